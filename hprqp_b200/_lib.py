@@ -1,0 +1,64 @@
+"""ctypes loader for libhprqp.so (the C ABI of include/hprqp.h).
+
+The library is loaded from this package directory.  There is no fallback:
+if it is missing or CUDA is unusable, calls raise (the reference silently
+fell back to its CPU path, src/utils.jl:14-31; this build does not).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from ._abi import Params, Result
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhprqp.so")
+
+# Every entry point declared in include/hprqp.h
+EXPORTS = ("hprqp_abi_info", "hprqp_default_params", "hprqp_create", "hprqp_load", "hprqp_prepare",
+           "hprqp_solve", "hprqp_set_trace", "hprqp_last_error", "hprqp_destroy")
+
+_lib = None
+
+
+class HPRQPError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"libhprqp error {code}: {msg}")
+        self.code = code
+
+
+def load():
+    """Load libhprqp.so (build it first with hprqp_b200.build if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise HPRQPError(-4, f"{LIB_PATH} not built; run `python -m hprqp_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.hprqp_abi_info.argtypes = [C.POINTER(C.c_int64)]
+    L.hprqp_abi_info.restype = C.c_int
+    L.hprqp_default_params.argtypes = [C.POINTER(Params)]
+    L.hprqp_default_params.restype = None
+    L.hprqp_create.argtypes = [C.POINTER(vp), C.c_int32]
+    L.hprqp_create.restype = C.c_int
+    L.hprqp_load.argtypes = [vp, vp]
+    L.hprqp_load.restype = C.c_int
+    L.hprqp_prepare.argtypes = [vp, C.POINTER(Params)]
+    L.hprqp_prepare.restype = C.c_int
+    L.hprqp_solve.argtypes = [vp, C.POINTER(Params), vp, vp, C.POINTER(Result), vp, vp, vp, vp]
+    L.hprqp_solve.restype = C.c_int
+    L.hprqp_set_trace.argtypes = [vp, C.c_int64, vp, vp, vp]
+    L.hprqp_set_trace.restype = C.c_int
+    L.hprqp_last_error.argtypes = [vp]
+    L.hprqp_last_error.restype = C.c_char_p
+    L.hprqp_destroy.argtypes = [vp]
+    L.hprqp_destroy.restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(rc, handle=None):
+    if rc != 0:
+        msg = load().hprqp_last_error(handle).decode(errors="replace")
+        raise HPRQPError(rc, msg)

@@ -1,0 +1,199 @@
+"""Python mirror of the reference solver API (src/algorithm.jl:1511-1554,
+src/structs.jl:195-309) over libhprqp.so.
+
+    model = build_from_QAbc(Q, c, A, AL, AU, l, u)
+    params = HPRQP_parameters(); params.stoptol = 1e-6
+    result = optimize(model, params)        # HPRQP_results
+
+Parameter names, defaults, status strings and result fields are the
+reference's.  Additions: params.precision ("fp64" | "fp32_polish"),
+params.polish_tol, params.lambda_max_A_override/_Q_override.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import Params, ProblemView, Result, STATUS_NAMES
+from ._lib import check, load
+
+
+@dataclass
+class HPRQP_parameters:
+    """HPRQP_parameters (src/structs.jl:195-275) with the reference defaults."""
+    stoptol: float = 1e-6
+    sigma: float = -1.0
+    max_iter: int = 2**31 - 1
+    sigma_fixed: bool = False
+    time_limit: float = 3600.0
+    eig_factor: float = 1.05
+    check_iter: int = 100
+    warm_up: bool = False
+    spmv_mode_Q: str = "auto"
+    spmv_mode_A: str = "auto"
+    print_frequency: int = -1
+    device_number: int = 0
+    use_Ruiz_scaling: bool = True
+    use_bc_scaling: bool = False
+    use_l2_scaling: bool = False
+    use_Pock_Chambolle_scaling: bool = True
+    problem_type: str = "QP"
+    lambda_: float = 0.0
+    initial_x: np.ndarray | None = None
+    initial_y: np.ndarray | None = None
+    auto_save: bool = False
+    save_filename: str = "hprqp_autosave.h5"
+    verbose: bool = True
+    use_gpu: bool = True
+    # extensions
+    precision: str = "fp64"
+    polish_tol: float = -1.0
+    lambda_max_A_override: float = -1.0
+    lambda_max_Q_override: float = -1.0
+
+    def to_struct(self) -> Params:
+        p = _abi.default_params()
+        for name in ("stoptol", "sigma", "time_limit", "eig_factor", "polish_tol",
+                     "lambda_max_A_override", "lambda_max_Q_override"):
+            setattr(p, name, float(getattr(self, name)))
+        p.lambda_ = float(self.lambda_)
+        p.max_iter = int(self.max_iter)
+        p.check_iter = int(self.check_iter)
+        p.print_frequency = int(self.print_frequency)
+        p.device_number = int(self.device_number)
+        for name in ("sigma_fixed", "warm_up", "use_Ruiz_scaling", "use_bc_scaling", "use_l2_scaling",
+                     "use_Pock_Chambolle_scaling", "auto_save", "verbose", "use_gpu"):
+            setattr(p, name, int(bool(getattr(self, name))))
+        p.spmv_mode_Q = _spmv_mode(self.spmv_mode_Q)
+        p.spmv_mode_A = _spmv_mode(self.spmv_mode_A)
+        if self.problem_type not in _abi.PROBLEM_TYPES:
+            raise ValueError(f"problem_type must be one of {list(_abi.PROBLEM_TYPES)}")
+        p.problem_type = _abi.PROBLEM_TYPES[self.problem_type]
+        if self.precision not in _abi.PRECISIONS:
+            raise ValueError(f"precision must be one of {list(_abi.PRECISIONS)}")
+        p.precision = _abi.PRECISIONS[self.precision]
+        return p
+
+
+def _spmv_mode(v) -> int:
+    """'auto' (autotuned), 'CUSPARSE'/'customized' (reference names, treated
+    as auto), or an explicit threads-per-row count 1..32."""
+    if isinstance(v, str):
+        return 0
+    t = int(v)
+    if t not in (1, 2, 4, 8, 16, 32):
+        raise ValueError("threads per row must be 1, 2, 4, 8, 16 or 32")
+    return int(np.log2(t)) + 1
+
+
+@dataclass
+class HPRQP_results:
+    """HPRQP_results (src/structs.jl:292-309) plus the library's extras."""
+    iter: int = 0
+    iter_4: int = 0
+    iter_6: int = 0
+    time: float = 0.0
+    time_4: float = 0.0
+    time_6: float = 0.0
+    power_time: float = 0.0
+    primal_obj: float = 0.0
+    residuals: float = 0.0
+    gap: float = 0.0
+    status: str = ""
+    x: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    y: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    z: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    w: np.ndarray = field(default_factory=lambda: np.zeros(0))
+    # extras
+    dual_obj: float = 0.0
+    err_Rp: float = 0.0
+    err_Rd: float = 0.0
+    setup_time: float = 0.0
+    sigma: float = 0.0
+    lambda_max_A: float = 0.0
+    lambda_max_Q: float = 0.0
+    restarts: int = 0
+    iter_fp32: int = 0
+    gpu_launches: int = 0
+    Q_is_diag: bool = False
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class Solver:
+    """A libhprqp handle bound to one device and one loaded model.  Reusing
+    it across solves keeps the scaled problem resident in HBM."""
+
+    def __init__(self, device: int = 0):
+        L = load()
+        h = C.c_void_p()
+        check(L.hprqp_create(C.byref(h), int(device)), None)
+        self._L, self.h = L, h
+        self.model = None
+        self._view = None
+
+    def load(self, model):
+        self._view = ProblemView(model)  # keeps the arrays alive during the copy
+        check(self._L.hprqp_load(self.h, C.addressof(self._view.struct)), self.h)
+        self.model = model
+        self._view = None
+        return self
+
+    def prepare(self, params: HPRQP_parameters):
+        check(self._L.hprqp_prepare(self.h, C.byref(params.to_struct())), self.h)
+
+    def set_trace(self, iters: int):
+        n, m = self.model.n, self.model.m
+        self._trace = (np.zeros((iters, n)), np.zeros((iters, m)), np.zeros((iters, n))) if iters else None
+        t = self._trace
+        check(self._L.hprqp_set_trace(self.h, iters, *( [_ptr(a) for a in t] if t else [None] * 3)), self.h)
+        return self._trace
+
+    def solve(self, params: HPRQP_parameters) -> HPRQP_results:
+        model = self.model
+        n, m = model.n, model.m
+        x, y, z, w = np.zeros(n), np.zeros(m), np.zeros(n), np.zeros(n)
+        x0 = None if params.initial_x is None else np.ascontiguousarray(params.initial_x, dtype=np.float64)
+        y0 = None if params.initial_y is None else np.ascontiguousarray(params.initial_y, dtype=np.float64)
+        if x0 is not None and len(x0) != n:
+            raise ValueError("initial_x has the wrong length")
+        if y0 is not None and len(y0) != m:
+            raise ValueError("initial_y has the wrong length")
+        r = Result()
+        check(self._L.hprqp_solve(self.h, C.byref(params.to_struct()), _ptr(x0), _ptr(y0), C.byref(r),
+                                  _ptr(x), _ptr(y), _ptr(z), _ptr(w)), self.h)
+        out = HPRQP_results()
+        for f, _ in Result._fields_:
+            if f == "status":
+                out.status = STATUS_NAMES[r.status]
+            elif hasattr(out, f):
+                setattr(out, f, getattr(r, f))
+        out.Q_is_diag = bool(r.Q_is_diag)
+        out.x, out.y, out.z, out.w = x, (y if m > 0 else np.zeros(0)), z, w
+        return out
+
+    def close(self):
+        if self.h:
+            self._L.hprqp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def optimize(model, params: HPRQP_parameters | None = None) -> HPRQP_results:
+    """optimize(model, params) (src/algorithm.jl:1511-1554) on the GPU."""
+    params = params or HPRQP_parameters()
+    s = Solver(params.device_number).load(model)
+    try:
+        return s.solve(params)
+    finally:
+        s.close()

@@ -1,0 +1,61 @@
+// common.cuh — shared device helpers for the HPR-QP iteration engine.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+
+namespace hprqp {
+
+// Error carrying an ABI return code; caught at the C boundary.
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define HPRQP_CUDA(call)                                                                  \
+  do {                                                                                    \
+    cudaError_t e_ = (call);                                                              \
+    if (e_ != cudaSuccess)                                                                \
+      throw ::hprqp::Error(e_ == cudaErrorMemoryAllocation ? -3 : -2,                     \
+                           std::string(#call) + ": " + cudaGetErrorString(e_) + " (" +   \
+                               __FILE__ + ":" + std::to_string(__LINE__) + ")");         \
+  } while (0)
+
+#define HPRQP_LAUNCH_CHECK() HPRQP_CUDA(cudaGetLastError())
+
+#ifdef __CUDACC__
+constexpr int kBlock = 256;  // threads per CTA for every row/element kernel
+
+// Device view of a CSR matrix (0-based, int32 indices).
+template <typename V>
+struct DCsr {
+  int rows = 0, cols = 0;
+  int64_t nnz = 0;
+  const int* ptr = nullptr;
+  const int* col = nullptr;
+  const V* val = nullptr;
+  int tpr = 4;  // threads cooperating on one row (1,2,4,8,16,32)
+};
+
+// Reduce `v` over the TPR lanes of a row group (lanes of a group are
+// consecutive and the group is aligned inside its warp).
+template <int TPR, typename T>
+__device__ __forceinline__ T group_sum(T v) {
+  if constexpr (TPR > 1) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned mask = (TPR == 32) ? 0xffffffffu
+                                      : (((1u << TPR) - 1u) << (lane & ~(unsigned)(TPR - 1)));
+#pragma unroll
+    for (int off = TPR / 2; off > 0; off >>= 1) v += __shfl_xor_sync(mask, v, off, TPR);
+  }
+  return v;
+}
+
+#endif  // __CUDACC__
+
+}  // namespace hprqp

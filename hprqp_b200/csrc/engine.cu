@@ -1,0 +1,755 @@
+// engine.cu — Engine<V>: uploads, launch wrappers and the device-side steps
+// of the HPR loop.  See engine.cuh.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <functional>
+
+#include "engine.cuh"
+
+namespace hprqp {
+
+constexpr int kMaxReduceGrid = 1184;  // 8 CTAs per SM on 148 SMs
+
+// ---------------------------------------------------------------------------
+// Common
+// ---------------------------------------------------------------------------
+void Common::init() {
+  HPRQP_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  if (cublasCreate(&cublas) != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cublasCreate failed");
+  cublasSetStream(cublas, stream);
+  d_scal = mem.alloc<double>(kNumSlots);
+  HPRQP_CUDA(cudaMemset(d_scal, 0, sizeof(double) * kNumSlots));
+  HPRQP_CUDA(cudaMallocHost(&h_scal, sizeof(double) * kNumSlots));
+  rws.partials = mem.alloc<double>((int64_t)kMaxReduceGrid * 16);
+  rws.counter = mem.alloc<unsigned>(4);
+  HPRQP_CUDA(cudaMemset(rws.counter, 0, sizeof(unsigned) * 4));
+  int dev = 0;
+  HPRQP_CUDA(cudaGetDevice(&dev));
+  HPRQP_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+}
+
+Common::~Common() {
+  if (h_scal) cudaFreeHost(h_scal);
+  if (cublas) cublasDestroy(cublas);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+void Common::sync_read(int first, int count) {
+  HPRQP_CUDA(cudaMemcpyAsync(h_scal + first, d_scal + first, sizeof(double) * count,
+                             cudaMemcpyDeviceToHost, stream));
+  HPRQP_CUDA(cudaStreamSynchronize(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Launch wrappers
+// ---------------------------------------------------------------------------
+template <int TPR, typename Acc, typename Src, typename Epi>
+static void rows_t(Common& cm, int nrows, const Src& src, const Epi& epi) {
+  const long long threads = (long long)nrows * TPR;
+  const int grid = (int)((threads + kBlock - 1) / kBlock);
+  k_row_pass<TPR, Acc, Src, Epi><<<grid, kBlock, 0, cm.stream>>>(nrows, src, epi);
+  cm.launches++;
+  HPRQP_LAUNCH_CHECK();
+}
+
+template <typename Acc, typename Src, typename Epi>
+static void rows(Common& cm, int tpr, int64_t nrows, const Src& src, const Epi& epi) {
+  if (nrows <= 0) return;
+  switch (tpr) {
+    case 1: rows_t<1, Acc>(cm, (int)nrows, src, epi); break;
+    case 2: rows_t<2, Acc>(cm, (int)nrows, src, epi); break;
+    case 4: rows_t<4, Acc>(cm, (int)nrows, src, epi); break;
+    case 8: rows_t<8, Acc>(cm, (int)nrows, src, epi); break;
+    case 16: rows_t<16, Acc>(cm, (int)nrows, src, epi); break;
+    case 32: rows_t<32, Acc>(cm, (int)nrows, src, epi); break;
+    default: throw Error(HPRQP_E_ARG, "bad threads-per-row");
+  }
+}
+
+template <int TPR, int K, unsigned MM, typename Acc, typename Src, typename Epi>
+static void reduce_t(Common& cm, int nrows, const Src& src, const Epi& epi, double* out) {
+  const long long threads = (long long)std::max(nrows, 1) * TPR;
+  const int grid = (int)std::min<long long>((threads + kBlock - 1) / kBlock, kMaxReduceGrid);
+  k_row_reduce<TPR, K, MM, Acc, Src, Epi><<<grid, kBlock, 0, cm.stream>>>(nrows, src, epi, cm.rws, out);
+  cm.launches++;
+  HPRQP_LAUNCH_CHECK();
+}
+
+template <int K, unsigned MM, typename Acc, typename Src, typename Epi>
+static void reduce(Common& cm, int tpr, int64_t nrows, const Src& src, const Epi& epi, double* out) {
+  switch (tpr) {
+    case 1: reduce_t<1, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
+    case 2: reduce_t<2, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
+    case 4: reduce_t<4, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
+    case 8: reduce_t<8, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
+    case 16: reduce_t<16, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
+    case 32: reduce_t<32, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
+    default: throw Error(HPRQP_E_ARG, "bad threads-per-row");
+  }
+}
+
+template <typename F>
+static void elem(Common& cm, int64_t len, const F& f) {
+  if (len <= 0) return;
+  const int grid = (int)((len + kBlock - 1) / kBlock);
+  k_elementwise<<<grid, kBlock, 0, cm.stream>>>((int)len, f);
+  cm.launches++;
+  HPRQP_LAUNCH_CHECK();
+}
+
+#define HPRQP_BOOL(cond, NAME, ...)   \
+  if (cond) {                         \
+    constexpr bool NAME = true;       \
+    __VA_ARGS__                       \
+  } else {                            \
+    constexpr bool NAME = false;      \
+    __VA_ARGS__                       \
+  }
+
+// ---------------------------------------------------------------------------
+// Extra epilogues / kernels local to the engine
+// ---------------------------------------------------------------------------
+
+// do_restart! (src/algorithm.jl:522-555), n-part: acc = (A' y_bar)_i
+template <typename V>
+struct EpiRestartN {
+  V *x, *w, *ATy, *ATy_bar, *Qw;
+  const V *x_bar, *w_bar, *Qw_bar;
+  double *last_x, *last_w, *last_ATy, *last_Qw;
+  bool has_m, noC;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const V xb = x_bar[i], wb = w_bar[i];
+    x[i] = xb;
+    w[i] = wb;
+    last_x[i] = (double)xb;
+    last_w[i] = (double)wb;
+    if (has_m) {
+      ATy_bar[i] = (V)acc;
+      last_ATy[i] = (double)(V)acc;
+      ATy[i] = (V)acc;
+    }
+    if (noC) {
+      Qw[i] = Qw_bar[i];
+      last_Qw[i] = (double)Qw_bar[i];
+    }
+  }
+};
+
+// Power method residual: sum (z - lambda q)^2, lambda read from the device.
+template <typename V>
+struct EpiPowerResid {
+  const V *q, *z;
+  const double* lam;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A, double (&r)[1]) const {
+    const double t = (double)z[i] - (*lam) * (double)q[i];
+    r[0] += t * t;
+  }
+};
+
+template <typename D, typename S>
+struct CastCopy {
+  D* dst;
+  const S* src;
+  __device__ __forceinline__ void operator()(int i) const { dst[i] = (D)src[i]; }
+};
+
+__global__ void k_power_log(double* scal, int k) {
+  const double lam = scal[S_POW + 1], zz = scal[S_POW + 2], rr = scal[S_POW + 3];
+  scal[S_POWLOG + 2 * k] = lam;
+  scal[S_POWLOG + 2 * k + 1] = sqrt(rr) / (sqrt(zz) + lam);
+}
+
+// Golden-section search of unified_golden_Q_diag (src/unified_operations.jl:
+// 348-386) on one CTA: f(x) = a x + b/x + x^2 sum_i c_i d_i / (1 + x Q_i).
+template <typename V>
+__global__ void __launch_bounds__(1024) k_golden_diag(int n, double a, double b, const V* Q,
+                                                      const V* cc, const V* dd, double lo, double hi,
+                                                      double tol, int maxiter, double* out) {
+  __shared__ double sh[32];
+  auto f = [&](double x) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      s += (double)cc[i] * ((double)dd[i] / (1.0 + x * (double)Q[i]));
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_down_sync(0xffffffffu, s, off);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = s;
+    __syncthreads();
+    double t = 0.0;
+    if (threadIdx.x < 32) {
+      t = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+      for (int off = 16; off > 0; off >>= 1) t += __shfl_down_sync(0xffffffffu, t, off);
+      if (threadIdx.x == 0) sh[0] = t;
+    }
+    __syncthreads();
+    t = sh[0];
+    return a * x + b / x + x * x * t;
+  };
+  const double phi = (sqrt(5.0) - 1.0) / 2.0;
+  double x1 = hi - phi * (hi - lo), x2 = lo + phi * (hi - lo);
+  double f1 = f(x1), f2 = f(x2);
+  int it = 0;
+  while (fabs(hi - lo) > tol * fmax(1.0, fabs(lo)) && it < maxiter) {
+    if (f1 > f2) {
+      lo = x1; x1 = x2; f1 = f2;
+      x2 = lo + phi * (hi - lo);
+      f2 = f(x2);
+    } else {
+      hi = x2; x2 = x1; f2 = f1;
+      x1 = hi - phi * (hi - lo);
+      f1 = f(x1);
+    }
+    ++it;
+  }
+  if (threadIdx.x == 0) *out = (f1 < f2) ? x1 : x2;
+}
+
+// ---------------------------------------------------------------------------
+// Engine: construction and uploads
+// ---------------------------------------------------------------------------
+template <typename V>
+static V* upload(DeviceMem& mem, const std::vector<double>& h, int64_t len) {
+  V* d = mem.alloc<V>(len);
+  if (len > 0) {
+    std::vector<V> t(h.begin(), h.begin() + len);
+    HPRQP_CUDA(cudaMemcpy(d, t.data(), sizeof(V) * len, cudaMemcpyHostToDevice));
+  }
+  return d;
+}
+
+template <typename V>
+void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode) {
+  d.rows = (int)h.rows;
+  d.cols = (int)h.cols;
+  d.nnz = h.nnz();
+  int* ptr = mem.alloc<int>(h.rows + 1);
+  int* col = mem.alloc<int>(d.nnz);
+  HPRQP_CUDA(cudaMemcpy(ptr, h.ptr.data(), sizeof(int) * (h.rows + 1), cudaMemcpyHostToDevice));
+  if (d.nnz) HPRQP_CUDA(cudaMemcpy(col, h.col.data(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice));
+  d.ptr = ptr;
+  d.col = col;
+  d.val = upload<V>(mem, h.val, d.nnz);
+  if (tpr_mode > 0) d.tpr = 1 << std::min(tpr_mode - 1, 5);
+  else d.tpr = autotune(d);
+}
+
+// Row-schedule autotuner: time the plain product for each threads-per-row
+// candidate on this matrix and keep the fastest (replaces the reference's
+// cuSPARSE-vs-inline micro-benchmark, src/algorithm.jl:1557-1752).
+template <typename V>
+int Engine<V>::autotune(DCsr<V>& d) {
+  if (d.rows <= 0 || d.nnz == 0) return 1;
+  const double avg = (double)d.nnz / d.rows;
+  static const int cand[] = {1, 2, 4, 8, 16, 32};
+  cudaEvent_t e0, e1;
+  HPRQP_CUDA(cudaEventCreate(&e0));
+  HPRQP_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_t = 4;
+  for (int t : cand) {
+    if (t == 1 && avg > 12) continue;
+    if (t == 32 && avg < 8) continue;
+    d.tpr = t;
+    spmv(d, pz, pt);
+    HPRQP_CUDA(cudaEventRecord(e0, cm.stream));
+    for (int r = 0; r < 3; ++r) spmv(d, pz, pt);
+    HPRQP_CUDA(cudaEventRecord(e1, cm.stream));
+    HPRQP_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    HPRQP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) { best = ms; best_t = t; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return best_t;
+}
+
+template <typename V>
+Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int path_, int tpr_Q, int tpr_A)
+    : cm(c_) {
+  n = hp.n;
+  m = hp.m;
+  path = path_;
+  Q_is_diag = pp.Q_is_diag;
+  is_qap = hp.Q_kind == HPRQP_Q_QAP;
+  is_lasso = hp.Q_kind == HPRQP_Q_LASSO;
+  has_Q_sparse = hp.Q_kind == HPRQP_Q_SPARSE;
+  b_scale = pp.b_scale;
+  c_scale = pp.c_scale;
+  norm_b_org = pp.norm_b_org;
+  norm_c_org = pp.norm_c_org;
+  lasso_lam = hp.lambda;
+  const int64_t mx = std::max(std::max(n, m), is_lasso ? hp.L.rows : (int64_t)0);
+  V** nv[] = {&x, &x_hat, &x_bar, &dx, &w, &w_bar, &dw, &z_bar, &Qw, &Qw_bar, &ATy, &ATy_bar, &ATdy,
+              &QATdy, &dQw, &Qx, &tempv, &fact1, &fact2, &fact, &fact_M};
+  for (V** p : nv) *p = mem.alloc<V>(n);
+  V** mv[] = {&y, &y_bar, &dy, &s, &Ax};
+  for (V** p : mv) *p = mem.alloc<V>(m);
+  for (double** p : {&last_x, &last_w, &last_ATy, &last_Qw}) *p = mem.alloc<double>(n);
+  last_y = mem.alloc<double>(m);
+  stage_n = mem.alloc<double>(n);
+  stage_m = mem.alloc<double>(m);
+  pz = mem.alloc<V>(mx);
+  pq = mem.alloc<V>(mx);
+  pt = mem.alloc<V>(mx);
+  HPRQP_CUDA(cudaMemset(pz, 0, sizeof(V) * mx));
+  c = upload<V>(mem, pp.c, n);
+  l = upload<V>(mem, pp.l, n);
+  u = upload<V>(mem, pp.u, n);
+  col_norm = upload<V>(mem, pp.col_norm, n);
+  diag_Q = upload<V>(mem, pp.diag_Q, n);
+  AL = upload<V>(mem, pp.AL, m);
+  AU = upload<V>(mem, pp.AU, m);
+  row_norm = upload<V>(mem, pp.row_norm, m);
+  upload_csr(pp.A, A, tpr_A);
+  upload_csr(pp.AT, AT, tpr_A);
+  if (has_Q_sparse) upload_csr(pp.Q, Q, tpr_Q);
+  if (is_lasso) {
+    ltemp = mem.alloc<V>(hp.L.rows);
+    upload_csr(hp.L, L, tpr_Q);
+    upload_csr(transpose(hp.L), LT, tpr_Q);
+  }
+  if (is_qap) {
+    const int64_t N2 = hp.qn * hp.qn;
+    qA = upload<V>(mem, hp.qA, N2);
+    qB = upload<V>(mem, hp.qB, N2);
+    qS = upload<V>(mem, hp.qS, N2);
+    qT = upload<V>(mem, hp.qT, N2);
+    qTmp = mem.alloc<V>(N2);
+  }
+  reset_state();
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+}
+
+template <typename V>
+void Engine<V>::reset_state() {
+  V* nv[] = {x, x_hat, x_bar, dx, w, w_bar, dw, z_bar, Qw, Qw_bar, ATy, ATy_bar, ATdy, QATdy, dQw, Qx, tempv};
+  for (V* p : nv) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(V) * n, cm.stream));
+  V* mv[] = {y, y_bar, dy, s, Ax};
+  for (V* p : mv)
+    if (m) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(V) * m, cm.stream));
+  for (double* p : {last_x, last_w, last_ATy, last_Qw}) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * n, cm.stream));
+  if (m) HPRQP_CUDA(cudaMemsetAsync(last_y, 0, sizeof(double) * m, cm.stream));
+}
+
+// ---------------------------------------------------------------------------
+// Products
+// ---------------------------------------------------------------------------
+template <typename V>
+void Engine<V>::spmv(const DCsr<V>& M, const V* xin, V* yout, double scale) {
+  rows<V>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, EpiStore<V>{yout, scale});
+}
+
+template <typename V>
+static cublasStatus_t gemm(cublasHandle_t h, int N, double alpha, const V* A, const V* B, double beta, V* C);
+template <>
+cublasStatus_t gemm<double>(cublasHandle_t h, int N, double alpha, const double* A, const double* B,
+                            double beta, double* C) {
+  return cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &alpha, A, N, B, N, &beta, C, N);
+}
+template <>
+cublasStatus_t gemm<float>(cublasHandle_t h, int N, double alpha, const float* A, const float* B, double beta,
+                           float* C) {
+  const float a = (float)alpha, b = (float)beta;
+  return cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &a, A, N, B, N, &b, C, N);
+}
+
+// QAP Qmap! (src/Q_operators/QAP_operator.jl:52-61): X = reshape(x, N, N)
+// column-major; TMP = A X; QX = 2 TMP B - 2 S X - 2 X T.
+template <typename V>
+void Engine<V>::qap_apply(const V* xin, V* yout) {
+  const int N = (int)std::lround(std::sqrt((double)n));
+  auto ck = [](cublasStatus_t s) {
+    if (s != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cuBLAS GEMM failed");
+  };
+  ck(gemm<V>(cm.cublas, N, 1.0, qA, xin, 0.0, qTmp));
+  ck(gemm<V>(cm.cublas, N, 2.0, qTmp, qB, 0.0, yout));
+  ck(gemm<V>(cm.cublas, N, -2.0, qS, xin, 1.0, yout));
+  ck(gemm<V>(cm.cublas, N, -2.0, xin, qT, 1.0, yout));
+  cm.launches += 4;
+}
+
+template <typename V>
+void Engine<V>::apply_Q(const V* xin, V* yout) {
+  if (is_lasso) {
+    spmv(L, xin, ltemp);
+    spmv(LT, ltemp, yout);
+  } else if (is_qap) {
+    qap_apply(xin, yout);
+  } else {
+    spmv(Q, xin, yout);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// One HPR iteration: main_update_cpu!/gpu! (src/algorithm.jl:945-972, 1250-1279)
+// ---------------------------------------------------------------------------
+template <typename V>
+void Engine<V>::step(bool full, double h1, double h2) {
+  const double f2s = 1.0 / (1.0 + sigma * lamQ), f1s = 1.0 - f2s;
+  const double fy1 = lamA * sigma, fy2 = 1.0 / fy1;
+  if (path == PATH_LASSO) {
+    spmv(L, w, ltemp);
+    HPRQP_BOOL(full, F, {
+      EpiLasso<V, F> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, c, last_x, last_w, sigma, lasso_lam, f1s, f2s, h1, h2};
+      rows<V>(cm, LT.tpr, n, CsrSrc<V, V>{LT.ptr, LT.col, LT.val, ltemp}, e);
+    })
+    return;
+  }
+  if (path == PATH_QP) {
+    HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
+      EpiZxw1<V, F, D> e{Qw, x, x_hat, w_bar, dx, x_bar, z_bar, ATy, c, l, u, w, fact1, fact2, last_x,
+                         sigma, f1s, f2s, h1, h2};
+      if (is_qap) {
+        qap_apply(w, Qw);
+        rows<V>(cm, 1, n, VecSrc<V>{Qw}, e);
+      } else {
+        rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w}, e);
+      }
+    }))
+    if (m > 0) {
+      EpiTempv<V> et{tempv, x_hat, Qw, sigma};
+      if (is_qap) {
+        qap_apply(w_bar, Qw_bar);
+        rows<V>(cm, 1, n, VecSrc<V>{Qw_bar}, et);
+      } else {
+        rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w_bar}, et);
+      }
+      HPRQP_BOOL(full, F, {
+        EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
+        rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, tempv}, ey);
+      })
+    }
+    const double fs = sigma / (1.0 + sigma * lamQ);
+    HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
+      EpiW2<V, F, D> e{w, ATy, w_bar, dw, ATdy, ATy_bar, fact, last_w, last_ATy, fs, h1, h2};
+      if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar}, e);
+      else rows<V>(cm, 1, n, ZeroSrc{}, e);
+    }))
+    return;
+  }
+  if (path == PATH_NOC) {
+    HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
+      EpiZxwNoC<V, F, D> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, Qw, c, l, u, fact1, fact2, last_x, last_w,
+                           sigma, f1s, f2s, h1, h2};
+      if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y}, e);
+      else rows<V>(cm, 1, n, ZeroSrc{}, e);
+    }))
+    HPRQP_BOOL(full, F, {
+      EpiTempvNoC<V, F> e{Qw, tempv, Qw_bar, x_hat, last_Qw, sigma, h1, h2};
+      if (is_qap) {
+        qap_apply(w_bar, Qw_bar);
+        rows<V>(cm, 1, n, VecSrc<V>{Qw_bar}, e);
+      } else {
+        rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w_bar}, e);
+      }
+    })
+    if (m > 0) {
+      HPRQP_BOOL(full, F, {
+        EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
+        rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, tempv}, ey);
+      })
+    }
+    return;
+  }
+  // PATH_LP
+  HPRQP_BOOL(full, F, {
+    EpiZxLP<V, F> e{x, x_hat, dx, x_bar, z_bar, c, l, u, last_x, sigma, h1, h2};
+    if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y}, e);
+    else rows<V>(cm, 1, n, ZeroSrc{}, e);
+  })
+  if (m > 0) {
+    HPRQP_BOOL(full, F, {
+      EpiY<V, F, false> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
+      rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, x_hat}, ey);
+    })
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Reductions
+// ---------------------------------------------------------------------------
+template <typename V>
+void Engine<V>::residuals_launch(bool) {
+  apply_Q(x_bar, Qx);
+  EpiResN<V> e{x_bar, Qx, c, z_bar, col_norm, l, u, lam_l1, c_scale, b_scale};
+  if (m > 0)
+    reduce<8, kResNMax, double>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar}, e, cm.d_scal + S_RES_N);
+  else
+    reduce<8, kResNMax, double>(cm, 1, n, ZeroSrc{}, e, cm.d_scal + S_RES_N);
+  if (m > 0) {
+    EpiResM<V> em{y_bar, s, AL, AU, row_norm, b_scale};
+    reduce<3, kResMMax, double>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, x_bar}, em, cm.d_scal + S_RES_M);
+  }
+}
+
+template <typename V>
+void Engine<V>::mnorm_launch(int slot) {
+  apply_Q(dw, dQw);
+  if (m > 0) {
+    spmv(AT, dy, ATdy);
+    apply_Q(ATdy, QATdy);
+  }
+  reduce<8, 0u, double>(cm, 1, n, ZeroSrc{}, EpiMnormN<V>{dx, dQw, ATdy, QATdy, fact_M, dw, m > 0}, cm.d_scal + slot);
+  reduce<1, 0u, double>(cm, 1, m, ZeroSrc{}, EpiSumSq<V>{dy}, cm.d_scal + slot + 8);
+}
+
+template <typename V>
+void Engine<V>::sigma_stats_launch() {
+  {
+    V *dx_ = dx, *dw_ = dw, *ATdy_ = ATdy;
+    const V *xb = x_bar, *wb = w_bar, *atyb = ATy_bar;
+    const double *lx = last_x, *lw = last_w, *laty = last_ATy;
+    const bool hm = m > 0;
+    elem(cm, n, [=] __device__(int i) {
+      dx_[i] = (V)((double)xb[i] - lx[i]);
+      dw_[i] = (V)((double)wb[i] - lw[i]);
+      if (hm) ATdy_[i] = (V)((double)atyb[i] - laty[i]);
+    });
+    V* dy_ = dy;
+    const V* yb = y_bar;
+    const double* ly = last_y;
+    elem(cm, m, [=] __device__(int i) { dy_[i] = (V)((double)yb[i] - ly[i]); });
+  }
+  apply_Q(dw, dQw);
+  if (m > 0) apply_Q(ATdy, QATdy);
+  reduce<5, 0u, double>(cm, 1, n, ZeroSrc{}, EpiSigmaN<V>{dx, dQw, ATdy, QATdy, dw, m > 0}, cm.d_scal + S_SIG);
+  reduce<1, 0u, double>(cm, 1, m, ZeroSrc{}, EpiSumSq<V>{dy}, cm.d_scal + S_SIG + 5);
+}
+
+template <typename V>
+void Engine<V>::golden_diag_launch(double a, double b) {
+  k_golden_diag<V><<<1, 1024, 0, cm.stream>>>((int)n, a, b, diag_Q, ATdy, QATdy, 1e-12, 1e12, 1e-13, 200,
+                                              cm.d_scal + S_GOLD);
+  cm.launches++;
+  HPRQP_LAUNCH_CHECK();
+}
+
+template <typename V>
+void Engine<V>::set_sigma(double sg) {
+  sigma = sg;
+  if (!Q_is_diag) return;
+  // unified_update_Q_factors! (src/unified_operations.jl:445-459)
+  V *f2 = fact2, *f = fact, *f1 = fact1, *fM = fact_M;
+  const V* dq = diag_Q;
+  const double s2 = sg * sg;
+  elem(cm, n, [=] __device__(int i) {
+    const double q = dq[i];
+    const double t2 = 1.0 / (1.0 + sg * q);
+    f2[i] = (V)t2;
+    f[i] = (V)(sg * t2);
+    f1[i] = (V)(sg * q * t2);
+    fM[i] = (V)(s2 * t2);
+  });
+}
+
+template <typename V>
+void Engine<V>::restart() {
+  EpiRestartN<V> e{x, w, ATy, ATy_bar, Qw, x_bar, w_bar, Qw_bar, last_x, last_w, last_ATy, last_Qw,
+                   m > 0, path == PATH_NOC};
+  if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar}, e);
+  else rows<V>(cm, 1, n, ZeroSrc{}, e);
+  V *y_ = y;
+  const V* yb = y_bar;
+  double* ly = last_y;
+  elem(cm, m, [=] __device__(int i) {
+    y_[i] = yb[i];
+    ly[i] = (double)yb[i];
+  });
+}
+
+// process_initial_points! (src/algorithm.jl:1783-1836)
+template <typename V>
+void Engine<V>::initial_points(const double* x0, const double* y0) {
+  if (x0) {
+    HPRQP_CUDA(cudaMemcpyAsync(stage_n, x0, sizeof(double) * n, cudaMemcpyHostToDevice, cm.stream));
+    V *x_ = x, *xb = x_bar, *w_ = w, *wb = w_bar;
+    double *lx = last_x, *lw = last_w;
+    const double* st = stage_n;
+    const V* cn = col_norm;
+    const double bs = b_scale;
+    elem(cm, n, [=] __device__(int i) {
+      const double v = st[i] * (double)cn[i] / bs;
+      x_[i] = xb[i] = w_[i] = wb[i] = (V)v;
+      lx[i] = lw[i] = (double)(V)v;
+    });
+  }
+  if (y0) {
+    if (m > 0) {
+      HPRQP_CUDA(cudaMemcpyAsync(stage_m, y0, sizeof(double) * m, cudaMemcpyHostToDevice, cm.stream));
+      V *y_ = y, *yb = y_bar;
+      double* ly = last_y;
+      const double* st = stage_m;
+      const V* rn = row_norm;
+      const double cs = c_scale;
+      elem(cm, m, [=] __device__(int i) {
+        const double v = st[i] * (double)rn[i] / cs;
+        y_[i] = yb[i] = (V)v;
+        ly[i] = (double)(V)v;
+      });
+      spmv(AT, y_bar, ATy_bar);
+      V* aty = ATy;
+      const V* atyb = ATy_bar;
+      double* laty = last_ATy;
+      elem(cm, n, [=] __device__(int i) {
+        aty[i] = atyb[i];
+        laty[i] = (double)atyb[i];
+      });
+    }
+    apply_Q(x_bar, Qx);
+    {
+      V* zb = z_bar;
+      const V *xb = x_bar, *qx = Qx, *atyb = ATy_bar, *cc = c;
+      const double sg = sigma;
+      elem(cm, n, [=] __device__(int i) {
+        const double tmp = -(double)qx[i] + (double)atyb[i] - (double)cc[i];
+        const double z_raw = (double)xb[i] + sg * tmp;
+        zb[i] = (V)(((double)xb[i] - z_raw) / sg);
+      });
+    }
+    if (m > 0) {
+      spmv(A, x_bar, Ax);
+      V* s_ = s;
+      const V *ax = Ax, *y_ = y, *al = AL, *au = AU;
+      const double f1 = lamA * sigma;
+      elem(cm, m, [=] __device__(int i) {
+        s_[i] = (V)clampd((double)ax[i] - f1 * (double)y_[i], (double)al[i], (double)au[i]);
+      });
+    }
+  }
+}
+
+// collect_results! (src/algorithm.jl:611-643)
+template <typename V>
+void Engine<V>::collect(double* xo, double* yo, double* zo, double* wo) {
+  const V *xb = x_bar, *wb = w_bar, *zb = z_bar, *cn = col_norm;
+  double* st = stage_n;
+  const double bs = b_scale, cs = c_scale;
+  auto copy_n = [&](double* dst) {
+    HPRQP_CUDA(cudaMemcpyAsync(dst, stage_n, sizeof(double) * n, cudaMemcpyDeviceToHost, cm.stream));
+    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+  };
+  if (xo) {
+    elem(cm, n, [=] __device__(int i) { st[i] = bs * ((double)xb[i] / (double)cn[i]); });
+    copy_n(xo);
+  }
+  if (wo) {
+    elem(cm, n, [=] __device__(int i) { st[i] = bs * ((double)wb[i] / (double)cn[i]); });
+    copy_n(wo);
+  }
+  if (zo) {
+    elem(cm, n, [=] __device__(int i) { st[i] = cs * ((double)zb[i] * (double)cn[i]); });
+    copy_n(zo);
+  }
+  if (yo && m > 0) {
+    const V *yb = y_bar, *rn = row_norm;
+    double* sm = stage_m;
+    elem(cm, m, [=] __device__(int i) { sm[i] = cs * ((double)yb[i] / (double)rn[i]); });
+    HPRQP_CUDA(cudaMemcpyAsync(yo, stage_m, sizeof(double) * m, cudaMemcpyDeviceToHost, cm.stream));
+  }
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+}
+
+template <typename V>
+void Engine<V>::trace_copy(double* xt, double* yt, double* wt) {
+  auto out = [&](const V* src, int64_t len, double* stage, double* dst) {
+    if (!dst || len == 0) return;
+    elem(cm, len, CastCopy<double, V>{stage, src});
+    HPRQP_CUDA(cudaMemcpyAsync(dst, stage, sizeof(double) * len, cudaMemcpyDeviceToHost, cm.stream));
+    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+  };
+  out(x, n, stage_n, xt);
+  out(y, m, stage_m, yt);
+  out(w, n, stage_n, wt);
+}
+
+// ---------------------------------------------------------------------------
+// Power method (src/utils.jl:1335-1461), chunked: the host checks the
+// per-iteration (lambda, err) log once per kPowChunk iterations.
+// ---------------------------------------------------------------------------
+template <typename V>
+static double power_common(Engine<V>& E, int64_t len, double tol, int max_it, int64_t* iters,
+                           const std::function<void(const V*, V*)>& op) {
+  Common& cm = E.cm;
+  {
+    std::vector<double> z0 = power_start_vector(len);
+    std::vector<V> zv(z0.begin(), z0.end());
+    HPRQP_CUDA(cudaMemcpy(E.pz, zv.data(), sizeof(V) * len, cudaMemcpyHostToDevice));
+  }
+  reduce<1, 0u, double>(cm, 1, len, ZeroSrc{}, EpiSumSq<V>{E.pz}, cm.d_scal + S_POW + 2);
+  double lam = 1.0;
+  int it = 0;
+  while (it < max_it) {
+    const int chunk = std::min<int>(kPowChunk, max_it - it);
+    for (int k = 0; k < chunk; ++k) {
+      V* q = E.pq;
+      const V* z = E.pz;
+      const double* zz = cm.d_scal + S_POW + 2;
+      elem(cm, len, [=] __device__(int i) { q[i] = (V)((double)z[i] / sqrt(*zz)); });
+      op(E.pq, E.pz);
+      reduce<2, 0u, double>(cm, 1, len, ZeroSrc{}, EpiPowerDot<V>{E.pq, E.pz}, cm.d_scal + S_POW + 1);
+      reduce<1, 0u, double>(cm, 1, len, ZeroSrc{}, EpiPowerResid<V>{E.pq, E.pz, cm.d_scal + S_POW + 1},
+                            cm.d_scal + S_POW + 3);
+      k_power_log<<<1, 1, 0, cm.stream>>>(cm.d_scal, k);
+      cm.launches++;
+      HPRQP_LAUNCH_CHECK();
+    }
+    cm.sync_read(S_POWLOG, 2 * chunk);
+    for (int k = 0; k < chunk; ++k) {
+      lam = cm.h_scal[S_POWLOG + 2 * k];
+      const double err = cm.h_scal[S_POWLOG + 2 * k + 1];
+      if (err < tol) {
+        *iters = it + k + 1;
+        return lam;
+      }
+    }
+    it += chunk;
+  }
+  *iters = it;
+  std::fprintf(stderr, "Power iteration did not converge within the specified tolerance.\n");
+  return lam;
+}
+
+template <typename V>
+double Engine<V>::power_A(double tol, int max_it, int64_t* iters) {
+  return power_common<V>(*this, m, tol, max_it, iters, [this](const V* q, V* z) {
+    spmv(AT, q, pt);
+    spmv(A, pt, z);
+  });
+}
+
+template <typename V>
+double Engine<V>::power_Q(double tol, int max_it, int64_t* iters) {
+  return power_common<V>(*this, n, tol, max_it, iters, [this](const V* q, V* z) { apply_Q(q, z); });
+}
+
+// FP32 -> FP64 hand-over of the full iteration state (precision switch)
+template <typename V>
+template <typename W>
+void Engine<V>::import_state(const Engine<W>& o) {
+  auto cv = [&](V* dst, const W* src, int64_t len) { elem(cm, len, CastCopy<V, W>{dst, src}); };
+  cv(x, o.x, n); cv(x_hat, o.x_hat, n); cv(x_bar, o.x_bar, n); cv(dx, o.dx, n);
+  cv(w, o.w, n); cv(w_bar, o.w_bar, n); cv(dw, o.dw, n); cv(z_bar, o.z_bar, n);
+  cv(Qw, o.Qw, n); cv(Qw_bar, o.Qw_bar, n); cv(ATy, o.ATy, n); cv(ATy_bar, o.ATy_bar, n);
+  cv(ATdy, o.ATdy, n); cv(tempv, o.tempv, n);
+  cv(y, o.y, m); cv(y_bar, o.y_bar, m); cv(dy, o.dy, m); cv(s, o.s, m);
+  auto cp = [&](double* dst, const double* src, int64_t len) {
+    if (len) HPRQP_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * len, cudaMemcpyDeviceToDevice, cm.stream));
+  };
+  cp(last_x, o.last_x, n); cp(last_w, o.last_w, n); cp(last_ATy, o.last_ATy, n); cp(last_Qw, o.last_Qw, n);
+  cp(last_y, o.last_y, m);
+  lamA = o.lamA;
+  lamQ = o.lamQ;
+  lam_l1 = o.lam_l1;
+  set_sigma(o.sigma);
+}
+
+template class Engine<double>;
+template class Engine<float>;
+template void Engine<double>::import_state<float>(const Engine<float>&);
+
+}  // namespace hprqp

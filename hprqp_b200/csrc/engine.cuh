@@ -1,0 +1,126 @@
+// engine.cuh — device state and kernel launch layer of the HPR-QP engine.
+//
+// Engine<V> owns the scaled problem and every iterate in HBM (V = double
+// for the FP64 path, float for the FP32 phase; Halpern anchors stay double)
+// and exposes the steps of the reference loop as stream-ordered launches:
+// step() = main_update (src/algorithm.jl:945-972), residuals() =
+// compute_residuals!, mnorm() = compute_M_norm!, sigma_stats() = the
+// reductions of update_sigma!, restart() = do_restart!, power_*() =
+// power_iteration_A/Q.  Scalars from reductions land in a device slot array
+// that the host reads once per residual check.
+#pragma once
+
+#include <cublas_v2.h>
+
+#include <memory>
+#include <vector>
+
+#include "host_setup.h"
+#include "kernels.cuh"
+
+namespace hprqp {
+
+enum Path { PATH_QP = 0, PATH_NOC = 1, PATH_LP = 2, PATH_LASSO = 3 };
+
+// Device scalar slot layout
+enum Slot {
+  S_RES_N = 0,     // 8 slots: EpiResN
+  S_RES_M = 8,     // 3 slots: EpiResM
+  S_MN_CUR = 16,   // 8 + 1 slots: M-norm for current_gap
+  S_MN_LAST = 32,  // 8 + 1 slots: M-norm for last_gap
+  S_SIG = 48,      // 5 + 1 slots: sigma statistics
+  S_GOLD = 56,     // golden-section result (diagonal Q)
+  S_POW = 64,      // power method working scalars (4)
+  S_POWLOG = 128,  // power method log: (lambda, err) per iteration
+  kPowChunk = 32,
+  kNumSlots = S_POWLOG + 2 * kPowChunk,
+};
+
+struct DeviceMem {  // owns cudaMalloc'ed blocks
+  std::vector<void*> blocks;
+  void* get(size_t bytes) {
+    void* p = nullptr;
+    if (bytes == 0) bytes = 16;
+    HPRQP_CUDA(cudaMalloc(&p, bytes));
+    blocks.push_back(p);
+    return p;
+  }
+  template <typename T>
+  T* alloc(int64_t count) { return (T*)get(sizeof(T) * (size_t)(count > 0 ? count : 1)); }
+  ~DeviceMem() {
+    for (void* p : blocks) cudaFree(p);
+  }
+};
+
+struct Common {  // per-handle resources shared by the engines
+  cudaStream_t stream = nullptr;
+  cublasHandle_t cublas = nullptr;
+  double* d_scal = nullptr;
+  double* h_scal = nullptr;  // pinned mirror
+  ReduceWs rws{};
+  int64_t launches = 0;
+  int num_sms = 148;
+  DeviceMem mem;
+  void init();
+  ~Common();
+  void sync_read(int first, int count);
+};
+
+struct PendingMnorm {
+  bool active = false;
+  int slot = 0;
+  double sigma = 0, lamA = 0, lamQ = 0;
+};
+
+template <typename V>
+class Engine {
+ public:
+  Engine(Common& cm, const HostProblem& hp, const Prepared& pp, int path, int tpr_mode_Q, int tpr_mode_A);
+  int64_t n, m;
+  int path;
+  bool Q_is_diag, has_Q_sparse, is_qap, is_lasso;
+  double b_scale, c_scale, norm_b_org, norm_c_org;
+  double sigma = 1.0, lamA = 0.0, lamQ = 0.0;
+  double lam_l1 = 0.0;   // lambda in the L1 objective term (problem_type LASSO)
+  double lasso_lam = 0;  // soft-threshold lambda
+
+  // iteration state (V) and anchors (double)
+  V *x, *x_hat, *x_bar, *dx, *w, *w_bar, *dw, *z_bar, *Qw, *Qw_bar, *ATy, *ATy_bar, *ATdy, *QATdy,
+      *dQw, *Qx, *tempv, *c, *l, *u, *col_norm, *fact1, *fact2, *fact, *fact_M, *diag_Q;
+  V *y, *y_bar, *dy, *s, *Ax, *AL, *AU, *row_norm;
+  double *last_x, *last_w, *last_ATy, *last_Qw, *last_y;
+  V* ltemp = nullptr;                 // LASSO A_d w
+  double *stage_n, *stage_m;          // FP64 staging for host copies
+  V *pz, *pq, *pt;                    // power method vectors
+
+  DCsr<V> A, AT, Q, L, LT;
+  V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;
+
+  void reset_state();
+  void set_sigma(double s);  // + diagonal factors (unified_update_Q_factors!)
+  void step(bool full, double h1, double h2);
+  void residuals_launch(bool with_bounds);
+  void mnorm_launch(int slot);
+  void sigma_stats_launch();
+  void golden_diag_launch(double a, double b);
+  void restart();
+  void initial_points(const double* x0, const double* y0);
+  void collect(double* x_out, double* y_out, double* z_out, double* w_out);
+  void trace_copy(double* xt, double* yt, double* wt);
+  double power_A(double tol, int max_it, int64_t* iters);
+  double power_Q(double tol, int max_it, int64_t* iters);
+  template <typename W>
+  void import_state(const Engine<W>& o);  // precision switch (FP32 -> FP64)
+
+  void apply_Q(const V* xin, V* yout);  // Qmap! into a vector
+  Common& cm;
+
+ private:
+  DeviceMem mem;
+  void upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode);
+  int autotune(DCsr<V>& d);
+  void spmv(const DCsr<V>& M, const V* xin, V* yout, double scale = 1.0);
+  void qap_apply(const V* xin, V* yout);
+};
+
+}  // namespace hprqp

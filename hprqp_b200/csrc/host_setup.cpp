@@ -1,0 +1,310 @@
+// host_setup.cpp — see host_setup.h.
+#include "host_setup.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <limits>
+
+#include "common.cuh"
+
+namespace hprqp {
+
+namespace {
+const double kInf = std::numeric_limits<double>::infinity();
+
+HCsr csc_to_csr(int64_t rows, int64_t cols, const int32_t* cp, const int32_t* rv, const double* nz,
+                int base, const char* what) {
+  HCsr M;
+  M.rows = rows;
+  M.cols = cols;
+  if (!cp) throw Error(HPRQP_E_ARG, std::string(what) + ": null colptr");
+  if (cp[0] != base) throw Error(HPRQP_E_ARG, std::string(what) + ": colptr[0] != index_base");
+  const int64_t nnz = (int64_t)cp[cols] - base;
+  if (nnz < 0 || nnz > INT32_MAX) throw Error(HPRQP_E_ARG, std::string(what) + ": bad nnz");
+  if (nnz > 0 && (!rv || !nz)) throw Error(HPRQP_E_ARG, std::string(what) + ": null rowval/nzval");
+  M.ptr.assign(rows + 1, 0);
+  M.col.resize(nnz);
+  M.val.resize(nnz);
+  for (int64_t j = 0; j < cols; ++j)
+    if (cp[j + 1] < cp[j]) throw Error(HPRQP_E_ARG, std::string(what) + ": colptr not monotone");
+  for (int64_t k = 0; k < nnz; ++k) {
+    const int64_t r = (int64_t)rv[k] - base;
+    if (r < 0 || r >= rows) throw Error(HPRQP_E_ARG, std::string(what) + ": row index out of range");
+    if (!std::isfinite(nz[k])) throw Error(HPRQP_E_ARG, std::string(what) + " contains NaN or Inf values.");
+    M.ptr[r + 1]++;
+  }
+  for (int64_t i = 0; i < rows; ++i) M.ptr[i + 1] += M.ptr[i];
+  std::vector<int> pos(M.ptr.begin(), M.ptr.end() - 1);
+  for (int64_t j = 0; j < cols; ++j)
+    for (int64_t k = cp[j] - base; k < cp[j + 1] - base; ++k) {
+      const int r = rv[k] - base;
+      M.col[pos[r]] = (int)j;
+      M.val[pos[r]] = nz[k];
+      pos[r]++;
+    }
+  // CSC rows sorted within each column give CSR columns sorted within rows.
+  return M;
+}
+
+std::vector<double> copy_vec(const double* p, int64_t len, const char* what, bool allow_inf) {
+  if (len > 0 && !p) throw Error(HPRQP_E_ARG, std::string(what) + ": null pointer");
+  std::vector<double> v(p, p + len);
+  for (double x : v) {
+    if (std::isnan(x)) throw Error(HPRQP_E_ARG, std::string(what) + " contains NaN values.");
+    if (!allow_inf && std::isinf(x)) throw Error(HPRQP_E_ARG, std::string(what) + " contains Inf values.");
+  }
+  return v;
+}
+
+double norm_b_of(const std::vector<double>& AL, const std::vector<double>& AU, bool inf) {
+  double s = 0.0;
+  for (size_t i = 0; i < AL.size(); ++i) {
+    const double a = AL[i] == -kInf ? 0.0 : AL[i];
+    const double b = AU[i] == kInf ? 0.0 : AU[i];
+    const double t = std::max(std::fabs(a), std::fabs(b));
+    s = inf ? std::max(s, t) : s + t * t;
+  }
+  return inf ? s : std::sqrt(s);
+}
+double norm2(const std::vector<double>& v) {
+  double s = 0.0;
+  for (double x : v) s += x * x;
+  return std::sqrt(s);
+}
+double norminf(const std::vector<double>& v) {
+  double s = 0.0;
+  for (double x : v) s = std::max(s, std::fabs(x));
+  return s;
+}
+
+// ((1/dr_i) * m_ij) * (1/dc_j): the entry order of DR * M * DC
+void scale_rows_cols(HCsr& M, const std::vector<double>* dr, const std::vector<double>* dc) {
+  for (int64_t i = 0; i < M.rows; ++i)
+    for (int k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
+      double v = M.val[k];
+      if (dr) v = (1.0 / (*dr)[i]) * v;
+      if (dc) v = v * (1.0 / (*dc)[M.col[k]]);
+      M.val[k] = v;
+    }
+}
+}  // namespace
+
+HCsr transpose(const HCsr& A) {
+  HCsr T;
+  T.rows = A.cols;
+  T.cols = A.rows;
+  const int64_t nnz = A.nnz();
+  T.ptr.assign(T.rows + 1, 0);
+  T.col.resize(nnz);
+  T.val.resize(nnz);
+  for (int64_t k = 0; k < nnz; ++k) T.ptr[A.col[k] + 1]++;
+  for (int64_t i = 0; i < T.rows; ++i) T.ptr[i + 1] += T.ptr[i];
+  std::vector<int> pos(T.ptr.begin(), T.ptr.end() - 1);
+  for (int64_t i = 0; i < A.rows; ++i)
+    for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) {
+      const int c = A.col[k];
+      T.col[pos[c]] = (int)i;
+      T.val[pos[c]] = A.val[k];
+      pos[c]++;
+    }
+  return T;
+}
+
+std::vector<double> power_start_vector(int64_t len) {
+  std::vector<double> z(len);
+  uint64_t s = 1;
+  auto next = [&s]() {
+    uint64_t v = (s += 0x9E3779B97F4A7C15ULL);
+    v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
+    return v ^ (v >> 31);
+  };
+  for (int64_t i = 0; i < len; ++i) {
+    const double u1 = ((next() >> 11) + 1.0) * 0x1.0p-53;
+    const double u2 = (next() >> 11) * 0x1.0p-53;
+    z[i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2) + 1e-8;
+  }
+  return z;
+}
+
+void load_problem(const hprqp_problem* pr, HostProblem& hp) {
+  if (!pr) throw Error(HPRQP_E_ARG, "null problem");
+  if (pr->n <= 0 || pr->m < 0 || pr->n > INT32_MAX || pr->m > INT32_MAX)
+    throw Error(HPRQP_E_ARG, "bad problem sizes (need n >= 1, m >= 0)");
+  if (pr->index_base != 0 && pr->index_base != 1) throw Error(HPRQP_E_ARG, "index_base must be 0 or 1");
+  HostProblem h;
+  h.n = pr->n;
+  h.m = pr->m;
+  const int base = pr->index_base;
+  h.Q_kind = pr->Q_kind;
+  if (h.m > 0) {
+    h.A = csc_to_csr(h.m, h.n, pr->A_colptr, pr->A_rowval, pr->A_nzval, base, "A matrix");
+  } else {
+    h.A.rows = 0;
+    h.A.cols = h.n;
+    h.A.ptr.assign(1, 0);
+  }
+  h.c = copy_vec(pr->c, h.n, "c vector", false);
+  h.AL = copy_vec(pr->AL, h.m, "Constraint bounds AL", true);
+  h.AU = copy_vec(pr->AU, h.m, "Constraint bounds AU", true);
+  h.l = copy_vec(pr->l, h.n, "Variable bounds l", true);
+  h.u = copy_vec(pr->u, h.n, "Variable bounds u", true);
+  for (int64_t i = 0; i < h.n; ++i)
+    if (h.l[i] > h.u[i]) throw Error(HPRQP_E_ARG, "Infeasible variable bounds: l > u at index " + std::to_string(i));
+  for (int64_t i = 0; i < h.m; ++i)
+    if (h.AL[i] > h.AU[i]) throw Error(HPRQP_E_ARG, "Infeasible constraint bounds: AL > AU at row " + std::to_string(i));
+  h.obj_constant = pr->obj_constant;
+  h.lambda = pr->lambda;
+  if (h.Q_kind == HPRQP_Q_SPARSE) {
+    if (pr->Q_colptr) h.Q = csc_to_csr(h.n, h.n, pr->Q_colptr, pr->Q_rowval, pr->Q_nzval, base, "Q matrix");
+    else { h.Q.rows = h.Q.cols = h.n; h.Q.ptr.assign(h.n + 1, 0); }
+  } else if (h.Q_kind == HPRQP_Q_LASSO) {
+    if (pr->lasso_m <= 0 || pr->lasso_m > INT32_MAX) throw Error(HPRQP_E_ARG, "LASSO: bad lasso_m");
+    h.L = csc_to_csr(pr->lasso_m, h.n, pr->L_colptr, pr->L_rowval, pr->L_nzval, base, "LASSO data matrix");
+  } else if (h.Q_kind == HPRQP_Q_QAP) {
+    const int64_t N = pr->qap_n;
+    if (N <= 0 || N * N != h.n) throw Error(HPRQP_E_ARG, "QAP: n must equal qap_n^2");
+    h.qn = N;
+    h.qA = copy_vec(pr->qap_A, N * N, "QAP A", false);
+    h.qB = copy_vec(pr->qap_B, N * N, "QAP B", false);
+    h.qS = copy_vec(pr->qap_S, N * N, "QAP S", false);
+    h.qT = copy_vec(pr->qap_T, N * N, "QAP T", false);
+  } else {
+    throw Error(HPRQP_E_ARG, "unknown Q_kind");
+  }
+  h.loaded = true;
+  hp = std::move(h);
+}
+
+void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& o) {
+  const int64_t n = hp.n, m = hp.m;
+  o = Prepared();
+  o.ruiz = p.use_Ruiz_scaling;
+  o.pc = p.use_Pock_Chambolle_scaling;
+  o.A = hp.A;
+  o.c = hp.c;
+  o.AL = hp.AL;
+  o.AU = hp.AU;
+  o.l = hp.l;
+  o.u = hp.u;
+  o.row_norm.assign(m, 1.0);
+  o.col_norm.assign(n, 1.0);
+  o.norm_b_org = m > 0 ? norm_b_of(o.AL, o.AU, true) : 0.0;
+  o.norm_c_org = norminf(o.c);
+  if (hp.Q_kind != HPRQP_Q_SPARSE) {
+    // Operator Q: no scaling at all (src/utils.jl:364-406)
+    o.AT = transpose(o.A);
+    o.norm_b = m > 0 ? norm_b_of(o.AL, o.AU, false) : 0.0;
+    o.norm_c = norm2(o.c);
+    o.diag_Q.assign(n, 0.0);
+    o.Q_is_diag = false;
+  } else {
+    o.Q = hp.Q;
+    HCsr& A = o.A;
+    HCsr& Q = o.Q;
+    std::vector<double> tr(m, 1.0), tc(n, 1.0);
+    auto apply = [&]() {
+      for (int64_t i = 0; i < m; ++i) o.row_norm[i] *= tr[i];
+      for (int64_t j = 0; j < n; ++j) o.col_norm[j] *= tc[j];
+      scale_rows_cols(Q, &tc, &tc);
+      if (m > 0) scale_rows_cols(A, &tr, &tc);
+      for (int64_t j = 0; j < n; ++j) o.c[j] /= tc[j];
+      for (int64_t i = 0; i < m; ++i) { o.AL[i] /= tr[i]; o.AU[i] /= tr[i]; }
+      for (int64_t j = 0; j < n; ++j) { o.l[j] *= tc[j]; o.u[j] *= tc[j]; }
+    };
+    if (p.use_Ruiz_scaling) {
+      for (int pass = 0; pass < 10; ++pass) {
+        std::vector<double> ca(n, 0.0), cq(n, 0.0);
+        for (int64_t i = 0; i < A.rows; ++i)
+          for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) ca[A.col[k]] = std::max(ca[A.col[k]], std::fabs(A.val[k]));
+        for (int64_t i = 0; i < Q.rows; ++i)
+          for (int k = Q.ptr[i]; k < Q.ptr[i + 1]; ++k) cq[Q.col[k]] = std::max(cq[Q.col[k]], std::fabs(Q.val[k]));
+        for (int64_t j = 0; j < n; ++j) {
+          tc[j] = std::sqrt(std::max(ca[j], cq[j]));
+          if (tc[j] == 0.0) tc[j] = 1.0;
+        }
+        for (int64_t i = 0; i < m; ++i) {
+          double r = 0.0;
+          for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) r = std::max(r, std::fabs(A.val[k]));
+          tr[i] = std::sqrt(r);
+          if (tr[i] == 0.0) tr[i] = 1.0;
+        }
+        apply();
+      }
+    }
+    if (p.use_Pock_Chambolle_scaling) {
+      std::vector<double> ca(n, 0.0), cq(n, 0.0);
+      HCsr AT = transpose(A), QT = transpose(Q);
+      for (int64_t j = 0; j < n; ++j) {
+        double s = 0.0;
+        for (int k = AT.ptr[j]; k < AT.ptr[j + 1]; ++k) s += std::fabs(AT.val[k]);
+        ca[j] = s;
+        s = 0.0;
+        for (int k = QT.ptr[j]; k < QT.ptr[j + 1]; ++k) s += std::fabs(QT.val[k]);
+        cq[j] = s;
+      }
+      for (int64_t j = 0; j < n; ++j) {
+        tc[j] = std::sqrt(ca[j] + cq[j]);
+        if (tc[j] == 0.0) tc[j] = 1.0;
+      }
+      for (int64_t i = 0; i < m; ++i) {
+        double r = 0.0;
+        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) r += std::fabs(A.val[k]);
+        tr[i] = std::sqrt(r);
+        if (tr[i] == 0.0) tr[i] = 1.0;
+      }
+      apply();
+    }
+    o.AT = transpose(A);
+    // Q = (Q + Q') / 2 (src/utils.jl:771-780)
+    {
+      HCsr QT = transpose(Q), S;
+      S.rows = S.cols = n;
+      S.ptr.assign(n + 1, 0);
+      S.col.reserve(Q.nnz());
+      S.val.reserve(Q.nnz());
+      for (int64_t i = 0; i < n; ++i) {
+        int a = Q.ptr[i], b = QT.ptr[i];
+        const int ae = Q.ptr[i + 1], be = QT.ptr[i + 1];
+        while (a < ae || b < be) {
+          const int ca = a < ae ? Q.col[a] : INT32_MAX;
+          const int cb = b < be ? QT.col[b] : INT32_MAX;
+          double v;
+          int cc;
+          if (ca == cb) { v = Q.val[a++] + QT.val[b++]; cc = ca; }
+          else if (ca < cb) { v = Q.val[a++]; cc = ca; }
+          else { v = QT.val[b++]; cc = cb; }
+          S.col.push_back(cc);
+          S.val.push_back(v / 2.0);
+        }
+        S.ptr[i + 1] = (int)S.col.size();
+      }
+      Q = std::move(S);
+    }
+    o.norm_b = norm_b_of(o.AL, o.AU, false);
+    o.norm_c = norm2(o.c);
+    // check_Q_diagonal on the scaled Q (src/utils.jl:827-855)
+    o.diag_Q.assign(n, 0.0);
+    std::vector<double> colsum(n, 0.0);
+    for (int64_t i = 0; i < n; ++i)
+      for (int k = Q.ptr[i]; k < Q.ptr[i + 1]; ++k) {
+        colsum[Q.col[k]] += std::fabs(Q.val[k]);
+        if (Q.col[k] == i) o.diag_Q[i] = Q.val[k];
+      }
+    const double rtol = std::sqrt(std::numeric_limits<double>::epsilon());
+    o.Q_is_diag = true;
+    for (int64_t j = 0; j < n && o.Q_is_diag; ++j) {
+      const double x = colsum[j], y = std::fabs(o.diag_Q[j]);
+      const bool ok = (x == y) || (std::isfinite(x) && std::isfinite(y) &&
+                                   std::fabs(x - y) <= rtol * std::max(std::fabs(x), std::fabs(y)));
+      if (!ok) o.Q_is_diag = false;
+    }
+    o.Q_maxval = Q.nnz() ? *std::max_element(Q.val.begin(), Q.val.end()) : 0.0;
+  }
+  int64_t nfree = 0;
+  for (int64_t i = 0; i < n; ++i) nfree += (hp.l[i] == -kInf && hp.u[i] == kInf);
+  o.noC = nfree > 0.8 * n;
+}
+
+}  // namespace hprqp

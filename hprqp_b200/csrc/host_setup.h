@@ -1,0 +1,59 @@
+// host_setup.h — host-side problem intake and scaling for libhprqp.
+//
+// Loading converts the caller's CSC arrays (QP_info_cpu, src/structs.jl:98-149)
+// into CSR and validates them.  Scaling restates the reference's scaling!
+// (src/utils.jl:350-804, CPU branch): 10 Ruiz passes on [Q; A], one
+// Pock-Chambolle pass, b/c scaling disabled, Q symmetrised afterwards, and
+// check_Q_diagonal (src/utils.jl:827-855).  It runs on the host once per
+// prepare; the scaled arrays are then uploaded to HBM.
+#pragma once
+
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/hprqp.h"
+
+namespace hprqp {
+
+struct HCsr {
+  int64_t rows = 0, cols = 0;
+  std::vector<int> ptr, col;
+  std::vector<double> val;
+  int64_t nnz() const { return (int64_t)val.size(); }
+};
+
+struct HostProblem {  // the loaded, unscaled problem
+  int64_t n = 0, m = 0;
+  int Q_kind = HPRQP_Q_SPARSE;
+  HCsr A;  // m x n
+  std::vector<double> c, AL, AU, l, u;
+  double obj_constant = 0.0, lambda = 0.0;
+  HCsr Q;  // n x n (sparse kind)
+  HCsr L;  // lasso data, lasso_m x n
+  int64_t qn = 0;
+  std::vector<double> qA, qB, qS, qT;  // column-major qn x qn
+  bool loaded = false;
+};
+
+struct Prepared {  // scaled problem + scaling info (Scaling_info_cpu)
+  HCsr A, AT, Q;
+  std::vector<double> c, AL, AU, l, u, row_norm, col_norm, diag_Q;
+  double norm_b = 0, norm_c = 0, norm_b_org = 0, norm_c_org = 0;
+  double b_scale = 1.0, c_scale = 1.0;
+  bool Q_is_diag = false;
+  double Q_maxval = 0.0;  // maximum(Q.nzval), lambda_max_Q of a diagonal Q
+  bool noC = false;
+  int ruiz = -1, pc = -1;
+};
+
+// Validate and copy; throws Error(HPRQP_E_ARG) on bad input.
+void load_problem(const hprqp_problem* pr, HostProblem& hp);
+// scaling! + check_Q_diagonal + the noC rule (src/algorithm.jl:1969-1974).
+void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& out);
+HCsr transpose(const HCsr& A);
+// splitmix64 + Box-Muller start vector of the power method (+1e-8).
+std::vector<double> power_start_vector(int64_t len);
+
+}  // namespace hprqp

@@ -1,0 +1,486 @@
+// kernels.cuh — sm_100a kernels of the HPR-QP iteration engine.
+//
+// Every iteration pass is ONE kernel: a CSR row product (TPR threads per
+// row, shuffle-reduced) whose per-row epilogue applies the projection /
+// prox / Halpern update of the reference's fused update kernels
+// (src/kernels.jl:261-1426).  The epilogues follow the reference CPU loops
+// (src/kernels.jl:2115-2832) expression by expression; `fma` stands where
+// the reference writes `muladd`.  Epilogue arithmetic is FP64; `V` is the
+// storage type of vectors and matrix values (double, or float in the FP32
+// phase), Halpern anchors (last_*) are always FP64.
+//
+// Reductions (KKT residuals, M-norm, sigma statistics, power method) are
+// single-pass: per-CTA shuffle/shared reduction, per-CTA partials, and the
+// last CTA to finish (atomic ticket) folds the partials in a fixed order, so
+// results are deterministic and stay on the device.
+#pragma once
+
+#include "common.cuh"
+
+namespace hprqp {
+
+// ---------------------------------------------------------------------------
+// Row sources: what the per-row accumulator is
+// ---------------------------------------------------------------------------
+template <typename V, typename X>
+struct CsrSrc {  // (M x)_row with M in CSR
+  const int* __restrict__ ptr;
+  const int* __restrict__ col;
+  const V* __restrict__ val;
+  const X* __restrict__ x;
+  template <int TPR, typename Acc>
+  __device__ __forceinline__ Acc dot(int row, int lane) const {
+    const int b = __ldg(ptr + row), e = __ldg(ptr + row + 1);
+    Acc s = Acc(0);
+#pragma unroll 4
+    for (int k = b + lane; k < e; k += TPR) s = fma((Acc)__ldg(val + k), (Acc)__ldg(x + __ldg(col + k)), s);
+    return group_sum<TPR>(s);
+  }
+};
+
+template <typename V>
+struct VecSrc {  // precomputed product (operator Q)
+  const V* __restrict__ v;
+  template <int TPR, typename Acc>
+  __device__ __forceinline__ Acc dot(int row, int) const { return (Acc)v[row]; }
+};
+
+struct ZeroSrc {
+  template <int TPR, typename Acc>
+  __device__ __forceinline__ Acc dot(int, int) const { return Acc(0); }
+};
+
+__device__ __forceinline__ double clampd(double v, double lo, double hi) { return fmin(fmax(v, lo), hi); }
+
+// ---------------------------------------------------------------------------
+// Generic row kernels
+// ---------------------------------------------------------------------------
+template <int TPR, typename Acc, typename Src, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_row_pass(int nrows, Src src, Epi epi) {
+  const long long g = (long long)blockIdx.x * kBlock + threadIdx.x;
+  const int row = (int)(g / TPR);
+  if (row >= nrows) return;  // whole row groups leave together
+  const int lane = threadIdx.x & (TPR - 1);
+  const Acc acc = src.template dot<TPR, Acc>(row, lane);
+  if (lane == 0) epi(row, acc);
+}
+
+// Block reduction of K slots; MaxMask bit k selects max (else sum).
+// Result valid in thread 0.
+template <int K, unsigned MaxMask>
+__device__ __forceinline__ void block_reduce(double (&r)[K]) {
+  __shared__ double sh[K][kBlock / 32];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    double v = r[k];
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, v, off);
+      v = ((MaxMask >> k) & 1u) ? fmax(v, o) : v + o;
+    }
+    if ((threadIdx.x & 31) == 0) sh[k][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double v = threadIdx.x < kBlock / 32 ? sh[k][threadIdx.x] : (((MaxMask >> k) & 1u) ? 0.0 : 0.0);
+#pragma unroll
+      for (int off = 16; off > 0; off >>= 1) {
+        const double o = __shfl_down_sync(0xffffffffu, v, off);
+        v = ((MaxMask >> k) & 1u) ? fmax(v, o) : v + o;
+      }
+      r[k] = v;
+    }
+  }
+  __syncthreads();
+}
+
+struct ReduceWs {  // partials (one K-vector per CTA) + ticket counter
+  double* partials;
+  unsigned* counter;
+};
+
+// Fold per-CTA partials in the last CTA; write K results to out.
+template <int K, unsigned MaxMask>
+__device__ __forceinline__ void grid_finish(double (&r)[K], ReduceWs ws, double* out) {
+  __shared__ bool am_last;
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) ws.partials[(size_t)blockIdx.x * K + k] = r[k];
+    __threadfence();
+    const unsigned t = atomicAdd(ws.counter, 1u);
+    am_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!am_last) return;
+  __threadfence();
+  double acc[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) acc[k] = 0.0;
+  for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const double v = __ldcg(ws.partials + (size_t)b * K + k);
+      acc[k] = ((MaxMask >> k) & 1u) ? fmax(acc[k], v) : acc[k] + v;
+    }
+  }
+  block_reduce<K, MaxMask>(acc);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) out[k] = acc[k];
+    *ws.counter = 0u;
+  }
+}
+
+// Row product + epilogue that also contributes to K reduction slots.
+// Grid-stride over rows; the grid is capped so the partials stay small.
+template <int TPR, int K, unsigned MaxMask, typename Acc, typename Src, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_row_reduce(int nrows, Src src, Epi epi, ReduceWs ws,
+                                                       double* out) {
+  double r[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) r[k] = 0.0;
+  const int lane = threadIdx.x & (TPR - 1);
+  const int rows_per_grid = (int)(gridDim.x * (kBlock / TPR));
+  for (int row = (int)((blockIdx.x * kBlock + threadIdx.x) / TPR); row < nrows; row += rows_per_grid) {
+    const Acc acc = src.template dot<TPR, Acc>(row, lane);
+    if (lane == 0) epi(row, acc, r);
+  }
+  block_reduce<K, MaxMask>(r);
+  grid_finish<K, MaxMask>(r, ws, out);
+}
+
+// ---------------------------------------------------------------------------
+// Epilogues of the iteration passes
+// ---------------------------------------------------------------------------
+
+// Plain product: y = scale * (M x)
+template <typename V>
+struct EpiStore {
+  V* __restrict__ y;
+  double scale;
+  __device__ __forceinline__ void operator()(int i, double acc) const { y[i] = (V)(scale * acc); }
+  __device__ __forceinline__ void operator()(int i, float acc) const { y[i] = (V)(scale * (double)acc); }
+};
+
+// QP step 1: Qw = Q w fused with update_zxw1_cpu! (src/kernels.jl:2301-2397)
+template <typename V, bool Full, bool Diag>
+struct EpiZxw1 {
+  V *Qw, *x, *x_hat, *w_bar, *dx, *x_bar, *z_bar;
+  const V *ATy, *c, *l, *u, *w, *fact1, *fact2;
+  const double* last_x;
+  double sigma, f1s, f2s, h1, h2;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const double qw = (double)acc;
+    Qw[i] = (V)qw;
+    const double x_i = x[i], w_i = w[i];
+    const double tmp = -qw + (double)ATy[i] - (double)c[i];
+    const double z_raw = x_i + sigma * tmp;
+    const double xb = clampd(z_raw, l[i], u[i]);
+    const double xh = 2.0 * xb - x_i;
+    const double xn = fma(h2, xh, h1 * last_x[i]);
+    const double wb = Diag ? fma((double)fact1[i], w_i, (double)fact2[i] * xh) : fma(f1s, w_i, f2s * xh);
+    if (Full) {
+      dx[i] = (V)(xb - x_i);
+      x_bar[i] = (V)xb;
+      z_bar[i] = (V)((xb - z_raw) / sigma);
+    }
+    x[i] = (V)xn;
+    x_hat[i] = (V)xh;
+    w_bar[i] = (V)wb;
+  }
+};
+
+// QP step 2: tempv = x_hat + sigma (Qw - Q w_bar)  (update_y_cpu!, kernels.jl:2690-2694)
+template <typename V>
+struct EpiTempv {
+  V* tempv;
+  const V *x_hat, *Qw;
+  double sigma;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    tempv[i] = (V)((double)x_hat[i] + sigma * ((double)Qw[i] - (double)acc));
+  }
+};
+
+// y step: A*v fused with update_y_cpu! / unified_update_y_cpu! /
+// unified_update_y_noQ_cpu! (src/kernels.jl:2242-2298, 2582-2658, 2682-2743).
+// YbarAlways: the QP / noC loops write y_bar in partial steps too, the LP
+// loop only in full steps.
+template <typename V, bool Full, bool YbarAlways>
+struct EpiY {
+  V *y, *y_bar, *s, *dy;
+  const V *AL, *AU;
+  const double* last_y;
+  double f1, f2, h1, h2;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const double yi = y[i];
+    const double s_raw = (double)acc - f1 * yi;
+    const double s_proj = clampd(s_raw, AL[i], AU[i]);
+    const double yb = f2 * (s_proj - s_raw);
+    const double yh = 2.0 * yb - yi;
+    const double yn = fma(h2, yh, h1 * last_y[i]);
+    if (Full) {
+      s[i] = (V)s_proj;
+      dy[i] = (V)(yb - yi);
+    }
+    if (Full || YbarAlways) y_bar[i] = (V)yb;
+    y[i] = (V)yn;
+  }
+};
+
+// QP step 4: A'y_bar fused with update_w2_cpu! (src/kernels.jl:2747-2832)
+template <typename V, bool Full, bool Diag>
+struct EpiW2 {
+  V *w, *ATy, *w_bar, *dw, *ATdy, *ATy_bar;
+  const V* fact;
+  const double *last_w, *last_ATy;
+  double fs, h1, h2;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const double atyb = (double)acc;
+    const double w_i = w[i], aty = ATy[i];
+    const double f = Diag ? (double)fact[i] : fs;
+    const double wbn = (double)w_bar[i] + f * (atyb - aty);
+    const double wn = h1 * last_w[i] + h2 * (2.0 * wbn - w_i);
+    const double atyn = h1 * last_ATy[i] + h2 * (2.0 * atyb - aty);
+    w[i] = (V)wn;
+    ATy[i] = (V)atyn;
+    if (Full) {
+      w_bar[i] = (V)wbn;
+      dw[i] = (V)(wbn - w_i);
+      ATdy[i] = (V)(atyb - aty);
+      ATy_bar[i] = (V)atyb;
+    }
+  }
+};
+
+// QP-noC step 1: A'y fused with unified_update_zxw_cpu! (kernels.jl:2117-2223)
+template <typename V, bool Full, bool Diag>
+struct EpiZxwNoC {
+  V *x, *x_hat, *w_bar, *w, *dx, *x_bar, *z_bar, *dw;
+  const V *Qw, *c, *l, *u, *fact1, *fact2;
+  const double *last_x, *last_w;
+  double sigma, f1s, f2s, h1, h2;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const double x_i = x[i], w_i = w[i];
+    const double tmp = -(double)Qw[i] + (double)acc - (double)c[i];
+    const double z_raw = x_i + sigma * tmp;
+    const double xb = clampd(z_raw, l[i], u[i]);
+    const double xh = 2.0 * xb - x_i;
+    const double xn = fma(h2, xh, h1 * last_x[i]);
+    const double wb = Diag ? fma((double)fact1[i], w_i, (double)fact2[i] * xh) : fma(f1s, w_i, f2s * xh);
+    const double wh = 2.0 * wb - w_i;
+    const double wn = fma(h2, wh, h1 * last_w[i]);
+    if (Full) {
+      dx[i] = (V)(xb - x_i);
+      x_bar[i] = (V)xb;
+      z_bar[i] = (V)((xb - z_raw) / sigma);
+      dw[i] = (V)(wb - w_i);
+    }
+    x[i] = (V)xn;
+    x_hat[i] = (V)xh;
+    w_bar[i] = (V)wb;
+    w[i] = (V)wn;
+  }
+};
+
+// QP-noC step 2: Q w_bar; Halpern-averaged Qw and tempv (kernels.jl:2226-2237)
+template <typename V, bool Full>
+struct EpiTempvNoC {
+  V *Qw, *tempv, *Qw_bar;
+  const V* x_hat;
+  const double* last_Qw;
+  double sigma, h1, h2;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const double qwb = (double)acc, qw = Qw[i];
+    const double qwh = 2.0 * qwb - qw;
+    Qw[i] = (V)fma(h2, qwh, h1 * last_Qw[i]);
+    tempv[i] = (V)((double)x_hat[i] + sigma * (qw - qwb));
+    if (Full) Qw_bar[i] = (V)qwb;
+  }
+};
+
+// LP step 1: A'y fused with unified_update_zx_cpu! (kernels.jl:2504-2578)
+template <typename V, bool Full>
+struct EpiZxLP {
+  V *x, *x_hat, *dx, *x_bar, *z_bar;
+  const V *c, *l, *u;
+  const double* last_x;
+  double sigma, h1, h2;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const double x_i = x[i];
+    const double z_raw = x_i + sigma * ((double)acc - (double)c[i]);
+    const double xb = clampd(z_raw, l[i], u[i]);
+    const double xh = 2.0 * xb - x_i;
+    const double xn = fma(h2, xh, h1 * last_x[i]);
+    if (Full) {
+      dx[i] = (V)(xb - x_i);
+      x_bar[i] = (V)xb;
+      z_bar[i] = (V)((xb - z_raw) / sigma);
+    }
+    x[i] = (V)xn;
+    x_hat[i] = (V)xh;
+  }
+};
+
+// LASSO: A_d'(A_d w) fused with update_zxw_LASSO_cpu! (kernels.jl:2400-2496)
+template <typename V, bool Full>
+struct EpiLasso {
+  V *x, *x_hat, *w_bar, *w, *dx, *x_bar, *z_bar, *dw;
+  const V* c;
+  const double *last_x, *last_w;
+  double sigma, lam, f1s, f2s, h1, h2;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    const double x_i = x[i], w_i = w[i];
+    const double tmp = -(double)acc + 0.0 - (double)c[i];  // A'y == 0 (m = 0)
+    const double z_raw = x_i + sigma * tmp;
+    const double shrink = fmax(fabs(z_raw) - lam * sigma, 0.0);
+    const double xb = copysign(shrink, z_raw);
+    const double xh = 2.0 * xb - x_i;
+    const double xn = fma(h2, xh, h1 * last_x[i]);
+    const double wb = fma(f1s, w_i, f2s * xh);
+    const double wn = fma(h2, 2.0 * wb - w_i, h1 * last_w[i]);
+    if (Full) {
+      dx[i] = (V)(xb - x_i);
+      x_bar[i] = (V)xb;
+      z_bar[i] = (V)((xb - z_raw) / sigma);
+      dw[i] = (V)(wb - w_i);
+    }
+    x[i] = (V)xn;
+    x_hat[i] = (V)xh;
+    w_bar[i] = (V)wb;
+    w[i] = (V)wn;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Reduction epilogues
+// ---------------------------------------------------------------------------
+
+// compute_residuals! n-part (algorithm.jl:55-79, kernels.jl:132-148,
+// algorithm.jl:127-133): acc = (A' y_bar)_i.
+// slots: 0 c'x  1 x'Qx  2 z'x  3 |lam x|_1  4 |Rd|inf  5 |A'y s|inf  6 |Qx s|inf  7 bound viol
+template <typename V>
+struct EpiResN {
+  const V *x_bar, *Qx, *c, *z_bar, *col_norm, *l, *u;
+  double lam, c_scale, b_scale;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, double (&r)[8]) const {
+    const double xb = x_bar[i], qx = Qx[i], ci = c[i], zb = z_bar[i];
+    const double aty = (double)acc;
+    const double f = (double)col_norm[i] * c_scale;
+    r[0] += ci * xb;
+    r[1] += xb * qx;
+    r[2] += zb * xb;
+    r[3] += fabs(lam * xb);
+    r[4] = fmax(r[4], fabs((qx + ci - aty - zb) * f));
+    r[5] = fmax(r[5], fabs(aty * f));
+    r[6] = fmax(r[6], fabs(qx * f));
+    const double viol = fmax((double)l[i] - xb, 0.0) + fmax(xb - (double)u[i], 0.0);
+    r[7] = fmax(r[7], fabs(viol * (b_scale / (double)col_norm[i])));
+  }
+};
+constexpr unsigned kResNMax = (1u << 4) | (1u << 5) | (1u << 6) | (1u << 7);
+
+// compute_residuals! m-part (algorithm.jl:62,82-85, kernels.jl:172-194):
+// acc = (A x_bar)_i.  slots: 0 y's  1 |Rp|inf  2 |Ax s|inf
+template <typename V>
+struct EpiResM {
+  const V *y_bar, *s, *AL, *AU, *row_norm;
+  double b_scale;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, double (&r)[3]) const {
+    const double ax = (double)acc;
+    const double corr = clampd(ax, AL[i], AU[i]) - ax;
+    const double f = (double)row_norm[i] * b_scale;
+    r[0] += (double)y_bar[i] * (double)s[i];
+    r[1] = fmax(r[1], fabs(corr * f));
+    r[2] = fmax(r[2], fabs(ax * f));
+  }
+};
+constexpr unsigned kResMMax = (1u << 1) | (1u << 2);
+
+// compute_M_norm! n-part (algorithm.jl:689-739).  slots:
+// 0 dx.dx 1 dQw.dx 2 dQw.ATdy 3 ATdy.dx 4 (ATdy*fact_M).QATdy 5 ATdy.QATdy 6 dQw.dQw 7 dw.dQw
+template <typename V>
+struct EpiMnormN {
+  const V *dx, *dQw, *ATdy, *QATdy, *fact_M, *dw;
+  bool has_m;
+  __device__ __forceinline__ void operator()(int i, double, double (&r)[8]) const {
+    const double ddx = dx[i], dqw = dQw[i], ddw = dw[i];
+    r[0] += ddx * ddx;
+    r[1] += dqw * ddx;
+    if (has_m) {
+      const double at = ATdy[i], qat = QATdy[i];
+      r[2] += dqw * at;
+      r[3] += at * ddx;
+      r[4] += (at * (double)fact_M[i]) * qat;
+      r[5] += at * qat;
+    }
+    r[6] += dqw * dqw;
+    r[7] += ddw * dqw;
+  }
+  __device__ __forceinline__ void operator()(int i, float a, double (&r)[8]) const { (*this)(i, (double)a, r); }
+};
+
+// sum of squares of an m-vector (dy.dy)
+template <typename V>
+struct EpiSumSq {
+  const V* v;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A, double (&r)[1]) const {
+    const double t = v[i];
+    r[0] += t * t;
+  }
+};
+
+// update_sigma! statistics (algorithm.jl:344-371). slots:
+// 0 dx.dx 1 dQw.ATdy 2 dQw.dQw 3 dw.dQw 4 ATdy.QATdy
+template <typename V>
+struct EpiSigmaN {
+  const V *dx, *dQw, *ATdy, *QATdy, *dw;
+  bool has_m;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A, double (&r)[5]) const {
+    const double ddx = dx[i], dqw = dQw[i], ddw = dw[i];
+    r[0] += ddx * ddx;
+    if (has_m) {
+      const double at = ATdy[i];
+      r[1] += dqw * at;
+      r[4] += at * (double)QATdy[i];
+    }
+    r[2] += dqw * dqw;
+    r[3] += ddw * dqw;
+  }
+};
+
+// Power method partial sums: 0 q.z  1 z.z   (q = zold/||zold||)
+template <typename V>
+struct EpiPowerDot {
+  const V *q, *z;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A, double (&r)[2]) const {
+    const double zi = z[i];
+    r[0] += (double)q[i] * zi;
+    r[1] += zi * zi;
+  }
+};
+
+// ---------------------------------------------------------------------------
+// Element-wise kernels
+// ---------------------------------------------------------------------------
+template <typename F>
+__global__ void __launch_bounds__(kBlock) k_elementwise(int len, F f) {
+  const int i = blockIdx.x * kBlock + threadIdx.x;
+  if (i < len) f(i);
+}
+
+}  // namespace hprqp

@@ -1,0 +1,555 @@
+// solver.cu — the HPR control loop and the C ABI of libhprqp.so.
+//
+// The loop restates solve() (src/algorithm.jl:1904-2039) on the host with
+// every vector in HBM: per iteration it only enqueues the fused passes of
+// Engine::step(); it synchronises with the device only on the residual
+// cadence of the reference (check_iter and the print schedule), reading the
+// residual, M-norm and sigma scalars in one copy.  Restart decisions, the
+// sigma blend and the scalar golden-section search (src/kernels.jl:1453-1486)
+// run on the host from those scalars.
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+
+#include "engine.cuh"
+
+namespace hprqp {
+
+namespace {
+const double kInf = std::numeric_limits<double>::infinity();
+thread_local std::string g_global_err;
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+double print_step(int64_t iter) {  // src/algorithm.jl:1173-1175
+  return std::max(std::pow(10.0, std::floor(std::log10((double)iter))) / 10.0, 10.0);
+}
+bool on_print_schedule(int64_t iter, const hprqp_params& p) {
+  if (p.print_frequency == -1) return std::fmod((double)iter, print_step(iter)) == 0.0;
+  return iter % p.print_frequency == 0;
+}
+
+// golden (src/kernels.jl:1453-1486)
+double golden(double ap, double bp, double cp, double dp, double lo, double hi, double tol, int maxiter = 200) {
+  auto f = [&](double x) { return ap * x + bp / x + cp * x * x / (1 + dp * x); };
+  const double phi = (std::sqrt(5.0) - 1.0) / 2.0;
+  double a = lo, b = hi, c = b - phi * (b - a), d = a + phi * (b - a);
+  double fc = f(c), fd = f(d);
+  for (int i = 0; i < maxiter; ++i) {
+    if (fd < fc) {
+      a = c; c = d; fc = fd;
+      d = a + phi * (b - a);
+      fd = f(d);
+    } else {
+      b = d; d = c; fd = fc;
+      c = b - phi * (b - a);
+      fc = f(c);
+    }
+    if ((b - a) < tol) break;
+  }
+  return 0.5 * (a + b);
+}
+}  // namespace
+
+struct RestartInfo {  // HPRQP_restart / initialize_restart (src/algorithm.jl:1154-1171)
+  bool first_restart = true;
+  double save_gap = kInf, current_gap = kInf, last_gap = kInf, best_gap = kInf;
+  double best_sigma = 1.0, weighted_norm = kInf;
+  int64_t inner = 0, times = 0, sufficient = 0, necessary = 0, long_ = 0;
+  int restart_flag = 0;
+};
+
+struct Residuals {
+  double err_Rp = 0, err_Rd = 0, KKT = kInf, pobj = 0, dobj = 0, gap = 0;
+};
+
+struct Handle {
+  int device = 0;
+  std::unique_ptr<Common> cm;
+  HostProblem hp;
+  Prepared pp;
+  bool prepared = false;
+  int key[5] = {-1, -1, -1, -1, -1};
+  int path = PATH_QP;
+  std::unique_ptr<Engine<double>> e64;
+  std::unique_ptr<Engine<float>> e32;
+  std::string err;
+  int64_t trace_iters = 0;
+  double *xt = nullptr, *yt = nullptr, *wt = nullptr;
+  double setup_time = 0.0;
+};
+
+struct LoopState {
+  int64_t iter = 0;
+  RestartInfo ri;
+  Residuals res;
+  double t0 = 0;
+  int64_t iter_4 = 0, iter_6 = 0;
+  double time_4 = 0, time_6 = 0;
+  bool first_4 = true, first_6 = true;
+  PendingMnorm pend_cur, pend_last;
+  double polish_tol = 0, best_kkt = kInf;
+  int stall = 0;
+  bool force_residuals = false;
+  int status = -1;
+};
+
+constexpr int kSwitch = -100;
+
+static double eval_mnorm(const Common& cm, const PendingMnorm& pm, bool has_m, bool diag, bool verbose) {
+  const double* s = cm.h_scal + pm.slot;
+  const double sg = pm.sigma;
+  double M1 = 0.0, M2 = (1.0 / sg) * s[0], M3 = 0.0;
+  M2 -= 2.0 * s[1];
+  if (has_m) {
+    M1 = sg * pm.lamA * s[8];
+    M1 -= 2.0 * sg * s[2];
+    M2 += 2.0 * s[3];
+    if (diag) {
+      M3 = s[4];
+      M1 += sg * s[6];
+    } else {
+      M3 = (sg * sg) / (1.0 + sg * pm.lamQ) * s[5];
+      M1 += sg * pm.lamQ * s[7];
+    }
+  } else if (!diag) {
+    M1 = sg * pm.lamQ * s[7];
+  }
+  M2 += std::max(M1, 0.0);
+  const double Mn = std::max(M2, 0.0) + std::max(M3, 0.0);
+  if (verbose && std::min(std::min(M1, M2), M3) < -1e-8)
+    std::printf("M_1 = %g, M_2 = %g, M_3 = %g, negative M norm due to numerical instability, consider increasing eig_factor\n",
+                M1, M2, M3);
+  return std::sqrt(Mn);
+}
+
+// One phase of the HPR loop on engine E (src/algorithm.jl:1977-2038).
+// Returns a final status, or kSwitch when the FP32 phase hands over.
+template <typename V>
+static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L, bool fp32_phase) {
+  Common& cm = *H.cm;
+  const int64_t n = E.n, m = E.m;
+  const int64_t check_iter = p.check_iter;
+  RestartInfo& ri = L.ri;
+  for (; L.iter <= p.max_iter; ++L.iter) {
+    const int64_t iter = L.iter;
+    const bool time_up = now_s() - L.t0 > p.time_limit;
+    const bool print_yes = on_print_schedule(iter, p) || iter == p.max_iter || time_up;
+    if (iter % check_iter == 0 || print_yes || L.force_residuals) {
+      L.force_residuals = false;
+      E.residuals_launch(iter == 0);
+      cm.sync_read(0, S_GOLD);
+      if (L.pend_cur.active) {
+        ri.current_gap = eval_mnorm(cm, L.pend_cur, m > 0, E.Q_is_diag, p.verbose);
+        L.pend_cur.active = false;
+      }
+      if (L.pend_last.active) {
+        ri.last_gap = eval_mnorm(cm, L.pend_last, m > 0, E.Q_is_diag, p.verbose);
+        L.pend_last.active = false;
+      }
+      // compute_residuals! (src/algorithm.jl:37-115) from the reduced slots
+      const double* r = cm.h_scal;
+      const double bc = E.b_scale * E.c_scale;
+      Residuals& R = L.res;
+      R.pobj = bc * (r[S_RES_N + 0] + 0.5 * r[S_RES_N + 1]) + H.hp.obj_constant;
+      R.dobj = bc * (-0.5 * r[S_RES_N + 1] + r[S_RES_N + 2]) + H.hp.obj_constant;
+      if (m > 0) R.dobj += bc * r[S_RES_M + 0];
+      if (p.problem_type == HPRQP_PROBLEM_LASSO && n > 0) {
+        R.pobj += bc * r[S_RES_N + 3];
+        R.dobj += bc * r[S_RES_N + 3];
+      }
+      R.gap = std::fabs(R.pobj - R.dobj) / (1.0 + std::max(std::fabs(R.pobj), std::fabs(R.dobj)));
+      R.err_Rd = r[S_RES_N + 4] / (1.0 + std::max(std::max(E.norm_c_org, r[S_RES_N + 5]), r[S_RES_N + 6]));
+      R.err_Rp = m > 0 ? r[S_RES_M + 1] / (1.0 + std::max(E.norm_b_org, r[S_RES_M + 2])) : 0.0;
+      if (iter == 0) R.err_Rp = std::max(R.err_Rp, r[S_RES_N + 7]);
+      R.KKT = std::max(std::max(R.err_Rp, R.err_Rd), R.gap);
+      if (!std::isfinite(R.KKT) || !std::isfinite(R.pobj) || !std::isfinite(R.dobj)) return HPRQP_STATUS_NUMERICAL_ERROR;
+      if (fp32_phase) {
+        if (R.KKT < L.polish_tol) return kSwitch;
+        if (R.KKT < 0.9 * L.best_kkt) {
+          L.best_kkt = R.KKT;
+          L.stall = 0;
+        } else if (++L.stall >= 50 && iter >= 1000) {
+          return kSwitch;
+        }
+      }
+    }
+    // check_break (src/algorithm.jl:558-576)
+    int status = -1;
+    if (L.res.KKT < p.stoptol) status = HPRQP_STATUS_OPTIMAL;
+    else if (iter == p.max_iter) status = HPRQP_STATUS_MAX_ITER;
+    else if (now_s() - L.t0 > p.time_limit) status = HPRQP_STATUS_TIME_LIMIT;
+    // check_restart (src/algorithm.jl:441-492)
+    ri.restart_flag = 0;
+    if (ri.first_restart) {
+      if (iter == check_iter) {
+        ri.first_restart = false;
+        ri.restart_flag = 1;
+        ri.weighted_norm = ri.current_gap;
+        ri.best_gap = ri.current_gap;
+        ri.best_sigma = E.sigma;
+      }
+    } else if (iter % check_iter == 0) {
+      if (ri.current_gap < 0) {
+        ri.current_gap = 1e-6;
+        if (p.verbose) std::printf("current_gap < 0\n");
+      }
+      if (ri.current_gap <= 0.2 * ri.last_gap) { ri.sufficient++; ri.restart_flag = 1; }
+      if (ri.current_gap <= 0.8 * ri.last_gap && ri.current_gap > 1.00 * ri.save_gap) {
+        ri.necessary++;
+        ri.restart_flag = 2;
+      }
+      const double fact = (ri.current_gap / ri.weighted_norm > 1e-1) ? 0.5 : 0.2;
+      if (ri.inner >= fact * iter) { ri.long_++; ri.restart_flag = 3; }
+      if (ri.best_gap > ri.current_gap) { ri.best_gap = ri.current_gap; ri.best_sigma = E.sigma; }
+      ri.save_gap = ri.current_gap;
+    }
+    // update_sigma! (src/algorithm.jl:323-423)
+    if (!p.sigma_fixed && ri.restart_flag >= 1) {
+      const double sigma_old = E.sigma;
+      E.sigma_stats_launch();
+      cm.sync_read(S_SIG, 6);
+      const double* s = cm.h_scal + S_SIG;
+      double a = 0.0, b = s[0], c = 0.0, d = 0.0;
+      if (m > 0) a = E.lamA * s[5] - 2 * s[1];
+      if (E.Q_is_diag) {
+        const double nq = std::sqrt(s[2]);
+        a += nq * nq;
+      } else {
+        a += E.lamQ * s[3];
+        if (m > 0) { c = s[4]; d = E.lamQ; }
+      }
+      a = std::max(a, 1e-12);
+      b = std::max(b, 1e-12);
+      double est;
+      if (E.Q_is_diag) {
+        if (m > 0) {
+          E.golden_diag_launch(a, b);
+          cm.sync_read(S_GOLD, 1);
+          est = cm.h_scal[S_GOLD];
+        } else {
+          est = std::sqrt(b / a);
+        }
+      } else {
+        est = m > 0 ? golden(a, b, c, d, 1e-12, 1e12, 1e-13) : std::sqrt(b / a);
+      }
+      const double fct = std::exp(-0.05 * (ri.current_gap / ri.best_gap));
+      const double temp1 = std::max(std::min(L.res.err_Rd, L.res.err_Rp), std::min(L.res.gap, ri.current_gap));
+      const double cand = std::exp(fct * std::log(est) + (1 - fct) * std::log(ri.best_sigma));
+      double kappa;
+      if (temp1 > 9e-10) kappa = 1.0;
+      else if (temp1 > 5e-10) kappa = std::min(std::max(std::sqrt(L.res.err_Rd / L.res.err_Rp), 1e-2), 100.0);
+      else kappa = std::min(std::max(L.res.err_Rd / L.res.err_Rp, 1e-2), 100.0);
+      const double sigma_new = kappa * cand;
+      if (E.Q_is_diag && std::fabs(sigma_old - sigma_new) > 1e-15) E.set_sigma(sigma_new);
+      else E.sigma = sigma_new;
+    }
+    // do_restart! (src/algorithm.jl:522-555)
+    if (ri.restart_flag > 0) {
+      E.restart();
+      ri.last_gap = ri.current_gap;
+      ri.save_gap = kInf;
+      ri.times++;
+      ri.inner = 0;
+    }
+    if ((print_yes || status >= 0) && p.verbose)
+      std::printf("%5lld    %3.2e    %3.2e    %+7.6e    %+7.6e    %3.2e    %3.2e    %6.2f\n", (long long)iter,
+                  L.res.err_Rp, L.res.err_Rd, L.res.pobj, L.res.dobj, L.res.gap, E.sigma, now_s() - L.t0);
+    if (L.res.KKT < 1e-4 && L.first_4) { L.time_4 = now_s() - L.t0; L.iter_4 = iter; L.first_4 = false; }
+    if (L.res.KKT < 1e-6 && L.first_6) { L.time_6 = now_s() - L.t0; L.iter_6 = iter; L.first_6 = false; }
+    if (status >= 0) return status;
+    const int64_t next = iter + 1;
+    const bool to_check = (next % check_iter == 0) || (ri.restart_flag > 0) || on_print_schedule(next, p);
+    // perform_iteration_step! (src/algorithm.jl:1881-1900)
+    const double h1 = 1.0 / (ri.inner + 2.0), h2 = 1.0 - h1;
+    E.step(to_check, h1, h2);
+    if (ri.restart_flag > 0) {
+      E.mnorm_launch(S_MN_LAST);
+      L.pend_last = PendingMnorm{true, S_MN_LAST, E.sigma, E.lamA, E.lamQ};
+    }
+    if ((iter + 1) % check_iter == 0) {
+      E.mnorm_launch(S_MN_CUR);
+      L.pend_cur = PendingMnorm{true, S_MN_CUR, E.sigma, E.lamA, E.lamQ};
+    }
+    ri.inner++;
+    if (next <= H.trace_iters)
+      E.trace_copy(H.xt ? H.xt + (next - 1) * n : nullptr, H.yt ? H.yt + (next - 1) * m : nullptr,
+                   H.wt ? H.wt + (next - 1) * n : nullptr);
+  }
+  return HPRQP_STATUS_MAX_ITER;
+}
+
+static void check_params(const hprqp_params& p) {
+  if (!(p.stoptol > 0)) throw Error(HPRQP_E_ARG, "stoptol must be positive");
+  if (p.check_iter <= 0) throw Error(HPRQP_E_ARG, "check_iter must be positive");
+  if (p.max_iter < 0) throw Error(HPRQP_E_ARG, "max_iter must be >= 0");
+  if (!(p.sigma == -1 || p.sigma > 0))
+    throw Error(HPRQP_E_ARG, "Invalid sigma value. It should be a positive number or -1 for automatic.");
+  if (!(p.print_frequency == -1 || p.print_frequency > 0))
+    throw Error(HPRQP_E_ARG, "Invalid print_frequency. It should be a positive integer or -1 for automatic printing.");
+  if (p.auto_save) throw Error(HPRQP_E_UNSUPPORTED, "auto_save (HDF5) is not implemented by libhprqp");
+  if (!p.use_gpu) throw Error(HPRQP_E_UNSUPPORTED, "use_gpu = false: libhprqp has no CPU path");
+  if (p.precision != HPRQP_PRECISION_FP64 && p.precision != HPRQP_PRECISION_FP32_POLISH)
+    throw Error(HPRQP_E_ARG, "unknown precision mode");
+  if (p.spmv_mode_Q < 0 || p.spmv_mode_Q > 6 || p.spmv_mode_A < 0 || p.spmv_mode_A > 6)
+    throw Error(HPRQP_E_ARG, "spmv_mode must be 0 (auto) or 1..6 (1,2,4,8,16,32 threads per row)");
+}
+
+static void prepare(Handle& H, const hprqp_params& p) {
+  if (!H.hp.loaded) throw Error(HPRQP_E_STATE, "no problem loaded");
+  check_params(p);
+  const int key[5] = {p.use_Ruiz_scaling, p.use_Pock_Chambolle_scaling, p.precision, p.spmv_mode_Q, p.spmv_mode_A};
+  if (H.prepared && std::memcmp(key, H.key, sizeof(key)) == 0) return;
+  const double t = now_s();
+  H.e64.reset();
+  H.e32.reset();
+  prepare_problem(H.hp, p, H.pp);
+  if (H.hp.Q_kind == HPRQP_Q_LASSO) H.path = PATH_LASSO;
+  else if (H.hp.Q_kind == HPRQP_Q_QAP || H.pp.Q.nnz() > 0) H.path = H.pp.noC ? PATH_NOC : PATH_QP;
+  else H.path = PATH_LP;
+  H.e64 = std::make_unique<Engine<double>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A);
+  if (p.precision == HPRQP_PRECISION_FP32_POLISH)
+    H.e32 = std::make_unique<Engine<float>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A);
+  std::memcpy(H.key, key, sizeof(key));
+  H.prepared = true;
+  H.setup_time = now_s() - t;
+}
+
+template <typename V>
+static void start_engine(Handle& H, Engine<V>& E, const hprqp_params& p, double lamA, double lamQ, double sigma0,
+                         const double* x0, const double* y0) {
+  E.reset_state();
+  E.lamA = lamA;
+  E.lamQ = lamQ;
+  E.lam_l1 = p.problem_type == HPRQP_PROBLEM_LASSO ? H.hp.lambda : 0.0;
+  E.sigma = sigma0;
+  E.initial_points(x0, y0);
+  if (E.Q_is_diag) E.set_sigma(sigma0);
+}
+
+static int solve(Handle& H, const hprqp_params& p, const double* x0, const double* y0, hprqp_result* res,
+                 double* xo, double* yo, double* zo, double* wo) {
+  const double setup_start = now_s();
+  prepare(H, p);
+  const double setup_time = now_s() - setup_start;
+  Common& cm = *H.cm;
+  const int64_t launches0 = cm.launches;
+  const Prepared& pp = H.pp;
+  const int64_t m = H.hp.m;
+  Engine<double>& E64 = *H.e64;
+  LoopState L;
+  L.t0 = now_s();
+  // estimate_eigenvalues (src/algorithm.jl:1407-1440)
+  double lamA = 0.0, lamQ = 0.0;
+  int64_t pit = 0;
+  if (m > 0) lamA = p.lambda_max_A_override > 0 ? p.lambda_max_A_override : E64.power_A(1e-4, 5000, &pit) * p.eig_factor;
+  if (H.hp.Q_kind != HPRQP_Q_SPARSE) {
+    lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : E64.power_Q(1e-4, 5000, &pit) * p.eig_factor;
+  } else if (pp.Q.nnz() > 0) {
+    if (!pp.Q_is_diag)
+      lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : E64.power_Q(1e-4, 5000, &pit) * p.eig_factor;
+    else
+      lamQ = pp.Q_maxval;
+  }
+  const double power_time = now_s() - L.t0;
+  // sigma of allocate_workspace (src/algorithm.jl:838-851)
+  double sigma0 = p.sigma > 0 ? p.sigma : 1.0;
+  if (p.sigma == -1)
+    sigma0 = (pp.norm_c > 1e-16 && pp.norm_b > 1e-16 && pp.norm_b < 1e16 && pp.norm_c < 1e16) ? pp.norm_b / pp.norm_c : 1.0;
+  L.ri.best_sigma = sigma0;
+  L.polish_tol = p.polish_tol > 0 ? p.polish_tol : 10.0 * p.stoptol;
+  int status;
+  int64_t iter_fp32 = 0;
+  bool final64 = true;
+  if (p.precision == HPRQP_PRECISION_FP32_POLISH) {
+    Engine<float>& E32 = *H.e32;
+    start_engine(H, E32, p, lamA, lamQ, sigma0, x0, y0);
+    status = run_loop(H, E32, p, L, true);
+    iter_fp32 = L.iter;
+    if (status == kSwitch) {
+      E64.import_state(E32);
+      L.force_residuals = true;
+      status = run_loop(H, E64, p, L, false);
+    } else {
+      final64 = false;
+    }
+  } else {
+    start_engine(H, E64, p, lamA, lamQ, sigma0, x0, y0);
+    status = run_loop(H, E64, p, L, false);
+  }
+  // handle_termination + collect_results! (src/algorithm.jl:1039-1097, 611-643)
+  if (final64) E64.collect(xo, yo, zo, wo);
+  else H.e32->collect(xo, yo, zo, wo);
+  const double t_end = now_s() - L.t0;
+  std::memset(res, 0, sizeof(*res));
+  res->iter = L.iter;
+  res->time = t_end;
+  res->power_time = power_time;
+  res->setup_time = setup_time > 0 ? std::max(setup_time, 0.0) : 0.0;
+  if (setup_time < 1e-9) res->setup_time = 0.0;
+  res->primal_obj = L.res.pobj;
+  res->dual_obj = L.res.dobj;
+  res->residuals = L.res.KKT;
+  res->gap = L.res.gap;
+  res->err_Rp = L.res.err_Rp;
+  res->err_Rd = L.res.err_Rd;
+  res->status = status;
+  res->Q_is_diag = pp.Q_is_diag;
+  res->sigma = final64 ? E64.sigma : H.e32->sigma;
+  res->lambda_max_A = lamA;
+  res->lambda_max_Q = lamQ;
+  res->restarts = L.ri.times;
+  res->time_4 = L.time_4 == 0.0 ? t_end : L.time_4;
+  res->iter_4 = L.iter_4 == 0 ? L.iter : L.iter_4;
+  res->time_6 = L.time_6 == 0.0 ? t_end : L.time_6;
+  res->iter_6 = L.iter_6 == 0 ? L.iter : L.iter_6;
+  res->iter_fp32 = iter_fp32;
+  res->gpu_launches = cm.launches - launches0;
+  if (p.verbose) {
+    static const char* names[] = {"OPTIMAL", "MAX_ITER", "TIME_LIMIT", "NUMERICAL_ERROR"};
+    std::printf("Status: %s  Iterations: %lld  Time: %.3f s  Primal Objective: %.12e  KKT: %.3e\n",
+                names[status], (long long)L.iter, t_end, L.res.pobj, L.res.KKT);
+  }
+  return HPRQP_OK;
+}
+
+}  // namespace hprqp
+
+using hprqp::Error;
+using hprqp::Handle;
+
+struct hprqp_ctx : hprqp::Handle {};
+
+#define HPRQP_GUARD(h, body)                                        \
+  try {                                                             \
+    if (h) cudaSetDevice(h->device);                                \
+    body;                                                           \
+    return HPRQP_OK;                                                \
+  } catch (const Error& e) {                                        \
+    (h ? h->err : hprqp::g_global_err) = e.what();                  \
+    return e.code;                                                  \
+  } catch (const std::exception& e) {                               \
+    (h ? h->err : hprqp::g_global_err) = e.what();                  \
+    return HPRQP_E_CUDA;                                            \
+  }
+
+extern "C" {
+
+void hprqp_default_params(hprqp_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->stoptol = 1e-6;
+  p->sigma = -1;
+  p->max_iter = 2147483647;
+  p->sigma_fixed = 0;
+  p->time_limit = 3600.0;
+  p->eig_factor = 1.05;
+  p->check_iter = 100;
+  p->warm_up = 0;
+  p->spmv_mode_Q = 0;
+  p->spmv_mode_A = 0;
+  p->print_frequency = -1;
+  p->device_number = 0;
+  p->use_Ruiz_scaling = 1;
+  p->use_bc_scaling = 0;
+  p->use_l2_scaling = 0;
+  p->use_Pock_Chambolle_scaling = 1;
+  p->problem_type = HPRQP_PROBLEM_QP;
+  p->lambda = 0.0;
+  p->auto_save = 0;
+  p->verbose = 1;
+  p->use_gpu = 1;
+  p->precision = HPRQP_PRECISION_FP64;
+  p->polish_tol = -1.0;
+  p->lambda_max_A_override = -1.0;
+  p->lambda_max_Q_override = -1.0;
+}
+
+int hprqp_abi_info(int64_t* out) {
+  if (!out) return HPRQP_E_ARG;
+  out[0] = HPRQP_ABI_VERSION;
+  out[1] = (int64_t)sizeof(hprqp_problem);
+  out[2] = (int64_t)sizeof(hprqp_params);
+  out[3] = (int64_t)sizeof(hprqp_result);
+  return HPRQP_OK;
+}
+
+int hprqp_create(hprqp_handle* out, int32_t device) {
+  hprqp_ctx* h = nullptr;
+  try {
+    if (!out) throw Error(HPRQP_E_ARG, "null handle pointer");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0)
+      throw Error(HPRQP_E_CUDA, std::string("CUDA is not functional: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "no device"));
+    if (device < 0 || device >= count)
+      throw Error(HPRQP_E_CUDA, "Invalid GPU device number " + std::to_string(device) + ". Valid range is [0, " +
+                                    std::to_string(count - 1) + "]");
+    HPRQP_CUDA(cudaSetDevice(device));
+    h = new hprqp_ctx();
+    h->device = device;
+    h->cm = std::make_unique<hprqp::Common>();
+    h->cm->init();
+    *out = h;
+    return HPRQP_OK;
+  } catch (const Error& e) {
+    hprqp::g_global_err = e.what();
+    delete h;
+    return e.code;
+  } catch (const std::exception& e) {
+    hprqp::g_global_err = e.what();
+    delete h;
+    return HPRQP_E_CUDA;
+  }
+}
+
+int hprqp_load(hprqp_handle h, const hprqp_problem* prob) {
+  if (!h) return HPRQP_E_ARG;
+  HPRQP_GUARD(h, {
+    h->prepared = false;
+    h->e64.reset();
+    h->e32.reset();
+    hprqp::load_problem(prob, h->hp);
+  })
+}
+
+int hprqp_prepare(hprqp_handle h, const hprqp_params* params) {
+  if (!h || !params) return HPRQP_E_ARG;
+  HPRQP_GUARD(h, { hprqp::prepare(*h, *params); })
+}
+
+int hprqp_solve(hprqp_handle h, const hprqp_params* params, const double* initial_x, const double* initial_y,
+                hprqp_result* result, double* x, double* y, double* z, double* w) {
+  if (!h || !params || !result) return HPRQP_E_ARG;
+  HPRQP_GUARD(h, { hprqp::solve(*h, *params, initial_x, initial_y, result, x, y, z, w); })
+}
+
+int hprqp_set_trace(hprqp_handle h, int64_t iters, double* x_trace, double* y_trace, double* w_trace) {
+  if (!h || iters < 0) return HPRQP_E_ARG;
+  h->trace_iters = iters;
+  h->xt = x_trace;
+  h->yt = y_trace;
+  h->wt = w_trace;
+  return HPRQP_OK;
+}
+
+const char* hprqp_last_error(hprqp_handle h) { return h ? h->err.c_str() : hprqp::g_global_err.c_str(); }
+
+int hprqp_destroy(hprqp_handle h) {
+  if (!h) return HPRQP_OK;
+  cudaSetDevice(h->device);
+  if (h->cm && h->cm->stream) cudaStreamSynchronize(h->cm->stream);
+  h->e32.reset();
+  h->e64.reset();
+  delete h;
+  return HPRQP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,218 @@
+/*
+ * hprqp.h — C ABI of libhprqp.so, the B200 (sm_100a) iteration engine of the
+ * HPR-QP solver (dual Halpern Peaceman–Rachford method for convex composite
+ * quadratic programs).
+ *
+ *     minimize    0.5 x'Qx + c'x + obj_constant  [+ lambda*||x||_1 for LASSO]
+ *     subject to  AL <= A x <= AU,   l <= x <= u
+ *
+ * The library replaces the `use_gpu = true` branch of the reference solver's
+ * `solve(model, params)` (src/algorithm.jl:1904-2039): everything after
+ * `prepare_model` (src/algorithm.jl:1326-1333) — scaling, eigenvalue
+ * estimation, warm start, the HPR loop, residuals, restarts, sigma updates
+ * and result collection — runs behind these entry points.  A Julia `ccall`
+ * shim (julia/HPRQPGPU.jl) or Python `ctypes` (hprqp_b200/_lib.py) binds it.
+ *
+ * Conventions
+ *  - Plain C types only; no exceptions cross the boundary.  Every function
+ *    returns 0 on success and a negative HPRQP_E* code on failure; the text
+ *    of the last failure is available from hprqp_last_error().
+ *  - The caller owns every host array.  hprqp_load() copies what it needs;
+ *    output arrays are caller-allocated.
+ *  - There is NO CPU fallback: if CUDA is unusable or the device number is
+ *    invalid, hprqp_create() fails with HPRQP_E_CUDA.  (The reference's
+ *    validate_gpu_parameters!, src/utils.jl:14-31, silently falls back to the
+ *    CPU instead.)
+ *  - A handle is not thread-safe; use one handle per host thread.
+ */
+#ifndef HPRQP_H
+#define HPRQP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HPRQP_ABI_VERSION 1
+
+/* ---- return codes -------------------------------------------------------- */
+#define HPRQP_OK             0
+#define HPRQP_E_ARG         -1   /* invalid argument (sizes, NaN data, l > u, ...) */
+#define HPRQP_E_CUDA        -2   /* CUDA unusable / kernel launch or copy failed   */
+#define HPRQP_E_OOM         -3   /* device allocation failed                        */
+#define HPRQP_E_STATE       -4   /* call order (solve before load, ...)             */
+#define HPRQP_E_UNSUPPORTED -5   /* option the library does not implement           */
+
+/* ---- solver status (reference strings, src/algorithm.jl:558-576) --------- */
+#define HPRQP_STATUS_OPTIMAL          0   /* "OPTIMAL"          */
+#define HPRQP_STATUS_MAX_ITER         1   /* "MAX_ITER"         */
+#define HPRQP_STATUS_TIME_LIMIT       2   /* "TIME_LIMIT"       */
+#define HPRQP_STATUS_NUMERICAL_ERROR  3   /* NaN/Inf in a residual (new)    */
+
+/* ---- kind of Q (the Q-operator plug-ins of src/Q_operators) ---------- */
+#define HPRQP_Q_SPARSE 0   /* explicit sparse Q (may have 0 nonzeros: LP)      */
+#define HPRQP_Q_LASSO  1   /* implicit Q = A_d' A_d  (LASSO_operator.jl)       */
+#define HPRQP_Q_QAP    2   /* implicit Q(X) = 2(A X B - S X - X T) (QAP_operator.jl) */
+
+/* ---- problem_type (reference params.problem_type string) ----------------- */
+#define HPRQP_PROBLEM_QP    0
+#define HPRQP_PROBLEM_LASSO 1
+#define HPRQP_PROBLEM_QAP   2
+
+/* ---- precision modes (new) ----------------------------------------------- */
+#define HPRQP_PRECISION_FP64        0  /* plain FP64 HPR, the reference arithmetic */
+#define HPRQP_PRECISION_FP32_POLISH 1  /* FP32 storage + FP64 anchors/reductions,
+                                          then FP64 polish to the tolerance        */
+
+/*
+ * Problem data: the fields of the reference's QP_info_cpu
+ * (src/structs.jl:98-149).  Sparse matrices are CSC with int32 indices, as a
+ * Julia SparseMatrixCSC{Float64,Int32}; `index_base` is 1 for Julia arrays
+ * passed as-is and 0 for scipy/C arrays.  Vectors are float64.  Infinite
+ * bounds are +-INFINITY.
+ */
+typedef struct hprqp_problem {
+    int64_t n;                 /* number of variables                          */
+    int64_t m;                 /* number of rows of A (0 allowed)              */
+    int32_t index_base;        /* 0 or 1, for every CSC array below            */
+    int32_t Q_kind;            /* HPRQP_Q_*                                    */
+    /* constraint matrix A (m x n), CSC */
+    const int32_t* A_colptr;   /* n+1                                          */
+    const int32_t* A_rowval;   /* nnz(A)                                       */
+    const double*  A_nzval;    /* nnz(A)                                       */
+    const double*  c;          /* n                                            */
+    const double*  AL;         /* m                                            */
+    const double*  AU;         /* m                                            */
+    const double*  l;          /* n                                            */
+    const double*  u;          /* n                                            */
+    double obj_constant;
+    double lambda;             /* LASSO regularisation (QP_info_cpu.lambda)    */
+    /* HPRQP_Q_SPARSE: Q (n x n), CSC, symmetric (as left by qp_formulation)  */
+    const int32_t* Q_colptr;
+    const int32_t* Q_rowval;
+    const double*  Q_nzval;
+    /* HPRQP_Q_LASSO: data matrix A_d (lasso_m x n), CSC                       */
+    int64_t lasso_m;
+    const int32_t* L_colptr;
+    const int32_t* L_rowval;
+    const double*  L_nzval;
+    /* HPRQP_Q_QAP: dense n_qap x n_qap column-major A, B, S, T; n = n_qap^2   */
+    int64_t qap_n;
+    const double* qap_A;
+    const double* qap_B;
+    const double* qap_S;
+    const double* qap_T;
+} hprqp_problem;
+
+/*
+ * Solver parameters: every field of HPRQP_parameters (src/structs.jl:195-275),
+ * strings mapped to ints, plus the library's own extensions at the end.
+ * hprqp_default_params() gives the reference defaults (src/structs.jl:274).
+ */
+typedef struct hprqp_params {
+    double  stoptol;                 /* 1e-6                                        */
+    double  sigma;                   /* -1 = automatic (||b||/||c|| after scaling)  */
+    int64_t max_iter;                /* typemax(Int32)                              */
+    int32_t sigma_fixed;             /* 0                                           */
+    double  time_limit;              /* 3600 s                                      */
+    double  eig_factor;              /* 1.05                                        */
+    int32_t check_iter;              /* 100                                         */
+    int32_t warm_up;                 /* 0; accepted, no JIT to warm                 */
+    int32_t spmv_mode_Q;             /* 0 = auto (autotuned row schedule)           */
+    int32_t spmv_mode_A;             /* 0 = auto                                    */
+    int32_t print_frequency;         /* -1 = adaptive (print_step)                  */
+    int32_t device_number;           /* 0                                           */
+    int32_t use_Ruiz_scaling;        /* 1                                           */
+    int32_t use_bc_scaling;          /* 0 (disabled in the reference, utils.jl:703) */
+    int32_t use_l2_scaling;          /* 0 (never read by the reference algorithm)   */
+    int32_t use_Pock_Chambolle_scaling; /* 1                                        */
+    int32_t problem_type;            /* HPRQP_PROBLEM_*; L1 term in the objective
+                                        only when LASSO (algorithm.jl:66)           */
+    double  lambda;                  /* params.lambda: never read (reference quirk) */
+    int32_t auto_save;               /* HDF5 auto-save: HPRQP_E_UNSUPPORTED if set  */
+    int32_t verbose;                 /* 1: iteration log on stdout                  */
+    int32_t use_gpu;                 /* must be 1 for this library                  */
+    /* ---- extensions ---- */
+    int32_t precision;               /* HPRQP_PRECISION_*                           */
+    double  polish_tol;              /* FP32 phase stops when KKT < polish_tol
+                                        (<= 0: automatic)                           */
+    double  lambda_max_A_override;   /* > 0: use instead of power iteration         */
+    double  lambda_max_Q_override;   /* > 0: use instead of power iteration         */
+} hprqp_params;
+
+/* Results: HPRQP_results (src/structs.jl:292-309) minus the vectors, which go
+ * to caller-allocated arrays in hprqp_solve(). */
+typedef struct hprqp_result {
+    int64_t iter, iter_4, iter_6;
+    double  time, time_4, time_6;    /* seconds from t_start_alg (after setup)     */
+    double  power_time, setup_time;
+    double  primal_obj, dual_obj;
+    double  residuals;               /* max(err_Rp, err_Rd, gap) (KKT)              */
+    double  gap, err_Rp, err_Rd;
+    int32_t status;                  /* HPRQP_STATUS_*                              */
+    int32_t Q_is_diag;
+    double  sigma;                   /* final sigma                                 */
+    double  lambda_max_A, lambda_max_Q;
+    int64_t restarts;
+    int64_t iter_fp32;               /* iterations done in the FP32 phase           */
+    int64_t gpu_launches;            /* kernels launched by this solve              */
+} hprqp_result;
+
+typedef struct hprqp_ctx* hprqp_handle;
+
+/* ---- entry points -------------------------------------------------------- */
+
+/* ABI self-description: out[0] = HPRQP_ABI_VERSION, out[1..3] =
+ * sizeof(hprqp_problem), sizeof(hprqp_params), sizeof(hprqp_result).  Lets
+ * a binding check its struct layouts.  No reference counterpart. */
+int hprqp_abi_info(int64_t* out);
+
+/* Reference defaults, HPRQP_parameters() (src/structs.jl:274). */
+void hprqp_default_params(hprqp_params* p);
+
+/* Bind a handle to CUDA device `device`.  Replaces validate_gpu_parameters! +
+ * CUDA.device! (src/utils.jl:14-31, src/algorithm.jl:1910-1912); an unusable
+ * device is an error, not a CPU fallback. */
+int hprqp_create(hprqp_handle* h, int32_t device);
+
+/* Copy a problem (QP_info_cpu, src/structs.jl:98-149) into the handle.
+ * Validates sizes, index ranges, NaN and l <= u, AL <= AU.  Replaces
+ * transfer_to_gpu (src/algorithm.jl:1284-1322) and the Q plug-ins' to_gpu
+ * (src/Q_operators). */
+int hprqp_load(hprqp_handle h, const hprqp_problem* prob);
+
+/* Setup only: scaling!, check_Q_diagonal, workspace allocation, upload and
+ * SpMV schedule selection (src/algorithm.jl:1914-1935).  Optional: hprqp_solve
+ * performs it when the handle is not prepared for these params.  Lets a
+ * caller time the iteration engine with the data already resident. */
+int hprqp_prepare(hprqp_handle h, const hprqp_params* params);
+
+/* optimize(model, params) for the loaded problem (src/algorithm.jl:1511-1554
+ * and 1904-2039).  initial_x (length n) / initial_y (length m) may be NULL
+ * (params.initial_x / initial_y = nothing).  x, z, w (length n) and y
+ * (length m) receive the unscaled solution (collect_results!,
+ * src/algorithm.jl:611-643); any of them may be NULL. */
+int hprqp_solve(hprqp_handle h, const hprqp_params* params,
+                const double* initial_x, const double* initial_y,
+                hprqp_result* result,
+                double* x, double* y, double* z, double* w);
+
+/* Parity hook: record the scaled working iterates x, y, w after each of the
+ * first `iters` HPR iterations of the next hprqp_solve() into caller-owned
+ * arrays of iters*n, iters*m, iters*n doubles (NULL entries are skipped).
+ * iters = 0 disables tracing.  Tracing synchronises every iteration. */
+int hprqp_set_trace(hprqp_handle h, int64_t iters,
+                    double* x_trace, double* y_trace, double* w_trace);
+
+/* Text of the last error on this handle ("" if none); valid until the next
+ * call on the handle.  h may be NULL for errors from hprqp_create. */
+const char* hprqp_last_error(hprqp_handle h);
+
+/* Free every device and host resource of the handle. */
+int hprqp_destroy(hprqp_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPRQP_H */
