@@ -50,6 +50,7 @@ class Params(C.Structure):
         ("auto_save", C.c_int32), ("verbose", C.c_int32), ("use_gpu", C.c_int32),
         ("precision", C.c_int32), ("polish_tol", C.c_double),
         ("lambda_max_A_override", C.c_double), ("lambda_max_Q_override", C.c_double),
+        ("profile_passes", C.c_int32),
     ]
 
 
@@ -64,6 +65,21 @@ class Result(C.Structure):
         ("status", C.c_int32), ("Q_is_diag", C.c_int32),
         ("sigma", C.c_double), ("lambda_max_A", C.c_double), ("lambda_max_Q", C.c_double),
         ("restarts", C.c_int64), ("iter_fp32", C.c_int64), ("gpu_launches", C.c_int64),
+        ("device_time", C.c_double), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+    ]
+
+
+MAX_PASSES = 8
+
+
+class PassStats(C.Structure):
+    _fields_ = [
+        ("npass", C.c_int32), ("path", C.c_int32),
+        ("name", (C.c_char * 32) * MAX_PASSES),
+        ("ms_per_launch", C.c_double * MAX_PASSES),
+        ("bytes_per_launch", C.c_double * MAX_PASSES),
+        ("threads_per_row", C.c_int32 * MAX_PASSES),
+        ("ms_per_iter", C.c_double), ("bytes_per_iter", C.c_double), ("iters", C.c_int64),
     ]
 
 
@@ -95,6 +111,7 @@ def default_params():
     p.polish_tol = -1.0
     p.lambda_max_A_override = -1.0
     p.lambda_max_Q_override = -1.0
+    p.profile_passes = 0
     return p
 
 

@@ -9,14 +9,15 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from ._abi import Params, Result
+from ._abi import Params, PassStats, Result
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libhprqp.so")
 
 # Every entry point declared in include/hprqp.h
 EXPORTS = ("hprqp_abi_info", "hprqp_default_params", "hprqp_create", "hprqp_load", "hprqp_prepare",
-           "hprqp_solve", "hprqp_set_trace", "hprqp_last_error", "hprqp_destroy")
+           "hprqp_solve", "hprqp_set_trace", "hprqp_profile_iterations", "hprqp_get_pass_stats",
+           "hprqp_last_error", "hprqp_destroy")
 
 _lib = None
 
@@ -50,6 +51,10 @@ def load():
     L.hprqp_solve.restype = C.c_int
     L.hprqp_set_trace.argtypes = [vp, C.c_int64, vp, vp, vp]
     L.hprqp_set_trace.restype = C.c_int
+    L.hprqp_profile_iterations.argtypes = [vp, C.POINTER(Params), C.c_int64, C.c_int32, C.POINTER(PassStats)]
+    L.hprqp_profile_iterations.restype = C.c_int
+    L.hprqp_get_pass_stats.argtypes = [vp, C.POINTER(PassStats), C.POINTER(PassStats)]
+    L.hprqp_get_pass_stats.restype = C.c_int
     L.hprqp_last_error.argtypes = [vp]
     L.hprqp_last_error.restype = C.c_char_p
     L.hprqp_destroy.argtypes = [vp]

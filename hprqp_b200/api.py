@@ -53,6 +53,7 @@ class HPRQP_parameters:
     polish_tol: float = -1.0
     lambda_max_A_override: float = -1.0
     lambda_max_Q_override: float = -1.0
+    profile_passes: bool = False
 
     def to_struct(self) -> Params:
         p = _abi.default_params()
@@ -65,7 +66,7 @@ class HPRQP_parameters:
         p.print_frequency = int(self.print_frequency)
         p.device_number = int(self.device_number)
         for name in ("sigma_fixed", "warm_up", "use_Ruiz_scaling", "use_bc_scaling", "use_l2_scaling",
-                     "use_Pock_Chambolle_scaling", "auto_save", "verbose", "use_gpu"):
+                     "use_Pock_Chambolle_scaling", "auto_save", "verbose", "use_gpu", "profile_passes"):
             setattr(p, name, int(bool(getattr(self, name))))
         p.spmv_mode_Q = _spmv_mode(self.spmv_mode_Q)
         p.spmv_mode_A = _spmv_mode(self.spmv_mode_A)
@@ -119,6 +120,15 @@ class HPRQP_results:
     iter_fp32: int = 0
     gpu_launches: int = 0
     Q_is_diag: bool = False
+
+
+def _stats_dict(st):
+    passes = []
+    for k in range(st.npass):
+        passes.append(dict(name=st.name[k].value.decode(), ms=st.ms_per_launch[k],
+                           bytes=st.bytes_per_launch[k], threads_per_row=st.threads_per_row[k]))
+    return dict(path=st.path, iters=st.iters, ms_per_iter=st.ms_per_iter, bytes_per_iter=st.bytes_per_iter,
+                passes=passes)
 
 
 def _ptr(a):
@@ -176,6 +186,20 @@ class Solver:
         out.Q_is_diag = bool(r.Q_is_diag)
         out.x, out.y, out.z, out.w = x, (y if m > 0 else np.zeros(0)), z, w
         return out
+
+    def pass_stats(self):
+        """Per-pass CUDA-event timings of the last solve run with
+        params.profile_passes (fp64 and fp32 engines)."""
+        a, b = _abi.PassStats(), _abi.PassStats()
+        check(self._L.hprqp_get_pass_stats(self.h, C.byref(a), C.byref(b)), self.h)
+        return {"fp64": _stats_dict(a), "fp32": _stats_dict(b)}
+
+    def profile_iterations(self, params: HPRQP_parameters, iters: int = 50, full: bool = False):
+        """Run `iters` HPR iterations from the zero state and time each pass."""
+        st = _abi.PassStats()
+        check(self._L.hprqp_profile_iterations(self.h, C.byref(params.to_struct()), iters, int(full),
+                                               C.byref(st)), self.h)
+        return _stats_dict(st)
 
     def close(self):
         if self.h:

@@ -38,8 +38,7 @@ Common::~Common() {
 }
 
 void Common::sync_read(int first, int count) {
-  HPRQP_CUDA(cudaMemcpyAsync(h_scal + first, d_scal + first, sizeof(double) * count,
-                             cudaMemcpyDeviceToHost, stream));
+  to_host(h_scal + first, d_scal + first, sizeof(double) * count);
   HPRQP_CUDA(cudaStreamSynchronize(stream));
 }
 
@@ -69,24 +68,25 @@ static void rows(Common& cm, int tpr, int64_t nrows, const Src& src, const Epi& 
   }
 }
 
-template <int TPR, int K, unsigned MM, typename Acc, typename Src, typename Epi>
-static void reduce_t(Common& cm, int nrows, const Src& src, const Epi& epi, double* out) {
+template <int TPR, int K, unsigned MM, typename Acc, typename Src, typename Epi, typename Fin>
+static void reduce_t(Common& cm, int nrows, const Src& src, const Epi& epi, double* out, const Fin& fin) {
   const long long threads = (long long)std::max(nrows, 1) * TPR;
   const int grid = (int)std::min<long long>((threads + kBlock - 1) / kBlock, kMaxReduceGrid);
-  k_row_reduce<TPR, K, MM, Acc, Src, Epi><<<grid, kBlock, 0, cm.stream>>>(nrows, src, epi, cm.rws, out);
+  k_row_reduce<TPR, K, MM, Acc, Src, Epi, Fin><<<grid, kBlock, 0, cm.stream>>>(nrows, src, epi, cm.rws, out, fin);
   cm.launches++;
   HPRQP_LAUNCH_CHECK();
 }
 
-template <int K, unsigned MM, typename Acc, typename Src, typename Epi>
-static void reduce(Common& cm, int tpr, int64_t nrows, const Src& src, const Epi& epi, double* out) {
+template <int K, unsigned MM, typename Acc, typename Src, typename Epi, typename Fin = NoFin>
+static void reduce(Common& cm, int tpr, int64_t nrows, const Src& src, const Epi& epi, double* out,
+                   const Fin& fin = Fin()) {
   switch (tpr) {
-    case 1: reduce_t<1, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
-    case 2: reduce_t<2, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
-    case 4: reduce_t<4, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
-    case 8: reduce_t<8, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
-    case 16: reduce_t<16, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
-    case 32: reduce_t<32, K, MM, Acc>(cm, (int)nrows, src, epi, out); break;
+    case 1: reduce_t<1, K, MM, Acc>(cm, (int)nrows, src, epi, out, fin); break;
+    case 2: reduce_t<2, K, MM, Acc>(cm, (int)nrows, src, epi, out, fin); break;
+    case 4: reduce_t<4, K, MM, Acc>(cm, (int)nrows, src, epi, out, fin); break;
+    case 8: reduce_t<8, K, MM, Acc>(cm, (int)nrows, src, epi, out, fin); break;
+    case 16: reduce_t<16, K, MM, Acc>(cm, (int)nrows, src, epi, out, fin); break;
+    case 32: reduce_t<32, K, MM, Acc>(cm, (int)nrows, src, epi, out, fin); break;
     default: throw Error(HPRQP_E_ARG, "bad threads-per-row");
   }
 }
@@ -139,30 +139,12 @@ struct EpiRestartN {
   }
 };
 
-// Power method residual: sum (z - lambda q)^2, lambda read from the device.
-template <typename V>
-struct EpiPowerResid {
-  const V *q, *z;
-  const double* lam;
-  template <typename A>
-  __device__ __forceinline__ void operator()(int i, A, double (&r)[1]) const {
-    const double t = (double)z[i] - (*lam) * (double)q[i];
-    r[0] += t * t;
-  }
-};
-
 template <typename D, typename S>
 struct CastCopy {
   D* dst;
   const S* src;
   __device__ __forceinline__ void operator()(int i) const { dst[i] = (D)src[i]; }
 };
-
-__global__ void k_power_log(double* scal, int k) {
-  const double lam = scal[S_POW + 1], zz = scal[S_POW + 2], rr = scal[S_POW + 3];
-  scal[S_POWLOG + 2 * k] = lam;
-  scal[S_POWLOG + 2 * k + 1] = sqrt(rr) / (sqrt(zz) + lam);
-}
 
 // Golden-section search of unified_golden_Q_diag (src/unified_operations.jl:
 // 348-386) on one CTA: f(x) = a x + b/x + x^2 sum_i c_i d_i / (1 + x Q_i).
@@ -212,11 +194,12 @@ __global__ void __launch_bounds__(1024) k_golden_diag(int n, double a, double b,
 // Engine: construction and uploads
 // ---------------------------------------------------------------------------
 template <typename V>
-static V* upload(DeviceMem& mem, const std::vector<double>& h, int64_t len) {
+static V* upload(Common& cm, DeviceMem& mem, const std::vector<double>& h, int64_t len) {
   V* d = mem.alloc<V>(len);
   if (len > 0) {
     std::vector<V> t(h.begin(), h.begin() + len);
-    HPRQP_CUDA(cudaMemcpy(d, t.data(), sizeof(V) * len, cudaMemcpyHostToDevice));
+    cm.to_dev(d, t.data(), sizeof(V) * len);
+    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   }
   return d;
 }
@@ -228,11 +211,11 @@ void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode) {
   d.nnz = h.nnz();
   int* ptr = mem.alloc<int>(h.rows + 1);
   int* col = mem.alloc<int>(d.nnz);
-  HPRQP_CUDA(cudaMemcpy(ptr, h.ptr.data(), sizeof(int) * (h.rows + 1), cudaMemcpyHostToDevice));
-  if (d.nnz) HPRQP_CUDA(cudaMemcpy(col, h.col.data(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice));
+  cm.to_dev(ptr, h.ptr.data(), sizeof(int) * (h.rows + 1));
+  cm.to_dev(col, h.col.data(), sizeof(int) * d.nnz);
   d.ptr = ptr;
   d.col = col;
-  d.val = upload<V>(mem, h.val, d.nnz);
+  d.val = upload<V>(cm, mem, h.val, d.nnz);
   if (tpr_mode > 0) d.tpr = 1 << std::min(tpr_mode - 1, 5);
   else d.tpr = autotune(d);
 }
@@ -297,14 +280,14 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   pq = mem.alloc<V>(mx);
   pt = mem.alloc<V>(mx);
   HPRQP_CUDA(cudaMemset(pz, 0, sizeof(V) * mx));
-  c = upload<V>(mem, pp.c, n);
-  l = upload<V>(mem, pp.l, n);
-  u = upload<V>(mem, pp.u, n);
-  col_norm = upload<V>(mem, pp.col_norm, n);
-  diag_Q = upload<V>(mem, pp.diag_Q, n);
-  AL = upload<V>(mem, pp.AL, m);
-  AU = upload<V>(mem, pp.AU, m);
-  row_norm = upload<V>(mem, pp.row_norm, m);
+  c = upload<V>(cm, mem, pp.c, n);
+  l = upload<V>(cm, mem, pp.l, n);
+  u = upload<V>(cm, mem, pp.u, n);
+  col_norm = upload<V>(cm, mem, pp.col_norm, n);
+  diag_Q = upload<V>(cm, mem, pp.diag_Q, n);
+  AL = upload<V>(cm, mem, pp.AL, m);
+  AU = upload<V>(cm, mem, pp.AU, m);
+  row_norm = upload<V>(cm, mem, pp.row_norm, m);
   upload_csr(pp.A, A, tpr_A);
   upload_csr(pp.AT, AT, tpr_A);
   if (has_Q_sparse) upload_csr(pp.Q, Q, tpr_Q);
@@ -315,10 +298,10 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   }
   if (is_qap) {
     const int64_t N2 = hp.qn * hp.qn;
-    qA = upload<V>(mem, hp.qA, N2);
-    qB = upload<V>(mem, hp.qB, N2);
-    qS = upload<V>(mem, hp.qS, N2);
-    qT = upload<V>(mem, hp.qT, N2);
+    qA = upload<V>(cm, mem, hp.qA, N2);
+    qB = upload<V>(cm, mem, hp.qB, N2);
+    qS = upload<V>(cm, mem, hp.qS, N2);
+    qT = upload<V>(cm, mem, hp.qT, N2);
     qTmp = mem.alloc<V>(N2);
   }
   reset_state();
@@ -392,12 +375,15 @@ template <typename V>
 void Engine<V>::step(bool full, double h1, double h2) {
   const double f2s = 1.0 / (1.0 + sigma * lamQ), f1s = 1.0 - f2s;
   const double fy1 = lamA * sigma, fy2 = 1.0 / fy1;
+  mark();
   if (path == PATH_LASSO) {
     spmv(L, w, ltemp);
+    mark();
     HPRQP_BOOL(full, F, {
       EpiLasso<V, F> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, c, last_x, last_w, sigma, lasso_lam, f1s, f2s, h1, h2};
       rows<V>(cm, LT.tpr, n, CsrSrc<V, V>{LT.ptr, LT.col, LT.val, ltemp}, e);
     })
+    mark();
     return;
   }
   if (path == PATH_QP) {
@@ -411,6 +397,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
         rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w}, e);
       }
     }))
+    mark();
     if (m > 0) {
       EpiTempv<V> et{tempv, x_hat, Qw, sigma};
       if (is_qap) {
@@ -419,10 +406,12 @@ void Engine<V>::step(bool full, double h1, double h2) {
       } else {
         rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w_bar}, et);
       }
+      mark();
       HPRQP_BOOL(full, F, {
         EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
         rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, tempv}, ey);
       })
+      mark();
     }
     const double fs = sigma / (1.0 + sigma * lamQ);
     HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
@@ -430,6 +419,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
       if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar}, e);
       else rows<V>(cm, 1, n, ZeroSrc{}, e);
     }))
+    mark();
     return;
   }
   if (path == PATH_NOC) {
@@ -439,6 +429,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
       if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y}, e);
       else rows<V>(cm, 1, n, ZeroSrc{}, e);
     }))
+    mark();
     HPRQP_BOOL(full, F, {
       EpiTempvNoC<V, F> e{Qw, tempv, Qw_bar, x_hat, last_Qw, sigma, h1, h2};
       if (is_qap) {
@@ -448,11 +439,13 @@ void Engine<V>::step(bool full, double h1, double h2) {
         rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w_bar}, e);
       }
     })
+    mark();
     if (m > 0) {
       HPRQP_BOOL(full, F, {
         EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
         rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, tempv}, ey);
       })
+      mark();
     }
     return;
   }
@@ -462,12 +455,51 @@ void Engine<V>::step(bool full, double h1, double h2) {
     if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y}, e);
     else rows<V>(cm, 1, n, ZeroSrc{}, e);
   })
+  mark();
   if (m > 0) {
     HPRQP_BOOL(full, F, {
       EpiY<V, F, false> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
       rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, x_hat}, ey);
     })
+    mark();
   }
+}
+
+// Name, algorithmic HBM bytes (plain iteration) and schedule of pass k.
+// CSR stream = nnz (sizeof(V) + 4) + 4 (rows + 1); every distinct vector is
+// counted once per pass at its storage size (FP64 anchors stay 8 bytes);
+// the gathered input vector is counted once.
+template <typename V>
+void Engine<V>::pass_info(int k, const char** name, double* bytes, int* tpr) const {
+  const double v = sizeof(V), d = 8.0;
+  auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
+  const double N = (double)n, M_ = (double)m;
+  const double dg = Q_is_diag ? 2 * N * v : 0.0;
+  *name = "?";
+  *bytes = 0;
+  *tpr = 1;
+  if (path == PATH_LASSO) {
+    if (k == 0) { *name = "lasso1 A_d*w"; *bytes = csr(L) + N * v + L.rows * v; *tpr = L.tpr; }
+    else { *name = "lasso2 A_d'*t+prox"; *bytes = csr(LT) + L.rows * v + 3 * N * v + 2 * N * d + 4 * N * v; *tpr = LT.tpr; }
+    return;
+  }
+  const double cq = is_qap ? 0.0 : csr(Q);
+  const int tq = is_qap ? 1 : Q.tpr;
+  if (path == PATH_QP) {
+    if (k == 0) { *name = "zxw1 Q*w"; *bytes = cq + N * v + 5 * N * v + N * d + dg + 4 * N * v; *tpr = tq; }
+    else if (m > 0 && k == 1) { *name = "tempv Q*w_bar"; *bytes = cq + N * v + 2 * N * v + N * v; *tpr = tq; }
+    else if (m > 0 && k == 2) { *name = "y A*tempv"; *bytes = csr(A) + N * v + 3 * M_ * v + M_ * d + 2 * M_ * v; *tpr = A.tpr; }
+    else { *name = "w2 A'*y_bar"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 3 * N * v + 2 * N * d + (Q_is_diag ? N * v : 0.0) + 2 * N * v; *tpr = m > 0 ? AT.tpr : 1; }
+    return;
+  }
+  if (path == PATH_NOC) {
+    if (k == 0) { *name = "zxw A'*y"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 6 * N * v + 2 * N * d + dg + 4 * N * v; *tpr = m > 0 ? AT.tpr : 1; }
+    else if (k == 1) { *name = "tempv Q*w_bar"; *bytes = cq + N * v + 2 * N * v + N * d + 2 * N * v; *tpr = tq; }
+    else { *name = "y A*tempv"; *bytes = csr(A) + N * v + 3 * M_ * v + M_ * d + 2 * M_ * v; *tpr = A.tpr; }
+    return;
+  }
+  if (k == 0) { *name = "zx A'*y"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 4 * N * v + N * d + 2 * N * v; *tpr = m > 0 ? AT.tpr : 1; }
+  else { *name = "y A*x_hat"; *bytes = m > 0 ? csr(A) + N * v + 3 * M_ * v + M_ * d + M_ * v : 0.0; *tpr = m > 0 ? A.tpr : 1; }
 }
 
 // ---------------------------------------------------------------------------
@@ -566,7 +598,7 @@ void Engine<V>::restart() {
 template <typename V>
 void Engine<V>::initial_points(const double* x0, const double* y0) {
   if (x0) {
-    HPRQP_CUDA(cudaMemcpyAsync(stage_n, x0, sizeof(double) * n, cudaMemcpyHostToDevice, cm.stream));
+    cm.to_dev(stage_n, x0, sizeof(double) * n);
     V *x_ = x, *xb = x_bar, *w_ = w, *wb = w_bar;
     double *lx = last_x, *lw = last_w;
     const double* st = stage_n;
@@ -580,7 +612,7 @@ void Engine<V>::initial_points(const double* x0, const double* y0) {
   }
   if (y0) {
     if (m > 0) {
-      HPRQP_CUDA(cudaMemcpyAsync(stage_m, y0, sizeof(double) * m, cudaMemcpyHostToDevice, cm.stream));
+      cm.to_dev(stage_m, y0, sizeof(double) * m);
       V *y_ = y, *yb = y_bar;
       double* ly = last_y;
       const double* st = stage_m;
@@ -630,7 +662,7 @@ void Engine<V>::collect(double* xo, double* yo, double* zo, double* wo) {
   double* st = stage_n;
   const double bs = b_scale, cs = c_scale;
   auto copy_n = [&](double* dst) {
-    HPRQP_CUDA(cudaMemcpyAsync(dst, stage_n, sizeof(double) * n, cudaMemcpyDeviceToHost, cm.stream));
+    cm.to_host(dst, stage_n, sizeof(double) * n);
     HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   };
   if (xo) {
@@ -649,7 +681,7 @@ void Engine<V>::collect(double* xo, double* yo, double* zo, double* wo) {
     const V *yb = y_bar, *rn = row_norm;
     double* sm = stage_m;
     elem(cm, m, [=] __device__(int i) { sm[i] = cs * ((double)yb[i] / (double)rn[i]); });
-    HPRQP_CUDA(cudaMemcpyAsync(yo, stage_m, sizeof(double) * m, cudaMemcpyDeviceToHost, cm.stream));
+    cm.to_host(yo, stage_m, sizeof(double) * m);
   }
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
 }
@@ -659,7 +691,7 @@ void Engine<V>::trace_copy(double* xt, double* yt, double* wt) {
   auto out = [&](const V* src, int64_t len, double* stage, double* dst) {
     if (!dst || len == 0) return;
     elem(cm, len, CastCopy<double, V>{stage, src});
-    HPRQP_CUDA(cudaMemcpyAsync(dst, stage, sizeof(double) * len, cudaMemcpyDeviceToHost, cm.stream));
+    cm.to_host(dst, stage, sizeof(double) * len);
     HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   };
   out(x, n, stage_n, xt);
@@ -668,63 +700,99 @@ void Engine<V>::trace_copy(double* xt, double* yt, double* wt) {
 }
 
 // ---------------------------------------------------------------------------
-// Power method (src/utils.jl:1335-1461), chunked: the host checks the
-// per-iteration (lambda, err) log once per kPowChunk iterations.
+// Power method (src/utils.jl:1335-1461).  One power step is one fused kernel
+// for a sparse Q (the product, z_next, and the q.z / z.z / q.q sums), two
+// for A A' and the LASSO operator, a GEMM chain + one reduction for QAP.
+// kPowChunk steps (z ping-pongs between two buffers, so an even chunk ends
+// where it started) are captured once in a CUDA graph and replayed; the host
+// reads the (lambda, err) log once per chunk and stops at the first step
+// with err < tol, returning that step's lambda.
 // ---------------------------------------------------------------------------
 template <typename V>
-static double power_common(Engine<V>& E, int64_t len, double tol, int max_it, int64_t* iters,
-                           const std::function<void(const V*, V*)>& op) {
-  Common& cm = E.cm;
+double Engine<V>::power_run(int which, double tol, int max_it, int64_t* iters) {
+  const int64_t len = which == 0 ? m : n;
   {
     std::vector<double> z0 = power_start_vector(len);
     std::vector<V> zv(z0.begin(), z0.end());
-    HPRQP_CUDA(cudaMemcpy(E.pz, zv.data(), sizeof(V) * len, cudaMemcpyHostToDevice));
+    cm.to_dev(pz, zv.data(), sizeof(V) * len);
   }
-  reduce<1, 0u, double>(cm, 1, len, ZeroSrc{}, EpiSumSq<V>{E.pz}, cm.d_scal + S_POW + 2);
+  double* zz = cm.d_scal + S_POW + 2;
+  double* log = cm.d_scal + S_POWLOG;
+  reduce<1, 0u, double>(cm, 1, len, ZeroSrc{}, EpiSumSq<V>{pz}, zz);
+  auto one_step = [&](int k, V* zc, V* zn) {
+    const PowerFin fin{log, k};
+    if (which == 0) {  // A A' (power_iteration_A)
+      rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, zc}, EpiStoreInvNorm<V>{pt, zz});
+      reduce<3, 0u, double>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, pt}, EpiPowerFused<V>{zc, zn, zz, false},
+                            cm.d_scal + S_POW + 1, fin);
+    } else if (is_lasso) {
+      rows<V>(cm, L.tpr, L.rows, CsrSrc<V, V>{L.ptr, L.col, L.val, zc}, EpiStoreInvNorm<V>{ltemp, zz});
+      reduce<3, 0u, double>(cm, LT.tpr, n, CsrSrc<V, V>{LT.ptr, LT.col, LT.val, ltemp},
+                            EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
+    } else if (is_qap) {
+      V* q = pt;
+      const V* z = zc;
+      elem(cm, n, [=] __device__(int i) { q[i] = (V)((double)z[i] / sqrt(*zz)); });
+      qap_apply(pt, zn);
+      reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
+    } else {
+      reduce<3, 0u, double>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, zc}, EpiPowerFused<V>{zc, zn, zz, true},
+                            cm.d_scal + S_POW + 1, fin);
+    }
+  };
+  // capture one chunk (cuBLAS calls of the QAP operator run eagerly instead)
+  cudaGraphExec_t exec = nullptr;
+  int64_t per_chunk_launches = 0;
+  if (!is_qap) {
+    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+    cudaGraph_t g = nullptr;
+    const int64_t l0 = cm.launches;
+    HPRQP_CUDA(cudaStreamBeginCapture(cm.stream, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < kPowChunk; ++k) one_step(k, (k & 1) ? pq : pz, (k & 1) ? pz : pq);
+    HPRQP_CUDA(cudaStreamEndCapture(cm.stream, &g));
+    per_chunk_launches = cm.launches - l0;
+    cm.launches = l0;
+    HPRQP_CUDA(cudaGraphInstantiate(&exec, g, 0));
+    cudaGraphDestroy(g);
+  }
   double lam = 1.0;
   int it = 0;
-  while (it < max_it) {
-    const int chunk = std::min<int>(kPowChunk, max_it - it);
-    for (int k = 0; k < chunk; ++k) {
-      V* q = E.pq;
-      const V* z = E.pz;
-      const double* zz = cm.d_scal + S_POW + 2;
-      elem(cm, len, [=] __device__(int i) { q[i] = (V)((double)z[i] / sqrt(*zz)); });
-      op(E.pq, E.pz);
-      reduce<2, 0u, double>(cm, 1, len, ZeroSrc{}, EpiPowerDot<V>{E.pq, E.pz}, cm.d_scal + S_POW + 1);
-      reduce<1, 0u, double>(cm, 1, len, ZeroSrc{}, EpiPowerResid<V>{E.pq, E.pz, cm.d_scal + S_POW + 1},
-                            cm.d_scal + S_POW + 3);
-      k_power_log<<<1, 1, 0, cm.stream>>>(cm.d_scal, k);
-      cm.launches++;
-      HPRQP_LAUNCH_CHECK();
+  int found = -1;
+  while (it < max_it && found < 0) {
+    if (exec) {
+      HPRQP_CUDA(cudaGraphLaunch(exec, cm.stream));
+      cm.launches += per_chunk_launches;
+    } else {
+      for (int k = 0; k < kPowChunk; ++k) one_step(k, (k & 1) ? pq : pz, (k & 1) ? pz : pq);
     }
-    cm.sync_read(S_POWLOG, 2 * chunk);
-    for (int k = 0; k < chunk; ++k) {
+    cm.sync_read(S_POWLOG, 2 * kPowChunk);
+    for (int k = 0; k < kPowChunk && it + k < max_it; ++k) {
       lam = cm.h_scal[S_POWLOG + 2 * k];
-      const double err = cm.h_scal[S_POWLOG + 2 * k + 1];
-      if (err < tol) {
-        *iters = it + k + 1;
-        return lam;
+      if (cm.h_scal[S_POWLOG + 2 * k + 1] < tol) {
+        found = it + k + 1;
+        break;
       }
     }
-    it += chunk;
+    it += kPowChunk;
   }
-  *iters = it;
-  std::fprintf(stderr, "Power iteration did not converge within the specified tolerance.\n");
+  if (exec) cudaGraphExecDestroy(exec);
+  if (found < 0) {
+    *iters = std::min(it, max_it);
+    std::fprintf(stderr, "Power iteration did not converge within the specified tolerance.\n");
+  } else {
+    *iters = found;
+  }
   return lam;
 }
 
 template <typename V>
 double Engine<V>::power_A(double tol, int max_it, int64_t* iters) {
-  return power_common<V>(*this, m, tol, max_it, iters, [this](const V* q, V* z) {
-    spmv(AT, q, pt);
-    spmv(A, pt, z);
-  });
+  return power_run(0, tol, max_it, iters);
 }
 
 template <typename V>
 double Engine<V>::power_Q(double tol, int max_it, int64_t* iters) {
-  return power_common<V>(*this, n, tol, max_it, iters, [this](const V* q, V* z) { apply_Q(q, z); });
+  return power_run(1, tol, max_it, iters);
 }
 
 // FP32 -> FP64 hand-over of the full iteration state (precision switch)

@@ -59,11 +59,22 @@ struct Common {  // per-handle resources shared by the engines
   double* h_scal = nullptr;  // pinned mirror
   ReduceWs rws{};
   int64_t launches = 0;
+  int64_t h2d = 0, d2h = 0;  // bytes copied host<->device
   int num_sms = 148;
   DeviceMem mem;
   void init();
   ~Common();
   void sync_read(int first, int count);
+  void to_dev(void* d, const void* h, size_t bytes) {
+    if (!bytes) return;
+    HPRQP_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream));
+    h2d += (int64_t)bytes;
+  }
+  void to_host(void* h, const void* d, size_t bytes) {
+    if (!bytes) return;
+    HPRQP_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, stream));
+    d2h += (int64_t)bytes;
+  }
 };
 
 struct PendingMnorm {
@@ -109,11 +120,24 @@ class Engine {
   void trace_copy(double* xt, double* yt, double* wt);
   double power_A(double tol, int max_it, int64_t* iters);
   double power_Q(double tol, int max_it, int64_t* iters);
+  double power_run(int which, double tol, int max_it, int64_t* iters);
   template <typename W>
   void import_state(const Engine<W>& o);  // precision switch (FP32 -> FP64)
 
   void apply_Q(const V* xin, V* yout);  // Qmap! into a vector
   Common& cm;
+
+  // pass profiling: when `prof` is set, step() records an event before the
+  // first pass and after every pass
+  std::vector<cudaEvent_t>* prof = nullptr;
+  size_t prof_k = 0;
+  void mark() {
+    if (prof && prof_k < prof->size()) HPRQP_CUDA(cudaEventRecord((*prof)[prof_k++], cm.stream));
+  }
+  int npasses() const {
+    return path == PATH_QP ? (m > 0 ? 4 : 2) : path == PATH_NOC ? (m > 0 ? 3 : 2) : path == PATH_LP ? (m > 0 ? 2 : 1) : 2;
+  }
+  void pass_info(int k, const char** name, double* bytes, int* tpr) const;
 
  private:
   DeviceMem mem;

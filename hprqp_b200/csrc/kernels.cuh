@@ -101,9 +101,15 @@ struct ReduceWs {  // partials (one K-vector per CTA) + ticket counter
   unsigned* counter;
 };
 
-// Fold per-CTA partials in the last CTA; write K results to out.
-template <int K, unsigned MaxMask>
-__device__ __forceinline__ void grid_finish(double (&r)[K], ReduceWs ws, double* out) {
+struct NoFin {
+  template <int K>
+  __device__ __forceinline__ void operator()(const double (&)[K]) const {}
+};
+
+// Fold per-CTA partials in the last CTA; write K results to out, then let
+// `fin` (thread 0 of the last CTA) derive further scalars from them.
+template <int K, unsigned MaxMask, typename Fin = NoFin>
+__device__ __forceinline__ void grid_finish(double (&r)[K], ReduceWs ws, double* out, Fin fin = Fin()) {
   __shared__ bool am_last;
   if (threadIdx.x == 0) {
 #pragma unroll
@@ -129,15 +135,16 @@ __device__ __forceinline__ void grid_finish(double (&r)[K], ReduceWs ws, double*
   if (threadIdx.x == 0) {
 #pragma unroll
     for (int k = 0; k < K; ++k) out[k] = acc[k];
+    fin(acc);
     *ws.counter = 0u;
   }
 }
 
 // Row product + epilogue that also contributes to K reduction slots.
 // Grid-stride over rows; the grid is capped so the partials stay small.
-template <int TPR, int K, unsigned MaxMask, typename Acc, typename Src, typename Epi>
+template <int TPR, int K, unsigned MaxMask, typename Acc, typename Src, typename Epi, typename Fin = NoFin>
 __global__ void __launch_bounds__(kBlock) k_row_reduce(int nrows, Src src, Epi epi, ReduceWs ws,
-                                                       double* out) {
+                                                       double* out, Fin fin = Fin()) {
   double r[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) r[k] = 0.0;
@@ -148,7 +155,7 @@ __global__ void __launch_bounds__(kBlock) k_row_reduce(int nrows, Src src, Epi e
     if (lane == 0) epi(row, acc, r);
   }
   block_reduce<K, MaxMask>(r);
-  grid_finish<K, MaxMask>(r, ws, out);
+  grid_finish<K, MaxMask, Fin>(r, ws, out, fin);
 }
 
 // ---------------------------------------------------------------------------
@@ -460,6 +467,52 @@ struct EpiSigmaN {
     r[2] += dqw * dqw;
     r[3] += ddw * dqw;
   }
+};
+
+// Power method, fused: acc is (M z_cur)_i (scale_acc: divide by ||z_cur||,
+// i.e. the product of the normalised q = z_cur/||z_cur||) or already the
+// product of q.  Stores z_next and accumulates 0 q.z_next  1 z_next.z_next
+// 2 q.q, so ||z_next - lambda q||^2 = zz - 2 lambda^2 + lambda^2 qq needs no
+// second pass (power_iteration_A/Q, src/utils.jl:1352-1372).
+template <typename V>
+struct EpiPowerFused {
+  const V* zc;
+  V* zn;
+  const double* zz;
+  bool scale_acc;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, double (&r)[3]) const {
+    const double inv = 1.0 / sqrt(*zz);
+    const double v = scale_acc ? (double)acc * inv : (double)acc;
+    zn[i] = (V)v;
+    const double q = (double)zc[i] * inv;
+    r[0] += q * v;
+    r[1] += v * v;
+    r[2] += q * q;
+  }
+};
+
+// y = (M x) / ||x||, the norm read from the device
+template <typename V>
+struct EpiStoreInvNorm {
+  V* y;
+  const double* zz;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc) const { y[i] = (V)((double)acc / sqrt(*zz)); }
+};
+
+// Last-CTA step of a power iteration: log (lambda, err) for iteration k.
+struct PowerFin {
+  double* log;
+  int k;
+  __device__ __forceinline__ void operator()(const double (&a)[3]) const {
+    const double lam = a[0], zz = a[1], qq = a[2];
+    const double rr = fmax(zz - 2.0 * lam * lam + lam * lam * qq, 0.0);
+    log[2 * k] = lam;
+    log[2 * k + 1] = sqrt(rr) / (sqrt(zz) + lam);
+  }
+  template <int K>
+  __device__ __forceinline__ void operator()(const double (&)[K]) const {}
 };
 
 // Power method partial sums: 0 q.z  1 z.z   (q = zold/||zold||)

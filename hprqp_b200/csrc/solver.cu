@@ -69,22 +69,6 @@ struct Residuals {
   double err_Rp = 0, err_Rd = 0, KKT = kInf, pobj = 0, dobj = 0, gap = 0;
 };
 
-struct Handle {
-  int device = 0;
-  std::unique_ptr<Common> cm;
-  HostProblem hp;
-  Prepared pp;
-  bool prepared = false;
-  int key[5] = {-1, -1, -1, -1, -1};
-  int path = PATH_QP;
-  std::unique_ptr<Engine<double>> e64;
-  std::unique_ptr<Engine<float>> e32;
-  std::string err;
-  int64_t trace_iters = 0;
-  double *xt = nullptr, *yt = nullptr, *wt = nullptr;
-  double setup_time = 0.0;
-};
-
 struct LoopState {
   int64_t iter = 0;
   RestartInfo ri;
@@ -101,6 +85,51 @@ struct LoopState {
 };
 
 constexpr int kSwitch = -100;
+
+// Live per-pass timing: a pool of event sets, one set (npass + 1 marks) per
+// recorded plain iteration, harvested after each residual synchronisation.
+struct PassProfiler {
+  bool on = false;
+  int np = 0;
+  static constexpr int kSets = 64;
+  std::vector<cudaEvent_t> ev;
+  int used = 0;  // sets recorded since the last harvest
+  double ms[HPRQP_MAX_PASSES] = {0};
+  int64_t count = 0;
+  void init(int npass) {
+    np = npass;
+    if (ev.empty()) {
+      ev.resize((size_t)kSets * (HPRQP_MAX_PASSES + 1));
+      for (auto& e : ev) HPRQP_CUDA(cudaEventCreate(&e));
+    }
+    used = 0;
+    count = 0;
+    for (double& v : ms) v = 0;
+  }
+  ~PassProfiler() {
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  // events of the next set, or false when the pool is full
+  bool begin(std::vector<cudaEvent_t>& view) {
+    if (used >= kSets) return false;
+    view.assign(ev.begin() + (size_t)used * (HPRQP_MAX_PASSES + 1),
+                ev.begin() + (size_t)used * (HPRQP_MAX_PASSES + 1) + np + 1);
+    ++used;
+    return true;
+  }
+  void harvest() {  // call only after a stream synchronisation
+    for (int s = 0; s < used; ++s) {
+      for (int k = 0; k < np; ++k) {
+        float t = 0;
+        HPRQP_CUDA(cudaEventElapsedTime(&t, ev[(size_t)s * (HPRQP_MAX_PASSES + 1) + k],
+                                        ev[(size_t)s * (HPRQP_MAX_PASSES + 1) + k + 1]));
+        ms[k] += t;
+      }
+      ++count;
+    }
+    used = 0;
+  }
+};
 
 static double eval_mnorm(const Common& cm, const PendingMnorm& pm, bool has_m, bool diag, bool verbose) {
   const double* s = cm.h_scal + pm.slot;
@@ -129,6 +158,25 @@ static double eval_mnorm(const Common& cm, const PendingMnorm& pm, bool has_m, b
   return std::sqrt(Mn);
 }
 
+struct Handle {
+  int device = 0;
+  std::unique_ptr<Common> cm;
+  HostProblem hp;
+  Prepared pp;
+  bool prepared = false;
+  int key[5] = {-1, -1, -1, -1, -1};
+  int path = PATH_QP;
+  std::unique_ptr<Engine<double>> e64;
+  std::unique_ptr<Engine<float>> e32;
+  std::string err;
+  int64_t trace_iters = 0;
+  double *xt = nullptr, *yt = nullptr, *wt = nullptr;
+  double setup_time = 0.0;
+  int64_t h2d_at_solve_start = 0;
+  PassProfiler prof64, prof32;
+  hprqp_pass_stats stats64{}, stats32{};
+};
+
 // One phase of the HPR loop on engine E (src/algorithm.jl:1977-2038).
 // Returns a final status, or kSwitch when the FP32 phase hands over.
 template <typename V>
@@ -137,6 +185,10 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
   const int64_t n = E.n, m = E.m;
   const int64_t check_iter = p.check_iter;
   RestartInfo& ri = L.ri;
+  PassProfiler& prof = sizeof(V) == 8 ? H.prof64 : H.prof32;
+  std::vector<cudaEvent_t> prof_view;
+  prof.on = p.profile_passes != 0;
+  if (prof.on) prof.init(E.npasses());
   for (; L.iter <= p.max_iter; ++L.iter) {
     const int64_t iter = L.iter;
     const bool time_up = now_s() - L.t0 > p.time_limit;
@@ -145,6 +197,7 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
       L.force_residuals = false;
       E.residuals_launch(iter == 0);
       cm.sync_read(0, S_GOLD);
+      if (prof.on) prof.harvest();
       if (L.pend_cur.active) {
         ri.current_gap = eval_mnorm(cm, L.pend_cur, m > 0, E.Q_is_diag, p.verbose);
         L.pend_cur.active = false;
@@ -268,7 +321,12 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
     const bool to_check = (next % check_iter == 0) || (ri.restart_flag > 0) || on_print_schedule(next, p);
     // perform_iteration_step! (src/algorithm.jl:1881-1900)
     const double h1 = 1.0 / (ri.inner + 2.0), h2 = 1.0 - h1;
+    if (prof.on && !to_check && prof.begin(prof_view)) {
+      E.prof = &prof_view;
+      E.prof_k = 0;
+    }
     E.step(to_check, h1, h2);
+    E.prof = nullptr;
     if (ri.restart_flag > 0) {
       E.mnorm_launch(S_MN_LAST);
       L.pend_last = PendingMnorm{true, S_MN_LAST, E.sigma, E.lamA, E.lamQ};
@@ -336,6 +394,7 @@ static void start_engine(Handle& H, Engine<V>& E, const hprqp_params& p, double 
 static int solve(Handle& H, const hprqp_params& p, const double* x0, const double* y0, hprqp_result* res,
                  double* xo, double* yo, double* zo, double* wo) {
   const double setup_start = now_s();
+  H.h2d_at_solve_start = H.cm->h2d;
   prepare(H, p);
   const double setup_time = now_s() - setup_start;
   Common& cm = *H.cm;
@@ -343,6 +402,11 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   const Prepared& pp = H.pp;
   const int64_t m = H.hp.m;
   Engine<double>& E64 = *H.e64;
+  const int64_t h2d0 = cm.h2d - (setup_time > 0 ? 0 : 0), d2h0 = cm.d2h;
+  cudaEvent_t ev0, ev1;
+  HPRQP_CUDA(cudaEventCreate(&ev0));
+  HPRQP_CUDA(cudaEventCreate(&ev1));
+  HPRQP_CUDA(cudaEventRecord(ev0, cm.stream));
   LoopState L;
   L.t0 = now_s();
   // estimate_eigenvalues (src/algorithm.jl:1407-1440)
@@ -384,6 +448,35 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
     status = run_loop(H, E64, p, L, false);
   }
   // handle_termination + collect_results! (src/algorithm.jl:1039-1097, 611-643)
+  HPRQP_CUDA(cudaEventRecord(ev1, cm.stream));
+  HPRQP_CUDA(cudaEventSynchronize(ev1));
+  float dev_ms = 0.0f;
+  HPRQP_CUDA(cudaEventElapsedTime(&dev_ms, ev0, ev1));
+  cudaEventDestroy(ev0);
+  cudaEventDestroy(ev1);
+  auto fill = [&](auto& E, PassProfiler& pr, hprqp_pass_stats& st) {
+    std::memset(&st, 0, sizeof(st));
+    if (!p.profile_passes || pr.count == 0) return;
+    pr.harvest();
+    st.npass = pr.np;
+    st.path = E.path;
+    st.iters = pr.count;
+    for (int k = 0; k < pr.np; ++k) {
+      const char* name;
+      double bytes;
+      int tpr;
+      E.pass_info(k, &name, &bytes, &tpr);
+      std::snprintf(st.name[k], sizeof(st.name[k]), "%s", name);
+      st.ms_per_launch[k] = pr.ms[k] / (double)pr.count;
+      st.bytes_per_launch[k] = bytes;
+      st.threads_per_row[k] = tpr;
+      st.ms_per_iter += st.ms_per_launch[k];
+      st.bytes_per_iter += bytes;
+    }
+  };
+  fill(E64, H.prof64, H.stats64);
+  if (H.e32) fill(*H.e32, H.prof32, H.stats32);
+  else std::memset(&H.stats32, 0, sizeof(H.stats32));
   if (final64) E64.collect(xo, yo, zo, wo);
   else H.e32->collect(xo, yo, zo, wo);
   const double t_end = now_s() - L.t0;
@@ -411,12 +504,84 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   res->iter_6 = L.iter_6 == 0 ? L.iter : L.iter_6;
   res->iter_fp32 = iter_fp32;
   res->gpu_launches = cm.launches - launches0;
+  res->device_time = dev_ms * 1e-3;
+  res->h2d_bytes = cm.h2d - H.h2d_at_solve_start;
+  res->d2h_bytes = cm.d2h - d2h0;
+  (void)h2d0;
   if (p.verbose) {
     static const char* names[] = {"OPTIMAL", "MAX_ITER", "TIME_LIMIT", "NUMERICAL_ERROR"};
     std::printf("Status: %s  Iterations: %lld  Time: %.3f s  Primal Objective: %.12e  KKT: %.3e\n",
                 names[status], (long long)L.iter, t_end, L.res.pobj, L.res.KKT);
   }
   return HPRQP_OK;
+}
+
+// Time `iters` HPR iterations pass by pass (CUDA events) from the zero state.
+static void profile(Handle& H, const hprqp_params& p, int64_t iters, bool full, hprqp_pass_stats* out) {
+  prepare(H, p);
+  Common& cm = *H.cm;
+  const Prepared& pp = H.pp;
+  Engine<double>& E64 = *H.e64;
+  double lamA = 0.0, lamQ = 0.0;
+  int64_t pit = 0;
+  if (H.hp.m > 0) lamA = p.lambda_max_A_override > 0 ? p.lambda_max_A_override : E64.power_A(1e-4, 5000, &pit) * p.eig_factor;
+  if (H.hp.Q_kind != HPRQP_Q_SPARSE || (pp.Q.nnz() > 0 && !pp.Q_is_diag))
+    lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : E64.power_Q(1e-4, 5000, &pit) * p.eig_factor;
+  else if (pp.Q.nnz() > 0)
+    lamQ = pp.Q_maxval;
+  double sigma0 = p.sigma > 0 ? p.sigma : 1.0;
+  if (p.sigma == -1)
+    sigma0 = (pp.norm_c > 1e-16 && pp.norm_b > 1e-16 && pp.norm_b < 1e16 && pp.norm_c < 1e16) ? pp.norm_b / pp.norm_c : 1.0;
+  auto run = [&](auto& E) {
+    start_engine(H, E, p, lamA, lamQ, sigma0, nullptr, nullptr);
+    const int np = E.npasses();
+    for (int w = 0; w < 5; ++w) E.step(full, 0.5, 0.5);
+    // whole iterations, no per-pass events
+    cudaEvent_t a, b;
+    HPRQP_CUDA(cudaEventCreate(&a));
+    HPRQP_CUDA(cudaEventCreate(&b));
+    HPRQP_CUDA(cudaEventRecord(a, cm.stream));
+    for (int64_t k = 0; k < iters; ++k) E.step(full, 1.0 / (k + 2.0), 1.0 - 1.0 / (k + 2.0));
+    HPRQP_CUDA(cudaEventRecord(b, cm.stream));
+    HPRQP_CUDA(cudaEventSynchronize(b));
+    float ms = 0;
+    HPRQP_CUDA(cudaEventElapsedTime(&ms, a, b));
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    // per pass: np + 1 marks per iteration
+    std::vector<cudaEvent_t> ev((size_t)iters * (np + 1));
+    for (auto& e : ev) HPRQP_CUDA(cudaEventCreate(&e));
+    E.prof = &ev;
+    E.prof_k = 0;
+    for (int64_t k = 0; k < iters; ++k) E.step(full, 1.0 / (k + 2.0), 1.0 - 1.0 / (k + 2.0));
+    E.prof = nullptr;
+    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+    std::memset(out, 0, sizeof(*out));
+    out->npass = np;
+    out->path = E.path;
+    out->iters = iters;
+    out->ms_per_iter = ms / (double)iters;
+    for (int k = 0; k < np && k < HPRQP_MAX_PASSES; ++k) {
+      double tot = 0.0;
+      for (int64_t it = 0; it < iters; ++it) {
+        float t = 0;
+        HPRQP_CUDA(cudaEventElapsedTime(&t, ev[it * (np + 1) + k], ev[it * (np + 1) + k + 1]));
+        tot += t;
+      }
+      const char* name;
+      double bytes;
+      int tpr;
+      E.pass_info(k, &name, &bytes, &tpr);
+      std::snprintf(out->name[k], sizeof(out->name[k]), "%s", name);
+      out->ms_per_launch[k] = tot / (double)iters;
+      out->bytes_per_launch[k] = bytes;
+      out->threads_per_row[k] = tpr;
+      out->bytes_per_iter += bytes;
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+  };
+  if (p.precision == HPRQP_PRECISION_FP32_POLISH) run(*H.e32);
+  else run(E64);
 }
 
 }  // namespace hprqp
@@ -469,6 +634,7 @@ void hprqp_default_params(hprqp_params* p) {
   p->polish_tol = -1.0;
   p->lambda_max_A_override = -1.0;
   p->lambda_max_Q_override = -1.0;
+  p->profile_passes = 0;
 }
 
 int hprqp_abi_info(int64_t* out) {
@@ -529,6 +695,19 @@ int hprqp_solve(hprqp_handle h, const hprqp_params* params, const double* initia
                 hprqp_result* result, double* x, double* y, double* z, double* w) {
   if (!h || !params || !result) return HPRQP_E_ARG;
   HPRQP_GUARD(h, { hprqp::solve(*h, *params, initial_x, initial_y, result, x, y, z, w); })
+}
+
+int hprqp_profile_iterations(hprqp_handle h, const hprqp_params* params, int64_t iters, int32_t full,
+                             hprqp_pass_stats* out) {
+  if (!h || !params || !out || iters <= 0) return HPRQP_E_ARG;
+  HPRQP_GUARD(h, { hprqp::profile(*h, *params, iters, full != 0, out); })
+}
+
+int hprqp_get_pass_stats(hprqp_handle h, hprqp_pass_stats* fp64, hprqp_pass_stats* fp32) {
+  if (!h) return HPRQP_E_ARG;
+  if (fp64) *fp64 = h->stats64;
+  if (fp32) *fp32 = h->stats32;
+  return HPRQP_OK;
 }
 
 int hprqp_set_trace(hprqp_handle h, int64_t iters, double* x_trace, double* y_trace, double* w_trace) {

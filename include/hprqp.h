@@ -139,6 +139,9 @@ typedef struct hprqp_params {
                                         (<= 0: automatic)                           */
     double  lambda_max_A_override;   /* > 0: use instead of power iteration         */
     double  lambda_max_Q_override;   /* > 0: use instead of power iteration         */
+    int32_t profile_passes;          /* 1: time each fused pass of plain iterations
+                                        with CUDA events during the solve (read
+                                        them with hprqp_get_pass_stats)            */
 } hprqp_params;
 
 /* Results: HPRQP_results (src/structs.jl:292-309) minus the vectors, which go
@@ -157,7 +160,23 @@ typedef struct hprqp_result {
     int64_t restarts;
     int64_t iter_fp32;               /* iterations done in the FP32 phase           */
     int64_t gpu_launches;            /* kernels launched by this solve              */
+    double  device_time;             /* CUDA-event time of the same span as `time`  */
+    int64_t h2d_bytes, d2h_bytes;    /* host<->device bytes moved by this call      */
 } hprqp_result;
+
+/* Per-pass timing of the hot loop (hprqp_profile_iterations). */
+#define HPRQP_MAX_PASSES 8
+typedef struct hprqp_pass_stats {
+    int32_t npass;
+    int32_t path;                        /* 0 QP, 1 QP-noC, 2 LP, 3 LASSO           */
+    char    name[HPRQP_MAX_PASSES][32];
+    double  ms_per_launch[HPRQP_MAX_PASSES];    /* CUDA events, averaged           */
+    double  bytes_per_launch[HPRQP_MAX_PASSES]; /* algorithmic HBM bytes           */
+    int32_t threads_per_row[HPRQP_MAX_PASSES];
+    double  ms_per_iter;                 /* whole iteration, timed without per-pass events */
+    double  bytes_per_iter;
+    int64_t iters;
+} hprqp_pass_stats;
 
 typedef struct hprqp_ctx* hprqp_handle;
 
@@ -204,6 +223,19 @@ int hprqp_solve(hprqp_handle h, const hprqp_params* params,
  * iters = 0 disables tracing.  Tracing synchronises every iteration. */
 int hprqp_set_trace(hprqp_handle h, int64_t iters,
                     double* x_trace, double* y_trace, double* w_trace);
+
+/* Measurement hook: prepare, estimate lambda_max, then run `iters` plain
+ * (partial, `full` = 0) or full HPR iterations of the loaded problem from
+ * the zero state and report the CUDA-event time and the algorithmic bytes
+ * of each fused pass.  Used by bench.py for the roofline; no reference
+ * counterpart. */
+int hprqp_profile_iterations(hprqp_handle h, const hprqp_params* params, int64_t iters,
+                             int32_t full, hprqp_pass_stats* out);
+
+/* Per-pass CUDA-event timings collected by the last hprqp_solve() run with
+ * params.profile_passes = 1: one hprqp_pass_stats per engine precision
+ * (fp64, fp32; npass = 0 when that engine did not run). */
+int hprqp_get_pass_stats(hprqp_handle h, hprqp_pass_stats* fp64, hprqp_pass_stats* fp32);
 
 /* Text of the last error on this handle ("" if none); valid until the next
  * call on the handle.  h may be NULL for errors from hprqp_create. */
