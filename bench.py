@@ -1,0 +1,334 @@
+#!/usr/bin/env python
+"""Benchmark: time to 1e-6 relative KKT on the 700x700 grid QP
+(n = 490,000, m = 974,408, nnz(A) = 2.92M, nnz(Q) = 2.45M), on B200.
+
+One step = one full HPR-QP solve from a cold start to 1e-6 relative KKT,
+timed like the reference's `time` (from after setup, power method included)
+with CUDA events on the engine's stream.  Inputs are resident in HBM when
+the timed region starts (the problem is loaded and prepared before it).
+The headline path is FP32 storage + FP64 polish; the plain FP64 path is
+timed on the same instance beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs one process per GPU (torchrun); the instance does not shard, so
+every rank solves its own replica ("scaling": "weak", replicas only) and
+the reported time is the max over ranks.  --impl reference times the
+reference CPU path's restatement (oracle/) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time to 1e-6 rel. KKT (s)"
+WORKLOAD = "grid_qp_700x700"
+HBM_FALLBACK_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--grid", type=int, default=700, help="grid side (700 = the benchmark configuration)")
+    ap.add_argument("--precision", default="fp32_polish", choices=["fp32_polish", "fp64"])
+    ap.add_argument("--cpu-sample-iters", type=int, default=40)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)), int(os.environ.get("WORLD_SIZE", 1))
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = tempfile.mktemp(suffix=".csv")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                t = [x.strip() for x in line.split(",")]
+                if len(t) >= 9:
+                    rows.append(t)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        smax = max((num(r[2]) or 0) for r in rows)
+        loaded = [v for v in sm if v > 0.5 * smax] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": smax, "reasons": reasons,
+                "samples": len(rows), "power_w_max": max((num(r[3]) or 0) for r in rows)}
+
+
+def cpu_sample(model, iters_to_target, threads, sample_iters):
+    """The oracle (restated reference CPU path) on the host cores: its power
+    method in full plus `sample_iters` HPR iterations, extrapolated to the
+    iteration count of the same FP64 method to 1e-6."""
+    from hprqp_b200._abi import default_params
+    from oracle import oracle as O
+    p = default_params()
+    p.verbose = 0
+    p.max_iter = sample_iters
+    t = time.time()
+    r = O.solve(model, p, threads=threads)
+    wall = time.time() - t
+    per_iter = (r.time - r.power_time) / max(r.iter, 1)
+    value = r.power_time + per_iter * iters_to_target
+    return value, dict(power_s=r.power_time, s_per_iter=per_iter, sample_wall_s=wall,
+                       lambda_max_A=r.lambda_max_A, lambda_max_Q=r.lambda_max_Q)
+
+
+def oracle_iters_fixture(grid):
+    path = os.path.join(ROOT, "tests", "golden", "grid_qp_oracle.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(str(grid))
+    except Exception:
+        return None
+
+
+def ncu_traffic(kernel_name):
+    """Per-launch DRAM bytes of a pass from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("#") or "=" not in line:
+                    continue
+                k, v = line.rsplit("=", 1)
+                if k.strip() == kernel_name:
+                    return float(v)
+    except FileNotFoundError:
+        pass
+    return None
+
+
+def run_reference(args):
+    rank, _, world = dist_env()
+    if rank != 0:
+        return 0
+    from hprqp_b200 import workloads as W
+    model = W.grid_qp(N=args.grid)
+    fx = oracle_iters_fixture(args.grid)
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):  # a tiny sample: builds caches, pages in the oracle
+        from hprqp_b200._abi import default_params
+        from oracle import oracle as O
+        p = default_params()
+        p.verbose = 0
+        p.max_iter = 2
+        p.lambda_max_A_override = 1.0
+        p.lambda_max_Q_override = 1.0
+        O.solve(model, p, threads=threads)
+    iters = fx["iter"] if fx else None
+    vals = []
+    det = None
+    for _ in range(args.steps):
+        v, det = cpu_sample(model, iters if iters else args.cpu_sample_iters, threads, args.cpu_sample_iters)
+        vals.append(v)
+    value = statistics.mean(vals)
+    sample = (f"oracle power method in full + {args.cpu_sample_iters} HPR iterations of {WORKLOAD}, "
+              f"extrapolated to {iters} iterations (oracle FP64 iteration count to 1e-6, "
+              "tests/golden/grid_qp_oracle.json)")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
+            "config": {"workload": WORKLOAD, "n": model.n, "m": model.m, "precision": "fp64",
+                       "implementation": "reference CPU path restated in C++ (oracle/), OpenMP"},
+            "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample,
+                             **det},
+            "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    rank, local_rank, world = dist_env()
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local_rank)
+        from datetime import timedelta
+        td.init_process_group("nccl", timeout=timedelta(seconds=600))
+        dist = td
+
+    def barrier_max(v):
+        if dist is None:
+            return v
+        import torch
+        t = torch.tensor([float(v)], device=f"cuda:{local_rank}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    from hprqp_b200 import HPRQP_parameters, Solver
+    from hprqp_b200 import workloads as W
+    model = W.grid_qp(N=args.grid)
+    nnzA, nnzQ = model.A.nnz, model.Q.Q.nnz
+    solver = Solver(local_rank).load(model)
+    modes = [args.precision] + (["fp64"] if args.precision != "fp64" else [])
+    params = {mode: HPRQP_parameters(verbose=False, precision=mode, profile_passes=True) for mode in modes}
+    for mode in modes:
+        solver.prepare(params[mode])       # setup (scaling + upload) outside the timed region
+    for _ in range(args.warmup):
+        for mode in modes:
+            solver.solve(params[mode])
+    sampler = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(local_rank)).split(",")[0])
+                           if "CUDA_VISIBLE_DEVICES" in os.environ else local_rank)
+    results = {mode: [] for mode in modes}
+    stats = {}
+    if dist:
+        dist.barrier()
+    sampler.start()
+    for mode in modes:
+        for _ in range(args.steps):
+            r = solver.solve(params[mode])
+            results[mode].append(r)
+        stats[mode] = solver.pass_stats()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+
+    def summarize(rs):
+        dev = barrier_max(statistics.mean(r.device_time for r in rs))
+        return dict(value=dev, wall=statistics.mean(r.time for r in rs), iters=rs[-1].iter,
+                    iter_fp32=rs[-1].iter_fp32, power_s=statistics.mean(r.power_time for r in rs),
+                    status=rs[-1].status, kkt=rs[-1].residuals, obj=rs[-1].primal_obj,
+                    launches=sum(r.gpu_launches for r in rs))
+
+    summ = {mode: summarize(results[mode]) for mode in modes}
+    head = summ[args.precision]
+    # roofline: dominant fused pass of the timed solves (live CUDA events)
+    peak, peak_kind = measured_peak()
+    best = None
+    for eng in ("fp64", "fp32"):
+        st = stats[args.precision][eng]
+        for p in st["passes"]:
+            share = p["ms"] / st["ms_per_iter"] if st["ms_per_iter"] else 0
+            cand = dict(kernel=f"{eng}:{p['name']}", ms=p["ms"], bytes=p["bytes"], share=share,
+                        threads_per_row=p["threads_per_row"], iters_timed=st["iters"])
+            if best is None or p["ms"] * st["iters"] > best["ms"] * best["iters_timed"]:
+                best = cand
+    roof = None
+    if best:
+        ach = best["bytes"] / (best["ms"] * 1e-3) / 1e9
+        roof = {"bound": "hbm", "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach / peak, 4), "traffic": ncu_traffic(best["kernel"]),
+                "kernel": best["kernel"], "algorithmic_bytes_per_launch": best["bytes"],
+                "ms_per_launch": best["ms"], "peak_source": peak_kind,
+                "share_of_iteration": round(best["share"], 3)}
+    # end to end through the public API from host buffers (load -> solve -> x,y,z,w on the host)
+    e2e_t, h2d, d2h = [], 0, 0
+    for _ in range(max(1, min(args.steps, 3))):
+        t = time.perf_counter()
+        s2 = Solver(local_rank).load(model)
+        r = s2.solve(HPRQP_parameters(verbose=False, precision=args.precision))
+        s2.close()
+        e2e_t.append(time.perf_counter() - t)
+        h2d, d2h = r.h2d_bytes, r.d2h_bytes
+    e2e = {"value": barrier_max(statistics.mean(e2e_t)), "unit": "s", "h2d_bytes_per_step": h2d,
+           "d2h_bytes_per_step": d2h,
+           "note": "hprqp_load + hprqp_solve from host arrays (host-side scaling, upload, solve, solution copy-back)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        fx = oracle_iters_fixture(args.grid)
+        threads = os.cpu_count() or 1
+        iters = fx["iter"] if fx else summ["fp64"]["iters"] if "fp64" in summ else head["iters"]
+        v, det = cpu_sample(model, iters, threads, args.cpu_sample_iters)
+        cpu = {"value": v, "unit": "s", "cores": threads, "kind": "port",
+               "sample": f"oracle power method in full + {args.cpu_sample_iters} HPR iterations, extrapolated "
+                         f"to {iters} iterations (FP64 iteration count to 1e-6)", **det}
+    fp64 = summ.get("fp64", head)
+    st64 = stats[args.precision]["fp64"]
+    loop_s = max(fp64["value"] - fp64["power_s"], 1e-9)
+    line = {
+        "metric": METRIC, "value": round(head["value"], 6), "unit": "s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(head["value"] * 1e3, 3), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32+f64 polish" if args.precision == "fp32_polish" else "f64",
+        "data": "synthetic (seeded generator with the configuration's shapes and distributions)",
+        "config": {"workload": WORKLOAD if args.grid == 700 else f"grid_qp_{args.grid}x{args.grid}",
+                   "n": model.n, "m": model.m, "nnz_A": nnzA, "nnz_Q": nnzQ, "stoptol": 1e-6,
+                   "precision": args.precision, "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (>= 168 MB streamed per iteration vs 126 MB L2)"},
+        "status": head["status"], "kkt": head["kkt"], "iters": head["iters"], "iters_fp32": head["iter_fp32"],
+        "power_method_s": head["power_s"],
+        "plain_fp64": {"time_s": fp64["value"], "iters": fp64["iters"], "power_method_s": fp64["power_s"],
+                       "iters_per_s": fp64["iters"] / loop_s,
+                       "hbm_gbs_plain_iteration": (st64["bytes_per_iter"] / (st64["ms_per_iter"] * 1e-3) / 1e9
+                                                   if st64["ms_per_iter"] else None),
+                       "ms_per_plain_iteration": st64["ms_per_iter"]},
+        "speedup_vs_plain_fp64": fp64["value"] / head["value"] if head["value"] else None,
+        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "gpu_launches": head["launches"],
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    solver.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -362,8 +362,13 @@ static void check_params(const hprqp_params& p) {
 static void prepare(Handle& H, const hprqp_params& p) {
   if (!H.hp.loaded) throw Error(HPRQP_E_STATE, "no problem loaded");
   check_params(p);
-  const int key[5] = {p.use_Ruiz_scaling, p.use_Pock_Chambolle_scaling, p.precision, p.spmv_mode_Q, p.spmv_mode_A};
-  if (H.prepared && std::memcmp(key, H.key, sizeof(key)) == 0) return;
+  const int key[5] = {p.use_Ruiz_scaling, p.use_Pock_Chambolle_scaling, 0, p.spmv_mode_Q, p.spmv_mode_A};
+  if (H.prepared && std::memcmp(key, H.key, sizeof(key)) == 0) {
+    // same scaling and schedule: only add the FP32 engine if it is missing
+    if (p.precision == HPRQP_PRECISION_FP32_POLISH && !H.e32)
+      H.e32 = std::make_unique<Engine<float>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A);
+    return;
+  }
   const double t = now_s();
   H.e64.reset();
   H.e32.reset();

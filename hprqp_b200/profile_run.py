@@ -1,0 +1,53 @@
+"""Run the iteration engine alone, for profilers (ncu) and quick timing.
+
+    python -m hprqp_b200.profile_run --grid 700 --precision fp64 --mode iterations --iters 10
+    python -m hprqp_b200.profile_run --grid 700 --precision fp32_polish --mode solve
+
+--mode iterations: prepare, then hprqp_profile_iterations (5 warm-up + 2 x iters
+                   plain HPR iterations from the zero state); lambda_max is
+                   injected (--lam-A/--lam-Q, defaults for the 700x700 grid from
+                   the oracle) so no power-method launches precede the passes.
+--mode solve:      one full solve to 1e-6 (power method included).
+Prints one JSON line with the per-pass CUDA-event times.
+"""
+import argparse
+import json
+import sys
+
+from . import HPRQP_parameters, Solver
+from . import workloads as W
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--grid", type=int, default=700)
+    ap.add_argument("--workload", default="grid", choices=["grid", "random_qp", "lasso"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_polish"])
+    ap.add_argument("--mode", default="iterations", choices=["iterations", "solve"])
+    ap.add_argument("--iters", type=int, default=10)
+    ap.add_argument("--lam-A", type=float, default=0.44866094653915195)
+    ap.add_argument("--lam-Q", type=float, default=0.8051445993716677)
+    a = ap.parse_args(argv)
+    if a.workload == "grid":
+        model, ptype = W.grid_qp(N=a.grid), "QP"
+    elif a.workload == "random_qp":
+        model, ptype = W.random_qp(), "QP"
+    else:
+        model, ptype = W.lasso(), "LASSO"
+    s = Solver(0).load(model)
+    if a.mode == "iterations":
+        p = HPRQP_parameters(verbose=False, precision=a.precision, problem_type=ptype,
+                             lambda_max_A_override=a.lam_A, lambda_max_Q_override=a.lam_Q)
+        out = s.profile_iterations(p, a.iters)
+    else:
+        p = HPRQP_parameters(verbose=False, precision=a.precision, problem_type=ptype, profile_passes=True)
+        r = s.solve(p)
+        out = dict(status=r.status, iter=r.iter, iter_fp32=r.iter_fp32, time=r.time, device_time=r.device_time,
+                   power_time=r.power_time, kkt=r.residuals, launches=r.gpu_launches, passes=s.pass_stats())
+    s.close()
+    print(json.dumps(out))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -183,3 +183,28 @@ def test_grid_qp_full_size_properties():
     for r in (r64, r32):
         k = kkt(m, r.x, r.y, r.z)
         assert k["err_Rp"] < 1e-5 and k["err_Rd"] < 1e-5 and k["gap"] < 1e-5
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_against_committed_golden_fixtures(name):
+    """The GPU path against the committed oracle fixtures (tests/golden/cases.npz)."""
+    import os
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cases.npz"))
+    m = model(name)
+    ptype = CASES[name][1]
+    lamA, lamQ = g[name + "/lam"]
+    s = Solver().load(m)
+    xt, yt, wt = s.set_trace(10)
+    s.solve(gpu_params(ptype, max_iter=10, lambda_max_A_override=lamA, lambda_max_Q_override=lamQ))
+    s.set_trace(0)
+    for k in range(10):
+        assert rel(xt[k], g[name + "/x_trace"][k]) < ITER_RTOL
+        if m.m:
+            assert rel(yt[k], g[name + "/y_trace"][k]) < ITER_RTOL
+    r = s.solve(gpu_params(ptype, max_iter=50000))
+    s.close()
+    assert r.status == "OPTIMAL" and int(g[name + "/status"]) == 0
+    pobj = float(g[name + "/pobj"])
+    assert abs(r.primal_obj - pobj) / (1 + abs(pobj)) < OBJ_RTOL
+    xg = g[name + "/x"]
+    assert np.max(np.abs(r.x - xg)) / max(1.0, np.max(np.abs(xg))) < 1e-3

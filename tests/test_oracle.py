@@ -135,3 +135,19 @@ def test_reference_mps_fixtures(name):
     assert r.status_name == "OPTIMAL" and r.residuals < 1e-6
     k = kkt(m, r.x, r.y, r.z)
     assert k["err_Rp"] < 1e-5 and k["err_Rd"] < 1e-5
+
+
+def test_oracle_reproduces_golden_fixtures():
+    """Regression pin: the committed fixtures (tests/golden/make_golden.py)."""
+    import os
+    from tests.test_gpu_parity import CASES, oracle_params
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cases.npz"))
+    for name in ("toy_diagQ", "lp", "random_lp", "lasso", "qap_n10"):
+        m = CASES[name][0]()
+        r = O.solve(m, oracle_params(CASES[name][1], max_iter=50000))
+        assert r.status == int(g[name + "/status"]) and r.iter == int(g[name + "/iter"])
+        assert abs(r.primal_obj - float(g[name + "/pobj"])) <= 1e-12 * (1 + abs(r.primal_obj))
+        lamA, lamQ = g[name + "/lam"]
+        t = O.solve(m, oracle_params(CASES[name][1], max_iter=10, lambda_max_A_override=lamA,
+                                     lambda_max_Q_override=lamQ), trace_iters=10)
+        assert np.array_equal(t.x_trace, g[name + "/x_trace"])
