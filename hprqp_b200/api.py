@@ -81,9 +81,9 @@ class HPRQP_parameters:
 
 def _spmv_mode(v) -> int:
     """'auto' (autotuned), 'CUSPARSE'/'customized' (reference names, treated
-    as auto), or an explicit threads-per-row count 1..32."""
+    as auto), 'sell' (SELL-32), or an explicit CSR threads-per-row 1..32."""
     if isinstance(v, str):
-        return 0
+        return 7 if v.lower() == "sell" else 0
     t = int(v)
     if t not in (1, 2, 4, 8, 16, 32):
         raise ValueError("threads per row must be 1, 2, 4, 8, 16 or 32")
@@ -120,6 +120,9 @@ class HPRQP_results:
     iter_fp32: int = 0
     gpu_launches: int = 0
     Q_is_diag: bool = False
+    device_time: float = 0.0
+    h2d_bytes: int = 0
+    d2h_bytes: int = 0
 
 
 def _stats_dict(st):

@@ -31,7 +31,11 @@ struct Error : std::runtime_error {
 #ifdef __CUDACC__
 constexpr int kBlock = 256;  // threads per CTA for every row/element kernel
 
-// Device view of a CSR matrix (0-based, int32 indices).
+// Device view of a sparse matrix: CSR (0-based, int32 indices), plus an
+// optional SELL-32 copy (slices of 32 consecutive rows stored column-major,
+// entry k of row r at sptr[r/32] + 32k + r%32) used when the row-schedule
+// autotuner finds it faster.  Row lengths come from the CSR ptr, so the
+// padding of a slice is never read.
 template <typename V>
 struct DCsr {
   int rows = 0, cols = 0;
@@ -40,7 +44,22 @@ struct DCsr {
   const int* col = nullptr;
   const V* val = nullptr;
   int tpr = 4;  // threads cooperating on one row (1,2,4,8,16,32)
+  bool sell = false;
+  const int* sptr = nullptr;
+  const int* scol = nullptr;
+  const V* sval = nullptr;
+  int64_t sell_len = 0;
 };
+
+// Programmatic dependent launch: wait until the previous kernel in the
+// stream has completed and flushed, then let the next kernel start its CTAs
+// (they wait in turn), so kernel boundaries overlap launch and tail.
+__device__ __forceinline__ void pdl_enter() {
+#if defined(__CUDA_ARCH__) && __CUDA_ARCH__ >= 900
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
 
 // Reduce `v` over the TPR lanes of a row group (lanes of a group are
 // consecutive and the group is aligned inside its warp).

@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <cstdlib>
 #include <functional>
 
 #include "engine.cuh"
@@ -29,6 +30,8 @@ void Common::init() {
   int dev = 0;
   HPRQP_CUDA(cudaGetDevice(&dev));
   HPRQP_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  const char* e = std::getenv("HPRQP_PDL");
+  pdl = !(e && e[0] == '0');
 }
 
 Common::~Common() {
@@ -43,15 +46,30 @@ void Common::sync_read(int first, int count) {
 }
 
 // ---------------------------------------------------------------------------
-// Launch wrappers
+// Launch wrappers.  Every kernel of the engine starts with pdl_enter(), so
+// all are launched with programmatic stream serialisation.
 // ---------------------------------------------------------------------------
+template <typename... KArgs, typename... Args>
+static void launch(Common& cm, void (*kernel)(KArgs...), int grid, int block, Args... args) {
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = cm.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = cm.pdl ? 1 : 0;
+  HPRQP_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+  cm.launches++;
+}
+
 template <int TPR, typename Acc, typename Src, typename Epi>
 static void rows_t(Common& cm, int nrows, const Src& src, const Epi& epi) {
   const long long threads = (long long)nrows * TPR;
   const int grid = (int)((threads + kBlock - 1) / kBlock);
-  k_row_pass<TPR, Acc, Src, Epi><<<grid, kBlock, 0, cm.stream>>>(nrows, src, epi);
-  cm.launches++;
-  HPRQP_LAUNCH_CHECK();
+  launch(cm, k_row_pass<TPR, Acc, Src, Epi>, grid, kBlock, nrows, src, epi);
 }
 
 template <typename Acc, typename Src, typename Epi>
@@ -72,9 +90,7 @@ template <int TPR, int K, unsigned MM, typename Acc, typename Src, typename Epi,
 static void reduce_t(Common& cm, int nrows, const Src& src, const Epi& epi, double* out, const Fin& fin) {
   const long long threads = (long long)std::max(nrows, 1) * TPR;
   const int grid = (int)std::min<long long>((threads + kBlock - 1) / kBlock, kMaxReduceGrid);
-  k_row_reduce<TPR, K, MM, Acc, Src, Epi, Fin><<<grid, kBlock, 0, cm.stream>>>(nrows, src, epi, cm.rws, out, fin);
-  cm.launches++;
-  HPRQP_LAUNCH_CHECK();
+  launch(cm, k_row_reduce<TPR, K, MM, Acc, Src, Epi, Fin>, grid, kBlock, nrows, src, epi, cm.rws, out, fin);
 }
 
 template <int K, unsigned MM, typename Acc, typename Src, typename Epi, typename Fin = NoFin>
@@ -95,9 +111,7 @@ template <typename F>
 static void elem(Common& cm, int64_t len, const F& f) {
   if (len <= 0) return;
   const int grid = (int)((len + kBlock - 1) / kBlock);
-  k_elementwise<<<grid, kBlock, 0, cm.stream>>>((int)len, f);
-  cm.launches++;
-  HPRQP_LAUNCH_CHECK();
+  launch(cm, k_elementwise<F>, grid, kBlock, (int)len, f);
 }
 
 #define HPRQP_BOOL(cond, NAME, ...)   \
@@ -216,8 +230,65 @@ void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode) {
   d.ptr = ptr;
   d.col = col;
   d.val = upload<V>(cm, mem, h.val, d.nnz);
-  if (tpr_mode > 0) d.tpr = 1 << std::min(tpr_mode - 1, 5);
-  else d.tpr = autotune(d);
+  d.sell = false;
+  if (tpr_mode == 7) {  // SELL-32 requested
+    build_sell(h, d);
+    d.sell = d.sell_len > 0;
+    d.tpr = d.sell ? 1 : 4;
+  } else if (tpr_mode > 0) {
+    d.tpr = 1 << std::min(tpr_mode - 1, 5);
+  } else {
+    build_sell(h, d);
+    d.tpr = autotune(d);
+  }
+}
+
+// SELL-32 copy of a CSR matrix; skipped when padding would exceed 50%.
+template <typename V>
+void Engine<V>::build_sell(const HCsr& h, DCsr<V>& d) {
+  d.sell_len = 0;
+  if (h.rows <= 0 || h.nnz() == 0) return;
+  const int64_t ns = (h.rows + 31) / 32;
+  std::vector<int> sptr(ns + 1, 0);
+  for (int64_t sl = 0; sl < ns; ++sl) {
+    int w = 0;
+    for (int64_t r = sl * 32; r < std::min<int64_t>(h.rows, sl * 32 + 32); ++r) w = std::max(w, h.ptr[r + 1] - h.ptr[r]);
+    sptr[sl + 1] = sptr[sl] + 32 * w;
+  }
+  const int64_t total = sptr[ns];
+  if (total > (int64_t)(1.5 * h.nnz()) + 64 || total > INT32_MAX) return;
+  std::vector<int> scol(total, 0);
+  std::vector<double> sval(total, 0.0);
+  for (int64_t r = 0; r < h.rows; ++r) {
+    const int64_t base = sptr[r / 32] + (r % 32);
+    for (int k = h.ptr[r]; k < h.ptr[r + 1]; ++k) {
+      const int64_t j = base + 32 * (int64_t)(k - h.ptr[r]);
+      scol[j] = h.col[k];
+      sval[j] = h.val[k];
+    }
+  }
+  int* dsp = mem.alloc<int>(ns + 1);
+  int* dsc = mem.alloc<int>(total);
+  cm.to_dev(dsp, sptr.data(), sizeof(int) * (ns + 1));
+  cm.to_dev(dsc, scol.data(), sizeof(int) * total);
+  d.sptr = dsp;
+  d.scol = dsc;
+  d.sval = upload<V>(cm, mem, sval, total);
+  d.sell_len = total;
+}
+
+template <typename V>
+template <typename Epi>
+void Engine<V>::mat_rows(const DCsr<V>& M, const V* xin, const Epi& e) {
+  if (M.sell) rows<V>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e);
+  else rows<V>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, e);
+}
+
+// Fused product + reduction on M's format (FP64 accumulation).
+template <int K, unsigned MM, typename V, typename Epi, typename Fin = NoFin>
+static void mat_reduce(Common& cm, const DCsr<V>& M, const V* xin, const Epi& e, double* out, const Fin& fin = Fin()) {
+  if (M.sell) reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
+  else reduce<K, MM, double>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, e, out, fin);
 }
 
 // Row-schedule autotuner: time the plain product for each threads-per-row
@@ -227,27 +298,36 @@ template <typename V>
 int Engine<V>::autotune(DCsr<V>& d) {
   if (d.rows <= 0 || d.nnz == 0) return 1;
   const double avg = (double)d.nnz / d.rows;
-  static const int cand[] = {1, 2, 4, 8, 16, 32};
   cudaEvent_t e0, e1;
   HPRQP_CUDA(cudaEventCreate(&e0));
   HPRQP_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = 4;
-  for (int t : cand) {
+  bool best_sell = false;
+  // candidate -1 = SELL-32 (one thread per row); each timed as the best of 3
+  // rounds of 4 back-to-back products, so a noisy round cannot decide.
+  for (int t : {-1, 1, 2, 4, 8, 16, 32}) {
+    if (t == -1 && d.sell_len == 0) continue;
     if (t == 1 && avg > 12) continue;
     if (t == 32 && avg < 8) continue;
-    d.tpr = t;
+    d.sell = (t == -1);
+    d.tpr = t == -1 ? 1 : t;
     spmv(d, pz, pt);
-    HPRQP_CUDA(cudaEventRecord(e0, cm.stream));
-    for (int r = 0; r < 3; ++r) spmv(d, pz, pt);
-    HPRQP_CUDA(cudaEventRecord(e1, cm.stream));
-    HPRQP_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    HPRQP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) { best = ms; best_t = t; }
+    float tbest = 1e30f;
+    for (int round = 0; round < 3; ++round) {
+      HPRQP_CUDA(cudaEventRecord(e0, cm.stream));
+      for (int r = 0; r < 4; ++r) spmv(d, pz, pt);
+      HPRQP_CUDA(cudaEventRecord(e1, cm.stream));
+      HPRQP_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      HPRQP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      tbest = std::min(tbest, ms);
+    }
+    if (tbest < best) { best = tbest; best_t = d.tpr; best_sell = d.sell; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  d.sell = best_sell;
   return best_t;
 }
 
@@ -324,7 +404,7 @@ void Engine<V>::reset_state() {
 // ---------------------------------------------------------------------------
 template <typename V>
 void Engine<V>::spmv(const DCsr<V>& M, const V* xin, V* yout, double scale) {
-  rows<V>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, EpiStore<V>{yout, scale});
+  mat_rows(M, xin, EpiStore<V>{yout, scale});
 }
 
 template <typename V>
@@ -381,7 +461,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
     mark();
     HPRQP_BOOL(full, F, {
       EpiLasso<V, F> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, c, last_x, last_w, sigma, lasso_lam, f1s, f2s, h1, h2};
-      rows<V>(cm, LT.tpr, n, CsrSrc<V, V>{LT.ptr, LT.col, LT.val, ltemp}, e);
+      mat_rows(LT, ltemp, e);
     })
     mark();
     return;
@@ -394,7 +474,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
         qap_apply(w, Qw);
         rows<V>(cm, 1, n, VecSrc<V>{Qw}, e);
       } else {
-        rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w}, e);
+        mat_rows(Q, w, e);
       }
     }))
     mark();
@@ -404,19 +484,19 @@ void Engine<V>::step(bool full, double h1, double h2) {
         qap_apply(w_bar, Qw_bar);
         rows<V>(cm, 1, n, VecSrc<V>{Qw_bar}, et);
       } else {
-        rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w_bar}, et);
+        mat_rows(Q, w_bar, et);
       }
       mark();
       HPRQP_BOOL(full, F, {
         EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
-        rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, tempv}, ey);
+        mat_rows(A, tempv, ey);
       })
       mark();
     }
     const double fs = sigma / (1.0 + sigma * lamQ);
     HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
       EpiW2<V, F, D> e{w, ATy, w_bar, dw, ATdy, ATy_bar, fact, last_w, last_ATy, fs, h1, h2};
-      if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar}, e);
+      if (m > 0) mat_rows(AT, y_bar, e);
       else rows<V>(cm, 1, n, ZeroSrc{}, e);
     }))
     mark();
@@ -426,7 +506,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
     HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
       EpiZxwNoC<V, F, D> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, Qw, c, l, u, fact1, fact2, last_x, last_w,
                            sigma, f1s, f2s, h1, h2};
-      if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y}, e);
+      if (m > 0) mat_rows(AT, y, e);
       else rows<V>(cm, 1, n, ZeroSrc{}, e);
     }))
     mark();
@@ -436,14 +516,14 @@ void Engine<V>::step(bool full, double h1, double h2) {
         qap_apply(w_bar, Qw_bar);
         rows<V>(cm, 1, n, VecSrc<V>{Qw_bar}, e);
       } else {
-        rows<V>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, w_bar}, e);
+        mat_rows(Q, w_bar, e);
       }
     })
     mark();
     if (m > 0) {
       HPRQP_BOOL(full, F, {
         EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
-        rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, tempv}, ey);
+        mat_rows(A, tempv, ey);
       })
       mark();
     }
@@ -452,14 +532,14 @@ void Engine<V>::step(bool full, double h1, double h2) {
   // PATH_LP
   HPRQP_BOOL(full, F, {
     EpiZxLP<V, F> e{x, x_hat, dx, x_bar, z_bar, c, l, u, last_x, sigma, h1, h2};
-    if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y}, e);
+    if (m > 0) mat_rows(AT, y, e);
     else rows<V>(cm, 1, n, ZeroSrc{}, e);
   })
   mark();
   if (m > 0) {
     HPRQP_BOOL(full, F, {
       EpiY<V, F, false> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
-      rows<V>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, x_hat}, ey);
+      mat_rows(A, x_hat, ey);
     })
     mark();
   }
@@ -473,33 +553,34 @@ template <typename V>
 void Engine<V>::pass_info(int k, const char** name, double* bytes, int* tpr) const {
   const double v = sizeof(V), d = 8.0;
   auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
+  auto sched = [](const DCsr<V>& M) { return M.sell ? 0 : M.tpr; };  // 0 = SELL-32
   const double N = (double)n, M_ = (double)m;
   const double dg = Q_is_diag ? 2 * N * v : 0.0;
   *name = "?";
   *bytes = 0;
   *tpr = 1;
   if (path == PATH_LASSO) {
-    if (k == 0) { *name = "lasso1 A_d*w"; *bytes = csr(L) + N * v + L.rows * v; *tpr = L.tpr; }
-    else { *name = "lasso2 A_d'*t+prox"; *bytes = csr(LT) + L.rows * v + 3 * N * v + 2 * N * d + 4 * N * v; *tpr = LT.tpr; }
+    if (k == 0) { *name = "lasso1 A_d*w"; *bytes = csr(L) + N * v + L.rows * v; *tpr = sched(L); }
+    else { *name = "lasso2 A_d'*t+prox"; *bytes = csr(LT) + L.rows * v + 3 * N * v + 2 * N * d + 4 * N * v; *tpr = sched(LT); }
     return;
   }
   const double cq = is_qap ? 0.0 : csr(Q);
-  const int tq = is_qap ? 1 : Q.tpr;
+  const int tq = is_qap ? 1 : sched(Q);
   if (path == PATH_QP) {
     if (k == 0) { *name = "zxw1 Q*w"; *bytes = cq + N * v + 5 * N * v + N * d + dg + 4 * N * v; *tpr = tq; }
     else if (m > 0 && k == 1) { *name = "tempv Q*w_bar"; *bytes = cq + N * v + 2 * N * v + N * v; *tpr = tq; }
-    else if (m > 0 && k == 2) { *name = "y A*tempv"; *bytes = csr(A) + N * v + 3 * M_ * v + M_ * d + 2 * M_ * v; *tpr = A.tpr; }
-    else { *name = "w2 A'*y_bar"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 3 * N * v + 2 * N * d + (Q_is_diag ? N * v : 0.0) + 2 * N * v; *tpr = m > 0 ? AT.tpr : 1; }
+    else if (m > 0 && k == 2) { *name = "y A*tempv"; *bytes = csr(A) + N * v + 3 * M_ * v + M_ * d + 2 * M_ * v; *tpr = sched(A); }
+    else { *name = "w2 A'*y_bar"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 3 * N * v + 2 * N * d + (Q_is_diag ? N * v : 0.0) + 2 * N * v; *tpr = m > 0 ? sched(AT) : 1; }
     return;
   }
   if (path == PATH_NOC) {
-    if (k == 0) { *name = "zxw A'*y"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 6 * N * v + 2 * N * d + dg + 4 * N * v; *tpr = m > 0 ? AT.tpr : 1; }
+    if (k == 0) { *name = "zxw A'*y"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 6 * N * v + 2 * N * d + dg + 4 * N * v; *tpr = m > 0 ? sched(AT) : 1; }
     else if (k == 1) { *name = "tempv Q*w_bar"; *bytes = cq + N * v + 2 * N * v + N * d + 2 * N * v; *tpr = tq; }
-    else { *name = "y A*tempv"; *bytes = csr(A) + N * v + 3 * M_ * v + M_ * d + 2 * M_ * v; *tpr = A.tpr; }
+    else { *name = "y A*tempv"; *bytes = csr(A) + N * v + 3 * M_ * v + M_ * d + 2 * M_ * v; *tpr = sched(A); }
     return;
   }
-  if (k == 0) { *name = "zx A'*y"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 4 * N * v + N * d + 2 * N * v; *tpr = m > 0 ? AT.tpr : 1; }
-  else { *name = "y A*x_hat"; *bytes = m > 0 ? csr(A) + N * v + 3 * M_ * v + M_ * d + M_ * v : 0.0; *tpr = m > 0 ? A.tpr : 1; }
+  if (k == 0) { *name = "zx A'*y"; *bytes = (m > 0 ? csr(AT) + M_ * v : 0.0) + 4 * N * v + N * d + 2 * N * v; *tpr = m > 0 ? sched(AT) : 1; }
+  else { *name = "y A*x_hat"; *bytes = m > 0 ? csr(A) + N * v + 3 * M_ * v + M_ * d + M_ * v : 0.0; *tpr = m > 0 ? sched(A) : 1; }
 }
 
 // ---------------------------------------------------------------------------
@@ -510,12 +591,12 @@ void Engine<V>::residuals_launch(bool) {
   apply_Q(x_bar, Qx);
   EpiResN<V> e{x_bar, Qx, c, z_bar, col_norm, l, u, lam_l1, c_scale, b_scale};
   if (m > 0)
-    reduce<8, kResNMax, double>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar}, e, cm.d_scal + S_RES_N);
+    mat_reduce<8, kResNMax>(cm, AT, y_bar, e, cm.d_scal + S_RES_N);
   else
     reduce<8, kResNMax, double>(cm, 1, n, ZeroSrc{}, e, cm.d_scal + S_RES_N);
   if (m > 0) {
     EpiResM<V> em{y_bar, s, AL, AU, row_norm, b_scale};
-    reduce<3, kResMMax, double>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, x_bar}, em, cm.d_scal + S_RES_M);
+    mat_reduce<3, kResMMax>(cm, A, x_bar, em, cm.d_scal + S_RES_M);
   }
 }
 
@@ -583,7 +664,7 @@ template <typename V>
 void Engine<V>::restart() {
   EpiRestartN<V> e{x, w, ATy, ATy_bar, Qw, x_bar, w_bar, Qw_bar, last_x, last_w, last_ATy, last_Qw,
                    m > 0, path == PATH_NOC};
-  if (m > 0) rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar}, e);
+  if (m > 0) mat_rows(AT, y_bar, e);
   else rows<V>(cm, 1, n, ZeroSrc{}, e);
   V *y_ = y;
   const V* yb = y_bar;
@@ -722,13 +803,11 @@ double Engine<V>::power_run(int which, double tol, int max_it, int64_t* iters) {
   auto one_step = [&](int k, V* zc, V* zn) {
     const PowerFin fin{log, k};
     if (which == 0) {  // A A' (power_iteration_A)
-      rows<V>(cm, AT.tpr, n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, zc}, EpiStoreInvNorm<V>{pt, zz});
-      reduce<3, 0u, double>(cm, A.tpr, m, CsrSrc<V, V>{A.ptr, A.col, A.val, pt}, EpiPowerFused<V>{zc, zn, zz, false},
-                            cm.d_scal + S_POW + 1, fin);
+      mat_rows(AT, zc, EpiStoreInvNorm<V>{pt, zz});
+      mat_reduce<3, 0u>(cm, A, pt, EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
     } else if (is_lasso) {
-      rows<V>(cm, L.tpr, L.rows, CsrSrc<V, V>{L.ptr, L.col, L.val, zc}, EpiStoreInvNorm<V>{ltemp, zz});
-      reduce<3, 0u, double>(cm, LT.tpr, n, CsrSrc<V, V>{LT.ptr, LT.col, LT.val, ltemp},
-                            EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
+      mat_rows(L, zc, EpiStoreInvNorm<V>{ltemp, zz});
+      mat_reduce<3, 0u>(cm, LT, ltemp, EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
     } else if (is_qap) {
       V* q = pt;
       const V* z = zc;
@@ -736,8 +815,7 @@ double Engine<V>::power_run(int which, double tol, int max_it, int64_t* iters) {
       qap_apply(pt, zn);
       reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
     } else {
-      reduce<3, 0u, double>(cm, Q.tpr, n, CsrSrc<V, V>{Q.ptr, Q.col, Q.val, zc}, EpiPowerFused<V>{zc, zn, zz, true},
-                            cm.d_scal + S_POW + 1, fin);
+      mat_reduce<3, 0u>(cm, Q, zc, EpiPowerFused<V>{zc, zn, zz, true}, cm.d_scal + S_POW + 1, fin);
     }
   };
   // capture one chunk (cuBLAS calls of the QAP operator run eagerly instead)

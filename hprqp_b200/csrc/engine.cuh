@@ -61,6 +61,7 @@ struct Common {  // per-handle resources shared by the engines
   int64_t launches = 0;
   int64_t h2d = 0, d2h = 0;  // bytes copied host<->device
   int num_sms = 148;
+  bool pdl = true;           // programmatic dependent launch between kernels
   DeviceMem mem;
   void init();
   ~Common();
@@ -125,6 +126,8 @@ class Engine {
   void import_state(const Engine<W>& o);  // precision switch (FP32 -> FP64)
 
   void apply_Q(const V* xin, V* yout);  // Qmap! into a vector
+  template <typename Epi>
+  void mat_rows(const DCsr<V>& M, const V* xin, const Epi& e);  // fused pass on M's format
   Common& cm;
 
   // pass profiling: when `prof` is set, step() records an event before the
@@ -144,6 +147,7 @@ class Engine {
   void upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode);
   int autotune(DCsr<V>& d);
   void spmv(const DCsr<V>& M, const V* xin, V* yout, double scale = 1.0);
+  void build_sell(const HCsr& h, DCsr<V>& d);
   void qap_apply(const V* xin, V* yout);
 };
 

@@ -38,6 +38,25 @@ struct CsrSrc {  // (M x)_row with M in CSR
   }
 };
 
+template <typename V, typename X>
+struct SellSrc {  // (M x)_row with M in SELL-32, one thread per row
+  const int* __restrict__ sptr;
+  const int* __restrict__ ptr;
+  const int* __restrict__ col;
+  const V* __restrict__ val;
+  const X* __restrict__ x;
+  template <int TPR, typename Acc>
+  __device__ __forceinline__ Acc dot(int row, int) const {
+    const int len = __ldg(ptr + row + 1) - __ldg(ptr + row);
+    const int base = __ldg(sptr + (row >> 5)) + (row & 31);
+    Acc s = Acc(0);
+#pragma unroll 4
+    for (int k = 0; k < len; ++k)
+      s = fma((Acc)__ldg(val + base + 32 * k), (Acc)__ldg(x + __ldg(col + base + 32 * k)), s);
+    return s;
+  }
+};
+
 template <typename V>
 struct VecSrc {  // precomputed product (operator Q)
   const V* __restrict__ v;
@@ -57,6 +76,7 @@ __device__ __forceinline__ double clampd(double v, double lo, double hi) { retur
 // ---------------------------------------------------------------------------
 template <int TPR, typename Acc, typename Src, typename Epi>
 __global__ void __launch_bounds__(kBlock) k_row_pass(int nrows, Src src, Epi epi) {
+  pdl_enter();
   const long long g = (long long)blockIdx.x * kBlock + threadIdx.x;
   const int row = (int)(g / TPR);
   if (row >= nrows) return;  // whole row groups leave together
@@ -145,6 +165,7 @@ __device__ __forceinline__ void grid_finish(double (&r)[K], ReduceWs ws, double*
 template <int TPR, int K, unsigned MaxMask, typename Acc, typename Src, typename Epi, typename Fin = NoFin>
 __global__ void __launch_bounds__(kBlock) k_row_reduce(int nrows, Src src, Epi epi, ReduceWs ws,
                                                        double* out, Fin fin = Fin()) {
+  pdl_enter();
   double r[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) r[k] = 0.0;
@@ -532,6 +553,7 @@ struct EpiPowerDot {
 // ---------------------------------------------------------------------------
 template <typename F>
 __global__ void __launch_bounds__(kBlock) k_elementwise(int len, F f) {
+  pdl_enter();
   const int i = blockIdx.x * kBlock + threadIdx.x;
   if (i < len) f(i);
 }

@@ -355,8 +355,8 @@ static void check_params(const hprqp_params& p) {
   if (!p.use_gpu) throw Error(HPRQP_E_UNSUPPORTED, "use_gpu = false: libhprqp has no CPU path");
   if (p.precision != HPRQP_PRECISION_FP64 && p.precision != HPRQP_PRECISION_FP32_POLISH)
     throw Error(HPRQP_E_ARG, "unknown precision mode");
-  if (p.spmv_mode_Q < 0 || p.spmv_mode_Q > 6 || p.spmv_mode_A < 0 || p.spmv_mode_A > 6)
-    throw Error(HPRQP_E_ARG, "spmv_mode must be 0 (auto) or 1..6 (1,2,4,8,16,32 threads per row)");
+  if (p.spmv_mode_Q < 0 || p.spmv_mode_Q > 7 || p.spmv_mode_A < 0 || p.spmv_mode_A > 7)
+    throw Error(HPRQP_E_ARG, "spmv_mode must be 0 (auto), 1..6 (CSR, 1..32 threads per row) or 7 (SELL-32)");
 }
 
 static void prepare(Handle& H, const hprqp_params& p) {
@@ -417,12 +417,17 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   // estimate_eigenvalues (src/algorithm.jl:1407-1440)
   double lamA = 0.0, lamQ = 0.0;
   int64_t pit = 0;
-  if (m > 0) lamA = p.lambda_max_A_override > 0 ? p.lambda_max_A_override : E64.power_A(1e-4, 5000, &pit) * p.eig_factor;
+  // The power method runs in the precision of the first phase: its 1e-4
+  // stopping test is far above FP32 rounding.
+  const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
+  auto powA = [&]() { return fp32 ? H.e32->power_A(1e-4, 5000, &pit) : E64.power_A(1e-4, 5000, &pit); };
+  auto powQ = [&]() { return fp32 ? H.e32->power_Q(1e-4, 5000, &pit) : E64.power_Q(1e-4, 5000, &pit); };
+  if (m > 0) lamA = p.lambda_max_A_override > 0 ? p.lambda_max_A_override : powA() * p.eig_factor;
   if (H.hp.Q_kind != HPRQP_Q_SPARSE) {
-    lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : E64.power_Q(1e-4, 5000, &pit) * p.eig_factor;
+    lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : powQ() * p.eig_factor;
   } else if (pp.Q.nnz() > 0) {
     if (!pp.Q_is_diag)
-      lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : E64.power_Q(1e-4, 5000, &pit) * p.eig_factor;
+      lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : powQ() * p.eig_factor;
     else
       lamQ = pp.Q_maxval;
   }

@@ -119,8 +119,10 @@ typedef struct hprqp_params {
     double  eig_factor;              /* 1.05                                        */
     int32_t check_iter;              /* 100                                         */
     int32_t warm_up;                 /* 0; accepted, no JIT to warm                 */
-    int32_t spmv_mode_Q;             /* 0 = auto (autotuned row schedule)           */
-    int32_t spmv_mode_A;             /* 0 = auto                                    */
+    int32_t spmv_mode_Q;             /* 0 = auto (autotuned row schedule); 1..6 =
+                                        CSR with 1,2,4,...,32 threads per row;
+                                        7 = SELL-32                                 */
+    int32_t spmv_mode_A;             /* same, for A and A'                          */
     int32_t print_frequency;         /* -1 = adaptive (print_step)                  */
     int32_t device_number;           /* 0                                           */
     int32_t use_Ruiz_scaling;        /* 1                                           */

@@ -1,0 +1,171 @@
+# HPRQPGPU.jl — Julia binding of libhprqp.so (include/hprqp.h) for HPR-QP.
+#
+# Drop-in for the `params.use_gpu == true` branch of HPRQP.solve
+# (src/algorithm.jl:1904-2039): the model built by build_from_* (QP_info_cpu)
+# crosses the C ABI unchanged — CSC arrays are passed as-is with
+# index_base = 1 — and the library returns an HPRQP_results-shaped record.
+# CUDA.jl, cuSPARSE and KernelAbstractions are not involved.
+#
+# This file is not executed in the build container (no Julia there); the
+# same ABI is exercised from Python (hprqp_b200/_lib.py) by the test-suite.
+
+module HPRQPGPU
+
+using SparseArrays
+
+const libhprqp = get(ENV, "HPRQP_LIB", joinpath(@__DIR__, "..", "hprqp_b200", "libhprqp.so"))
+
+const Q_SPARSE, Q_LASSO, Q_QAP = Int32(0), Int32(1), Int32(2)
+const STATUS = Dict(0 => "OPTIMAL", 1 => "MAX_ITER", 2 => "TIME_LIMIT", 3 => "NUMERICAL_ERROR")
+
+# mirrors `hprqp_problem`
+struct CProblem
+    n::Int64
+    m::Int64
+    index_base::Int32
+    Q_kind::Int32
+    A_colptr::Ptr{Int32}
+    A_rowval::Ptr{Int32}
+    A_nzval::Ptr{Float64}
+    c::Ptr{Float64}
+    AL::Ptr{Float64}
+    AU::Ptr{Float64}
+    l::Ptr{Float64}
+    u::Ptr{Float64}
+    obj_constant::Float64
+    lambda::Float64
+    Q_colptr::Ptr{Int32}
+    Q_rowval::Ptr{Int32}
+    Q_nzval::Ptr{Float64}
+    lasso_m::Int64
+    L_colptr::Ptr{Int32}
+    L_rowval::Ptr{Int32}
+    L_nzval::Ptr{Float64}
+    qap_n::Int64
+    qap_A::Ptr{Float64}
+    qap_B::Ptr{Float64}
+    qap_S::Ptr{Float64}
+    qap_T::Ptr{Float64}
+end
+
+# mirrors `hprqp_params`
+mutable struct CParams
+    stoptol::Float64
+    sigma::Float64
+    max_iter::Int64
+    sigma_fixed::Int32
+    time_limit::Float64
+    eig_factor::Float64
+    check_iter::Int32
+    warm_up::Int32
+    spmv_mode_Q::Int32
+    spmv_mode_A::Int32
+    print_frequency::Int32
+    device_number::Int32
+    use_Ruiz_scaling::Int32
+    use_bc_scaling::Int32
+    use_l2_scaling::Int32
+    use_Pock_Chambolle_scaling::Int32
+    problem_type::Int32
+    lambda::Float64
+    auto_save::Int32
+    verbose::Int32
+    use_gpu::Int32
+    precision::Int32
+    polish_tol::Float64
+    lambda_max_A_override::Float64
+    lambda_max_Q_override::Float64
+    profile_passes::Int32
+end
+
+# mirrors `hprqp_result`
+mutable struct CResult
+    iter::Int64; iter_4::Int64; iter_6::Int64
+    time::Float64; time_4::Float64; time_6::Float64
+    power_time::Float64; setup_time::Float64
+    primal_obj::Float64; dual_obj::Float64
+    residuals::Float64; gap::Float64; err_Rp::Float64; err_Rd::Float64
+    status::Int32; Q_is_diag::Int32
+    sigma::Float64; lambda_max_A::Float64; lambda_max_Q::Float64
+    restarts::Int64; iter_fp32::Int64; gpu_launches::Int64
+    device_time::Float64; h2d_bytes::Int64; d2h_bytes::Int64
+    CResult() = new()
+end
+
+i32(v) = convert(Vector{Int32}, v)
+lasterr(h) = unsafe_string(ccall((:hprqp_last_error, libhprqp), Cstring, (Ptr{Cvoid},), h))
+check(rc, h) = rc == 0 || error("libhprqp error $rc: $(lasterr(h))")
+
+function cparams(p)
+    c = CParams(zeros(26)...)  # filled by hprqp_default_params, then overwritten
+    ccall((:hprqp_default_params, libhprqp), Cvoid, (Ref{CParams},), c)
+    c.stoptol = p.stoptol; c.sigma = p.sigma; c.max_iter = p.max_iter
+    c.sigma_fixed = p.sigma_fixed; c.time_limit = p.time_limit; c.eig_factor = p.eig_factor
+    c.check_iter = p.check_iter; c.warm_up = p.warm_up; c.print_frequency = p.print_frequency
+    c.device_number = p.device_number
+    c.use_Ruiz_scaling = p.use_Ruiz_scaling; c.use_bc_scaling = p.use_bc_scaling
+    c.use_l2_scaling = p.use_l2_scaling; c.use_Pock_Chambolle_scaling = p.use_Pock_Chambolle_scaling
+    c.problem_type = p.problem_type == "LASSO" ? 1 : p.problem_type == "QAP" ? 2 : 0
+    c.lambda = p.lambda; c.auto_save = p.auto_save; c.verbose = p.verbose; c.use_gpu = 1
+    return c
+end
+
+"""
+    solve_gpu(model::QP_info_cpu, params::HPRQP_parameters) -> NamedTuple
+
+The GPU body of `solve` through libhprqp.  Fields match HPRQP_results.
+"""
+function solve_gpu(model, params)
+    m, n = size(model.A)
+    A = model.A
+    Acp, Arv = i32(A.colptr), i32(A.rowval)
+    keep = Any[Acp, Arv, A.nzval, model.c, model.AL, model.AU, model.l, model.u]
+    Qk = Q_SPARSE
+    Qcp = Qrv = Ptr{Int32}(0); Qnz = Ptr{Float64}(0)
+    lm = 0; Lcp = Lrv = Ptr{Int32}(0); Lnz = Ptr{Float64}(0)
+    qn = 0; qA = qB = qS = qT = Ptr{Float64}(0)
+    Q = model.Q
+    if Q isa SparseMatrixCSC
+        a, b = i32(Q.colptr), i32(Q.rowval); push!(keep, a, b, Q.nzval)
+        Qcp, Qrv, Qnz = pointer(a), pointer(b), pointer(Q.nzval)
+    elseif nameof(typeof(Q)) == :LASSO_Q_operator_cpu
+        Qk = Q_LASSO
+        a, b = i32(Q.A.colptr), i32(Q.A.rowval); push!(keep, a, b, Q.A.nzval)
+        lm = size(Q.A, 1); Lcp, Lrv, Lnz = pointer(a), pointer(b), pointer(Q.A.nzval)
+    elseif nameof(typeof(Q)) == :QAP_Q_operator_cpu
+        Qk = Q_QAP
+        push!(keep, Q.A, Q.B, Q.S, Q.T)
+        qn = Q.n; qA, qB, qS, qT = pointer(Q.A), pointer(Q.B), pointer(Q.S), pointer(Q.T)
+    else
+        error("custom Q operators need the device-callback ABI (not provided)")
+    end
+    x = zeros(n); y = zeros(m); z = zeros(n); w = zeros(n)
+    res = CResult()
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve keep begin
+        prob = CProblem(n, m, Int32(1), Qk, pointer(Acp), pointer(Arv), pointer(A.nzval),
+                        pointer(model.c), pointer(model.AL), pointer(model.AU), pointer(model.l),
+                        pointer(model.u), model.obj_constant, model.lambda,
+                        Qcp, Qrv, Qnz, lm, Lcp, Lrv, Lnz, qn, qA, qB, qS, qT)
+        check(ccall((:hprqp_create, libhprqp), Cint, (Ref{Ptr{Cvoid}}, Int32), h, params.device_number), C_NULL)
+        try
+            check(ccall((:hprqp_load, libhprqp), Cint, (Ptr{Cvoid}, Ref{CProblem}), h[], prob), h[])
+            x0 = params.initial_x === nothing ? C_NULL : pointer(params.initial_x)
+            y0 = params.initial_y === nothing ? C_NULL : pointer(params.initial_y)
+            GC.@preserve params begin
+                check(ccall((:hprqp_solve, libhprqp), Cint,
+                            (Ptr{Cvoid}, Ref{CParams}, Ptr{Float64}, Ptr{Float64}, Ref{CResult},
+                             Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                            h[], cparams(params), x0, y0, res, x, y, z, w), h[])
+            end
+        finally
+            ccall((:hprqp_destroy, libhprqp), Cint, (Ptr{Cvoid},), h[])
+        end
+    end
+    return (iter = res.iter, iter_4 = res.iter_4, iter_6 = res.iter_6, time = res.time,
+            time_4 = res.time_4, time_6 = res.time_6, power_time = res.power_time,
+            primal_obj = res.primal_obj, residuals = res.residuals, gap = res.gap,
+            status = STATUS[res.status], x = x, y = m > 0 ? y : Float64[], z = z, w = w)
+end
+
+end # module
