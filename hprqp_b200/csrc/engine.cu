@@ -12,7 +12,6 @@
 
 namespace hprqp {
 
-constexpr int kMaxReduceGrid = 1184;  // 8 CTAs per SM on 148 SMs
 
 // ---------------------------------------------------------------------------
 // Common

@@ -111,20 +111,24 @@ HCsr transpose(const HCsr& A) {
   return T;
 }
 
-std::vector<double> power_start_vector(int64_t len) {
-  std::vector<double> z(len);
-  uint64_t s = 1;
-  auto next = [&s]() {
+void StartVectorStream::fill(double* out, int64_t count) {
+  auto next = [this]() {
     uint64_t v = (s += 0x9E3779B97F4A7C15ULL);
     v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
     v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
     return v ^ (v >> 31);
   };
-  for (int64_t i = 0; i < len; ++i) {
+  for (int64_t i = 0; i < count; ++i) {
     const double u1 = ((next() >> 11) + 1.0) * 0x1.0p-53;
     const double u2 = (next() >> 11) * 0x1.0p-53;
-    z[i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2) + 1e-8;
+    out[i] = std::sqrt(-2.0 * std::log(u1)) * std::cos(6.283185307179586 * u2) + 1e-8;
   }
+}
+
+std::vector<double> power_start_vector(int64_t len) {
+  std::vector<double> z(len);
+  StartVectorStream g;
+  g.fill(z.data(), len);
   return z;
 }
 

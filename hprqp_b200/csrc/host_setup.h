@@ -55,5 +55,10 @@ void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& out
 HCsr transpose(const HCsr& A);
 // splitmix64 + Box-Muller start vector of the power method (+1e-8).
 std::vector<double> power_start_vector(int64_t len);
+// The same stream, produced incrementally into a caller buffer.
+struct StartVectorStream {
+  uint64_t s = 1;
+  void fill(double* out, int64_t count);
+};
 
 }  // namespace hprqp

@@ -116,6 +116,8 @@ __device__ __forceinline__ void block_reduce(double (&r)[K]) {
   __syncthreads();
 }
 
+constexpr int kMaxReduceGrid = 1184;  // reduction grids: at most 8 CTAs per SM on 148 SMs
+
 struct ReduceWs {  // partials (one K-vector per CTA) + ticket counter
   double* partials;
   unsigned* counter;

@@ -57,6 +57,8 @@ double golden(double ap, double bp, double cp, double dp, double lo, double hi, 
 }
 }  // namespace
 
+void set_global_error(const std::string& msg) { g_global_err = msg; }
+
 struct RestartInfo {  // HPRQP_restart / initialize_restart (src/algorithm.jl:1154-1171)
   bool first_restart = true;
   double save_gap = kInf, current_gap = kInf, last_gap = kInf, best_gap = kInf;

@@ -239,6 +239,33 @@ int hprqp_profile_iterations(hprqp_handle h, const hprqp_params* params, int64_t
  * (fp64, fp32; npass = 0 when that engine did not run). */
 int hprqp_get_pass_stats(hprqp_handle h, hprqp_pass_stats* fp64, hprqp_pass_stats* fp32);
 
+/* lambda_max(A A') by the power method, for a CSR matrix A (m x n, int32,
+ * 0-based) and its transpose A' (n x m) that the caller already holds in
+ * device memory.  It allocates nothing; use it when device memory cannot be
+ * allocated where the estimate is needed (inside a graph capture that must
+ * not allocate, under another framework's memory pool, in a loop that must
+ * not allocate after start-up).  No counterpart in the reference.
+ *  - Scratch: a fixed block inside the library (8 MiB of work vectors plus
+ *    256 KiB of control), reserved on every GPU that loads the library until
+ *    the process exits.  Requires 2m + n <= 1,048,576; larger problems get
+ *    HPRQP_E_ARG with the reason in hprqp_last_error(NULL).
+ *  - The first call on each device looks up the scratch address there;
+ *    make that call before any stream capture.
+ *  - All calls share the scratch: calls that overlap on the GPU (different
+ *    streams, threads or processes on one device) race.  Each call clears
+ *    what must start at zero.
+ *  - Same start vector, kernels and stopping test (err < tol, at most
+ *    max_iter steps) as the solver's power method (threads_per_row 1..32
+ *    selects the CSR schedule), so lambda matches hprqp_solve's
+ *    lambda_max_A / eig_factor for the same matrix and schedule.
+ *  - stream: a cudaStream_t (NULL = legacy default stream); the call
+ *    returns after the stream has finished the work.  */
+int hprqp_power_lambda_noalloc(int64_t m, int64_t n,
+                               const int32_t* A_rowptr, const int32_t* A_colind, const double* A_val,
+                               const int32_t* AT_rowptr, const int32_t* AT_colind, const double* AT_val,
+                               int32_t threads_per_row, double tol, int32_t max_iter,
+                               void* stream, double* lambda_out, int32_t* iters_out);
+
 /* Text of the last error on this handle ("" if none); valid until the next
  * call on the handle.  h may be NULL for errors from hprqp_create. */
 const char* hprqp_last_error(hprqp_handle h);
