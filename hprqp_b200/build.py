@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libhprqp.so")
-SOURCES = ["engine.cu", "solver.cu", "host_setup.cpp", "noalloc.cu"]
+SOURCES = ["engine.cu", "solver.cu", "host_setup.cpp", "noalloc.cu", "mlp.cu", "batch.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -37,7 +37,7 @@ def _stale(obj, src):
     if not os.path.exists(obj):
         return True
     deps = [src] + [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
-    deps.append(os.path.join(ROOT, "include", "hprqp.h"))
+    deps += [os.path.join(ROOT, "include", f) for f in os.listdir(os.path.join(ROOT, "include"))]
     t = os.path.getmtime(obj)
     return any(os.path.getmtime(d) > t for d in deps)
 

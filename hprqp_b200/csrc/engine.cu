@@ -18,6 +18,7 @@ namespace hprqp {
 // ---------------------------------------------------------------------------
 void Common::init() {
   HPRQP_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  HPRQP_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
   if (cublasCreate(&cublas) != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cublasCreate failed");
   cublasSetStream(cublas, stream);
   d_scal = mem.alloc<double>(kNumSlots);
@@ -26,6 +27,9 @@ void Common::init() {
   rws.partials = mem.alloc<double>((int64_t)kMaxReduceGrid * 16);
   rws.counter = mem.alloc<unsigned>(4);
   HPRQP_CUDA(cudaMemset(rws.counter, 0, sizeof(unsigned) * 4));
+  rws2.partials = mem.alloc<double>((int64_t)kMaxReduceGrid * 16);
+  rws2.counter = mem.alloc<unsigned>(4);
+  HPRQP_CUDA(cudaMemset(rws2.counter, 0, sizeof(unsigned) * 4));
   int dev = 0;
   HPRQP_CUDA(cudaGetDevice(&dev));
   HPRQP_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -37,6 +41,7 @@ Common::~Common() {
   if (h_scal) cudaFreeHost(h_scal);
   if (cublas) cublasDestroy(cublas);
   if (stream) cudaStreamDestroy(stream);
+  if (stream2) cudaStreamDestroy(stream2);
 }
 
 void Common::sync_read(int first, int count) {
@@ -87,8 +92,7 @@ static void rows(Common& cm, int tpr, int64_t nrows, const Src& src, const Epi& 
 
 template <int TPR, int K, unsigned MM, typename Acc, typename Src, typename Epi, typename Fin>
 static void reduce_t(Common& cm, int nrows, const Src& src, const Epi& epi, double* out, const Fin& fin) {
-  const long long threads = (long long)std::max(nrows, 1) * TPR;
-  const int grid = (int)std::min<long long>((threads + kBlock - 1) / kBlock, kMaxReduceGrid);
+  const int grid = reduce_grid(nrows, TPR);
   launch(cm, k_row_reduce<TPR, K, MM, Acc, Src, Epi, Fin>, grid, kBlock, nrows, src, epi, cm.rws, out, fin);
 }
 
@@ -359,6 +363,10 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   pq = mem.alloc<V>(mx);
   pt = mem.alloc<V>(mx);
   HPRQP_CUDA(cudaMemset(pz, 0, sizeof(V) * mx));
+  pz2 = mem.alloc<V>(n);
+  pq2 = mem.alloc<V>(n);
+  pt2 = mem.alloc<V>(n);
+  ltemp2 = is_lasso ? mem.alloc<V>(hp.L.rows) : nullptr;
   c = upload<V>(cm, mem, pp.c, n);
   l = upload<V>(cm, mem, pp.l, n);
   u = upload<V>(cm, mem, pp.u, n);
@@ -789,87 +797,143 @@ void Engine<V>::trace_copy(double* xt, double* yt, double* wt) {
 // with err < tol, returning that step's lambda.
 // ---------------------------------------------------------------------------
 template <typename V>
-double Engine<V>::power_run(int which, double tol, int max_it, int64_t* iters) {
-  const int64_t len = which == 0 ? m : n;
-  {
-    std::vector<double> z0 = power_start_vector(len);
+struct ScaleInvNorm {  // q = z / ||z||, the norm read from the device
+  V* q;
+  const V* z;
+  const double* zz;
+  __device__ __forceinline__ void operator()(int i) const { q[i] = (V)((double)z[i] / sqrt(*zz)); }
+};
+
+template <typename V>
+void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, double* lamA_out, double* lamQ_out,
+                           int64_t* itA, int64_t* itQ) {
+  struct Chain {
+    bool on;
+    int which;  // 0 = A A', 1 = Q
+    V *z0, *z1, *t;
+    double *scal, *log;
+    ReduceWs ws;
+    cudaStream_t st;
+    int64_t len;
+    double lam;
+    int found;
+  };
+  const cudaStream_t main = cm.stream;
+  const ReduceWs main_ws = cm.rws;
+  // the QAP operator's cuBLAS calls are bound to the main stream: one stream then
+  const cudaStream_t qst = is_qap ? main : cm.stream2;
+  Chain ca{want_A && m > 0, 0, pz, pq, pt, cm.d_scal + S_POW, cm.d_scal + S_POWLOG, cm.rws, main, m, 1.0, -1};
+  Chain cq{want_Q, 1, pz2, pq2, pt2, cm.d_scal + S_POW_Q, cm.d_scal + S_POWLOG_Q, cm.rws2, qst, n, 1.0, -1};
+  auto use = [&](const Chain& c, cudaStream_t st) {
+    cm.stream = st;
+    cm.rws = c.ws;
+  };
+  auto restore = [&]() {
+    cm.stream = main;
+    cm.rws = main_ws;
+  };
+  for (Chain* c : {&ca, &cq}) {
+    if (!c->on) continue;
+    std::vector<double> z0 = power_start_vector(c->len);
     std::vector<V> zv(z0.begin(), z0.end());
-    cm.to_dev(pz, zv.data(), sizeof(V) * len);
+    cm.to_dev(c->z0, zv.data(), sizeof(V) * c->len);
+    HPRQP_CUDA(cudaStreamSynchronize(main));
+    use(*c, main);
+    reduce<1, 0u, double>(cm, 1, c->len, ZeroSrc{}, EpiSumSq<V>{c->z0}, c->scal + 2);
+    restore();
   }
-  double* zz = cm.d_scal + S_POW + 2;
-  double* log = cm.d_scal + S_POWLOG;
-  reduce<1, 0u, double>(cm, 1, len, ZeroSrc{}, EpiSumSq<V>{pz}, zz);
-  auto one_step = [&](int k, V* zc, V* zn) {
-    const PowerFin fin{log, k};
-    if (which == 0) {  // A A' (power_iteration_A)
-      mat_rows(AT, zc, EpiStoreInvNorm<V>{pt, zz});
-      mat_reduce<3, 0u>(cm, A, pt, EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
+  auto step = [&](const Chain& c, cudaStream_t st, int k) {
+    use(c, st);
+    V* zc = (k & 1) ? c.z1 : c.z0;
+    V* zn = (k & 1) ? c.z0 : c.z1;
+    double* zz = c.scal + 2;
+    const PowerFin fin{c.log, k};
+    if (c.which == 0) {  // A A' (power_iteration_A)
+      mat_rows(AT, zc, EpiStoreInvNorm<V>{c.t, zz});
+      mat_reduce<3, 0u>(cm, A, c.t, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
     } else if (is_lasso) {
-      mat_rows(L, zc, EpiStoreInvNorm<V>{ltemp, zz});
-      mat_reduce<3, 0u>(cm, LT, ltemp, EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
+      mat_rows(L, zc, EpiStoreInvNorm<V>{ltemp2, zz});
+      mat_reduce<3, 0u>(cm, LT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
     } else if (is_qap) {
-      V* q = pt;
-      const V* z = zc;
-      elem(cm, n, [=] __device__(int i) { q[i] = (V)((double)z[i] / sqrt(*zz)); });
-      qap_apply(pt, zn);
-      reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false}, cm.d_scal + S_POW + 1, fin);
+      elem(cm, n, ScaleInvNorm<V>{c.t, zc, zz});
+      qap_apply(c.t, zn);
+      reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
     } else {
-      mat_reduce<3, 0u>(cm, Q, zc, EpiPowerFused<V>{zc, zn, zz, true}, cm.d_scal + S_POW + 1, fin);
+      mat_reduce<3, 0u>(cm, Q, zc, EpiPowerFused<V>{zc, zn, zz, true}, c.scal + 1, fin);
+    }
+    restore();
+  };
+  // one chunk = kPowChunk steps of every active chain; A on the main stream,
+  // Q forked onto the second stream when both run (captured in a graph)
+  cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
+  int64_t graph_launches[4] = {0, 0, 0, 0};
+  cudaEvent_t fork = nullptr, join = nullptr;
+  HPRQP_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
+  HPRQP_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
+  auto issue_chunk = [&](bool doA, bool doQ) {
+    const bool two = doA && doQ && qst != main;
+    if (two) {
+      HPRQP_CUDA(cudaEventRecord(fork, main));
+      HPRQP_CUDA(cudaStreamWaitEvent(qst, fork, 0));
+    }
+    for (int k = 0; k < kPowChunk; ++k) {
+      if (doA) step(ca, main, k);
+      if (doQ) step(cq, two ? qst : main, k);
+    }
+    if (two) {
+      HPRQP_CUDA(cudaEventRecord(join, qst));
+      HPRQP_CUDA(cudaStreamWaitEvent(main, join, 0));
     }
   };
-  // capture one chunk (cuBLAS calls of the QAP operator run eagerly instead)
-  cudaGraphExec_t exec = nullptr;
-  int64_t per_chunk_launches = 0;
-  if (!is_qap) {
-    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
-    cudaGraph_t g = nullptr;
-    const int64_t l0 = cm.launches;
-    HPRQP_CUDA(cudaStreamBeginCapture(cm.stream, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < kPowChunk; ++k) one_step(k, (k & 1) ? pq : pz, (k & 1) ? pz : pq);
-    HPRQP_CUDA(cudaStreamEndCapture(cm.stream, &g));
-    per_chunk_launches = cm.launches - l0;
-    cm.launches = l0;
-    HPRQP_CUDA(cudaGraphInstantiate(&exec, g, 0));
-    cudaGraphDestroy(g);
-  }
-  double lam = 1.0;
   int it = 0;
-  int found = -1;
-  while (it < max_it && found < 0) {
-    if (exec) {
-      HPRQP_CUDA(cudaGraphLaunch(exec, cm.stream));
-      cm.launches += per_chunk_launches;
+  while (it < max_it && ((ca.on && ca.found < 0) || (cq.on && cq.found < 0))) {
+    const bool doA = ca.on && ca.found < 0, doQ = cq.on && cq.found < 0;
+    const int gi = (doA ? 1 : 0) | (doQ ? 2 : 0);
+    if (is_qap) {
+      issue_chunk(doA, doQ);  // cuBLAS inside: run eagerly
     } else {
-      for (int k = 0; k < kPowChunk; ++k) one_step(k, (k & 1) ? pq : pz, (k & 1) ? pz : pq);
+      if (!graphs[gi]) {
+        HPRQP_CUDA(cudaStreamSynchronize(main));
+        HPRQP_CUDA(cudaStreamSynchronize(cm.stream2));
+        cudaGraph_t g = nullptr;
+        const int64_t l0 = cm.launches;
+        HPRQP_CUDA(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+        issue_chunk(doA, doQ);
+        HPRQP_CUDA(cudaStreamEndCapture(main, &g));
+        graph_launches[gi] = cm.launches - l0;
+        cm.launches = l0;
+        HPRQP_CUDA(cudaGraphInstantiate(&graphs[gi], g, 0));
+        cudaGraphDestroy(g);
+      }
+      HPRQP_CUDA(cudaGraphLaunch(graphs[gi], main));
+      cm.launches += graph_launches[gi];
     }
-    cm.sync_read(S_POWLOG, 2 * kPowChunk);
-    for (int k = 0; k < kPowChunk && it + k < max_it; ++k) {
-      lam = cm.h_scal[S_POWLOG + 2 * k];
-      if (cm.h_scal[S_POWLOG + 2 * k + 1] < tol) {
-        found = it + k + 1;
-        break;
+    cm.sync_read(S_POWLOG, 4 * kPowChunk);
+    for (Chain* c : {&ca, &cq}) {
+      if (!c->on || c->found >= 0) continue;
+      const double* lg = cm.h_scal + (c->which == 0 ? S_POWLOG : S_POWLOG_Q);
+      for (int k = 0; k < kPowChunk && it + k < max_it; ++k) {
+        c->lam = lg[2 * k];
+        if (lg[2 * k + 1] < tol) {
+          c->found = it + k + 1;
+          break;
+        }
       }
     }
     it += kPowChunk;
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (found < 0) {
-    *iters = std::min(it, max_it);
-    std::fprintf(stderr, "Power iteration did not converge within the specified tolerance.\n");
-  } else {
-    *iters = found;
-  }
-  return lam;
-}
-
-template <typename V>
-double Engine<V>::power_A(double tol, int max_it, int64_t* iters) {
-  return power_run(0, tol, max_it, iters);
-}
-
-template <typename V>
-double Engine<V>::power_Q(double tol, int max_it, int64_t* iters) {
-  return power_run(1, tol, max_it, iters);
+  for (auto& g : graphs)
+    if (g) cudaGraphExecDestroy(g);
+  cudaEventDestroy(fork);
+  cudaEventDestroy(join);
+  for (Chain* c : {&ca, &cq})
+    if (c->on && c->found < 0)
+      std::fprintf(stderr, "Power iteration (%s) did not converge within the specified tolerance.\n",
+                   c->which == 0 ? "A" : "Q");
+  if (lamA_out) *lamA_out = ca.lam;
+  if (lamQ_out) *lamQ_out = cq.lam;
+  if (itA) *itA = ca.found >= 0 ? ca.found : std::min(it, max_it);
+  if (itQ) *itQ = cq.found >= 0 ? cq.found : std::min(it, max_it);
 }
 
 // FP32 -> FP64 hand-over of the full iteration state (precision switch)

@@ -30,10 +30,12 @@ enum Slot {
   S_MN_LAST = 32,  // 8 + 1 slots: M-norm for last_gap
   S_SIG = 48,      // 5 + 1 slots: sigma statistics
   S_GOLD = 56,     // golden-section result (diagonal Q)
-  S_POW = 64,      // power method working scalars (4)
-  S_POWLOG = 128,  // power method log: (lambda, err) per iteration
+  S_POW = 64,      // power method (A A') working scalars (4)
+  S_POW_Q = 72,    // power method (Q) working scalars (4)
+  S_POWLOG = 128,  // power method log A A': (lambda, err) per iteration
   kPowChunk = 32,
-  kNumSlots = S_POWLOG + 2 * kPowChunk,
+  S_POWLOG_Q = S_POWLOG + 2 * kPowChunk,  // power method log Q
+  kNumSlots = S_POWLOG_Q + 2 * kPowChunk,
 };
 
 struct DeviceMem {  // owns cudaMalloc'ed blocks
@@ -54,10 +56,11 @@ struct DeviceMem {  // owns cudaMalloc'ed blocks
 
 struct Common {  // per-handle resources shared by the engines
   cudaStream_t stream = nullptr;
+  cudaStream_t stream2 = nullptr;  // second chain of the power method
   cublasHandle_t cublas = nullptr;
   double* d_scal = nullptr;
   double* h_scal = nullptr;  // pinned mirror
-  ReduceWs rws{};
+  ReduceWs rws{}, rws2{};
   int64_t launches = 0;
   int64_t h2d = 0, d2h = 0;  // bytes copied host<->device
   int num_sms = 148;
@@ -102,6 +105,7 @@ class Engine {
   V *y, *y_bar, *dy, *s, *Ax, *AL, *AU, *row_norm;
   double *last_x, *last_w, *last_ATy, *last_Qw, *last_y;
   V* ltemp = nullptr;                 // LASSO A_d w
+  V* ltemp2 = nullptr;                // LASSO A_d z of the Q power chain
   double *stage_n, *stage_m;          // FP64 staging for host copies
   V *pz, *pq, *pt;                    // power method vectors
 
@@ -119,9 +123,11 @@ class Engine {
   void initial_points(const double* x0, const double* y0);
   void collect(double* x_out, double* y_out, double* z_out, double* w_out);
   void trace_copy(double* xt, double* yt, double* wt);
-  double power_A(double tol, int max_it, int64_t* iters);
-  double power_Q(double tol, int max_it, int64_t* iters);
-  double power_run(int which, double tol, int max_it, int64_t* iters);
+  // Both power methods (A A' and Q) at once, on two streams; want_* select
+  // which run.  Returns lambda estimates (not yet times eig_factor).
+  void power_both(bool want_A, bool want_Q, double tol, int max_it, double* lamA_out, double* lamQ_out,
+                  int64_t* itA, int64_t* itQ);
+  V *pz2 = nullptr, *pq2 = nullptr, *pt2 = nullptr;  // Q chain vectors
   template <typename W>
   void import_state(const Engine<W>& o);  // precision switch (FP32 -> FP64)
 

@@ -1,0 +1,457 @@
+// mlp.cu — the warm-start network: a 3-layer MLP (ReLU) with BF16 weights
+// and activations, FP32 accumulation, FP32 master weights and Adam, with
+// hand-written forward, backward and update kernels.
+//
+// It maps instance features of a problem family to a proposed solution and
+// log sigma; the HPR engine then starts from that proposal and certifies the
+// result itself, so a poor proposal costs iterations, never correctness.
+//
+// Layout: every matrix is row-major with leading dimensions padded to
+// multiples of 64 (zero padding stays zero: padded inputs are zero, padded
+// weight rows/columns start at zero and receive zero gradient).  Products
+// run on the tensor cores through WMMA 16x16x16 BF16 fragments with FP32
+// accumulators; one warp owns a 32x32 output tile, a CTA of 4 warps 64x64.
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <mma.h>
+
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/hprqp.h"
+#include "../../include/hprqp_mlp.h"
+#include "common.cuh"
+
+namespace hprqp {
+namespace mlp {
+
+using bf16 = __nv_bfloat16;
+using namespace nvcuda;
+
+constexpr int kTile = 64;
+inline int64_t pad64(int64_t v) { return (v + 63) / 64 * 64; }
+
+// C[M x N] (+)= opA(A) opB(B), fp32 out.  TA: A is stored K x M (row-major)
+// i.e. used transposed; TB: B is stored N x K (row-major) and used transposed.
+// All of M, N, K are multiples of 64; lda/ldb/ldc are the row strides.
+template <bool TA, bool TB>
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const bf16* __restrict__ A, int lda,
+                                              const bf16* __restrict__ B, int ldb, float* __restrict__ C, int ldc,
+                                              bool accumulate) {
+  using LA = typename std::conditional<TA, wmma::col_major, wmma::row_major>::type;
+  using LB = typename std::conditional<TB, wmma::col_major, wmma::row_major>::type;
+  const int warp = threadIdx.x >> 5;
+  const int row0 = blockIdx.y * kTile + (warp >> 1) * 32;
+  const int col0 = blockIdx.x * kTile + (warp & 1) * 32;
+  if (row0 >= M || col0 >= N) return;
+  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      if (accumulate) wmma::load_matrix_sync(acc[i][j], C + (size_t)(row0 + 16 * i) * ldc + col0 + 16 * j, ldc, wmma::mem_row_major);
+      else wmma::fill_fragment(acc[i][j], 0.0f);
+    }
+  for (int k = 0; k < K; k += 16) {
+    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, LA> a[2];
+    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, LB> b[2];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+      const bf16* pa = TA ? A + (size_t)k * lda + row0 + 16 * i : A + (size_t)(row0 + 16 * i) * lda + k;
+      wmma::load_matrix_sync(a[i], pa, lda);
+    }
+#pragma unroll
+    for (int j = 0; j < 2; ++j) {
+      const bf16* pb = TB ? B + (size_t)(col0 + 16 * j) * ldb + k : B + (size_t)k * ldb + col0 + 16 * j;
+      wmma::load_matrix_sync(b[j], pb, ldb);
+    }
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) wmma::mma_sync(acc[i][j], a[i], b[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 2; ++j)
+      wmma::store_matrix_sync(C + (size_t)(row0 + 16 * i) * ldc + col0 + 16 * j, acc[i][j], ldc, wmma::mem_row_major);
+}
+
+// Z = Z + bias (per column); relu -> H (bf16); keeps Z for the ReLU mask.
+__global__ void k_bias_act(int rows, int cols, int ld, float* Z, const float* bias, bf16* H, bool relu) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (int64_t)rows * ld) return;
+  const int c = (int)(i % ld);
+  float v = Z[i] + (c < cols ? bias[c] : 0.0f);
+  if (c >= cols) v = 0.0f;
+  Z[i] = v;
+  if (H) H[i] = __float2bfloat16(relu ? fmaxf(v, 0.0f) : v);
+}
+
+// dY = (Y - T) / B on real rows/columns (zero elsewhere); returns squared error partials.
+__global__ void k_loss_grad(int rows_real, int rows, int cols, int ld, const float* Y, const float* T, float invB,
+                            bf16* dY, float* dYf, double* sq) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  double e2 = 0.0;
+  if (i < (int64_t)rows * ld) {
+    const int r = (int)(i / ld), c = (int)(i % ld);
+    float g = 0.0f;
+    if (r < rows_real && c < cols) {
+      const float e = Y[i] - T[i];
+      e2 = (double)e * e;
+      g = e * invB;
+    }
+    dY[i] = __float2bfloat16(g);
+    dYf[i] = g;
+  }
+  for (int off = 16; off > 0; off >>= 1) e2 += __shfl_down_sync(0xffffffffu, e2, off);
+  if ((threadIdx.x & 31) == 0 && e2 != 0.0) atomicAdd(sq, e2);
+}
+
+// dZ = dH * (Z > 0), as bf16 for the next products
+__global__ void k_relu_back(int64_t total, const float* dH, const float* Z, bf16* dZ) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < total) dZ[i] = __float2bfloat16(Z[i] > 0.0f ? dH[i] : 0.0f);
+}
+
+// db[c] = sum_r dZ[r, c]
+__global__ void k_colsum(int rows, int cols, int ld, const bf16* dZ, float* db) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.0f;
+  for (int r = 0; r < rows; ++r) s += __bfloat162float(dZ[(size_t)r * ld + c]);
+  db[c] = s;
+}
+
+__global__ void k_f32_to_bf16(int64_t n, const float* src, bf16* dst) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = __float2bfloat16(src[i]);
+}
+
+// Adam on the FP32 master weights, then refresh the BF16 working copy.
+__global__ void k_adam(int64_t n, float* w, const float* g, float* m, float* v, bf16* wb, float lr, float b1, float b2,
+                       float c1, float c2, float eps) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.0f - b1) * gi;
+  const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+  w[i] = wi;
+  if (wb) wb[i] = __float2bfloat16(wi);
+}
+
+struct Layer {
+  int in, out, ldi, ldo;  // real and padded sizes
+  float *W, *b, *gW, *gb, *mW, *vW, *mb, *vb;  // fp32 [ldo x ldi], [ldo]
+  bf16* Wb;                                    // bf16 working copy
+};
+
+struct Net {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int n_in, width, n_out, batch;
+  std::vector<Layer> L;
+  // activations for one batch (rows padded to 64)
+  bf16 *X = nullptr, *H1 = nullptr, *H2 = nullptr, *dYb = nullptr, *dZ2 = nullptr, *dZ1 = nullptr;
+  float *Z1 = nullptr, *Z2 = nullptr, *Y = nullptr, *T = nullptr, *dYf = nullptr, *dH2 = nullptr, *dH1 = nullptr;
+  double* sq = nullptr;
+  int64_t step = 0;
+  std::vector<void*> blocks;
+  std::string err;
+  template <typename T>
+  T* alloc(int64_t n) {
+    void* p = nullptr;
+    HPRQP_CUDA(cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    blocks.push_back(p);
+    return (T*)p;
+  }
+  ~Net() {
+    for (void* p : blocks) cudaFree(p);
+    if (st) cudaStreamDestroy(st);
+  }
+};
+
+static void gemm(Net& N, bool TA, bool TB, int M, int Ncols, int K, const bf16* A, int lda, const bf16* B, int ldb,
+                 float* C, int ldc, bool acc) {
+  dim3 grid(Ncols / kTile, M / kTile);
+  if (!TA && TB) k_gemm<false, true><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
+  else if (!TA && !TB) k_gemm<false, false><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
+  else if (TA && !TB) k_gemm<true, false><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
+  else k_gemm<true, true><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
+  HPRQP_LAUNCH_CHECK();
+}
+
+static inline int blocks(int64_t n) { return (int)((n + 255) / 256); }
+
+// Forward for `rows_real` rows already in N.X; fills Z1, H1, Z2, H2, Y.
+static void forward(Net& N) {
+  const int R = N.batch;
+  Layer &l1 = N.L[0], &l2 = N.L[1], &l3 = N.L[2];
+  gemm(N, false, true, R, l1.ldo, l1.ldi, N.X, l1.ldi, l1.Wb, l1.ldi, N.Z1, l1.ldo, false);
+  k_bias_act<<<blocks((int64_t)R * l1.ldo), 256, 0, N.st>>>(R, l1.out, l1.ldo, N.Z1, l1.b, N.H1, true);
+  gemm(N, false, true, R, l2.ldo, l2.ldi, N.H1, l2.ldi, l2.Wb, l2.ldi, N.Z2, l2.ldo, false);
+  k_bias_act<<<blocks((int64_t)R * l2.ldo), 256, 0, N.st>>>(R, l2.out, l2.ldo, N.Z2, l2.b, N.H2, true);
+  gemm(N, false, true, R, l3.ldo, l3.ldi, N.H2, l3.ldi, l3.Wb, l3.ldi, N.Y, l3.ldo, false);
+  k_bias_act<<<blocks((int64_t)R * l3.ldo), 256, 0, N.st>>>(R, l3.out, l3.ldo, N.Y, l3.b, nullptr, false);
+  HPRQP_LAUNCH_CHECK();
+}
+
+// Backward for rows_real samples of the batch; gradients into gW/gb.
+static void backward(Net& N, int rows_real) {
+  const int R = N.batch;
+  Layer &l1 = N.L[0], &l2 = N.L[1], &l3 = N.L[2];
+  HPRQP_CUDA(cudaMemsetAsync(N.sq, 0, sizeof(double), N.st));
+  k_loss_grad<<<blocks((int64_t)R * l3.ldo), 256, 0, N.st>>>(rows_real, R, l3.out, l3.ldo, N.Y, N.T,
+                                                            1.0f / (float)rows_real, N.dYb, N.dYf, N.sq);
+  // layer 3: gW3 = dY^T H2 ; gb3 = colsum dY ; dH2 = dY W3
+  gemm(N, true, false, l3.ldo, l3.ldi, R, N.dYb, l3.ldo, N.H2, l3.ldi, l3.gW, l3.ldi, false);
+  k_colsum<<<blocks(l3.ldo), 256, 0, N.st>>>(R, l3.out, l3.ldo, N.dYb, l3.gb);
+  gemm(N, false, false, R, l3.ldi, l3.ldo, N.dYb, l3.ldo, l3.Wb, l3.ldi, N.dH2, l3.ldi, false);
+  k_relu_back<<<blocks((int64_t)R * l2.ldo), 256, 0, N.st>>>((int64_t)R * l2.ldo, N.dH2, N.Z2, N.dZ2);
+  // layer 2
+  gemm(N, true, false, l2.ldo, l2.ldi, R, N.dZ2, l2.ldo, N.H1, l2.ldi, l2.gW, l2.ldi, false);
+  k_colsum<<<blocks(l2.ldo), 256, 0, N.st>>>(R, l2.out, l2.ldo, N.dZ2, l2.gb);
+  gemm(N, false, false, R, l2.ldi, l2.ldo, N.dZ2, l2.ldo, l2.Wb, l2.ldi, N.dH1, l2.ldi, false);
+  k_relu_back<<<blocks((int64_t)R * l1.ldo), 256, 0, N.st>>>((int64_t)R * l1.ldo, N.dH1, N.Z1, N.dZ1);
+  // layer 1
+  gemm(N, true, false, l1.ldo, l1.ldi, R, N.dZ1, l1.ldo, N.X, l1.ldi, l1.gW, l1.ldi, false);
+  k_colsum<<<blocks(l1.ldo), 256, 0, N.st>>>(R, l1.out, l1.ldo, N.dZ1, l1.gb);
+  HPRQP_LAUNCH_CHECK();
+}
+
+static void upload_rows(Net& N, bf16* dst, float* dstf, int ld, const float* src, int rows, int cols) {
+  // host rows (cols wide) -> padded device rows; rows beyond `rows` zero
+  std::vector<float> buf((size_t)N.batch * ld, 0.0f);
+  for (int r = 0; r < rows; ++r) std::memcpy(&buf[(size_t)r * ld], src + (size_t)r * cols, sizeof(float) * cols);
+  if (dstf) HPRQP_CUDA(cudaMemcpyAsync(dstf, buf.data(), sizeof(float) * buf.size(), cudaMemcpyHostToDevice, N.st));
+  if (dst) {
+    std::vector<bf16> bb(buf.size());
+    for (size_t i = 0; i < buf.size(); ++i) bb[i] = __float2bfloat16(buf[i]);
+    HPRQP_CUDA(cudaMemcpyAsync(dst, bb.data(), sizeof(bf16) * bb.size(), cudaMemcpyHostToDevice, N.st));
+    HPRQP_CUDA(cudaStreamSynchronize(N.st));
+  }
+  HPRQP_CUDA(cudaStreamSynchronize(N.st));
+}
+
+}  // namespace mlp
+}  // namespace hprqp
+
+using namespace hprqp;
+using namespace hprqp::mlp;
+
+struct hprqp_mlp : Net {};
+static thread_local std::string g_mlp_err;
+
+#define MLP_GUARD(h, ...)                        \
+  try {                                          \
+    if (h) cudaSetDevice(h->device);             \
+    __VA_ARGS__;                                 \
+    return HPRQP_OK;                             \
+  } catch (const Error& e) {                     \
+    (h ? h->err : g_mlp_err) = e.what();         \
+    return e.code;                               \
+  }
+
+extern "C" {
+
+int hprqp_mlp_create(hprqp_mlp_handle* out, int32_t device, int32_t n_in, int32_t width, int32_t n_out,
+                     int32_t batch, uint64_t seed) {
+  hprqp_mlp* h = nullptr;
+  try {
+    if (!out || n_in <= 0 || width <= 0 || n_out <= 0 || batch <= 0) throw Error(HPRQP_E_ARG, "bad MLP sizes");
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count)
+      throw Error(HPRQP_E_CUDA, "CUDA device unavailable");
+    HPRQP_CUDA(cudaSetDevice(device));
+    h = new hprqp_mlp();
+    h->device = device;
+    HPRQP_CUDA(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+    h->n_in = n_in;
+    h->width = width;
+    h->n_out = n_out;
+    h->batch = (int)pad64(batch);
+    const int dims[4] = {n_in, width, width, n_out};
+    uint64_t s = seed ? seed : 1;
+    auto rnd = [&s]() {  // splitmix64 -> uniform (-1, 1)
+      uint64_t v = (s += 0x9E3779B97F4A7C15ULL);
+      v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
+      v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
+      v ^= v >> 31;
+      return (double)(v >> 11) * 0x1.0p-52 - 1.0;
+    };
+    for (int k = 0; k < 3; ++k) {
+      Layer l{};
+      l.in = dims[k];
+      l.out = dims[k + 1];
+      l.ldi = (int)pad64(l.in);
+      l.ldo = (int)pad64(l.out);
+      const int64_t nw = (int64_t)l.ldo * l.ldi;
+      l.W = h->alloc<float>(nw);
+      l.gW = h->alloc<float>(nw);
+      l.mW = h->alloc<float>(nw);
+      l.vW = h->alloc<float>(nw);
+      l.Wb = h->alloc<bf16>(nw);
+      l.b = h->alloc<float>(l.ldo);
+      l.gb = h->alloc<float>(l.ldo);
+      l.mb = h->alloc<float>(l.ldo);
+      l.vb = h->alloc<float>(l.ldo);
+      // He-uniform init on the real block, zero padding
+      std::vector<float> w(nw, 0.0f);
+      const double a = std::sqrt(6.0 / l.in);
+      for (int o = 0; o < l.out; ++o)
+        for (int i = 0; i < l.in; ++i) w[(size_t)o * l.ldi + i] = (float)(a * rnd());
+      std::vector<bf16> wb(nw);
+      for (int64_t i = 0; i < nw; ++i) wb[i] = __float2bfloat16(w[i]);
+      HPRQP_CUDA(cudaMemcpy(l.W, w.data(), sizeof(float) * nw, cudaMemcpyHostToDevice));
+      HPRQP_CUDA(cudaMemcpy(l.Wb, wb.data(), sizeof(bf16) * nw, cudaMemcpyHostToDevice));
+      h->L.push_back(l);
+    }
+    const int R = h->batch;
+    Layer &l1 = h->L[0], &l2 = h->L[1], &l3 = h->L[2];
+    h->X = h->alloc<bf16>((int64_t)R * l1.ldi);
+    h->Z1 = h->alloc<float>((int64_t)R * l1.ldo);
+    h->H1 = h->alloc<bf16>((int64_t)R * l1.ldo);
+    h->Z2 = h->alloc<float>((int64_t)R * l2.ldo);
+    h->H2 = h->alloc<bf16>((int64_t)R * l2.ldo);
+    h->Y = h->alloc<float>((int64_t)R * l3.ldo);
+    h->T = h->alloc<float>((int64_t)R * l3.ldo);
+    h->dYb = h->alloc<bf16>((int64_t)R * l3.ldo);
+    h->dYf = h->alloc<float>((int64_t)R * l3.ldo);
+    h->dH2 = h->alloc<float>((int64_t)R * l2.ldo);
+    h->dZ2 = h->alloc<bf16>((int64_t)R * l2.ldo);
+    h->dH1 = h->alloc<float>((int64_t)R * l1.ldo);
+    h->dZ1 = h->alloc<bf16>((int64_t)R * l1.ldo);
+    h->sq = h->alloc<double>(1);
+    *out = h;
+    return HPRQP_OK;
+  } catch (const Error& e) {
+    g_mlp_err = e.what();
+    delete h;
+    return e.code;
+  }
+}
+
+int hprqp_mlp_train_batch(hprqp_mlp_handle h, const float* X, const float* T, int32_t rows, float lr,
+                          double* loss_out) {
+  if (!h || !X || !T || rows <= 0) return HPRQP_E_ARG;
+  MLP_GUARD(h, {
+    if (rows > h->batch) throw Error(HPRQP_E_ARG, "rows exceed the batch size");
+    upload_rows(*h, h->X, nullptr, h->L[0].ldi, X, rows, h->n_in);
+    upload_rows(*h, nullptr, h->T, h->L[2].ldo, T, rows, h->n_out);
+    forward(*h);
+    backward(*h, rows);
+    h->step++;
+    const float b1 = 0.9f, b2 = 0.999f;
+    const float c1 = 1.0f - std::pow(b1, (float)h->step), c2 = 1.0f - std::pow(b2, (float)h->step);
+    for (auto& l : h->L) {
+      const int64_t nw = (int64_t)l.ldo * l.ldi;
+      k_adam<<<blocks(nw), 256, 0, h->st>>>(nw, l.W, l.gW, l.mW, l.vW, l.Wb, lr, b1, b2, c1, c2, 1e-8f);
+      k_adam<<<blocks(l.ldo), 256, 0, h->st>>>(l.ldo, l.b, l.gb, l.mb, l.vb, nullptr, lr, b1, b2, c1, c2, 1e-8f);
+    }
+    HPRQP_LAUNCH_CHECK();
+    double sq = 0;
+    HPRQP_CUDA(cudaMemcpyAsync(&sq, h->sq, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    HPRQP_CUDA(cudaStreamSynchronize(h->st));
+    if (loss_out) *loss_out = 0.5 * sq / rows;
+  })
+}
+
+int hprqp_mlp_gradients(hprqp_mlp_handle h, const float* X, const float* T, int32_t rows, float* grads,
+                        double* loss_out) {
+  if (!h || !X || !T || rows <= 0 || !grads) return HPRQP_E_ARG;
+  MLP_GUARD(h, {
+    if (rows > h->batch) throw Error(HPRQP_E_ARG, "rows exceed the batch size");
+    upload_rows(*h, h->X, nullptr, h->L[0].ldi, X, rows, h->n_in);
+    upload_rows(*h, nullptr, h->T, h->L[2].ldo, T, rows, h->n_out);
+    forward(*h);
+    backward(*h, rows);
+    double sq = 0;
+    HPRQP_CUDA(cudaMemcpyAsync(&sq, h->sq, sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    HPRQP_CUDA(cudaStreamSynchronize(h->st));
+    if (loss_out) *loss_out = 0.5 * sq / rows;
+    // unpadded [W1, b1, W2, b2, W3, b3], W row-major out x in
+    size_t off = 0;
+    for (auto& l : h->L) {
+      std::vector<float> g((size_t)l.ldo * l.ldi), gb(l.ldo);
+      HPRQP_CUDA(cudaMemcpy(g.data(), l.gW, sizeof(float) * g.size(), cudaMemcpyDeviceToHost));
+      HPRQP_CUDA(cudaMemcpy(gb.data(), l.gb, sizeof(float) * gb.size(), cudaMemcpyDeviceToHost));
+      for (int o = 0; o < l.out; ++o)
+        for (int i = 0; i < l.in; ++i) grads[off++] = g[(size_t)o * l.ldi + i];
+      for (int o = 0; o < l.out; ++o) grads[off++] = gb[o];
+    }
+  })
+}
+
+int hprqp_mlp_predict(hprqp_mlp_handle h, const float* X, int64_t rows, float* Y) {
+  if (!h || !X || !Y || rows < 0) return HPRQP_E_ARG;
+  MLP_GUARD(h, {
+    const Layer& l3 = h->L[2];
+    std::vector<float> out((size_t)h->batch * l3.ldo);
+    for (int64_t r0 = 0; r0 < rows; r0 += h->batch) {
+      const int cnt = (int)std::min<int64_t>(h->batch, rows - r0);
+      upload_rows(*h, h->X, nullptr, h->L[0].ldi, X + (size_t)r0 * h->n_in, cnt, h->n_in);
+      forward(*h);
+      HPRQP_CUDA(cudaMemcpyAsync(out.data(), h->Y, sizeof(float) * out.size(), cudaMemcpyDeviceToHost, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
+      for (int r = 0; r < cnt; ++r)
+        std::memcpy(Y + (size_t)(r0 + r) * h->n_out, &out[(size_t)r * l3.ldo], sizeof(float) * h->n_out);
+    }
+  })
+}
+
+int hprqp_mlp_get_params(hprqp_mlp_handle h, float* params, int64_t* count) {
+  if (!h || !count) return HPRQP_E_ARG;
+  MLP_GUARD(h, {
+    int64_t total = 0;
+    for (auto& l : h->L) total += (int64_t)l.out * l.in + l.out;
+    if (params) {
+      size_t off = 0;
+      for (auto& l : h->L) {
+        std::vector<float> w((size_t)l.ldo * l.ldi), b(l.ldo);
+        HPRQP_CUDA(cudaMemcpy(w.data(), l.W, sizeof(float) * w.size(), cudaMemcpyDeviceToHost));
+        HPRQP_CUDA(cudaMemcpy(b.data(), l.b, sizeof(float) * b.size(), cudaMemcpyDeviceToHost));
+        for (int o = 0; o < l.out; ++o)
+          for (int i = 0; i < l.in; ++i) params[off++] = w[(size_t)o * l.ldi + i];
+        for (int o = 0; o < l.out; ++o) params[off++] = b[o];
+      }
+    }
+    *count = total;
+  })
+}
+
+int hprqp_mlp_set_params(hprqp_mlp_handle h, const float* params) {
+  if (!h || !params) return HPRQP_E_ARG;
+  MLP_GUARD(h, {
+    size_t off = 0;
+    for (auto& l : h->L) {
+      std::vector<float> w((size_t)l.ldo * l.ldi, 0.0f), b(l.ldo, 0.0f);
+      for (int o = 0; o < l.out; ++o)
+        for (int i = 0; i < l.in; ++i) w[(size_t)o * l.ldi + i] = params[off++];
+      for (int o = 0; o < l.out; ++o) b[o] = params[off++];
+      std::vector<bf16> wb(w.size());
+      for (size_t i = 0; i < w.size(); ++i) wb[i] = __float2bfloat16(w[i]);
+      HPRQP_CUDA(cudaMemcpy(l.W, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice));
+      HPRQP_CUDA(cudaMemcpy(l.Wb, wb.data(), sizeof(bf16) * wb.size(), cudaMemcpyHostToDevice));
+      HPRQP_CUDA(cudaMemcpy(l.b, b.data(), sizeof(float) * b.size(), cudaMemcpyHostToDevice));
+    }
+  })
+}
+
+const char* hprqp_mlp_last_error(hprqp_mlp_handle h) { return h ? h->err.c_str() : g_mlp_err.c_str(); }
+
+int hprqp_mlp_destroy(hprqp_mlp_handle h) {
+  if (h) {
+    cudaSetDevice(h->device);
+    delete h;
+  }
+  return HPRQP_OK;
+}
+
+}  // extern "C"

@@ -79,8 +79,7 @@ int power_steps(int m, int n, CsrSrc<double, double> At_z, CsrSrc<double, double
     k_row_pass<TPR, double><<<grid, kBlock, 0, st>>>(n, At_z, EpiStoreInvNorm<double>{t, zz});
   }
   {
-    const long long threads = (long long)std::max(m, 1) * TPR;
-    const int grid = (int)std::min<long long>((threads + kBlock - 1) / kBlock, kMaxReduceGrid);
+    const int grid = reduce_grid(m, TPR);
     k_row_reduce<TPR, 3, 0u, double><<<grid, kBlock, 0, st>>>(m, A_t, EpiPowerFused<double>{zc, zn, zz, false}, ws,
                                                                scal + 1, PowerFin{log, k % kChunk});
   }
@@ -141,7 +140,7 @@ extern "C" int hprqp_power_lambda_noalloc(int64_t m, int64_t n, const int32_t* A
     NA_CHECK(cudaStreamSynchronize(st));  // the staging buffer is reused
   }
   {
-    const int grid = (int)std::min<long long>(((long long)m + kBlock - 1) / kBlock, kMaxReduceGrid);
+    const int grid = reduce_grid(m, 1);
     k_row_reduce<1, 1, 0u, double><<<grid, kBlock, 0, st>>>((int)m, ZeroSrc{}, EpiSumSq<double>{za}, ws, scal + 2);
     NA_CHECK(cudaGetLastError());
   }

@@ -386,6 +386,26 @@ static void prepare(Handle& H, const hprqp_params& p) {
   H.setup_time = now_s() - t;
 }
 
+// estimate_eigenvalues + compute_lambda_max_Q (src/algorithm.jl:1407-1440,
+// src/unified_operations.jl:703-718): the power methods for A A' and Q run
+// together, in the precision of the first phase (their 1e-4 stopping test is
+// far above FP32 rounding).
+static void estimate_lambdas(Handle& H, const hprqp_params& p, bool fp32, double* lamA, double* lamQ) {
+  const Prepared& pp = H.pp;
+  const bool needA = H.hp.m > 0 && !(p.lambda_max_A_override > 0);
+  const bool opQ = H.hp.Q_kind != HPRQP_Q_SPARSE || (pp.Q.nnz() > 0 && !pp.Q_is_diag);
+  const bool needQ = opQ && !(p.lambda_max_Q_override > 0);
+  double a = 0.0, q = 0.0;
+  int64_t ia = 0, iq = 0;
+  if (needA || needQ) {
+    if (fp32) H.e32->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
+    else H.e64->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
+  }
+  *lamA = H.hp.m > 0 ? (needA ? a * p.eig_factor : p.lambda_max_A_override) : 0.0;
+  if (opQ) *lamQ = needQ ? q * p.eig_factor : p.lambda_max_Q_override;
+  else *lamQ = pp.Q.nnz() > 0 ? pp.Q_maxval : 0.0;
+}
+
 template <typename V>
 static void start_engine(Handle& H, Engine<V>& E, const hprqp_params& p, double lamA, double lamQ, double sigma0,
                          const double* x0, const double* y0) {
@@ -422,17 +442,7 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   // The power method runs in the precision of the first phase: its 1e-4
   // stopping test is far above FP32 rounding.
   const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
-  auto powA = [&]() { return fp32 ? H.e32->power_A(1e-4, 5000, &pit) : E64.power_A(1e-4, 5000, &pit); };
-  auto powQ = [&]() { return fp32 ? H.e32->power_Q(1e-4, 5000, &pit) : E64.power_Q(1e-4, 5000, &pit); };
-  if (m > 0) lamA = p.lambda_max_A_override > 0 ? p.lambda_max_A_override : powA() * p.eig_factor;
-  if (H.hp.Q_kind != HPRQP_Q_SPARSE) {
-    lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : powQ() * p.eig_factor;
-  } else if (pp.Q.nnz() > 0) {
-    if (!pp.Q_is_diag)
-      lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : powQ() * p.eig_factor;
-    else
-      lamQ = pp.Q_maxval;
-  }
+  estimate_lambdas(H, p, fp32, &lamA, &lamQ);
   const double power_time = now_s() - L.t0;
   // sigma of allocate_workspace (src/algorithm.jl:838-851)
   double sigma0 = p.sigma > 0 ? p.sigma : 1.0;
@@ -535,12 +545,7 @@ static void profile(Handle& H, const hprqp_params& p, int64_t iters, bool full, 
   const Prepared& pp = H.pp;
   Engine<double>& E64 = *H.e64;
   double lamA = 0.0, lamQ = 0.0;
-  int64_t pit = 0;
-  if (H.hp.m > 0) lamA = p.lambda_max_A_override > 0 ? p.lambda_max_A_override : E64.power_A(1e-4, 5000, &pit) * p.eig_factor;
-  if (H.hp.Q_kind != HPRQP_Q_SPARSE || (pp.Q.nnz() > 0 && !pp.Q_is_diag))
-    lamQ = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : E64.power_Q(1e-4, 5000, &pit) * p.eig_factor;
-  else if (pp.Q.nnz() > 0)
-    lamQ = pp.Q_maxval;
+  estimate_lambdas(H, p, p.precision == HPRQP_PRECISION_FP32_POLISH, &lamA, &lamQ);
   double sigma0 = p.sigma > 0 ? p.sigma : 1.0;
   if (p.sigma == -1)
     sigma0 = (pp.norm_c > 1e-16 && pp.norm_b > 1e-16 && pp.norm_b < 1e16 && pp.norm_c < 1e16) ? pp.norm_b / pp.norm_c : 1.0;

@@ -1,0 +1,45 @@
+/*
+ * hprqp_batch.h — batched HPR solves of a LASSO family in one launch
+ * sequence (libhprqp).  Every instance is a LASSO problem as built by the
+ * reference's build_from_Ab_lambda (src/utils.jl:1222-1267): Q = A_k' A_k,
+ * c_k = -A_k' b_k, no constraints (m = 0), lambda_k.  The instances are
+ * concatenated block-diagonally and each HPR pass is one kernel over all of
+ * them; converged instances drop out through a per-instance mask.  Each
+ * instance follows the reference's control logic on its own (restarts,
+ * sigma, stopping), so its result is the one hprqp_solve would return.
+ * No counterpart in the reference (which solves one model per call).
+ */
+#ifndef HPRQP_BATCH_H
+#define HPRQP_BATCH_H
+
+#include <stdint.h>
+
+#include "hprqp.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct hprqp_batch* hprqp_batch_handle;
+
+int hprqp_batch_create(hprqp_batch_handle* h, int32_t device);
+
+/* Copy `count` LASSO problems (Q_kind = HPRQP_Q_LASSO, m = 0). */
+int hprqp_batch_load_lasso(hprqp_batch_handle h, int32_t count, const hprqp_problem* problems);
+
+/* Solve all instances.  initial_x: NULL or `count` pointers (entries may be
+ * NULL) to length-n_k warm starts; sigma0: NULL or `count` initial sigmas
+ * (<= 0: the parameter rule).  results: `count` records; x_out: NULL or
+ * `count` pointers to length-n_k outputs (entries may be NULL).  params has
+ * the meaning of hprqp_solve's, including precision (FP32 + FP64 polish
+ * switches per instance). */
+int hprqp_batch_solve(hprqp_batch_handle h, const hprqp_params* params, const double* const* initial_x,
+                      const double* sigma0, hprqp_result* results, double* const* x_out);
+
+const char* hprqp_batch_last_error(hprqp_batch_handle h);
+int hprqp_batch_destroy(hprqp_batch_handle h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPRQP_BATCH_H */
