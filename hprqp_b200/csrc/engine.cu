@@ -9,6 +9,7 @@
 #include <functional>
 
 #include "engine.cuh"
+#include "power.cuh"
 
 namespace hprqp {
 
@@ -35,6 +36,12 @@ void Common::init() {
   HPRQP_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
   const char* e = std::getenv("HPRQP_PDL");
   pdl = !(e && e[0] == '0');
+  pow_part = mem.alloc<double>(2 * 2 * kPowMaxGrid * 3);
+  pow_bar = mem.alloc<unsigned>(4);
+  const char* pe = std::getenv("HPRQP_POWER_PERSISTENT");
+  pow_persistent = !(pe && pe[0] == '0');
+  const char* pc = std::getenv("HPRQP_POWER_CTAS_PER_SM");
+  if (pc) pow_ctas_per_sm = std::atoi(pc);
 }
 
 Common::~Common() {
@@ -804,6 +811,93 @@ struct ScaleInvNorm {  // q = z / ||z||, the norm read from the device
   __device__ __forceinline__ void operator()(int i) const { q[i] = (V)((double)z[i] / sqrt(*zz)); }
 };
 
+// Both chains in one persistent cooperative kernel (power.cuh).  The start
+// vectors and ||z_0||^2 are in place (power_both).  Returns false when the
+// kernel cannot be co-resident on this GPU (the caller then runs the
+// graph-captured chains).
+template <typename V>
+bool Engine<V>::power_persistent(bool onA, bool onQ, double tol, int max_it, double* lamA_out, double* lamQ_out,
+                                 int64_t* itA, int64_t* itQ) {
+  int per = 0;
+  HPRQP_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_power_persistent<V>, kPowBlock, 0));
+  if (cm.pow_ctas_per_sm > 0) per = std::min(per, cm.pow_ctas_per_sm);
+  else per = std::min(per, 2);
+  const int grid = std::min(per * cm.num_sms, kPowMaxGrid);
+  if (grid < 1) return false;
+  PowArgs<V> pa{};
+  if (onA) {
+    PowChain<V>& c = pa.ch[0];
+    c.kind = 2;
+    c.M1 = AT;
+    c.M2 = A;
+    c.z0 = pz;
+    c.z1 = pq;
+    c.t = pt;
+    c.zz0 = cm.d_scal + S_POW + 2;
+  }
+  if (onQ) {
+    PowChain<V>& c = pa.ch[1];
+    if (is_lasso) {
+      c.kind = 2;
+      c.M1 = L;
+      c.M2 = LT;
+      c.t = ltemp2;
+    } else {
+      c.kind = 1;
+      c.M1 = Q;
+    }
+    c.z0 = pz2;
+    c.z1 = pq2;
+    c.zz0 = cm.d_scal + S_POW_Q + 2;
+  }
+  pa.tol = tol;
+  pa.max_it = max_it;
+  pa.partials = cm.pow_part;
+  pa.bar = cm.pow_bar;
+  pa.status = reinterpret_cast<int*>(cm.pow_bar + 1);
+  pa.out = cm.d_scal + S_POWLOG;
+  HPRQP_CUDA(cudaMemsetAsync(cm.pow_bar, 0, 2 * sizeof(unsigned), cm.stream));
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = dim3((unsigned)grid);
+  cfg.blockDim = dim3((unsigned)kPowBlock);
+  cfg.stream = cm.stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  HPRQP_CUDA(cudaLaunchKernelEx(&cfg, k_power_persistent<V>, pa));
+  cm.launches++;
+  cm.sync_read(S_POWLOG, 9);
+  const double* o = cm.h_scal + S_POWLOG;
+  if (o[8] != 0.0) throw Error(HPRQP_E_CUDA, "power method: a grid barrier wait timed out");
+  const bool on[2] = {onA, onQ};
+  for (int c = 0; c < 2; ++c) {
+    if (!on[c]) continue;
+    const double lam = o[4 * c], found = o[4 * c + 1], steps = o[4 * c + 2];
+    if (found < 0)
+      std::fprintf(stderr, "Power iteration (%s) did not converge within the specified tolerance.\n",
+                   c == 0 ? "A" : "Q");
+    const int64_t it = (int64_t)(found >= 0 ? found : steps);
+    if (c == 0) {
+      if (lamA_out) *lamA_out = lam;
+      if (itA) *itA = it;
+    } else {
+      if (lamQ_out) *lamQ_out = lam;
+      if (itQ) *itQ = it;
+    }
+  }
+  if (!onA) {
+    if (lamA_out) *lamA_out = 1.0;
+    if (itA) *itA = 0;
+  }
+  if (!onQ) {
+    if (lamQ_out) *lamQ_out = 1.0;
+    if (itQ) *itQ = 0;
+  }
+  return true;
+}
+
 template <typename V>
 void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, double* lamA_out, double* lamQ_out,
                            int64_t* itA, int64_t* itQ) {
@@ -842,6 +936,8 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     reduce<1, 0u, double>(cm, 1, c->len, ZeroSrc{}, EpiSumSq<V>{c->z0}, c->scal + 2);
     restore();
   }
+  if (cm.pow_persistent && !is_qap && power_persistent(ca.on, cq.on, tol, max_it, lamA_out, lamQ_out, itA, itQ))
+    return;
   auto step = [&](const Chain& c, cudaStream_t st, int k) {
     use(c, st);
     V* zc = (k & 1) ? c.z1 : c.z0;

@@ -65,6 +65,12 @@ struct Common {  // per-handle resources shared by the engines
   int64_t h2d = 0, d2h = 0;  // bytes copied host<->device
   int num_sms = 148;
   bool pdl = true;           // programmatic dependent launch between kernels
+  // persistent power method: partials [2][2][grid][3], barrier counter +
+  // status word; CTAs per SM (0 = as many as fit, capped at 2)
+  double* pow_part = nullptr;
+  unsigned* pow_bar = nullptr;
+  int pow_ctas_per_sm = 0;
+  bool pow_persistent = true;
   DeviceMem mem;
   void init();
   ~Common();
@@ -127,6 +133,8 @@ class Engine {
   // which run.  Returns lambda estimates (not yet times eig_factor).
   void power_both(bool want_A, bool want_Q, double tol, int max_it, double* lamA_out, double* lamQ_out,
                   int64_t* itA, int64_t* itQ);
+  bool power_persistent(bool onA, bool onQ, double tol, int max_it, double* lamA_out, double* lamQ_out,
+                        int64_t* itA, int64_t* itQ);
   V *pz2 = nullptr, *pq2 = nullptr, *pt2 = nullptr;  // Q chain vectors
   template <typename W>
   void import_state(const Engine<W>& o);  // precision switch (FP32 -> FP64)

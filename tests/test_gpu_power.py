@@ -1,0 +1,71 @@
+"""GPU tests of the power method (src/utils.jl:1335-1461).
+
+The engine runs both chains (A A' and Q, or the LASSO operator) in one
+persistent cooperative kernel.  Its lambda_max estimates must agree with
+the oracle's power method (same start vector, same stopping rule, FP64) and
+with the engine's graph-captured one-launch-per-product chains, which
+HPRQP_POWER_PERSISTENT=0 selects."""
+import json
+import os
+import subprocess
+import sys
+
+import pytest
+
+from hprqp_b200 import HPRQP_parameters, Solver
+from hprqp_b200 import workloads as W
+from oracle import oracle as O
+from tests.test_gpu_parity import oracle_params
+
+pytestmark = pytest.mark.gpu
+
+LAM_RTOL = 1e-8  # same iteration from the same start vector in FP64
+
+CASES = {
+    "random_qp_n2000": (W.random_qp, "QP"),
+    "random_lp": (W.random_lp, "QP"),
+    "lasso": (W.small_lasso, "LASSO"),
+    "grid_60x60": (lambda: W.grid_qp(N=60), "QP"),
+}
+
+
+def gpu_lambdas(name, precision="fp64"):
+    fn, ptype = CASES[name]
+    s = Solver(0).load(fn())
+    r = s.solve(HPRQP_parameters(verbose=False, problem_type=ptype, max_iter=0, precision=precision))
+    s.close()
+    return r.lambda_max_A, r.lambda_max_Q
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_power_method_matches_oracle(name):
+    fn, ptype = CASES[name]
+    ref = O.solve(fn(), oracle_params(ptype, max_iter=0))
+    lamA, lamQ = gpu_lambdas(name)
+    for got, want in ((lamA, ref.lambda_max_A), (lamQ, ref.lambda_max_Q)):
+        assert abs(got - want) <= LAM_RTOL * max(abs(want), 1e-300), (name, got, want)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_power_method_fp32_within_method_tolerance(name):
+    fn, ptype = CASES[name]
+    ref = O.solve(fn(), oracle_params(ptype, max_iter=0))
+    lamA, lamQ = gpu_lambdas(name, precision="fp32_polish")
+    for got, want in ((lamA, ref.lambda_max_A), (lamQ, ref.lambda_max_Q)):
+        assert abs(got - want) <= 1e-3 * max(abs(want), 1e-300), (name, got, want)
+
+
+def test_persistent_kernel_matches_launch_chain():
+    code = ("import json; from tests.test_gpu_power import gpu_lambdas, CASES; "
+            "print(json.dumps({k: gpu_lambdas(k) for k in CASES}))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for flag in ("1", "0"):
+        env = dict(os.environ, HPRQP_POWER_PERSISTENT=flag)
+        r = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[flag] = json.loads(r.stdout.strip().splitlines()[-1])
+    for k in CASES:
+        for a, b in zip(out["1"][k], out["0"][k]):
+            assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (k, a, b)
