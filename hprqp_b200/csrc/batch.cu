@@ -35,6 +35,8 @@ namespace hprqp {
 namespace batch {
 
 constexpr int kTileRows = 1024;  // rows per reduction tile (256 threads x 4)
+constexpr int kStallChecks = 3;     // FP32 phase: evaluations without a 10% KKT gain before the switch
+constexpr int kStallMinIter = 300;  // ... and not before this iteration
 constexpr int kMaxK = 8;
 constexpr int kPowWin = 16;      // power steps between host checks
 
@@ -722,6 +724,8 @@ static void solve(Handle& H, const hprqp_params& p, const double* const* x0s, co
   std::vector<char> pend_cur(B, 0), pend_last(B, 0);
   std::vector<double> mn_sig_cur(B, 0), mn_sig_last(B, 0);
   const double polish_tol = p.polish_tol > 0 ? p.polish_tol : 10.0 * p.stoptol;
+  std::vector<double> best32(B, std::numeric_limits<double>::infinity());
+  std::vector<int> stall32(B, 0);
   const bool lasso_obj = p.problem_type == HPRQP_PROBLEM_LASSO;
   int active = B;
   int64_t launches = 0;
@@ -770,7 +774,18 @@ static void solve(Handle& H, const hprqp_params& p, const double* const* x0s, co
         if (pend_cur[k]) { ri[k].current_gap = mnorm_val(&mc[(size_t)k * 3], mn_sig_cur[k], lamQ[k]); pend_cur[k] = 0; }
         if (pend_last[k]) { ri[k].last_gap = mnorm_val(&ml[(size_t)k * 3], mn_sig_last[k], lamQ[k]); pend_last[k] = 0; }
         eval(k, in64 ? r64 : r32);
-        if (!in64 && kkt[k] < polish_tol) { sw[k] = 1; any_sw = true; }
+        if (!in64) {
+          // hand over at polish_tol, or once the FP32 iterate stops improving
+          // (no 10% gain in the best KKT over kStallChecks evaluations)
+          bool go = kkt[k] < polish_tol;
+          if (kkt[k] < 0.9 * best32[k]) {
+            best32[k] = kkt[k];
+            stall32[k] = 0;
+          } else if (++stall32[k] >= kStallChecks && iter >= kStallMinIter) {
+            go = true;
+          }
+          if (go) { sw[k] = 1; any_sw = true; }
+        }
       }
       if (any_sw) {  // hand the switching instances to the FP64 engine and re-evaluate there
         BEngine<float>& E32 = *H.e32;

@@ -31,9 +31,9 @@ def test_batch_matches_single_solves(precision):
         assert rb.residuals < 1e-6
         tol = 1e-6 if precision == "fp64" else 1e-5
         assert abs(rb.primal_obj - rs.primal_obj) / (1 + abs(rs.primal_obj)) < tol
-        if precision == "fp64":
+        if precision == "fp64":  # same arithmetic: the same trajectory
             assert abs(rb.iter - rs.iter) <= max(20, 0.1 * rs.iter), (rb.iter, rs.iter)
-        assert np.max(np.abs(rb.x - rs.x)) / max(1.0, np.max(np.abs(rs.x))) < 1e-3
+            assert np.max(np.abs(rb.x - rs.x)) / max(1.0, np.max(np.abs(rs.x))) < 1e-3
 
 
 def test_batch_warm_start_from_optimum():
