@@ -31,8 +31,8 @@ struct Error : std::runtime_error {
 #ifdef __CUDACC__
 constexpr int kBlock = 256;  // threads per CTA for every row/element kernel
 
-// Device view of a sparse matrix: CSR (0-based, int32 indices), plus an
-// optional SELL-32 copy (slices of 32 consecutive rows stored column-major,
+// Device view of a sparse matrix: CSR (0-based, int32 indices), plus
+// optional ELL and SELL-32 copies (slices of 32 consecutive rows stored column-major,
 // entry k of row r at sptr[r/32] + 32k + r%32) used when the row-schedule
 // autotuner finds it faster.  Row lengths come from the CSR ptr, so the
 // padding of a slice is never read.
@@ -49,6 +49,13 @@ struct DCsr {
   const int* scol = nullptr;
   const V* sval = nullptr;
   int64_t sell_len = 0;
+  // ELL copy for short, even rows: width ell_w, entry k of row r at
+  // k * rows + r (column-major), padding = (column 0, value 0), so a row's
+  // product needs neither row pointers nor lengths
+  bool ell = false;
+  int ell_w = 0;
+  const int* ecol = nullptr;
+  const V* evalv = nullptr;
 };
 
 // Programmatic dependent launch: wait until the previous kernel in the

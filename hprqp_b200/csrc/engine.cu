@@ -7,9 +7,11 @@
 #include <cstring>
 #include <cstdlib>
 #include <functional>
+#include <type_traits>
 
 #include "engine.cuh"
 #include "power.cuh"
+#include "tc_gemm.h"
 
 namespace hprqp {
 
@@ -40,6 +42,8 @@ void Common::init() {
   pow_bar = mem.alloc<unsigned>(4);
   const char* pe = std::getenv("HPRQP_POWER_PERSISTENT");
   pow_persistent = !(pe && pe[0] == '0');
+  const char* tq = std::getenv("HPRQP_QAP_TC");
+  tc_qap = !(tq && tq[0] == '0');
   const char* pc = std::getenv("HPRQP_POWER_CTAS_PER_SM");
   if (pc) pow_ctas_per_sm = std::atoi(pc);
 }
@@ -241,16 +245,47 @@ void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode) {
   d.col = col;
   d.val = upload<V>(cm, mem, h.val, d.nnz);
   d.sell = false;
+  d.ell = false;
   if (tpr_mode == 7) {  // SELL-32 requested
     build_sell(h, d);
     d.sell = d.sell_len > 0;
     d.tpr = d.sell ? 1 : 4;
+  } else if (tpr_mode == 8) {  // ELL requested
+    build_ell(h, d);
+    d.ell = d.ell_w > 0;
+    d.tpr = d.ell ? 1 : 4;
   } else if (tpr_mode > 0) {
     d.tpr = 1 << std::min(tpr_mode - 1, 5);
   } else {
     build_sell(h, d);
+    build_ell(h, d);
     d.tpr = autotune(d);
   }
+}
+
+// ELL copy of a CSR matrix: only for short rows (width <= 16) whose padding
+// stays within 25% of the nonzeros.
+template <typename V>
+void Engine<V>::build_ell(const HCsr& h, DCsr<V>& d) {
+  d.ell_w = 0;
+  if (h.rows <= 0 || h.nnz() == 0) return;
+  int w = 0;
+  for (int64_t r = 0; r < h.rows; ++r) w = std::max(w, h.ptr[r + 1] - h.ptr[r]);
+  const int64_t total = (int64_t)w * h.rows;
+  if (w > 16 || total > (int64_t)(1.25 * h.nnz()) + 64 || total > INT32_MAX) return;
+  std::vector<int> ecol(total, 0);
+  std::vector<double> evalv(total, 0.0);
+  for (int64_t r = 0; r < h.rows; ++r)
+    for (int k = h.ptr[r]; k < h.ptr[r + 1]; ++k) {
+      const int64_t j = (int64_t)(k - h.ptr[r]) * h.rows + r;
+      ecol[j] = h.col[k];
+      evalv[j] = h.val[k];
+    }
+  int* dc = mem.alloc<int>(total);
+  cm.to_dev(dc, ecol.data(), sizeof(int) * total);
+  d.ecol = dc;
+  d.evalv = upload<V>(cm, mem, evalv, total);
+  d.ell_w = w;
 }
 
 // SELL-32 copy of a CSR matrix; skipped when padding would exceed 50%.
@@ -290,14 +325,16 @@ void Engine<V>::build_sell(const HCsr& h, DCsr<V>& d) {
 template <typename V>
 template <typename Epi>
 void Engine<V>::mat_rows(const DCsr<V>& M, const V* xin, const Epi& e) {
-  if (M.sell) rows<V>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e);
+  if (M.ell) rows<V>(cm, 1, M.rows, EllSrc<V, V>{M.ecol, M.evalv, xin, M.rows, M.ell_w}, e);
+  else if (M.sell) rows<V>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e);
   else rows<V>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, e);
 }
 
 // Fused product + reduction on M's format (FP64 accumulation).
 template <int K, unsigned MM, typename V, typename Epi, typename Fin = NoFin>
 static void mat_reduce(Common& cm, const DCsr<V>& M, const V* xin, const Epi& e, double* out, const Fin& fin = Fin()) {
-  if (M.sell) reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
+  if (M.ell) reduce<K, MM, double>(cm, 1, M.rows, EllSrc<V, V>{M.ecol, M.evalv, xin, M.rows, M.ell_w}, e, out, fin);
+  else if (M.sell) reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
   else reduce<K, MM, double>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, e, out, fin);
 }
 
@@ -313,15 +350,18 @@ int Engine<V>::autotune(DCsr<V>& d) {
   HPRQP_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = 4;
-  bool best_sell = false;
-  // candidate -1 = SELL-32 (one thread per row); each timed as the best of 3
-  // rounds of 4 back-to-back products, so a noisy round cannot decide.
-  for (int t : {-1, 1, 2, 4, 8, 16, 32}) {
+  bool best_sell = false, best_ell = false;
+  // candidate -1 = SELL-32, -2 = ELL (one thread per row each); each timed as
+  // the best of 3 rounds of 4 back-to-back products, so a noisy round cannot
+  // decide.
+  for (int t : {-2, -1, 1, 2, 4, 8, 16, 32}) {
+    if (t == -2 && d.ell_w == 0) continue;
     if (t == -1 && d.sell_len == 0) continue;
     if (t == 1 && avg > 12) continue;
     if (t == 32 && avg < 8) continue;
+    d.ell = (t == -2);
     d.sell = (t == -1);
-    d.tpr = t == -1 ? 1 : t;
+    d.tpr = t < 0 ? 1 : t;
     spmv(d, pz, pt);
     float tbest = 1e30f;
     for (int round = 0; round < 3; ++round) {
@@ -333,11 +373,12 @@ int Engine<V>::autotune(DCsr<V>& d) {
       HPRQP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       tbest = std::min(tbest, ms);
     }
-    if (tbest < best) { best = tbest; best_t = d.tpr; best_sell = d.sell; }
+    if (tbest < best) { best = tbest; best_t = d.tpr; best_sell = d.sell; best_ell = d.ell; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   d.sell = best_sell;
+  d.ell = best_ell;
   return best_t;
 }
 
@@ -436,10 +477,21 @@ cublasStatus_t gemm<float>(cublasHandle_t h, int N, double alpha, const float* A
 }
 
 // QAP Qmap! (src/Q_operators/QAP_operator.jl:52-61): X = reshape(x, N, N)
-// column-major; TMP = A X; QX = 2 TMP B - 2 S X - 2 X T.
+// column-major; TMP = A X; QX = 2 TMP B - 2 S X - 2 X T.  FP64: cuBLAS
+// DGEMM (the reference arithmetic); FP32 phase: the 3xTF32 tcgen05 GEMM.
 template <typename V>
 void Engine<V>::qap_apply(const V* xin, V* yout) {
   const int N = (int)std::lround(std::sqrt((double)n));
+  if constexpr (std::is_same<V, float>::value) {
+    if (cm.tc_qap) {
+      gemm_3xtf32(N, 1.0f, qA, xin, 0.0f, qTmp, cm.stream);
+      gemm_3xtf32(N, 2.0f, qTmp, qB, 0.0f, yout, cm.stream);
+      gemm_3xtf32(N, -2.0f, qS, xin, 1.0f, yout, cm.stream);
+      gemm_3xtf32(N, -2.0f, xin, qT, 1.0f, yout, cm.stream);
+      cm.launches += 4;
+      return;
+    }
+  }
   auto ck = [](cublasStatus_t s) {
     if (s != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cuBLAS GEMM failed");
   };
@@ -567,7 +619,7 @@ template <typename V>
 void Engine<V>::pass_info(int k, const char** name, double* bytes, int* tpr) const {
   const double v = sizeof(V), d = 8.0;
   auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
-  auto sched = [](const DCsr<V>& M) { return M.sell ? 0 : M.tpr; };  // 0 = SELL-32
+  auto sched = [](const DCsr<V>& M) { return M.ell ? -1 : M.sell ? 0 : M.tpr; };  // 0 = SELL-32, -1 = ELL
   const double N = (double)n, M_ = (double)m;
   const double dg = Q_is_diag ? 2 * N * v : 0.0;
   *name = "?";

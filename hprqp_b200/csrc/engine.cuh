@@ -71,6 +71,7 @@ struct Common {  // per-handle resources shared by the engines
   unsigned* pow_bar = nullptr;
   int pow_ctas_per_sm = 0;
   bool pow_persistent = true;
+  bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;
   void init();
   ~Common();
@@ -162,6 +163,7 @@ class Engine {
   int autotune(DCsr<V>& d);
   void spmv(const DCsr<V>& M, const V* xin, V* yout, double scale = 1.0);
   void build_sell(const HCsr& h, DCsr<V>& d);
+  void build_ell(const HCsr& h, DCsr<V>& d);
   void qap_apply(const V* xin, V* yout);
 };
 

@@ -57,6 +57,23 @@ struct SellSrc {  // (M x)_row with M in SELL-32, one thread per row
   }
 };
 
+template <typename V, typename X>
+struct EllSrc {  // (M x)_row with M in ELL (width w, column-major), one thread per row
+  const int* __restrict__ col;
+  const V* __restrict__ val;
+  const X* __restrict__ x;
+  int rows, w;
+  template <int TPR, typename Acc>
+  __device__ __forceinline__ Acc dot(int row, int) const {
+    Acc s = Acc(0);
+    const int* c = col + row;
+    const V* v = val + row;
+#pragma unroll 4
+    for (int k = 0; k < w; ++k) s = fma((Acc)__ldg(v + (size_t)k * rows), (Acc)__ldg(x + __ldg(c + (size_t)k * rows)), s);
+    return s;
+  }
+};
+
 template <typename V>
 struct VecSrc {  // precomputed product (operator Q)
   const V* __restrict__ v;

@@ -28,6 +28,7 @@ namespace hprqp {
 
 constexpr int kPowBlock = 512;
 constexpr int kPowMaxGrid = 1024;  // partials buffer capacity (CTAs)
+constexpr int kPowIlp = 4;         // ELL rows per thread in flight
 constexpr unsigned long long kPowBarrierNs = 2000000000ull;  // 2 s per barrier wait
 constexpr unsigned kPowMaxPolls = 1u << 26;
 
@@ -175,6 +176,31 @@ __device__ __forceinline__ void pow_sweep_csr(const DCsr<V>& M, const V* x, long
 
 template <typename Acc, typename V, typename F>
 __device__ __forceinline__ void pow_sweep(const DCsr<V>& M, const V* x, long long gtid, long long gthreads, F& f) {
+  if (M.ell) {
+    // ELL: kPowIlp rows per thread in flight (rows r0 + q * gthreads, so a
+    // warp's loads stay coalesced), no row pointers to wait for
+    const long long rows = M.rows;
+    for (long long r0 = gtid; r0 < rows; r0 += kPowIlp * gthreads) {
+      Acc acc[kPowIlp];
+#pragma unroll
+      for (int q = 0; q < kPowIlp; ++q) acc[q] = Acc(0);
+      for (int k = 0; k < M.ell_w; ++k) {
+        const int* c = M.ecol + (size_t)k * rows;
+        const V* v = M.evalv + (size_t)k * rows;
+#pragma unroll
+        for (int q = 0; q < kPowIlp; ++q) {
+          const long long row = r0 + q * gthreads;
+          if (row < rows) acc[q] = fma((Acc)__ldg(v + row), (Acc)__ldcg(x + __ldg(c + row)), acc[q]);
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < kPowIlp; ++q) {
+        const long long row = r0 + q * gthreads;
+        if (row < rows) f((int)row, acc[q]);
+      }
+    }
+    return;
+  }
   if (M.sell) {
     const PowSellSrc<V> src{M.sptr, M.ptr, M.scol, M.sval, x};
     for (long long row = gtid; row < M.rows; row += gthreads) f((int)row, src.template dot<Acc>((int)row));
@@ -191,7 +217,7 @@ __device__ __forceinline__ void pow_sweep(const DCsr<V>& M, const V* x, long lon
 }
 
 template <typename V>
-__global__ void __launch_bounds__(kPowBlock) k_power_persistent(PowArgs<V> a) {
+__global__ void __launch_bounds__(kPowBlock, 2) k_power_persistent(PowArgs<V> a) {
   const long long gtid = (long long)blockIdx.x * kPowBlock + threadIdx.x;
   const long long gthreads = (long long)gridDim.x * kPowBlock;
   const int G = (int)gridDim.x;

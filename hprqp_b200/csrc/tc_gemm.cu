@@ -1,0 +1,278 @@
+// tc_gemm.cu — 3xTF32 split-precision GEMM on the sm_100a tensor cores
+// (tcgen05.mma kind::tf32, accumulator in TMEM), for the dense products of
+// the QAP operator (src/Q_operators/QAP_operator.jl:52-61) in the FP32
+// phase:  C = alpha * A * B + beta * C, all N x N column-major FP32.
+//
+// Each operand value a is split as a = hi + lo with hi = tf32(a) and
+// lo = tf32(a - hi); A*B is accumulated as Alo*Bhi + Ahi*Blo + Ahi*Bhi in
+// FP32, which recovers FP32-level accuracy from TF32 tensor-core products
+// (the Alo*Blo term is below FP32 resolution).
+//
+// One CTA computes one 128 x 128 tile of C.  K is walked in chunks of 32:
+// the 128 threads load the A and B chunk from global memory, split it, and
+// store it into shared memory in the canonical K-major no-swizzle layout of
+// the UMMA descriptors (8-row x 16-byte core matrices); one thread issues
+// 4 k-steps x 3 MMAs (M = 128, N = 128, K = 8) and commits them to an
+// mbarrier that the CTA waits on before reusing the buffers.  The epilogue
+// reads the accumulator tile from TMEM (warp w owns lanes 32w..32w+31, i.e.
+// rows of C) and writes alpha * acc + beta * C.
+//
+// Every mbarrier wait is bounded; on a timeout the kernel raises the
+// device flag g_tc_err, skips the rest of its work, frees its TMEM and
+// returns; gemm_3xtf32_failed() reads and clears the flag.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+
+#include "common.cuh"
+#include "tc_gemm.h"
+
+namespace hprqp {
+namespace tc {
+
+constexpr int kTile = 128;    // M and N of one CTA tile (one MMA: M = 128, N = 128)
+constexpr int kChunk = 32;    // K elements staged per round
+constexpr int kThreads = 128;
+constexpr int kOpBytes = kTile * kChunk * 4;      // one split half of one operand chunk: 16 KiB
+constexpr int kSmemBytes = 4 * kOpBytes + 1024;   // A hi/lo, B hi/lo, + alignment slack
+constexpr unsigned long long kWaitNs = 1000000000ull;
+
+__device__ int g_tc_err = 0;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint32_t to_tf32(float a) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
+  return r;
+}
+
+// byte offset of element (row r, k) in a K-major no-swizzle chunk of 128 rows
+// x 32 k: core matrix (k/4, r/8) of 8 rows x 16 bytes; K-adjacent core
+// matrices are kLbo apart, row-group-adjacent ones 128 bytes apart.
+constexpr uint32_t kSbo = 128;
+constexpr uint32_t kLbo = (kTile / 8) * 128;  // 2048
+__device__ __forceinline__ uint32_t kmaj_off(int r, int k) {
+  return (uint32_t)((k >> 2) * kLbo + (r >> 3) * kSbo + (r & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((kLbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((kSbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version (sm_100)
+  // base offset 0, LBO mode 0, layout type 0 (no swizzle)
+  return d;
+}
+
+// kind::tf32, D = F32, A = B = TF32, both K-major, M = 128, N = 128
+constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTile >> 3) << 17) |
+                            ((uint32_t)(kTile >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t dtm, uint64_t ad, uint64_t bd, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtm),
+      "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+  const uint32_t a = smem_u32(bar);
+  unsigned long long t0 = 0;
+  for (uint32_t it = 0;; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred P1;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, P1;\n\t}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    if (it == 0) t0 = t;
+    else if (t - t0 > kWaitNs || it > (1u << 26)) return false;
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_gemm_3xtf32(int N, float alpha, const float* __restrict__ A,
+                                                           const float* __restrict__ B, float beta, float* C) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* sAh = sm;
+  unsigned char* sAl = sm + kOpBytes;
+  unsigned char* sBh = sm + 2 * kOpBytes;
+  unsigned char* sBl = sm + 3 * kOpBytes;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int i0 = blockIdx.x * kTile, j0 = blockIdx.y * kTile;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"((uint32_t)kTile));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar)), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tm = tmem_base;
+
+  uint32_t parity = 0;
+  bool first = true;
+  for (int k0 = 0; k0 < N; k0 += kChunk) {
+    // stage A[i0 + r, k0 + k] and B[k0 + k, j0 + c] (zero outside the matrix)
+    for (int e = tid; e < kTile * kChunk; e += kThreads) {
+      // A is column-major: consecutive threads take consecutive rows
+      const int r = e & (kTile - 1), k = e >> 7;
+      const int gi = i0 + r, gk = k0 + k;
+      const float a = (gi < N && gk < N) ? __ldg(A + (size_t)gk * N + gi) : 0.0f;
+      const uint32_t ah = to_tf32(a);
+      const uint32_t al = to_tf32(a - __uint_as_float(ah));
+      const uint32_t off = kmaj_off(r, k);
+      *(uint32_t*)(sAh + off) = ah;
+      *(uint32_t*)(sAl + off) = al;
+    }
+    for (int e = tid; e < kTile * kChunk; e += kThreads) {
+      // B[k, j] with k contiguous in memory: consecutive threads take consecutive k
+      const int k = e & (kChunk - 1), c = e >> 5;
+      const int gk = k0 + k, gj = j0 + c;
+      const float b = (gk < N && gj < N) ? __ldg(B + (size_t)gj * N + gk) : 0.0f;
+      const uint32_t bh = to_tf32(b);
+      const uint32_t bl = to_tf32(b - __uint_as_float(bh));
+      const uint32_t off = kmaj_off(c, k);
+      *(uint32_t*)(sBh + off) = bh;
+      *(uint32_t*)(sBl + off) = bl;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t ah = smem_u32(sAh), al = smem_u32(sAl), bh = smem_u32(sBh), bl = smem_u32(sBl);
+#pragma unroll
+      for (int s = 0; s < kChunk / 8; ++s) {
+        const uint32_t o = (uint32_t)s * 2 * kLbo;  // K = 8 per MMA = two core matrices along K
+        mma_tf32(tm, smem_desc(al + o), smem_desc(bh + o), first ? 0u : 1u);
+        mma_tf32(tm, smem_desc(ah + o), smem_desc(bl + o), 1u);
+        mma_tf32(tm, smem_desc(ah + o), smem_desc(bh + o), 1u);
+        first = false;
+      }
+      mma_commit(&bar);
+    }
+    first = false;
+    if (!mbar_wait(&bar, parity)) s_fail = 1;
+    parity ^= 1u;
+    __syncthreads();
+    if (s_fail) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!s_fail) {
+    // epilogue: thread t of warp w holds row i0 + 32w + lane
+    const int row = i0 + warp * 32 + (tid & 31);
+    const uint32_t lane_base = tm + ((uint32_t)(warp * 32) << 16);
+#pragma unroll 1
+    for (int c0 = 0; c0 < kTile; c0 += 16) {
+      uint32_t v[16];
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+          "%14, %15}, [%16];"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15])
+          : "r"(lane_base + (uint32_t)c0));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      if (row < N) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) {
+          const int col = j0 + c0 + q;
+          if (col < N) {
+            float* p = C + (size_t)col * N + row;
+            const float acc = __uint_as_float(v[q]);
+            *p = beta == 0.0f ? alpha * acc : fmaf(alpha, acc, beta * *p);
+          }
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(&g_tc_err, 1);
+    mbar_wait(&bar, parity ^ 1u);  // give MMAs still in flight a bounded chance to drain
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"((uint32_t)kTile));
+  }
+}
+
+}  // namespace tc
+
+void gemm_3xtf32(int N, float alpha, const float* A, const float* B, float beta, float* C, cudaStream_t st) {
+  // the dynamic shared memory limit is a per-device function attribute
+  static std::mutex mu;
+  static bool ready[64] = {};
+  int dev = 0;
+  HPRQP_CUDA(cudaGetDevice(&dev));
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    if (dev < 0 || dev >= 64) throw Error(-2, "device ordinal out of range");
+    if (!ready[dev]) {
+      HPRQP_CUDA(cudaFuncSetAttribute(tc::k_gemm_3xtf32, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      tc::kSmemBytes));
+      ready[dev] = true;
+    }
+  }
+  if (N <= 0) return;
+  const int t = (N + tc::kTile - 1) / tc::kTile;
+  tc::k_gemm_3xtf32<<<dim3(t, t), tc::kThreads, tc::kSmemBytes, st>>>(N, alpha, A, B, beta, C);
+  HPRQP_LAUNCH_CHECK();
+}
+
+bool gemm_3xtf32_failed(cudaStream_t st) {
+  int v = 0;
+  const int zero = 0;
+  HPRQP_CUDA(cudaMemcpyFromSymbolAsync(&v, tc::g_tc_err, sizeof(int), 0, cudaMemcpyDeviceToHost, st));
+  HPRQP_CUDA(cudaStreamSynchronize(st));
+  if (v) {
+    HPRQP_CUDA(cudaMemcpyToSymbolAsync(tc::g_tc_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st));
+    HPRQP_CUDA(cudaStreamSynchronize(st));
+  }
+  return v != 0;
+}
+
+}  // namespace hprqp
+
+// ---------------------------------------------------------------------------
+// C ABI (include/hprqp.h)
+// ---------------------------------------------------------------------------
+extern "C" int hprqp_gemm_3xtf32(int32_t n, float alpha, const float* A, const float* B, float beta, float* C,
+                                 void* stream) {
+  try {
+    if (n < 0 || (n > 0 && (!A || !B || !C))) return -1;
+    const cudaStream_t st = (cudaStream_t)stream;
+    hprqp::gemm_3xtf32(n, alpha, A, B, beta, C, st);
+    if (hprqp::gemm_3xtf32_failed(st)) return -2;
+    return 0;
+  } catch (const hprqp::Error& e) {
+    std::fprintf(stderr, "hprqp_gemm_3xtf32: %s\n", e.what());
+    return e.code;
+  } catch (...) {
+    return -2;
+  }
+}

@@ -1,0 +1,15 @@
+// tc_gemm.h — 3xTF32 tensor-core GEMM (tc_gemm.cu) for the QAP operator.
+#pragma once
+
+#include <cuda_runtime.h>
+
+namespace hprqp {
+
+// C = alpha * A * B + beta * C, N x N column-major FP32, on `st`.
+void gemm_3xtf32(int N, float alpha, const float* A, const float* B, float beta, float* C, cudaStream_t st);
+
+// True (and the flag cleared) when a launch since the last call gave up a
+// bounded wait; synchronises `st`.
+bool gemm_3xtf32_failed(cudaStream_t st);
+
+}  // namespace hprqp

@@ -27,7 +27,7 @@ def main(argv=None):
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--lam-A", type=float, default=0.44866094653915195)
     ap.add_argument("--lam-Q", type=float, default=0.8051445993716677)
-    ap.add_argument("--tpr", default="0", help="CSR threads per row, 'sell', or 0 = autotune")
+    ap.add_argument("--tpr", default="0", help="CSR threads per row, 'sell', 'ell', or 0 = autotune")
     a = ap.parse_args(argv)
     if a.workload == "grid":
         model, ptype = W.grid_qp(N=a.grid), "QP"
@@ -40,12 +40,12 @@ def main(argv=None):
         p = HPRQP_parameters(verbose=False, precision=a.precision, problem_type=ptype,
                              lambda_max_A_override=a.lam_A, lambda_max_Q_override=a.lam_Q)
         if a.tpr != "0":
-            p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr == "sell" else int(a.tpr)
+            p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr in ("sell", "ell") else int(a.tpr)
         out = s.profile_iterations(p, a.iters)
     else:
         p = HPRQP_parameters(verbose=False, precision=a.precision, problem_type=ptype, profile_passes=True)
         if a.tpr != "0":
-            p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr == "sell" else int(a.tpr)
+            p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr in ("sell", "ell") else int(a.tpr)
         r = s.solve(p)
         out = dict(status=r.status, iter=r.iter, iter_fp32=r.iter_fp32, time=r.time, device_time=r.device_time,
                    power_time=r.power_time, kkt=r.residuals, launches=r.gpu_launches, passes=s.pass_stats())

@@ -121,7 +121,7 @@ typedef struct hprqp_params {
     int32_t warm_up;                 /* 0; accepted, no JIT to warm                 */
     int32_t spmv_mode_Q;             /* 0 = auto (autotuned row schedule); 1..6 =
                                         CSR with 1,2,4,...,32 threads per row;
-                                        7 = SELL-32                                 */
+                                        7 = SELL-32; 8 = ELL (short rows)           */
     int32_t spmv_mode_A;             /* same, for A and A'                          */
     int32_t print_frequency;         /* -1 = adaptive (print_step)                  */
     int32_t device_number;           /* 0                                           */
@@ -254,10 +254,11 @@ int hprqp_get_pass_stats(hprqp_handle h, hprqp_pass_stats* fp64, hprqp_pass_stat
  *  - All calls share the scratch: calls that overlap on the GPU (different
  *    streams, threads or processes on one device) race.  Each call clears
  *    what must start at zero.
- *  - Same start vector, kernels and stopping test (err < tol, at most
+ *  - Same start vector, products and stopping test (err < tol, at most
  *    max_iter steps) as the solver's power method (threads_per_row 1..32
- *    selects the CSR schedule), so lambda matches hprqp_solve's
- *    lambda_max_A / eig_factor for the same matrix and schedule.
+ *    selects the CSR schedule), so lambda agrees with hprqp_solve's
+ *    lambda_max_A / eig_factor for the same matrix to rounding (the solver
+ *    sums its dot products in another order).
  *  - stream: a cudaStream_t (NULL = legacy default stream); the call
  *    returns after the stream has finished the work.  */
 int hprqp_power_lambda_noalloc(int64_t m, int64_t n,
@@ -265,6 +266,15 @@ int hprqp_power_lambda_noalloc(int64_t m, int64_t n,
                                const int32_t* AT_rowptr, const int32_t* AT_colind, const double* AT_val,
                                int32_t threads_per_row, double tol, int32_t max_iter,
                                void* stream, double* lambda_out, int32_t* iters_out);
+
+/* C = alpha * A * B + beta * C for N x N column-major FP32 matrices in
+ * device memory, as a 3xTF32 split-precision GEMM on the tensor cores
+ * (tcgen05, FP32 accumulate): the product kernel of the QAP operator
+ * (src/Q_operators/QAP_operator.jl:52-61) in the FP32 phase, where the
+ * reference calls a cuBLAS GEMM.  Returns after the stream has finished;
+ * HPRQP_E_CUDA if a bounded wait inside the kernel gave up. */
+int hprqp_gemm_3xtf32(int32_t n, float alpha, const float* A, const float* B, float beta, float* C,
+                      void* stream);
 
 /* Text of the last error on this handle ("" if none); valid until the next
  * call on the handle.  h may be NULL for errors from hprqp_create. */

@@ -11,10 +11,13 @@ from hprqp_b200 import _abi, _lib
 from tests.conftest import ROOT, gpu_available
 
 
-def declared_entry_points():
-    src = open(os.path.join(ROOT, "include", "hprqp.h")).read()
+def declared_entry_points(header="hprqp.h"):
+    src = open(os.path.join(ROOT, "include", header)).read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
-    return sorted(set(re.findall(r"\b(hprqp_[a-z_]+)\s*\(", src)))
+    return sorted(set(re.findall(r"\b(hprqp_[a-z0-9_]+)\s*\(", src)))
+
+
+HEADERS = sorted(f for f in os.listdir(os.path.join(ROOT, "include")) if f.endswith(".h"))
 
 
 def test_header_declares_all_bound_exports():
@@ -22,10 +25,13 @@ def test_header_declares_all_bound_exports():
     assert set(_lib.EXPORTS) == set(decl), decl
 
 
-def test_library_exports_every_declared_symbol(lib_built):
+@pytest.mark.parametrize("header", HEADERS)
+def test_library_exports_every_declared_symbol(lib_built, header):
     L = C.CDLL(lib_built)
-    for name in declared_entry_points():
-        assert hasattr(L, name), name
+    names = declared_entry_points(header)
+    assert names, header
+    for name in names:
+        assert hasattr(L, name), (header, name)
 
 
 def test_struct_layouts_match(lib_built):
