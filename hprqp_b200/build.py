@@ -29,7 +29,7 @@ def nvcc():
 
 
 def _flags():
-    return ARCH + ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC",
+    return ARCH + ["-O3", "-lineinfo", "-std=c++17", "--extended-lambda", "-Xcompiler", "-fPIC,-fopenmp",
                    "-I" + os.path.join(ROOT, "include"), "-ccbin", "/usr/bin/g++"]
 
 
@@ -68,7 +68,7 @@ def build(verbose=False, force=False):
             print(o)
     objs = [os.path.join(BUILD, s + ".o") for s in SOURCES]
     if jobs or not os.path.exists(LIB):
-        run([cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcublas", "-ccbin", "/usr/bin/g++"])
+        run([cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcublas", "-lgomp", "-ccbin", "/usr/bin/g++"])
     return LIB
 
 

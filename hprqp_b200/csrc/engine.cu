@@ -44,6 +44,8 @@ void Common::init() {
   pow_persistent = !(pe && pe[0] == '0');
   const char* tq = std::getenv("HPRQP_QAP_TC");
   tc_qap = !(tq && tq[0] == '0');
+  const char* pel = std::getenv("HPRQP_POWER_ELL");
+  pow_prefer_ell = !(pel && pel[0] == '0');
   const char* pc = std::getenv("HPRQP_POWER_CTAS_PER_SM");
   if (pc) pow_ctas_per_sm = std::atoi(pc);
 }
@@ -877,11 +879,21 @@ bool Engine<V>::power_persistent(bool onA, bool onQ, double tol, int max_it, dou
   const int grid = std::min(per * cm.num_sms, kPowMaxGrid);
   if (grid < 1) return false;
   PowArgs<V> pa{};
+  // the persistent sweeps keep kPowIlp rows in flight only on ELL: use it
+  // wherever the matrix has an ELL copy
+  auto pick = [&](const DCsr<V>& M) {
+    DCsr<V> d = M;
+    if (cm.pow_prefer_ell && d.ell_w > 0) {
+      d.ell = true;
+      d.sell = false;
+    }
+    return d;
+  };
   if (onA) {
     PowChain<V>& c = pa.ch[0];
     c.kind = 2;
-    c.M1 = AT;
-    c.M2 = A;
+    c.M1 = pick(AT);
+    c.M2 = pick(A);
     c.z0 = pz;
     c.z1 = pq;
     c.t = pt;
@@ -891,12 +903,12 @@ bool Engine<V>::power_persistent(bool onA, bool onQ, double tol, int max_it, dou
     PowChain<V>& c = pa.ch[1];
     if (is_lasso) {
       c.kind = 2;
-      c.M1 = L;
-      c.M2 = LT;
+      c.M1 = pick(L);
+      c.M2 = pick(LT);
       c.t = ltemp2;
     } else {
       c.kind = 1;
-      c.M1 = Q;
+      c.M1 = pick(Q);
     }
     c.z0 = pz2;
     c.z1 = pq2;

@@ -71,6 +71,7 @@ struct Common {  // per-handle resources shared by the engines
   unsigned* pow_bar = nullptr;
   int pow_ctas_per_sm = 0;
   bool pow_persistent = true;
+  bool pow_prefer_ell = true;
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;
   void init();

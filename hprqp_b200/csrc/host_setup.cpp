@@ -47,6 +47,34 @@ HCsr csc_to_csr(int64_t rows, int64_t cols, const int32_t* cp, const int32_t* rv
   return M;
 }
 
+// The caller's CSC of M (rows x cols) read directly as the CSR of M'
+// (cols x rows): the column pointers are the row pointers.  Returns false
+// (and leaves T empty) when some column's row indices are not strictly
+// increasing, in which case the caller transposes the CSR instead.
+bool csc_as_transpose(int64_t rows, int64_t cols, const int32_t* cp, const int32_t* rv, const double* nz, int base,
+                      HCsr& T) {
+  const int64_t nnz = (int64_t)cp[cols] - base;
+  bool sorted = true;
+#pragma omp parallel for schedule(static) reduction(&& : sorted)
+  for (int64_t j = 0; j < cols; ++j)
+    for (int64_t k = cp[j] - base + 1; k < cp[j + 1] - base; ++k)
+      if (rv[k] <= rv[k - 1]) sorted = false;
+  if (!sorted) return false;
+  T.rows = cols;
+  T.cols = rows;
+  T.ptr.resize(cols + 1);
+  T.col.resize(nnz);
+  T.val.resize(nnz);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j <= cols; ++j) T.ptr[j] = cp[j] - base;
+#pragma omp parallel for schedule(static)
+  for (int64_t k = 0; k < nnz; ++k) {
+    T.col[k] = rv[k] - base;
+    T.val[k] = nz[k];
+  }
+  return true;
+}
+
 std::vector<double> copy_vec(const double* p, int64_t len, const char* what, bool allow_inf) {
   if (len > 0 && !p) throw Error(HPRQP_E_ARG, std::string(what) + ": null pointer");
   std::vector<double> v(p, p + len);
@@ -79,14 +107,61 @@ double norminf(const std::vector<double>& v) {
 }
 
 // ((1/dr_i) * m_ij) * (1/dc_j): the entry order of DR * M * DC
+// M <- diag(1/dr) M diag(1/dc), computed as ((1/dr_i) * v) * (1/dc_j);
+// the reciprocals are formed once per call (the same values).
+std::vector<double> recip(const std::vector<double>& d) {
+  std::vector<double> r(d.size());
+  for (size_t i = 0; i < d.size(); ++i) r[i] = 1.0 / d[i];
+  return r;
+}
+
 void scale_rows_cols(HCsr& M, const std::vector<double>* dr, const std::vector<double>* dc) {
+  const std::vector<double> ir = dr ? recip(*dr) : std::vector<double>(), ic = dc ? recip(*dc) : std::vector<double>();
+#pragma omp parallel for schedule(static)
   for (int64_t i = 0; i < M.rows; ++i)
     for (int k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
       double v = M.val[k];
-      if (dr) v = (1.0 / (*dr)[i]) * v;
-      if (dc) v = v * (1.0 / (*dc)[M.col[k]]);
+      if (dr) v = ir[i] * v;
+      if (dc) v = v * ic[M.col[k]];
       M.val[k] = v;
     }
+}
+
+// The same update on the transpose T = M' (entry (j, i) holds M(i, j)):
+// identical arithmetic in identical order, so T stays bitwise M'.
+void scale_rows_cols_T(HCsr& T, const std::vector<double>* dr, const std::vector<double>* dc) {
+  const std::vector<double> ir = dr ? recip(*dr) : std::vector<double>(), ic = dc ? recip(*dc) : std::vector<double>();
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < T.rows; ++j)
+    for (int k = T.ptr[j]; k < T.ptr[j + 1]; ++k) {
+      double v = T.val[k];
+      if (dr) v = ir[T.col[k]] * v;
+      if (dc) v = v * ic[j];
+      T.val[k] = v;
+    }
+}
+
+// row-wise max |v| (or sum |v|) of M, in stored order
+std::vector<double> row_absmax(const HCsr& M) {
+  std::vector<double> r(M.rows, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < M.rows; ++i) {
+    double x = 0.0;
+    for (int k = M.ptr[i]; k < M.ptr[i + 1]; ++k) x = std::max(x, std::fabs(M.val[k]));
+    r[i] = x;
+  }
+  return r;
+}
+
+std::vector<double> row_abssum(const HCsr& M) {
+  std::vector<double> r(M.rows, 0.0);
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < M.rows; ++i) {
+    double x = 0.0;
+    for (int k = M.ptr[i]; k < M.ptr[i + 1]; ++k) x += std::fabs(M.val[k]);
+    r[i] = x;
+  }
+  return r;
 }
 }  // namespace
 
@@ -144,10 +219,14 @@ void load_problem(const hprqp_problem* pr, HostProblem& hp) {
   h.Q_kind = pr->Q_kind;
   if (h.m > 0) {
     h.A = csc_to_csr(h.m, h.n, pr->A_colptr, pr->A_rowval, pr->A_nzval, base, "A matrix");
+    if (!csc_as_transpose(h.m, h.n, pr->A_colptr, pr->A_rowval, pr->A_nzval, base, h.AT)) h.AT = transpose(h.A);
   } else {
     h.A.rows = 0;
     h.A.cols = h.n;
     h.A.ptr.assign(1, 0);
+    h.AT.rows = h.n;
+    h.AT.cols = 0;
+    h.AT.ptr.assign(h.n + 1, 0);
   }
   h.c = copy_vec(pr->c, h.n, "c vector", false);
   h.AL = copy_vec(pr->AL, h.m, "Constraint bounds AL", true);
@@ -161,8 +240,14 @@ void load_problem(const hprqp_problem* pr, HostProblem& hp) {
   h.obj_constant = pr->obj_constant;
   h.lambda = pr->lambda;
   if (h.Q_kind == HPRQP_Q_SPARSE) {
-    if (pr->Q_colptr) h.Q = csc_to_csr(h.n, h.n, pr->Q_colptr, pr->Q_rowval, pr->Q_nzval, base, "Q matrix");
-    else { h.Q.rows = h.Q.cols = h.n; h.Q.ptr.assign(h.n + 1, 0); }
+    if (pr->Q_colptr) {
+      h.Q = csc_to_csr(h.n, h.n, pr->Q_colptr, pr->Q_rowval, pr->Q_nzval, base, "Q matrix");
+      if (!csc_as_transpose(h.n, h.n, pr->Q_colptr, pr->Q_rowval, pr->Q_nzval, base, h.QT)) h.QT = transpose(h.Q);
+    } else {
+      h.Q.rows = h.Q.cols = h.n;
+      h.Q.ptr.assign(h.n + 1, 0);
+      h.QT = h.Q;
+    }
   } else if (h.Q_kind == HPRQP_Q_LASSO) {
     if (pr->lasso_m <= 0 || pr->lasso_m > INT32_MAX) throw Error(HPRQP_E_ARG, "LASSO: bad lasso_m");
     h.L = csc_to_csr(pr->lasso_m, h.n, pr->L_colptr, pr->L_rowval, pr->L_nzval, base, "LASSO data matrix");
@@ -198,78 +283,65 @@ void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& o) 
   o.norm_c_org = norminf(o.c);
   if (hp.Q_kind != HPRQP_Q_SPARSE) {
     // Operator Q: no scaling at all (src/utils.jl:364-406)
-    o.AT = transpose(o.A);
+    o.AT = hp.AT;
     o.norm_b = m > 0 ? norm_b_of(o.AL, o.AU, false) : 0.0;
     o.norm_c = norm2(o.c);
     o.diag_Q.assign(n, 0.0);
     o.Q_is_diag = false;
   } else {
     o.Q = hp.Q;
+    o.AT = hp.AT;
     HCsr& A = o.A;
+    HCsr& AT = o.AT;
     HCsr& Q = o.Q;
+    HCsr QT = hp.QT;
     std::vector<double> tr(m, 1.0), tc(n, 1.0);
     auto apply = [&]() {
       for (int64_t i = 0; i < m; ++i) o.row_norm[i] *= tr[i];
       for (int64_t j = 0; j < n; ++j) o.col_norm[j] *= tc[j];
       scale_rows_cols(Q, &tc, &tc);
-      if (m > 0) scale_rows_cols(A, &tr, &tc);
+      scale_rows_cols_T(QT, &tc, &tc);
+      if (m > 0) {
+        scale_rows_cols(A, &tr, &tc);
+        scale_rows_cols_T(AT, &tr, &tc);
+      }
       for (int64_t j = 0; j < n; ++j) o.c[j] /= tc[j];
       for (int64_t i = 0; i < m; ++i) { o.AL[i] /= tr[i]; o.AU[i] /= tr[i]; }
       for (int64_t j = 0; j < n; ++j) { o.l[j] *= tc[j]; o.u[j] *= tc[j]; }
     };
     if (p.use_Ruiz_scaling) {
       for (int pass = 0; pass < 10; ++pass) {
-        std::vector<double> ca(n, 0.0), cq(n, 0.0);
-        for (int64_t i = 0; i < A.rows; ++i)
-          for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) ca[A.col[k]] = std::max(ca[A.col[k]], std::fabs(A.val[k]));
-        for (int64_t i = 0; i < Q.rows; ++i)
-          for (int k = Q.ptr[i]; k < Q.ptr[i + 1]; ++k) cq[Q.col[k]] = std::max(cq[Q.col[k]], std::fabs(Q.val[k]));
+        // column maxima of A and Q = row maxima of A' and Q'
+        const std::vector<double> ca = row_absmax(AT), cq = row_absmax(QT), ra = row_absmax(A);
         for (int64_t j = 0; j < n; ++j) {
           tc[j] = std::sqrt(std::max(ca[j], cq[j]));
           if (tc[j] == 0.0) tc[j] = 1.0;
         }
         for (int64_t i = 0; i < m; ++i) {
-          double r = 0.0;
-          for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) r = std::max(r, std::fabs(A.val[k]));
-          tr[i] = std::sqrt(r);
+          tr[i] = std::sqrt(ra[i]);
           if (tr[i] == 0.0) tr[i] = 1.0;
         }
         apply();
       }
     }
     if (p.use_Pock_Chambolle_scaling) {
-      std::vector<double> ca(n, 0.0), cq(n, 0.0);
-      HCsr AT = transpose(A), QT = transpose(Q);
-      for (int64_t j = 0; j < n; ++j) {
-        double s = 0.0;
-        for (int k = AT.ptr[j]; k < AT.ptr[j + 1]; ++k) s += std::fabs(AT.val[k]);
-        ca[j] = s;
-        s = 0.0;
-        for (int k = QT.ptr[j]; k < QT.ptr[j + 1]; ++k) s += std::fabs(QT.val[k]);
-        cq[j] = s;
-      }
+      // column abs-sums in increasing row order = row sums of the transposes
+      const std::vector<double> ca = row_abssum(AT), cq = row_abssum(QT), ra = row_abssum(A);
       for (int64_t j = 0; j < n; ++j) {
         tc[j] = std::sqrt(ca[j] + cq[j]);
         if (tc[j] == 0.0) tc[j] = 1.0;
       }
       for (int64_t i = 0; i < m; ++i) {
-        double r = 0.0;
-        for (int k = A.ptr[i]; k < A.ptr[i + 1]; ++k) r += std::fabs(A.val[k]);
-        tr[i] = std::sqrt(r);
+        tr[i] = std::sqrt(ra[i]);
         if (tr[i] == 0.0) tr[i] = 1.0;
       }
       apply();
     }
-    o.AT = transpose(A);
-    // Q = (Q + Q') / 2 (src/utils.jl:771-780)
+    // Q = (Q + Q') / 2 (src/utils.jl:771-780): row-wise merge, counted first
     {
-      HCsr QT = transpose(Q), S;
-      S.rows = S.cols = n;
-      S.ptr.assign(n + 1, 0);
-      S.col.reserve(Q.nnz());
-      S.val.reserve(Q.nnz());
-      for (int64_t i = 0; i < n; ++i) {
-        int a = Q.ptr[i], b = QT.ptr[i];
+      std::vector<int> len(n, 0);
+      auto merge = [&](int64_t i, int* cols, double* vals) {
+        int a = Q.ptr[i], b = QT.ptr[i], cnt = 0;
         const int ae = Q.ptr[i + 1], be = QT.ptr[i + 1];
         while (a < ae || b < be) {
           const int ca = a < ae ? Q.col[a] : INT32_MAX;
@@ -279,11 +351,24 @@ void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& o) 
           if (ca == cb) { v = Q.val[a++] + QT.val[b++]; cc = ca; }
           else if (ca < cb) { v = Q.val[a++]; cc = ca; }
           else { v = QT.val[b++]; cc = cb; }
-          S.col.push_back(cc);
-          S.val.push_back(v / 2.0);
+          if (cols) {
+            cols[cnt] = cc;
+            vals[cnt] = v / 2.0;
+          }
+          ++cnt;
         }
-        S.ptr[i + 1] = (int)S.col.size();
-      }
+        return cnt;
+      };
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; ++i) len[i] = merge(i, nullptr, nullptr);
+      HCsr S;
+      S.rows = S.cols = n;
+      S.ptr.assign(n + 1, 0);
+      for (int64_t i = 0; i < n; ++i) S.ptr[i + 1] = S.ptr[i] + len[i];
+      S.col.resize(S.ptr[n]);
+      S.val.resize(S.ptr[n]);
+#pragma omp parallel for schedule(static)
+      for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], S.val.data() + S.ptr[i]);
       Q = std::move(S);
     }
     o.norm_b = norm_b_of(o.AL, o.AU, false);

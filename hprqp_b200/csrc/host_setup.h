@@ -5,7 +5,10 @@
 // (src/utils.jl:350-804, CPU branch): 10 Ruiz passes on [Q; A], one
 // Pock-Chambolle pass, b/c scaling disabled, Q symmetrised afterwards, and
 // check_Q_diagonal (src/utils.jl:827-855).  It runs on the host once per
-// prepare; the scaled arrays are then uploaded to HBM.
+// prepare, row-parallel (OpenMP): A and A', Q and Q' are scaled side by
+// side with the same arithmetic, so column maxima and sums are row sweeps
+// of the transposes and every result is bitwise the sequential one.  The
+// scaled arrays are then uploaded to HBM.
 #pragma once
 
 #include <stdint.h>
@@ -27,7 +30,9 @@ struct HCsr {
 struct HostProblem {  // the loaded, unscaled problem
   int64_t n = 0, m = 0;
   int Q_kind = HPRQP_Q_SPARSE;
-  HCsr A;  // m x n
+  HCsr A;   // m x n
+  HCsr AT;  // n x m: the caller's CSC of A read as CSR of A'
+  HCsr QT;  // n x n: the caller's CSC of Q read as CSR of Q' (sparse kind)
   std::vector<double> c, AL, AU, l, u;
   double obj_constant = 0.0, lambda = 0.0;
   HCsr Q;  // n x n (sparse kind)

@@ -8,6 +8,10 @@
                    injected (--lam-A/--lam-Q, defaults for the 700x700 grid from
                    the oracle) so no power-method launches precede the passes.
 --mode solve:      one full solve to 1e-6 (power method included).
+--mode gemm:       the 3xTF32 tensor-core GEMM of the FP32 QAP operator on
+                   --n x --n FP32 matrices (--iters timed launches after 3
+                   warm-up launches); reports time and TFLOP/s (2 n^3 per
+                   product; the tensor pipe executes 3x that).
 Prints one JSON line with the per-pass CUDA-event times.
 """
 import argparse
@@ -23,12 +27,16 @@ def main(argv=None):
     ap.add_argument("--grid", type=int, default=700)
     ap.add_argument("--workload", default="grid", choices=["grid", "random_qp", "lasso"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_polish"])
-    ap.add_argument("--mode", default="iterations", choices=["iterations", "solve"])
+    ap.add_argument("--mode", default="iterations", choices=["iterations", "solve", "gemm"])
+    ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--lam-A", type=float, default=0.44866094653915195)
     ap.add_argument("--lam-Q", type=float, default=0.8051445993716677)
     ap.add_argument("--tpr", default="0", help="CSR threads per row, 'sell', 'ell', or 0 = autotune")
     a = ap.parse_args(argv)
+    if a.mode == "gemm":
+        print(json.dumps(_gemm(a.n, a.iters)))
+        return 0
     if a.workload == "grid":
         model, ptype = W.grid_qp(N=a.grid), "QP"
     elif a.workload == "random_qp":
@@ -52,6 +60,33 @@ def main(argv=None):
     s.close()
     print(json.dumps(out))
     return 0
+
+
+def _gemm(n, iters):
+    import ctypes as C
+
+    import torch
+
+    from ._lib import load
+    L = load()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A, B, Cm = (torch.randn(n * n, device="cuda", generator=g) for _ in range(3))
+    st = torch.cuda.current_stream()
+    call = lambda: L.hprqp_gemm_3xtf32(n, C.c_float(1.0), A.data_ptr(), B.data_ptr(), C.c_float(0.0),
+                                       Cm.data_ptr(), C.c_void_p(st.cuda_stream))
+    for _ in range(3):
+        assert call() == 0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ms = []
+    for _ in range(iters):
+        e0.record(st)
+        assert call() == 0
+        e1.record(st)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    ms.sort()
+    t = ms[len(ms) // 2] / 1e3
+    return dict(n=n, ms=t * 1e3, tflops=2.0 * n ** 3 / t / 1e12, tensor_tflops=6.0 * n ** 3 / t / 1e12)
 
 
 if __name__ == "__main__":
