@@ -20,10 +20,13 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <memory>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/hprqp.h"
@@ -335,8 +338,16 @@ struct BEngine {
     V* v = mem.alloc<V>(d.nnz);
     HPRQP_CUDA(cudaMemcpy(p, h.ptr.data(), sizeof(int) * (h.rows + 1), cudaMemcpyHostToDevice));
     if (d.nnz) HPRQP_CUDA(cudaMemcpy(cc, h.col.data(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice));
-    std::vector<V> vv(h.val.begin(), h.val.end());
-    if (d.nnz) HPRQP_CUDA(cudaMemcpy(v, vv.data(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
+    if (d.nnz) {
+      if constexpr (std::is_same<V, double>::value) {
+        HPRQP_CUDA(cudaMemcpy(v, h.val.data(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
+      } else {
+        std::vector<V> vv(d.nnz);
+#pragma omp parallel for schedule(static)
+        for (int64_t q = 0; q < d.nnz; ++q) vv[q] = (V)h.val[q];
+        HPRQP_CUDA(cudaMemcpy(v, vv.data(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
+      }
+    }
     d.ptr = p;
     d.col = cc;
     d.val = v;
@@ -610,16 +621,32 @@ static void build_family(int count, const hprqp_problem* probs, Family& F) {
   F.B = count;
   F.noff.assign(count + 1, 0);
   F.roff.assign(count + 1, 0);
-  std::vector<HCsr> Ls(count);
+  for (int k = 0; k < count; ++k)
+    if (probs[k].Q_kind != HPRQP_Q_LASSO || probs[k].m != 0)
+      throw Error(HPRQP_E_ARG, "batch: every instance must be a LASSO problem (m = 0)");
+  // per-instance intake and transpose, in parallel (instances are independent)
+  std::vector<HostProblem> hps(count);
+  std::vector<HCsr> LTs(count);
+  std::vector<int> codes(count, 0);
+  std::vector<std::string> errs(count);
+#pragma omp parallel for schedule(dynamic, 1)
   for (int k = 0; k < count; ++k) {
-    const hprqp_problem& p = probs[k];
-    if (p.Q_kind != HPRQP_Q_LASSO || p.m != 0) throw Error(HPRQP_E_ARG, "batch: every instance must be a LASSO problem (m = 0)");
-    HostProblem hp;
-    load_problem(&p, hp);
-    Ls[k] = std::move(hp.L);
+    try {
+      load_problem(&probs[k], hps[k]);
+      LTs[k] = transpose(hps[k].L);
+    } catch (const Error& e) {
+      codes[k] = e.code;
+      errs[k] = e.what();
+    }
+  }
+  for (int k = 0; k < count; ++k)
+    if (codes[k]) throw Error(codes[k], "batch instance " + std::to_string(k) + ": " + errs[k]);
+  std::vector<int64_t> zoff(count + 1, 0);  // nonzero offsets
+  for (int k = 0; k < count; ++k) {
+    const HostProblem& hp = hps[k];
     F.noff[k + 1] = F.noff[k] + hp.n;
-    F.roff[k + 1] = F.roff[k] + Ls[k].rows;
-    F.c.insert(F.c.end(), hp.c.begin(), hp.c.end());
+    F.roff[k + 1] = F.roff[k] + hp.L.rows;
+    zoff[k + 1] = zoff[k] + hp.L.nnz();
     F.lam.push_back(hp.lambda);
     F.obj_constant.push_back(hp.obj_constant);
     double nc = 0;
@@ -628,23 +655,36 @@ static void build_family(int count, const hprqp_problem* probs, Family& F) {
   }
   F.N = F.noff[count];
   F.R = F.roff[count];
-  if (F.N > INT32_MAX || F.R > INT32_MAX) throw Error(HPRQP_E_ARG, "batch too large");
+  if (F.N > INT32_MAX || F.R > INT32_MAX || zoff[count] > INT32_MAX) throw Error(HPRQP_E_ARG, "batch too large");
+  F.c.resize(F.N);
   HCsr& L = F.L;
-  L.rows = F.R;
-  L.cols = F.N;
+  HCsr& LT = F.LT;
+  L.rows = LT.cols = F.R;
+  L.cols = LT.rows = F.N;
   L.ptr.assign(F.R + 1, 0);
+  LT.ptr.assign(F.N + 1, 0);
+  L.col.resize(zoff[count]);
+  L.val.resize(zoff[count]);
+  LT.col.resize(zoff[count]);
+  LT.val.resize(zoff[count]);
+  // block-diagonal concatenation: block k shifted by (roff[k], noff[k])
+#pragma omp parallel for schedule(dynamic, 1)
   for (int k = 0; k < count; ++k) {
-    const HCsr& Lk = Ls[k];
-    for (int64_t r = 0; r < Lk.rows; ++r) {
-      for (int q = Lk.ptr[r]; q < Lk.ptr[r + 1]; ++q) {
-        L.col.push_back((int)(Lk.col[q] + F.noff[k]));
-        L.val.push_back(Lk.val[q]);
-      }
-      L.ptr[F.roff[k] + r + 1] = (int)L.col.size();
+    const HCsr& Lk = hps[k].L;
+    const HCsr& Tk = LTs[k];
+    const int64_t z = zoff[k];
+    for (int64_t r = 0; r < Lk.rows; ++r) L.ptr[F.roff[k] + r + 1] = (int)(z + Lk.ptr[r + 1]);
+    for (int64_t q = 0; q < Lk.nnz(); ++q) {
+      L.col[z + q] = (int)(Lk.col[q] + F.noff[k]);
+      L.val[z + q] = Lk.val[q];
     }
+    for (int64_t r = 0; r < Tk.rows; ++r) LT.ptr[F.noff[k] + r + 1] = (int)(z + Tk.ptr[r + 1]);
+    for (int64_t q = 0; q < Tk.nnz(); ++q) {
+      LT.col[z + q] = (int)(Tk.col[q] + F.roff[k]);
+      LT.val[z + q] = Tk.val[q];
+    }
+    std::copy(hps[k].c.begin(), hps[k].c.end(), F.c.begin() + F.noff[k]);
   }
-  if ((int64_t)L.col.size() > INT32_MAX) throw Error(HPRQP_E_ARG, "batch too large");
-  F.LT = transpose(L);
 }
 
 template <typename V>
@@ -694,8 +734,10 @@ static void solve(Handle& H, const hprqp_params& p, const double* const* x0s, co
   const Family& F = H.F;
   const int B = F.B;
   const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
+  const double tc0 = now_s();
   if (!H.e64) H.e64 = std::make_unique<BEngine<double>>(F, H.st);
   if (fp32 && !H.e32) H.e32 = std::make_unique<BEngine<float>>(F, H.st);
+  const double t_engines = now_s() - tc0;
   BEngine<double>& E64 = *H.e64;
   const double t0 = now_s();
   // lambda_max(Q_k) per instance
@@ -927,6 +969,10 @@ static void solve(Handle& H, const hprqp_params& p, const double* const* x0s, co
   }
   HPRQP_CUDA(cudaStreamSynchronize(H.st));
   const double t_all = now_s() - t0;
+  if (const char* tv = std::getenv("HPRQP_TIMING"))
+    if (tv[0] == '1')
+      std::fprintf(stderr, "batch solve: engines %.3f s, power %.3f s, loop %.3f s\n", t_engines, power_time,
+                   t_all - power_time);
   launches = E64.launches + (H.e32 ? H.e32->launches : 0);
   // collect_results! (operator Q: x = x_bar)
   std::vector<double> x64(F.N), x32(fp32 ? F.N : 0);
@@ -1013,7 +1059,10 @@ int hprqp_batch_load_lasso(hprqp_batch_handle h, int32_t count, const hprqp_prob
   BATCH_GUARD(h, {
     h->e64.reset();
     h->e32.reset();
+    const double t = hprqp::batch::now_s();
     hprqp::batch::build_family(count, problems, h->F);
+    if (const char* tv = std::getenv("HPRQP_TIMING"))
+      if (tv[0] == '1') std::fprintf(stderr, "batch load: %.3f s\n", hprqp::batch::now_s() - t);
   })
 }
 

@@ -27,10 +27,10 @@ void Common::init() {
   d_scal = mem.alloc<double>(kNumSlots);
   HPRQP_CUDA(cudaMemset(d_scal, 0, sizeof(double) * kNumSlots));
   HPRQP_CUDA(cudaMallocHost(&h_scal, sizeof(double) * kNumSlots));
-  rws.partials = mem.alloc<double>((int64_t)kMaxReduceGrid * 16);
+  rws.partials = mem.alloc<double>((int64_t)kReduceGridLimit * 16);
   rws.counter = mem.alloc<unsigned>(4);
   HPRQP_CUDA(cudaMemset(rws.counter, 0, sizeof(unsigned) * 4));
-  rws2.partials = mem.alloc<double>((int64_t)kMaxReduceGrid * 16);
+  rws2.partials = mem.alloc<double>((int64_t)kReduceGridLimit * 16);
   rws2.counter = mem.alloc<unsigned>(4);
   HPRQP_CUDA(cudaMemset(rws2.counter, 0, sizeof(unsigned) * 4));
   int dev = 0;
@@ -41,9 +41,11 @@ void Common::init() {
   pow_part = mem.alloc<double>(2 * 2 * kPowMaxGrid * 3);
   pow_bar = mem.alloc<unsigned>(4);
   const char* pe = std::getenv("HPRQP_POWER_PERSISTENT");
-  pow_persistent = !(pe && pe[0] == '0');
+  pow_persistent = pe && pe[0] == '1';
   const char* tq = std::getenv("HPRQP_QAP_TC");
   tc_qap = !(tq && tq[0] == '0');
+  const char* rc = std::getenv("HPRQP_REDUCE_CAP");
+  if (rc) reduce_cap = std::max(1, std::min(std::atoi(rc), kReduceGridLimit));
   const char* pel = std::getenv("HPRQP_POWER_ELL");
   pow_prefer_ell = !(pel && pel[0] == '0');
   const char* pc = std::getenv("HPRQP_POWER_CTAS_PER_SM");
@@ -105,7 +107,7 @@ static void rows(Common& cm, int tpr, int64_t nrows, const Src& src, const Epi& 
 
 template <int TPR, int K, unsigned MM, typename Acc, typename Src, typename Epi, typename Fin>
 static void reduce_t(Common& cm, int nrows, const Src& src, const Epi& epi, double* out, const Fin& fin) {
-  const int grid = reduce_grid(nrows, TPR);
+  const int grid = reduce_grid(nrows, TPR, cm.reduce_cap);
   launch(cm, k_row_reduce<TPR, K, MM, Acc, Src, Epi, Fin>, grid, kBlock, nrows, src, epi, cm.rws, out, fin);
 }
 

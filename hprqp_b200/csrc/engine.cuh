@@ -70,7 +70,10 @@ struct Common {  // per-handle resources shared by the engines
   double* pow_part = nullptr;
   unsigned* pow_bar = nullptr;
   int pow_ctas_per_sm = 0;
-  bool pow_persistent = true;
+  // the graph-captured chains measured faster than the persistent kernel on
+  // the 700x700 grid (99 vs 112 ms); HPRQP_POWER_PERSISTENT=1 selects it
+  bool pow_persistent = false;
+  int reduce_cap = kMaxReduceGrid;  // CTAs of a grid-stride reduction (HPRQP_REDUCE_CAP)
   bool pow_prefer_ell = true;
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;

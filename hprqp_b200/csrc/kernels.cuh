@@ -133,14 +133,15 @@ __device__ __forceinline__ void block_reduce(double (&r)[K]) {
   __syncthreads();
 }
 
-constexpr int kMaxReduceGrid = 1184;  // reduction grids: at most 8 CTAs per SM on 148 SMs
+constexpr int kMaxReduceGrid = 1184;   // default cap of reduction grids: 8 CTAs per SM on 148 SMs
+constexpr int kReduceGridLimit = 8192;  // largest cap the engine's partials buffers hold
 
 // Grid of a grid-stride reduction: the fewest CTAs (<= kMaxReduceGrid) that
 // give every thread the same number of row groups, so the last sweep is not
 // left to a fraction of the threads.
-inline int reduce_grid(long long nrows, int tpr) {
+inline int reduce_grid(long long nrows, int tpr, int max_grid = kMaxReduceGrid) {
   const long long threads = (nrows > 0 ? nrows : 1) * tpr;
-  const long long cap = (long long)kMaxReduceGrid * kBlock;
+  const long long cap = (long long)max_grid * kBlock;
   const long long per = (threads + cap - 1) / cap;           // row groups per thread
   const long long grid = (threads + (long long)kBlock * per - 1) / ((long long)kBlock * per);
   return (int)(grid < 1 ? 1 : grid);
