@@ -80,6 +80,7 @@ class PassStats(C.Structure):
         ("bytes_per_launch", C.c_double * MAX_PASSES),
         ("threads_per_row", C.c_int32 * MAX_PASSES),
         ("ms_per_iter", C.c_double), ("bytes_per_iter", C.c_double), ("iters", C.c_int64),
+        ("ms_back_to_back", C.c_double * MAX_PASSES),
     ]
 
 

@@ -130,7 +130,8 @@ def _stats_dict(st):
     passes = []
     for k in range(st.npass):
         passes.append(dict(name=st.name[k].value.decode(), ms=st.ms_per_launch[k],
-                           bytes=st.bytes_per_launch[k], threads_per_row=st.threads_per_row[k]))
+                           bytes=st.bytes_per_launch[k], threads_per_row=st.threads_per_row[k],
+                           ms_back_to_back=st.ms_back_to_back[k]))
     return dict(path=st.path, iters=st.iters, ms_per_iter=st.ms_per_iter, bytes_per_iter=st.bytes_per_iter,
                 passes=passes)
 

@@ -343,7 +343,7 @@ struct BEngine {
         HPRQP_CUDA(cudaMemcpy(v, h.val.data(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
       } else {
         std::vector<V> vv(d.nnz);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(d.nnz))
         for (int64_t q = 0; q < d.nnz; ++q) vv[q] = (V)h.val[q];
         HPRQP_CUDA(cudaMemcpy(v, vv.data(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
       }
@@ -629,7 +629,7 @@ static void build_family(int count, const hprqp_problem* probs, Family& F) {
   std::vector<HCsr> LTs(count);
   std::vector<int> codes(count, 0);
   std::vector<std::string> errs(count);
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(host_threads((int64_t)count * 4096))
   for (int k = 0; k < count; ++k) {
     try {
       load_problem(&probs[k], hps[k]);
@@ -668,7 +668,7 @@ static void build_family(int count, const hprqp_problem* probs, Family& F) {
   LT.col.resize(zoff[count]);
   LT.val.resize(zoff[count]);
   // block-diagonal concatenation: block k shifted by (roff[k], noff[k])
-#pragma omp parallel for schedule(dynamic, 1)
+#pragma omp parallel for schedule(dynamic, 1) num_threads(host_threads(zoff[count]))
   for (int k = 0; k < count; ++k) {
     const HCsr& Lk = hps[k].L;
     const HCsr& Tk = LTs[k];

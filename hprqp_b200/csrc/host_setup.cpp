@@ -6,6 +6,8 @@
 #include <cstring>
 #include <limits>
 
+#include <omp.h>
+
 #include "common.cuh"
 
 namespace hprqp {
@@ -55,7 +57,7 @@ bool csc_as_transpose(int64_t rows, int64_t cols, const int32_t* cp, const int32
                       HCsr& T) {
   const int64_t nnz = (int64_t)cp[cols] - base;
   bool sorted = true;
-#pragma omp parallel for schedule(static) reduction(&& : sorted)
+#pragma omp parallel for schedule(static) reduction(&& : sorted) num_threads(host_threads(cols))
   for (int64_t j = 0; j < cols; ++j)
     for (int64_t k = cp[j] - base + 1; k < cp[j + 1] - base; ++k)
       if (rv[k] <= rv[k - 1]) sorted = false;
@@ -65,9 +67,9 @@ bool csc_as_transpose(int64_t rows, int64_t cols, const int32_t* cp, const int32
   T.ptr.resize(cols + 1);
   T.col.resize(nnz);
   T.val.resize(nnz);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(cols))
   for (int64_t j = 0; j <= cols; ++j) T.ptr[j] = cp[j] - base;
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(nnz))
   for (int64_t k = 0; k < nnz; ++k) {
     T.col[k] = rv[k] - base;
     T.val[k] = nz[k];
@@ -117,7 +119,7 @@ std::vector<double> recip(const std::vector<double>& d) {
 
 void scale_rows_cols(HCsr& M, const std::vector<double>* dr, const std::vector<double>* dc) {
   const std::vector<double> ir = dr ? recip(*dr) : std::vector<double>(), ic = dc ? recip(*dc) : std::vector<double>();
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(M.rows))
   for (int64_t i = 0; i < M.rows; ++i)
     for (int k = M.ptr[i]; k < M.ptr[i + 1]; ++k) {
       double v = M.val[k];
@@ -131,7 +133,7 @@ void scale_rows_cols(HCsr& M, const std::vector<double>* dr, const std::vector<d
 // identical arithmetic in identical order, so T stays bitwise M'.
 void scale_rows_cols_T(HCsr& T, const std::vector<double>* dr, const std::vector<double>* dc) {
   const std::vector<double> ir = dr ? recip(*dr) : std::vector<double>(), ic = dc ? recip(*dc) : std::vector<double>();
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(T.rows))
   for (int64_t j = 0; j < T.rows; ++j)
     for (int k = T.ptr[j]; k < T.ptr[j + 1]; ++k) {
       double v = T.val[k];
@@ -144,7 +146,7 @@ void scale_rows_cols_T(HCsr& T, const std::vector<double>* dr, const std::vector
 // row-wise max |v| (or sum |v|) of M, in stored order
 std::vector<double> row_absmax(const HCsr& M) {
   std::vector<double> r(M.rows, 0.0);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(M.rows))
   for (int64_t i = 0; i < M.rows; ++i) {
     double x = 0.0;
     for (int k = M.ptr[i]; k < M.ptr[i + 1]; ++k) x = std::max(x, std::fabs(M.val[k]));
@@ -155,7 +157,7 @@ std::vector<double> row_absmax(const HCsr& M) {
 
 std::vector<double> row_abssum(const HCsr& M) {
   std::vector<double> r(M.rows, 0.0);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(M.rows))
   for (int64_t i = 0; i < M.rows; ++i) {
     double x = 0.0;
     for (int k = M.ptr[i]; k < M.ptr[i + 1]; ++k) x += std::fabs(M.val[k]);
@@ -164,6 +166,11 @@ std::vector<double> row_abssum(const HCsr& M) {
   return r;
 }
 }  // namespace
+
+int host_threads(int64_t work) {
+  if (work < 65536) return 1;
+  return std::max(1, std::min(16, omp_get_max_threads()));
+}
 
 HCsr transpose(const HCsr& A) {
   HCsr T;
@@ -359,7 +366,7 @@ void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& o) 
         }
         return cnt;
       };
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(n))
       for (int64_t i = 0; i < n; ++i) len[i] = merge(i, nullptr, nullptr);
       HCsr S;
       S.rows = S.cols = n;
@@ -367,7 +374,7 @@ void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& o) 
       for (int64_t i = 0; i < n; ++i) S.ptr[i + 1] = S.ptr[i] + len[i];
       S.col.resize(S.ptr[n]);
       S.val.resize(S.ptr[n]);
-#pragma omp parallel for schedule(static)
+#pragma omp parallel for schedule(static) num_threads(host_threads(n))
       for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], S.val.data() + S.ptr[i]);
       Q = std::move(S);
     }

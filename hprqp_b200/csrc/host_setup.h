@@ -58,6 +58,10 @@ void load_problem(const hprqp_problem* pr, HostProblem& hp);
 // scaling! + check_Q_diagonal + the noC rule (src/algorithm.jl:1969-1974).
 void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& out);
 HCsr transpose(const HCsr& A);
+// Host threads for a row-parallel loop over `work` items: 1 below ~64k
+// items (a parallel region costs more than it saves there), else at most
+// 16 (the loops are memory-bound; more threads only add wake-up cost).
+int host_threads(int64_t work);
 // splitmix64 + Box-Muller start vector of the power method (+1e-8).
 std::vector<double> power_start_vector(int64_t len);
 // The same stream, produced incrementally into a caller buffer.

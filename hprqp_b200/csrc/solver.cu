@@ -8,6 +8,7 @@
 // sigma blend and the scalar golden-section search (src/kernels.jl:1453-1486)
 // run on the host from those scalars.
 #include <chrono>
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -539,6 +540,82 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
 }
 
 // Time `iters` HPR iterations pass by pass (CUDA events) from the zero state.
+// Per-kernel time of each pass without the launch gap that an event between
+// passes adds: one iteration is captured into a CUDA graph, its kernel nodes
+// are ordered along the graph's edges, and each node's kernel is launched
+// alone kReps times back to back with programmatic dependent launch (as in
+// the loop); the CUDA-event time / kReps goes to ms[k].  Skipped (ms stays 0)
+// when the iteration is not exactly one kernel per pass (e.g. the QAP
+// operator's GEMMs).  The repeated launches overwrite iterates: profiling
+// only.
+template <typename F>
+static void back_to_back(Common& cm, int np, F one_iteration, double* ms) {
+  constexpr int kReps = 50;
+  cudaGraph_t g = nullptr;
+  HPRQP_CUDA(cudaStreamBeginCapture(cm.stream, cudaStreamCaptureModeThreadLocal));
+  const int64_t l0 = cm.launches;
+  one_iteration();
+  cm.launches = l0;
+  HPRQP_CUDA(cudaStreamEndCapture(cm.stream, &g));
+  size_t nn = 0, ne = 0;
+  HPRQP_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
+  std::vector<cudaGraphNode_t> nodes(nn);
+  HPRQP_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
+  HPRQP_CUDA(cudaGraphGetEdges(g, nullptr, nullptr, &ne));
+  std::vector<cudaGraphNode_t> from(ne), to(ne);
+  if (ne) HPRQP_CUDA(cudaGraphGetEdges(g, from.data(), to.data(), &ne));
+  // topological order (Kahn), kernel nodes only
+  std::vector<int> indeg(nn, 0);
+  auto idx = [&](cudaGraphNode_t x) { return (int)(std::find(nodes.begin(), nodes.end(), x) - nodes.begin()); };
+  for (size_t e = 0; e < ne; ++e) indeg[idx(to[e])]++;
+  std::vector<int> order, ready;
+  for (size_t i = 0; i < nn; ++i)
+    if (!indeg[i]) ready.push_back((int)i);
+  while (!ready.empty()) {
+    const int i = ready.front();
+    ready.erase(ready.begin());
+    order.push_back(i);
+    for (size_t e = 0; e < ne; ++e)
+      if (from[e] == nodes[i] && --indeg[idx(to[e])] == 0) ready.push_back(idx(to[e]));
+  }
+  std::vector<cudaGraphNode_t> kern;
+  for (int i : order) {
+    cudaGraphNodeType t;
+    HPRQP_CUDA(cudaGraphNodeGetType(nodes[i], &t));
+    if (t == cudaGraphNodeTypeKernel) kern.push_back(nodes[i]);
+  }
+  if ((int)kern.size() == np && np <= HPRQP_MAX_PASSES) {
+    cudaEvent_t a, b;
+    HPRQP_CUDA(cudaEventCreate(&a));
+    HPRQP_CUDA(cudaEventCreate(&b));
+    for (int k = 0; k < np; ++k) {
+      cudaKernelNodeParams kp{};
+      HPRQP_CUDA(cudaGraphKernelNodeGetParams(kern[k], &kp));
+      cudaLaunchConfig_t cfg{};
+      cfg.gridDim = kp.gridDim;
+      cfg.blockDim = kp.blockDim;
+      cfg.dynamicSmemBytes = kp.sharedMemBytes;
+      cfg.stream = cm.stream;
+      cudaLaunchAttribute attr[1];
+      attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      attr[0].val.programmaticStreamSerializationAllowed = 1;
+      cfg.attrs = attr;
+      cfg.numAttrs = cm.pdl ? 1 : 0;
+      for (int r = 0; r < 3; ++r) HPRQP_CUDA(cudaLaunchKernelExC(&cfg, kp.func, kp.kernelParams));
+      HPRQP_CUDA(cudaEventRecord(a, cm.stream));
+      for (int r = 0; r < kReps; ++r) HPRQP_CUDA(cudaLaunchKernelExC(&cfg, kp.func, kp.kernelParams));
+      HPRQP_CUDA(cudaEventRecord(b, cm.stream));
+      HPRQP_CUDA(cudaEventSynchronize(b));
+      float t = 0;
+      HPRQP_CUDA(cudaEventElapsedTime(&t, a, b));
+      ms[k] = t / kReps;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+  }
+  cudaGraphDestroy(g);
+}
+
 static void profile(Handle& H, const hprqp_params& p, int64_t iters, bool full, hprqp_pass_stats* out) {
   prepare(H, p);
   Common& cm = *H.cm;
@@ -596,6 +673,7 @@ static void profile(Handle& H, const hprqp_params& p, int64_t iters, bool full, 
       out->bytes_per_iter += bytes;
     }
     for (auto& e : ev) cudaEventDestroy(e);
+    back_to_back(cm, np, [&] { E.step(full, 0.5, 0.5); }, out->ms_back_to_back);
   };
   if (p.precision == HPRQP_PRECISION_FP32_POLISH) run(*H.e32);
   else run(E64);

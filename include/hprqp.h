@@ -178,6 +178,10 @@ typedef struct hprqp_pass_stats {
     double  ms_per_iter;                 /* whole iteration, timed without per-pass events */
     double  bytes_per_iter;
     int64_t iters;
+    double  ms_back_to_back[HPRQP_MAX_PASSES]; /* hprqp_profile_iterations only: the
+                                        pass kernel launched alone, back to back
+                                        (programmatic dependent launch as in the
+                                        loop), per launch; 0 when not measured */
 } hprqp_pass_stats;
 
 typedef struct hprqp_ctx* hprqp_handle;
