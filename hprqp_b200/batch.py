@@ -1,9 +1,11 @@
-"""Batched solves of a LASSO family (include/hprqp_batch.h): all instances
-advance together, one kernel per HPR pass over the concatenated instances,
-with per-instance restarts, sigma, stopping and (optionally) the per-instance
-FP32 -> FP64 polish switch.
+"""Batched solves (include/hprqp_batch.h) of a LASSO family
+(build_from_Ab_lambda models) or of QAP relaxations of uneven size
+(build_from_ABST models): all instances advance together, one kernel per HPR
+pass over the concatenated instances, with per-instance restarts, sigma,
+stopping and (optionally) the per-instance FP32 -> FP64 polish switch.
 
     results = solve_batch(models, HPRQP_parameters(problem_type="LASSO"))
+    results = solve_batch(qap_models, HPRQP_parameters(problem_type="QAP"))
 """
 from __future__ import annotations
 
@@ -12,6 +14,8 @@ import ctypes as C
 import numpy as np
 
 from ._abi import ProblemView, Result, STATUS_NAMES
+
+Q_LASSO, Q_QAP = 1, 2  # hprqp_problem.Q_kind (include/hprqp.h)
 from ._lib import HPRQPError, load
 from .api import HPRQP_parameters, HPRQP_results
 
@@ -25,11 +29,13 @@ def _lib():
         vp = C.c_void_p
         L.hprqp_batch_create.argtypes = [C.POINTER(vp), C.c_int32]
         L.hprqp_batch_load_lasso.argtypes = [vp, C.c_int32, vp]
+        L.hprqp_batch_load_qap.argtypes = [vp, C.c_int32, vp]
         L.hprqp_batch_solve.argtypes = [vp, vp, vp, vp, vp, vp]
         L.hprqp_batch_last_error.argtypes = [vp]
         L.hprqp_batch_last_error.restype = C.c_char_p
         L.hprqp_batch_destroy.argtypes = [vp]
-        for f in ("hprqp_batch_create", "hprqp_batch_load_lasso", "hprqp_batch_solve", "hprqp_batch_destroy"):
+        for f in ("hprqp_batch_create", "hprqp_batch_load_lasso", "hprqp_batch_load_qap", "hprqp_batch_solve",
+                  "hprqp_batch_destroy"):
             getattr(L, f).restype = C.c_int
         _blib = L
     return _blib
@@ -44,8 +50,12 @@ class BatchSolver:
             raise HPRQPError(rc, L.hprqp_batch_last_error(None).decode())
         self.L, self.h, self.models = L, h, list(models)
         views = [ProblemView(m) for m in self.models]
+        kinds = {v.struct.Q_kind for v in views}
+        if len(kinds) != 1 or kinds.pop() not in (Q_LASSO, Q_QAP):
+            raise ValueError("a batch is either all LASSO models or all QAP models")
         arr = (type(views[0].struct) * len(views))(*[v.struct for v in views])
-        self._check(L.hprqp_batch_load_lasso(h, len(views), C.addressof(arr)))
+        load = L.hprqp_batch_load_qap if views[0].struct.Q_kind == Q_QAP else L.hprqp_batch_load_lasso
+        self._check(load(h, len(views), C.addressof(arr)))
         del views
 
     def _check(self, rc):
@@ -94,7 +104,9 @@ class BatchSolver:
 
 
 def solve_batch(models, params: HPRQP_parameters | None = None, initial_x=None, sigma0=None, device=0):
-    params = params or HPRQP_parameters(verbose=False, problem_type="LASSO")
+    if params is None:
+        qap = ProblemView(models[0]).struct.Q_kind == Q_QAP
+        params = HPRQP_parameters(verbose=False, problem_type="QAP" if qap else "LASSO")
     s = BatchSolver(models, device)
     try:
         return s.solve(params, initial_x, sigma0)

@@ -31,6 +31,7 @@
 
 #include "../../include/hprqp.h"
 #include "../../include/hprqp_batch.h"
+#include "batch_qp.h"
 #include "host_setup.h"
 #include "kernels.cuh"
 
@@ -508,10 +509,13 @@ struct Handle {
   Family F;
   std::unique_ptr<BEngine<double>> e64;
   std::unique_ptr<BEngine<float>> e32;
+  bqp::QpBatch* qp = nullptr;  // the QAP family (batch_qp.cu), when loaded
+  bool qap = false;            // which family the handle holds
   std::string err;
   ~Handle() {
     e64.reset();
     e32.reset();
+    if (qp) bqp::destroy(qp);
     if (st) cudaStreamDestroy(st);
   }
 };
@@ -1060,9 +1064,26 @@ int hprqp_batch_load_lasso(hprqp_batch_handle h, int32_t count, const hprqp_prob
     h->e64.reset();
     h->e32.reset();
     const double t = hprqp::batch::now_s();
+    h->qap = false;
     hprqp::batch::build_family(count, problems, h->F);
     if (const char* tv = std::getenv("HPRQP_TIMING"))
       if (tv[0] == '1') std::fprintf(stderr, "batch load: %.3f s\n", hprqp::batch::now_s() - t);
+  })
+}
+
+int hprqp_batch_load_qap(hprqp_batch_handle h, int32_t count, const hprqp_problem* problems) {
+  if (!h) return HPRQP_E_ARG;
+  BATCH_GUARD(h, {
+    const double t = hprqp::batch::now_s();
+    h->e64.reset();
+    h->e32.reset();
+    h->F = hprqp::batch::Family();
+    if (!h->qp) h->qp = hprqp::bqp::create(h->st);
+    h->qap = false;
+    hprqp::bqp::load(h->qp, count, problems);
+    h->qap = true;
+    if (const char* tv = std::getenv("HPRQP_TIMING"))
+      if (tv[0] == '1') std::fprintf(stderr, "qp batch load: %.3f s\n", hprqp::batch::now_s() - t);
   })
 }
 
@@ -1070,8 +1091,13 @@ int hprqp_batch_solve(hprqp_batch_handle h, const hprqp_params* params, const do
                       const double* sigma0, hprqp_result* results, double* const* x_out) {
   if (!h || !params || !results) return HPRQP_E_ARG;
   BATCH_GUARD(h, {
-    if (h->F.B == 0) throw hprqp::Error(HPRQP_E_STATE, "no batch loaded");
-    hprqp::batch::solve(*h, *params, initial_x, sigma0, results, x_out);
+    if (h->qap) {
+      if (hprqp::bqp::count(h->qp) == 0) throw hprqp::Error(HPRQP_E_STATE, "no batch loaded");
+      hprqp::bqp::solve(h->qp, *params, initial_x, sigma0, results, x_out);
+    } else {
+      if (h->F.B == 0) throw hprqp::Error(HPRQP_E_STATE, "no batch loaded");
+      hprqp::batch::solve(*h, *params, initial_x, sigma0, results, x_out);
+    }
   })
 }
 

@@ -1,0 +1,1249 @@
+// batch_qp.cu — batched HPR solves of QAP relaxations in one launch sequence.
+//
+// B instances of build_from_ABST (src/utils.jl:1133-1180): x = vec(X_k)
+// (n_k^2 entries, column-major), 2 n_k doubly-stochastic rows in A,
+// l = 0 <= x, Q_k(X) = 2 (A_k X B_k - S_k X - X T_k)
+// (src/Q_operators/QAP_operator.jl:52-61).  An operator Q means no scaling
+// (src/utils.jl:364-406) and, with l finite, the QP path (noC false).
+//
+// The variables and the constraint rows of all instances are concatenated:
+// A and A' are block-diagonal CSR, every vector has one segment per
+// instance.  Each HPR pass (src/algorithm.jl:945-972: zxw1, tempv, y, w2) is
+// one kernel over all rows; its epilogue is the single-instance epilogue
+// (kernels.cuh) with the instance's sigma, lambda_A, lambda_Q and Halpern
+// counter filled in per row; rows of finished instances return at once.
+// The Q operator is one batched kernel pair over all active instances
+// (TMP = A_k X_k, then 2 TMP B_k - 2 S_k X_k - 2 X_k T_k).  Residuals,
+// M-norm, sigma statistics and the power method reduce per instance in
+// fixed-order segmented reductions.  The control logic -- residual
+// cadence, check_restart, update_sigma! with the golden search, do_restart!,
+// check_break (src/algorithm.jl:323-576, 1977-2038) -- runs per instance on
+// the host from those scalars, all instances in lockstep.  With FP32 +
+// polish every instance moves to the FP64 engine by itself.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "batch_qp.h"
+#include "host_setup.h"
+#include "kernels.cuh"
+
+namespace hprqp {
+namespace bqp {
+
+namespace {
+const double kInf = std::numeric_limits<double>::infinity();
+constexpr int kTileRows = 1024;  // rows per reduction tile
+constexpr int kMaxK = 8;         // reduction slots
+constexpr int kPowWin = 16;      // power steps between host checks
+constexpr int kQapCols = 16;     // output columns per CTA of the Q-operator kernels
+constexpr int kStallChecks = 3;  // FP32 phase: evaluations without a 10% KKT gain before the switch
+constexpr int kStallMinIter = 300;
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+double print_step(int64_t iter) {  // src/algorithm.jl:1173-1175
+  return std::max(std::pow(10.0, std::floor(std::log10((double)iter))) / 10.0, 10.0);
+}
+// golden (src/kernels.jl:1453-1486)
+double golden(double ap, double bp, double cp, double dp, double lo, double hi, double tol, int maxiter = 200) {
+  auto f = [&](double x) { return ap * x + bp / x + cp * x * x / (1 + dp * x); };
+  const double phi = (std::sqrt(5.0) - 1.0) / 2.0;
+  double a = lo, b = hi, c = b - phi * (b - a), d = a + phi * (b - a);
+  double fc = f(c), fd = f(d);
+  for (int i = 0; i < maxiter; ++i) {
+    if (fd < fc) {
+      a = c; c = d; fc = fd;
+      d = a + phi * (b - a);
+      fd = f(d);
+    } else {
+      b = d; d = c; fd = fc;
+      c = b - phi * (b - a);
+      fc = f(c);
+    }
+    if ((b - a) < tol) break;
+  }
+  return 0.5 * (a + b);
+}
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+struct Gate {  // row -> instance, and which instances take part
+  const int* inst;
+  const unsigned char* on;
+};
+
+template <int TPR, typename Acc, typename Src, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_rows(int nrows, Gate G, Src src, Epi epi) {
+  const long long g = (long long)blockIdx.x * kBlock + threadIdx.x;
+  const int row = (int)(g / TPR);
+  if (row >= nrows) return;
+  const int k = G.inst[row];
+  if (!G.on[k]) return;  // uniform over the row group
+  const int lane = threadIdx.x & (TPR - 1);
+  const Acc acc = src.template dot<TPR, Acc>(row, lane);
+  if (lane == 0) epi(row, k, acc);
+}
+
+struct IS {  // per-instance iteration scalars
+  const double *sigma, *lamA, *lamQ;
+  const int* rit;  // iteration of the instance's last restart
+  int iter;
+  __device__ __forceinline__ void halpern(int k, double& h1, double& h2) const {
+    h1 = 1.0 / ((double)(iter - rit[k]) + 2.0);  // 1 / (inner + 2)
+    h2 = 1.0 - h1;
+  }
+};
+
+// The single-instance epilogues with the instance's scalars filled in
+// (the same expressions as the host computes them in Engine::step).
+template <typename V, bool F>
+struct BZxw1 {
+  EpiZxw1<V, F, false> e;
+  IS S;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, int k, A acc) const {
+    EpiZxw1<V, F, false> t = e;
+    const double sg = S.sigma[k];
+    t.sigma = sg;
+    t.f2s = 1.0 / (1.0 + sg * S.lamQ[k]);
+    t.f1s = 1.0 - t.f2s;
+    S.halpern(k, t.h1, t.h2);
+    t(i, acc);
+  }
+};
+template <typename V>
+struct BTempv {
+  EpiTempv<V> e;
+  IS S;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, int k, A acc) const {
+    EpiTempv<V> t = e;
+    t.sigma = S.sigma[k];
+    t(i, acc);
+  }
+};
+template <typename V, bool F>
+struct BY {
+  EpiY<V, F, true> e;
+  IS S;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, int k, A acc) const {
+    EpiY<V, F, true> t = e;
+    t.f1 = S.lamA[k] * S.sigma[k];
+    t.f2 = 1.0 / t.f1;
+    S.halpern(k, t.h1, t.h2);
+    t(i, acc);
+  }
+};
+template <typename V, bool F>
+struct BW2 {
+  EpiW2<V, F, false> e;
+  IS S;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, int k, A acc) const {
+    EpiW2<V, F, false> t = e;
+    const double sg = S.sigma[k];
+    t.fs = sg / (1.0 + sg * S.lamQ[k]);
+    S.halpern(k, t.h1, t.h2);
+    t(i, acc);
+  }
+};
+template <typename Epi>
+struct Plain {  // an instance-independent epilogue
+  Epi e;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, int, A acc) const { e(i, acc); }
+};
+template <typename V>
+struct StoreInvNorm {  // y = (M x) / ||z_k||
+  V* y;
+  const double* zz;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, int k, A acc) const { y[i] = (V)((double)acc / sqrt(zz[k])); }
+};
+
+// segmented reduction: one CTA per tile (instance, rows [b, e))
+template <int K, unsigned MM, typename Src, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_seg(const int* tile_inst, const int* tile_begin, const int* tile_end,
+                                                const unsigned char* on, Src src, Epi epi, double* partials) {
+  const int t = blockIdx.x;
+  const int k = tile_inst[t];
+  double r[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) r[j] = 0.0;
+  if (on[k]) {
+    for (int i = tile_begin[t] + threadIdx.x; i < tile_end[t]; i += kBlock) {
+      const double acc = src.template dot<1, double>(i, 0);
+      epi(i, acc, r);
+    }
+  }
+  block_reduce<K, MM>(r);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) partials[(size_t)t * K + j] = r[j];
+  }
+}
+
+// fold: one warp per instance sums its tiles in a fixed order
+template <int K, unsigned MM, typename Fin>
+__global__ void k_fold(int B, const int* inst_tiles, const unsigned char* on, const double* partials, double* out,
+                       Fin fin) {
+  const int k = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (k >= B || !on[k]) return;
+  const int t0 = inst_tiles[k], t1 = inst_tiles[k + 1];
+  double acc[K];
+#pragma unroll
+  for (int j = 0; j < K; ++j) acc[j] = 0.0;
+  for (int t = t0 + lane; t < t1; t += 32)
+#pragma unroll
+    for (int j = 0; j < K; ++j) {
+      const double v = partials[(size_t)t * K + j];
+      acc[j] = ((MM >> j) & 1u) ? fmax(acc[j], v) : acc[j] + v;
+    }
+#pragma unroll
+  for (int j = 0; j < K; ++j)
+    for (int off = 16; off > 0; off >>= 1) {
+      const double o = __shfl_down_sync(0xffffffffu, acc[j], off);
+      acc[j] = ((MM >> j) & 1u) ? fmax(acc[j], o) : acc[j] + o;
+    }
+  if (lane == 0) {
+#pragma unroll
+    for (int j = 0; j < K; ++j) out[(size_t)k * K + j] = acc[j];
+    fin(k, acc);
+  }
+}
+
+struct NoFin {
+  template <int K>
+  __device__ void operator()(int, const double (&)[K]) const {}
+};
+
+struct PowFin {  // per instance: lambda, err into the log; ||z_next||^2 for the next step
+  double* zz;
+  double* log;  // [kPowWin][B][2]
+  int B, step;
+  __device__ void operator()(int k, const double (&a)[3]) const {
+    const double lam = a[0], z2 = a[1], qq = a[2];
+    const double rr = fmax(z2 - 2.0 * lam * lam + lam * lam * qq, 0.0);
+    log[2 * ((size_t)step * B + k)] = lam;
+    log[2 * ((size_t)step * B + k) + 1] = sqrt(rr) / (sqrt(z2) + lam);
+    zz[k] = z2;
+  }
+  template <int K>
+  __device__ void operator()(int, const double (&)[K]) const {}
+};
+struct ZzFin {
+  double* zz;
+  __device__ void operator()(int k, const double (&a)[1]) const { zz[k] = a[0]; }
+  template <int K>
+  __device__ void operator()(int, const double (&)[K]) const {}
+};
+
+// power-method reduction epilogue: acc = (M q)_i already formed with
+// q = z / ||z||; sums q.v, v.v, q.q (utils.jl:1335-1461)
+template <typename V>
+struct PowDots {
+  const V* zc;
+  V* zn;
+  const double* zz;
+  const int* inst;
+  __device__ __forceinline__ void operator()(int i, double acc, double (&r)[3]) const {
+    const double inv = 1.0 / sqrt(zz[inst[i]]);
+    zn[i] = (V)acc;
+    const double q = (double)zc[i] * inv;
+    r[0] += q * acc;
+    r[1] += acc * acc;
+    r[2] += q * q;
+  }
+};
+template <typename V>
+struct SumSq {
+  const V* v;
+  __device__ __forceinline__ void operator()(int i, double, double (&r)[1]) const {
+    const double t = v[i];
+    r[0] += t * t;
+  }
+};
+template <typename Epi>
+struct SegPlain {  // adapt epi(i, acc, r) (kernels.cuh reductions)
+  Epi e;
+  template <int K>
+  __device__ __forceinline__ void operator()(int i, double acc, double (&r)[K]) const { e(i, acc, r); }
+};
+
+template <typename F>
+__global__ void k_each(int64_t len, F f) {
+  const int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (i < len) f(i);
+}
+
+// Q operator, stage 1: TMP_k = A_k X_k for every active instance
+// (blockIdx.x = instance, blockIdx.y = block of kQapCols output columns).
+// Sums run over l in increasing order, accumulated in V.
+template <typename V>
+__global__ void __launch_bounds__(256) k_qap_tmp(const int* qn, const int64_t* off, const unsigned char* on,
+                                                 const V* __restrict__ QA, const V* X, V* TMP) {
+  const int k = blockIdx.x;
+  if (!on[k]) return;
+  const int n = qn[k];
+  const int j0 = blockIdx.y * kQapCols;
+  if (j0 >= n) return;
+  const int64_t o = off[k];
+  const V* Ak = QA + o;
+  const V* Xk = X + o;
+  V* Tk = TMP + o;
+  const int jn = min(kQapCols, n - j0);
+  for (int e = threadIdx.x; e < n * jn; e += blockDim.x) {
+    const int i = e % n, j = j0 + e / n;
+    V s = V(0);
+    for (int l = 0; l < n; ++l) s = fma(Ak[i + (int64_t)l * n], Xk[l + (int64_t)j * n], s);
+    Tk[i + (int64_t)j * n] = s;
+  }
+}
+
+// stage 2: Y_k = 2 TMP_k B_k - 2 S_k X_k - 2 X_k T_k, in the order of the
+// single-instance operator (Y = 2 TMP B; Y += -2 S X; Y += -2 X T)
+template <typename V>
+__global__ void __launch_bounds__(256) k_qap_out(const int* qn, const int64_t* off, const unsigned char* on,
+                                                 const V* __restrict__ QB, const V* __restrict__ QS,
+                                                 const V* __restrict__ QT, const V* X, const V* TMP, V* Y) {
+  const int k = blockIdx.x;
+  if (!on[k]) return;
+  const int n = qn[k];
+  const int j0 = blockIdx.y * kQapCols;
+  if (j0 >= n) return;
+  const int64_t o = off[k];
+  const V *Bk = QB + o, *Sk = QS + o, *Tk = QT + o, *Xk = X + o, *Pk = TMP + o;
+  V* Yk = Y + o;
+  const int jn = min(kQapCols, n - j0);
+  for (int e = threadIdx.x; e < n * jn; e += blockDim.x) {
+    const int i = e % n, j = j0 + e / n;
+    V a = V(0), b = V(0), c = V(0);
+    for (int l = 0; l < n; ++l) {
+      a = fma(Pk[i + (int64_t)l * n], Bk[l + (int64_t)j * n], a);
+      b = fma(Sk[i + (int64_t)l * n], Xk[l + (int64_t)j * n], b);
+      c = fma(Xk[i + (int64_t)l * n], Tk[l + (int64_t)j * n], c);
+    }
+    V y = V(2) * a;
+    y = fma(V(-2), b, y);
+    y = fma(V(-2), c, y);
+    Yk[i + (int64_t)j * n] = y;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+struct Mem {
+  std::vector<void*> blocks;
+  template <typename T>
+  T* alloc(int64_t n) {
+    void* p = nullptr;
+    HPRQP_CUDA(cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    blocks.push_back(p);
+    return (T*)p;
+  }
+  ~Mem() {
+    for (void* p : blocks) cudaFree(p);
+  }
+};
+
+struct Tiles {  // reduction tiles over a concatenated row space
+  int* inst = nullptr;
+  int* begin = nullptr;
+  int* end = nullptr;
+  int* inst_tiles = nullptr;  // [B+1]
+  int count = 0;
+};
+
+struct Family {  // host copy of the batch
+  int B = 0;
+  int64_t N = 0, M = 0;            // total variables, total constraint rows
+  std::vector<int64_t> noff, moff;  // [B+1]
+  std::vector<int> qn;
+  int nmax = 0;
+  HCsr A, AT;
+  std::vector<double> QA, QB, QS, QT;  // n_k x n_k column-major blocks at noff[k]
+  std::vector<double> c, l, u, AL, AU;
+  std::vector<double> obj_constant, norm_b_org, norm_c_org, norm_b, norm_c;
+};
+
+static void build_family(int count, const hprqp_problem* probs, Family& F) {
+  if (count <= 0 || !probs) throw Error(HPRQP_E_ARG, "empty batch");
+  for (int k = 0; k < count; ++k)
+    if (probs[k].Q_kind != HPRQP_Q_QAP || probs[k].m <= 0)
+      throw Error(HPRQP_E_ARG, "QP batch: every instance must be a QAP relaxation (Q_kind QAP, m > 0)");
+  F = Family();
+  F.B = count;
+  std::vector<HostProblem> hps(count);
+  std::vector<Prepared> pps(count);
+  std::vector<int> codes(count, 0);
+  std::vector<std::string> errs(count);
+  hprqp_params prm;
+  hprqp_default_params(&prm);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(host_threads((int64_t)count * 4096))
+  for (int k = 0; k < count; ++k) {
+    try {
+      load_problem(&probs[k], hps[k]);
+      prepare_problem(hps[k], prm, pps[k]);  // operator Q: no scaling, A' and the norms
+    } catch (const Error& e) {
+      codes[k] = e.code;
+      errs[k] = e.what();
+    }
+  }
+  for (int k = 0; k < count; ++k)
+    if (codes[k]) throw Error(codes[k], "batch instance " + std::to_string(k) + ": " + errs[k]);
+  F.noff.assign(count + 1, 0);
+  F.moff.assign(count + 1, 0);
+  std::vector<int64_t> zoff(count + 1, 0);
+  for (int k = 0; k < count; ++k) {
+    const HostProblem& hp = hps[k];
+    const Prepared& pp = pps[k];
+    F.noff[k + 1] = F.noff[k] + hp.n;
+    F.moff[k + 1] = F.moff[k] + hp.m;
+    zoff[k + 1] = zoff[k] + hp.A.nnz();
+    F.qn.push_back((int)hp.qn);
+    F.nmax = std::max(F.nmax, (int)hp.qn);
+    F.obj_constant.push_back(hp.obj_constant);
+    F.norm_b_org.push_back(pp.norm_b_org);
+    F.norm_c_org.push_back(pp.norm_c_org);
+    F.norm_b.push_back(pp.norm_b);
+    F.norm_c.push_back(pp.norm_c);
+  }
+  F.N = F.noff[count];
+  F.M = F.moff[count];
+  if (F.N > INT32_MAX || F.M > INT32_MAX || zoff[count] > INT32_MAX) throw Error(HPRQP_E_ARG, "batch too large");
+  for (auto* v : {&F.c, &F.l, &F.u, &F.QA, &F.QB, &F.QS, &F.QT}) v->resize(F.N);
+  F.AL.resize(F.M);
+  F.AU.resize(F.M);
+  HCsr& A = F.A;
+  HCsr& AT = F.AT;
+  A.rows = AT.cols = F.M;
+  A.cols = AT.rows = F.N;
+  A.ptr.assign(F.M + 1, 0);
+  AT.ptr.assign(F.N + 1, 0);
+  for (auto* v : {&A.col, &AT.col}) v->resize(zoff[count]);
+  for (auto* v : {&A.val, &AT.val}) v->resize(zoff[count]);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(host_threads(zoff[count]))
+  for (int k = 0; k < count; ++k) {
+    const HostProblem& hp = hps[k];
+    const HCsr& Ak = hp.A;
+    const HCsr& Tk = pps[k].AT;
+    const int64_t z = zoff[k], no = F.noff[k], mo = F.moff[k];
+    for (int64_t r = 0; r < Ak.rows; ++r) A.ptr[mo + r + 1] = (int)(z + Ak.ptr[r + 1]);
+    for (int64_t q = 0; q < Ak.nnz(); ++q) {
+      A.col[z + q] = (int)(Ak.col[q] + no);
+      A.val[z + q] = Ak.val[q];
+    }
+    for (int64_t r = 0; r < Tk.rows; ++r) AT.ptr[no + r + 1] = (int)(z + Tk.ptr[r + 1]);
+    for (int64_t q = 0; q < Tk.nnz(); ++q) {
+      AT.col[z + q] = (int)(Tk.col[q] + mo);
+      AT.val[z + q] = Tk.val[q];
+    }
+    std::copy(hp.c.begin(), hp.c.end(), F.c.begin() + no);
+    std::copy(hp.l.begin(), hp.l.end(), F.l.begin() + no);
+    std::copy(hp.u.begin(), hp.u.end(), F.u.begin() + no);
+    std::copy(hp.qA.begin(), hp.qA.end(), F.QA.begin() + no);
+    std::copy(hp.qB.begin(), hp.qB.end(), F.QB.begin() + no);
+    std::copy(hp.qS.begin(), hp.qS.end(), F.QS.begin() + no);
+    std::copy(hp.qT.begin(), hp.qT.end(), F.QT.begin() + no);
+    std::copy(hp.AL.begin(), hp.AL.end(), F.AL.begin() + mo);
+    std::copy(hp.AU.begin(), hp.AU.end(), F.AU.begin() + mo);
+  }
+}
+
+template <typename V>
+struct Engine {
+  cudaStream_t st = nullptr;
+  Mem mem;
+  int B;
+  int64_t N, M;
+  int nmax;
+  DCsr<V> A, AT;
+  int tprA = 32;
+  int *qn, *inst_n, *inst_m, *rit;
+  int64_t* off;
+  V *QA, *QB, *QS, *QT, *qtmp;
+  V *x, *x_hat, *x_bar, *dx, *w, *w_bar, *dw, *z_bar, *Qw, *Qw_bar, *ATy, *ATy_bar, *ATdy, *QATdy, *dQw, *Qx,
+      *tempv, *c, *l, *u, *ones_n, *zeros_n, *pt, *pz2, *pq2, *pn;
+  V *y, *y_bar, *dy, *s, *AL, *AU, *ones_m, *pz, *pq;
+  double *last_x, *last_w, *last_ATy, *last_y, *stage;
+  unsigned char *on, *mask, *maskA, *maskQ;
+  double *sigma, *lamA, *lamQ, *zzA, *zzQ, *logA, *logQ;
+  Tiles tn, tm;
+  double *part_n, *part_m;
+  double *out_rn, *out_rm, *out_mn_cur, *out_mn_last, *out_mm_cur, *out_mm_last, *out_sn, *out_sm, *out_tmp;
+  int64_t launches = 0;
+
+  template <typename T>
+  T* up(const std::vector<T>& h) {
+    T* d = mem.alloc<T>((int64_t)h.size());
+    if (!h.empty()) HPRQP_CUDA(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    return d;
+  }
+  V* upv(const std::vector<double>& h) {
+    std::vector<V> t(h.size());
+#pragma omp parallel for schedule(static) num_threads(host_threads((int64_t)h.size()))
+    for (int64_t i = 0; i < (int64_t)h.size(); ++i) t[i] = (V)h[i];
+    return up(t);
+  }
+  void upload_csr(const HCsr& h, DCsr<V>& d) {
+    d.rows = (int)h.rows;
+    d.cols = (int)h.cols;
+    d.nnz = h.nnz();
+    d.ptr = up(h.ptr);
+    d.col = up(h.col);
+    d.val = upv(h.val);
+  }
+  Tiles tiles(const std::vector<int64_t>& offs) {
+    std::vector<int> ti, tb, te, it(B + 1, 0);
+    for (int k = 0; k < B; ++k) {
+      it[k] = (int)ti.size();
+      for (int64_t b = offs[k]; b < offs[k + 1]; b += kTileRows) {
+        ti.push_back(k);
+        tb.push_back((int)b);
+        te.push_back((int)std::min<int64_t>(b + kTileRows, offs[k + 1]));
+      }
+    }
+    it[B] = (int)ti.size();
+    Tiles t;
+    t.count = (int)ti.size();
+    t.inst = up(ti);
+    t.begin = up(tb);
+    t.end = up(te);
+    t.inst_tiles = up(it);
+    return t;
+  }
+
+  Engine(const Family& F, cudaStream_t s_) : st(s_), B(F.B), N(F.N), M(F.M), nmax(F.nmax) {
+    upload_csr(F.A, A);
+    upload_csr(F.AT, AT);
+    const double avg = F.M ? (double)F.A.nnz() / F.M : 1.0;
+    tprA = avg > 48 ? 32 : avg > 24 ? 16 : avg > 12 ? 8 : avg > 6 ? 4 : 2;
+    qn = up(F.qn);
+    off = up(F.noff);
+    QA = upv(F.QA);
+    QB = upv(F.QB);
+    QS = upv(F.QS);
+    QT = upv(F.QT);
+    for (V** p : {&qtmp, &x, &x_hat, &x_bar, &dx, &w, &w_bar, &dw, &z_bar, &Qw, &Qw_bar, &ATy, &ATy_bar, &ATdy,
+                  &QATdy, &dQw, &Qx, &tempv, &zeros_n, &pt, &pz2, &pq2, &pn})
+      *p = mem.alloc<V>(N);
+    for (V** p : {&y, &y_bar, &dy, &s, &pz, &pq}) *p = mem.alloc<V>(M);
+    c = upv(F.c);
+    l = upv(F.l);
+    u = upv(F.u);
+    AL = upv(F.AL);
+    AU = upv(F.AU);
+    ones_n = upv(std::vector<double>(N, 1.0));
+    ones_m = upv(std::vector<double>(M, 1.0));
+    for (double** p : {&last_x, &last_w, &last_ATy, &stage}) *p = mem.alloc<double>(N);
+    last_y = mem.alloc<double>(M);
+    std::vector<int> in(N), im(M);
+    for (int k = 0; k < B; ++k) {
+      for (int64_t i = F.noff[k]; i < F.noff[k + 1]; ++i) in[i] = k;
+      for (int64_t i = F.moff[k]; i < F.moff[k + 1]; ++i) im[i] = k;
+    }
+    inst_n = up(in);
+    inst_m = up(im);
+    for (unsigned char** p : {&on, &mask, &maskA, &maskQ}) *p = mem.alloc<unsigned char>(B);
+    for (double** p : {&sigma, &lamA, &lamQ, &zzA, &zzQ}) *p = mem.alloc<double>(B);
+    logA = mem.alloc<double>(2 * (int64_t)B * kPowWin);
+    logQ = mem.alloc<double>(2 * (int64_t)B * kPowWin);
+    rit = mem.alloc<int>(B);
+    tn = tiles(F.noff);
+    tm = tiles(F.moff);
+    part_n = mem.alloc<double>((int64_t)tn.count * kMaxK);
+    part_m = mem.alloc<double>((int64_t)tm.count * kMaxK);
+    for (double** o : {&out_rn, &out_rm, &out_mn_cur, &out_mn_last, &out_mm_cur, &out_mm_last, &out_sn, &out_sm,
+                       &out_tmp})
+      *o = mem.alloc<double>((int64_t)B * kMaxK);
+  }
+
+  void check() {
+    launches++;
+    HPRQP_LAUNCH_CHECK();
+  }
+  // Q operator for the instances in `mk`: yout = Q_k(xin)
+  void qmap(const V* xin, V* yout, const unsigned char* mk) {
+    const dim3 g(B, (nmax + kQapCols - 1) / kQapCols);
+    k_qap_tmp<V><<<g, 256, 0, st>>>(qn, off, mk, QA, xin, qtmp);
+    check();
+    k_qap_out<V><<<g, 256, 0, st>>>(qn, off, mk, QB, QS, QT, xin, qtmp, yout);
+    check();
+  }
+  template <typename Src, typename Epi>
+  void rows_n(const Src& src, const Epi& e, const unsigned char* mk) {  // one thread per n-space row
+    k_rows<1, V><<<(int)((N + kBlock - 1) / kBlock), kBlock, 0, st>>>((int)N, Gate{inst_n, mk}, src, e);
+    check();
+  }
+  template <typename Epi>
+  void rows_AT(const V* xin, const Epi& e, const unsigned char* mk) {  // A' rows: 2 entries each
+    rows_n(CsrSrc<V, V>{AT.ptr, AT.col, AT.val, xin}, e, mk);
+  }
+  template <typename Epi>
+  void rows_A(const V* xin, const Epi& e, const unsigned char* mk) {
+    const Gate G{inst_m, mk};
+    const CsrSrc<V, V> src{A.ptr, A.col, A.val, xin};
+    const int grid = (int)((M * tprA + kBlock - 1) / kBlock);
+    switch (tprA) {
+      case 2: k_rows<2, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;
+      case 4: k_rows<4, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;
+      case 8: k_rows<8, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;
+      case 16: k_rows<16, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;
+      default: k_rows<32, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;
+    }
+    check();
+  }
+  template <int K, unsigned MM, typename Src, typename Epi, typename Fin = NoFin>
+  void seg(const Tiles& t, double* part, const Src& src, const Epi& e, const unsigned char* mk, double* dst,
+           const Fin& fin = Fin()) {
+    k_seg<K, MM><<<t.count, kBlock, 0, st>>>(t.inst, t.begin, t.end, mk, src, e, part);
+    check();
+    k_fold<K, MM><<<(B + 7) / 8, 256, 0, st>>>(B, t.inst_tiles, mk, part, dst, fin);
+    check();
+  }
+  template <typename Fn>
+  void each(int64_t len, const Fn& f) {
+    if (len <= 0) return;
+    k_each<<<(int)((len + kBlock - 1) / kBlock), kBlock, 0, st>>>(len, f);
+    check();
+  }
+
+  // one HPR iteration (QP path, main_update, src/algorithm.jl:945-972)
+  void step(bool full, int iter) {
+    const IS S{sigma, lamA, lamQ, rit, iter};
+    qmap(w, Qw, on);
+    if (full)
+      rows_n(VecSrc<V>{Qw}, BZxw1<V, true>{{Qw, x, x_hat, w_bar, dx, x_bar, z_bar, ATy, c, l, u, w, nullptr, nullptr,
+                                            last_x, 0, 0, 0, 0, 0}, S}, on);
+    else
+      rows_n(VecSrc<V>{Qw}, BZxw1<V, false>{{Qw, x, x_hat, w_bar, dx, x_bar, z_bar, ATy, c, l, u, w, nullptr, nullptr,
+                                             last_x, 0, 0, 0, 0, 0}, S}, on);
+    qmap(w_bar, Qw_bar, on);
+    rows_n(VecSrc<V>{Qw_bar}, BTempv<V>{{tempv, x_hat, Qw, 0}, S}, on);
+    if (full) {
+      rows_A(tempv, BY<V, true>{{y, y_bar, s, dy, AL, AU, last_y, 0, 0, 0, 0}, S}, on);
+      rows_AT(y_bar, BW2<V, true>{{w, ATy, w_bar, dw, ATdy, ATy_bar, nullptr, last_w, last_ATy, 0, 0, 0}, S}, on);
+    } else {
+      rows_A(tempv, BY<V, false>{{y, y_bar, s, dy, AL, AU, last_y, 0, 0, 0, 0}, S}, on);
+      rows_AT(y_bar, BW2<V, false>{{w, ATy, w_bar, dw, ATdy, ATy_bar, nullptr, last_w, last_ATy, 0, 0, 0}, S}, on);
+    }
+  }
+  // compute_residuals! parts (src/algorithm.jl:37-115): out_rn[k*8+j], out_rm[k*3+j]
+  void residuals(const unsigned char* mk) {
+    qmap(x_bar, Qx, mk);
+    seg<8, kResNMax>(tn, part_n, CsrSrc<V, V>{AT.ptr, AT.col, AT.val, y_bar},
+                     SegPlain<EpiResN<V>>{{x_bar, Qx, c, z_bar, ones_n, l, u, 0.0, 1.0, 1.0}}, mk, out_rn);
+    seg<3, kResMMax>(tm, part_m, CsrSrc<V, V>{A.ptr, A.col, A.val, x_bar},
+                     SegPlain<EpiResM<V>>{{y_bar, s, AL, AU, ones_m, 1.0}}, mk, out_rm);
+  }
+  // compute_M_norm! parts (src/algorithm.jl:689-739)
+  void mnorm(double* dn, double* dm, const unsigned char* mk) {
+    qmap(dw, dQw, mk);
+    rows_AT(dy, Plain<EpiStore<V>>{{ATdy, 1.0}}, mk);
+    qmap(ATdy, QATdy, mk);
+    seg<8, 0u>(tn, part_n, ZeroSrc{}, SegPlain<EpiMnormN<V>>{{dx, dQw, ATdy, QATdy, zeros_n, dw, true}}, mk, dn);
+    seg<1, 0u>(tm, part_m, ZeroSrc{}, SumSq<V>{dy}, mk, dm);
+  }
+  // update_sigma! statistics (src/algorithm.jl:344-371): out_sn[k*5+j], out_sm[k]
+  void sigma_stats(const unsigned char* mk) {
+    V *dx_ = dx, *dw_ = dw, *ATdy_ = ATdy, *dy_ = dy;
+    const V *xb = x_bar, *wb = w_bar, *atyb = ATy_bar, *yb = y_bar;
+    const double *lx = last_x, *lw = last_w, *laty = last_ATy, *ly = last_y;
+    const int *in = inst_n, *im = inst_m;
+    const unsigned char* m_ = mk;
+    each(N, [=] __device__(int64_t i) {
+      if (!m_[in[i]]) return;
+      dx_[i] = (V)((double)xb[i] - lx[i]);
+      dw_[i] = (V)((double)wb[i] - lw[i]);
+      ATdy_[i] = (V)((double)atyb[i] - laty[i]);
+    });
+    each(M, [=] __device__(int64_t i) {
+      if (!m_[im[i]]) return;
+      dy_[i] = (V)((double)yb[i] - ly[i]);
+    });
+    qmap(dw, dQw, mk);
+    qmap(ATdy, QATdy, mk);
+    seg<5, 0u>(tn, part_n, ZeroSrc{}, SegPlain<EpiSigmaN<V>>{{dx, dQw, ATdy, QATdy, dw, true}}, mk, out_sn);
+    seg<1, 0u>(tm, part_m, ZeroSrc{}, SumSq<V>{dy}, mk, out_sm);
+  }
+  // do_restart! (src/algorithm.jl:522-555) for the instances in mk
+  void restart(const unsigned char* mk) {
+    rows_AT(y_bar, Plain<EpiRestartQP>{{x, w, ATy, ATy_bar, x_bar, w_bar, last_x, last_w, last_ATy}}, mk);
+    V* y_ = y;
+    const V* yb = y_bar;
+    double* ly = last_y;
+    const int* im = inst_m;
+    const unsigned char* m_ = mk;
+    each(M, [=] __device__(int64_t i) {
+      if (!m_[im[i]]) return;
+      y_[i] = yb[i];
+      ly[i] = (double)yb[i];
+    });
+  }
+  struct EpiRestartQP {
+    V *x, *w, *ATy, *ATy_bar;
+    const V *x_bar, *w_bar;
+    double *last_x, *last_w, *last_ATy;
+    template <typename A>
+    __device__ __forceinline__ void operator()(int i, A acc) const {
+      const V xb = x_bar[i], wb = w_bar[i];
+      x[i] = xb;
+      w[i] = wb;
+      last_x[i] = (double)xb;
+      last_w[i] = (double)wb;
+      ATy_bar[i] = (V)acc;
+      last_ATy[i] = (double)(V)acc;
+      ATy[i] = (V)acc;
+    }
+  };
+  // state reset + process_initial_points! (x only; operator Q: no scaling)
+  void init(const std::vector<double>& x0all, bool has_x0) {
+    for (V* p : {x, x_hat, x_bar, dx, w, w_bar, dw, z_bar, Qw, Qw_bar, ATy, ATy_bar, ATdy, QATdy, dQw, Qx, tempv})
+      HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(V) * N, st));
+    for (V* p : {y, y_bar, dy, s}) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(V) * M, st));
+    for (double* p : {last_x, last_w, last_ATy}) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * N, st));
+    HPRQP_CUDA(cudaMemsetAsync(last_y, 0, sizeof(double) * M, st));
+    if (has_x0) {
+      HPRQP_CUDA(cudaMemcpyAsync(stage, x0all.data(), sizeof(double) * N, cudaMemcpyHostToDevice, st));
+      HPRQP_CUDA(cudaStreamSynchronize(st));
+      V *x_ = x, *xb = x_bar, *w_ = w, *wb = w_bar;
+      double *lx = last_x, *lw = last_w;
+      const double* sg = stage;
+      each(N, [=] __device__(int64_t i) {
+        const V v = (V)sg[i];
+        x_[i] = xb[i] = w_[i] = wb[i] = v;
+        lx[i] = lw[i] = (double)v;
+      });
+    }
+  }
+};
+
+// lambda_max(A_k A_k') and lambda_max(Q_k) for every instance, in lockstep
+// (power_iteration_A/Q, src/utils.jl:1335-1461; the start vectors are the
+// single-instance ones)
+template <typename V>
+static void power_batch(Engine<V>& E, const Family& F, double tol, int max_it, std::vector<double>& lamA,
+                        std::vector<double>& lamQ) {
+  const int B = F.B;
+  std::vector<double> za(E.M), zq(E.N);
+  for (int k = 0; k < B; ++k) {
+    const std::vector<double> a = power_start_vector(F.moff[k + 1] - F.moff[k]);
+    const std::vector<double> q = power_start_vector(F.noff[k + 1] - F.noff[k]);
+    std::copy(a.begin(), a.end(), za.begin() + F.moff[k]);
+    std::copy(q.begin(), q.end(), zq.begin() + F.noff[k]);
+  }
+  std::vector<V> va(za.begin(), za.end()), vq(zq.begin(), zq.end());
+  HPRQP_CUDA(cudaMemcpyAsync(E.pz, va.data(), sizeof(V) * E.M, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaMemcpyAsync(E.pz2, vq.data(), sizeof(V) * E.N, cudaMemcpyHostToDevice, E.st));
+  std::vector<unsigned char> onA(B, 1), onQ(B, 1);
+  HPRQP_CUDA(cudaMemcpyAsync(E.maskA, onA.data(), B, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaMemcpyAsync(E.maskQ, onQ.data(), B, cudaMemcpyHostToDevice, E.st));
+  E.template seg<1, 0u>(E.tm, E.part_m, ZeroSrc{}, SumSq<V>{E.pz}, E.maskA, E.out_tmp, ZzFin{E.zzA});
+  E.template seg<1, 0u>(E.tn, E.part_n, ZeroSrc{}, SumSq<V>{E.pz2}, E.maskQ, E.out_tmp, ZzFin{E.zzQ});
+  lamA.assign(B, 1.0);
+  lamQ.assign(B, 1.0);
+  std::vector<int> doneA(B, 0), doneQ(B, 0);
+  int activeA = B, activeQ = B;
+  std::vector<double> la(2 * (size_t)B * kPowWin), lq(2 * (size_t)B * kPowWin);
+  V *za_c = E.pz, *za_n = E.pq, *zq_c = E.pz2, *zq_n = E.pq2;
+  int it = 0;
+  while (it < max_it && (activeA > 0 || activeQ > 0)) {
+    const int win = std::min(kPowWin, max_it - it);
+    for (int sidx = 0; sidx < win; ++sidx) {
+      if (activeA > 0) {  // t = A' z / ||z||, z' = A t, dots
+        E.rows_AT(za_c, StoreInvNorm<V>{E.pt, E.zzA}, E.maskA);
+        E.template seg<3, 0u>(E.tm, E.part_m, CsrSrc<V, V>{E.A.ptr, E.A.col, E.A.val, E.pt},
+                     PowDots<V>{za_c, za_n, E.zzA, E.inst_m}, E.maskA, E.out_tmp, PowFin{E.zzA, E.logA, B, sidx});
+        std::swap(za_c, za_n);
+      }
+      if (activeQ > 0) {  // q = z / ||z||, z' = Q q, dots
+        V* pn = E.pn;
+        const V* zc = zq_c;
+        const double* zz = E.zzQ;
+        const int* in = E.inst_n;
+        const unsigned char* mq = E.maskQ;
+        E.each(E.N, [=] __device__(int64_t i) {
+          const int k = in[i];
+          if (mq[k]) pn[i] = (V)((double)zc[i] / sqrt(zz[k]));
+        });
+        E.qmap(E.pn, zq_n, E.maskQ);
+        E.template seg<3, 0u>(E.tn, E.part_n, VecSrc<V>{zq_n}, PowDots<V>{zq_c, zq_n, E.zzQ, E.inst_n}, E.maskQ, E.out_tmp,
+                     PowFin{E.zzQ, E.logQ, B, sidx});
+        std::swap(zq_c, zq_n);
+      }
+    }
+    HPRQP_CUDA(cudaMemcpyAsync(la.data(), E.logA, sizeof(double) * la.size(), cudaMemcpyDeviceToHost, E.st));
+    HPRQP_CUDA(cudaMemcpyAsync(lq.data(), E.logQ, sizeof(double) * lq.size(), cudaMemcpyDeviceToHost, E.st));
+    HPRQP_CUDA(cudaStreamSynchronize(E.st));
+    auto scan = [&](std::vector<double>& lg, std::vector<int>& done, std::vector<double>& lam, int& active,
+                    std::vector<unsigned char>& onv) {
+      if (active == 0) return;
+      for (int k = 0; k < B; ++k) {
+        if (done[k]) continue;
+        for (int sidx = 0; sidx < win; ++sidx) {
+          lam[k] = lg[2 * ((size_t)sidx * B + k)];
+          if (lg[2 * ((size_t)sidx * B + k) + 1] < tol) {
+            done[k] = 1;
+            break;
+          }
+        }
+        if (done[k]) {
+          onv[k] = 0;
+          --active;
+        }
+      }
+    };
+    scan(la, doneA, lamA, activeA, onA);
+    scan(lq, doneQ, lamQ, activeQ, onQ);
+    HPRQP_CUDA(cudaMemcpyAsync(E.maskA, onA.data(), B, cudaMemcpyHostToDevice, E.st));
+    HPRQP_CUDA(cudaMemcpyAsync(E.maskQ, onQ.data(), B, cudaMemcpyHostToDevice, E.st));
+    it += win;
+  }
+}
+
+struct RI {  // HPRQP_restart per instance (src/algorithm.jl:1154-1171)
+  bool first = true;
+  double save_gap = kInf, current_gap = kInf, last_gap = kInf, best_gap = kInf, best_sigma = 1.0, weighted = kInf;
+  int64_t inner = 0, times = 0;
+};
+struct Res {
+  double err_Rp = 0, err_Rd = 0, KKT = kInf, pobj = 0, dobj = 0, gap = 0;
+};
+struct Pend {
+  bool on = false;
+  double sigma = 0, lamA = 0, lamQ = 0;
+};
+
+struct QpBatch {
+  cudaStream_t st = nullptr;
+  Family F;
+  std::unique_ptr<Engine<double>> e64;
+  std::unique_ptr<Engine<float>> e32;
+};
+
+QpBatch* create(cudaStream_t st) {
+  QpBatch* q = new QpBatch();
+  q->st = st;
+  return q;
+}
+void destroy(QpBatch* q) { delete q; }
+void load(QpBatch* q, int count, const hprqp_problem* problems) {
+  q->e64.reset();
+  q->e32.reset();
+  build_family(count, problems, q->F);
+}
+int count(const QpBatch* q) { return q ? q->F.B : 0; }
+
+template <typename V>
+static void upload(Engine<V>& E, const std::vector<unsigned char>& on, const std::vector<double>& sigma,
+                   const std::vector<double>& lamA, const std::vector<double>& lamQ, const std::vector<int>& rit) {
+  const int B = E.B;
+  HPRQP_CUDA(cudaMemcpyAsync(E.on, on.data(), B, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaMemcpyAsync(E.sigma, sigma.data(), sizeof(double) * B, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaMemcpyAsync(E.lamA, lamA.data(), sizeof(double) * B, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaMemcpyAsync(E.lamQ, lamQ.data(), sizeof(double) * B, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaMemcpyAsync(E.rit, rit.data(), sizeof(int) * B, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaStreamSynchronize(E.st));  // the host vectors may change right after
+}
+
+template <typename V>
+static std::vector<double> read(Engine<V>& E, const double* d, int64_t count) {
+  std::vector<double> h((size_t)count);
+  HPRQP_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double) * count, cudaMemcpyDeviceToHost, E.st));
+  HPRQP_CUDA(cudaStreamSynchronize(E.st));
+  return h;
+}
+
+template <typename D, typename S>
+struct CopyMasked {  // FP32 -> FP64 hand-over of the instances in the mask
+  D* dst;
+  const S* src;
+  const int* inst;
+  const unsigned char* mk;
+  __device__ void operator()(int64_t i) const {
+    if (mk[inst[i]]) dst[i] = (D)src[i];
+  }
+};
+
+void solve(QpBatch* H, const hprqp_params& p, const double* const* x0s, const double* sig0, hprqp_result* res,
+           double* const* xs) {
+  if (p.auto_save) throw Error(HPRQP_E_UNSUPPORTED, "auto_save is not implemented");
+  if (!(p.stoptol > 0) || p.check_iter <= 0 || !(p.print_frequency == -1 || p.print_frequency > 0))
+    throw Error(HPRQP_E_ARG, "bad parameters");
+  if (!(p.sigma == -1 || p.sigma > 0)) throw Error(HPRQP_E_ARG, "bad sigma");
+  const Family& F = H->F;
+  const int B = F.B;
+  const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
+  const double tc0 = now_s();
+  if (!H->e64) H->e64 = std::make_unique<Engine<double>>(F, H->st);
+  if (fp32 && !H->e32) H->e32 = std::make_unique<Engine<float>>(F, H->st);
+  Engine<double>& E64 = *H->e64;
+  const double t_engines = now_s() - tc0;
+  const double t0 = now_s();
+  // lambda_A, lambda_Q per instance, in the precision of the first phase
+  std::vector<double> lA, lQ;
+  if (fp32) power_batch(*H->e32, F, 1e-4, 5000, lA, lQ);
+  else power_batch(E64, F, 1e-4, 5000, lA, lQ);
+  std::vector<double> lamA(B), lamQ(B);
+  for (int k = 0; k < B; ++k) {
+    lamA[k] = p.lambda_max_A_override > 0 ? p.lambda_max_A_override : lA[k] * p.eig_factor;
+    lamQ[k] = p.lambda_max_Q_override > 0 ? p.lambda_max_Q_override : lQ[k] * p.eig_factor;
+  }
+  const double power_time = now_s() - t0;
+  // sigma of allocate_workspace (src/algorithm.jl:838-851), or per instance
+  std::vector<double> sigma(B);
+  for (int k = 0; k < B; ++k) {
+    double s0 = p.sigma > 0 ? p.sigma : 1.0;
+    if (p.sigma == -1) {
+      const double nb = F.norm_b[k], nc = F.norm_c[k];
+      s0 = (nc > 1e-16 && nb > 1e-16 && nb < 1e16 && nc < 1e16) ? nb / nc : 1.0;
+    }
+    sigma[k] = (sig0 && sig0[k] > 0) ? sig0[k] : s0;
+  }
+  std::vector<double> x0all;
+  bool has_x0 = false;
+  if (x0s) {
+    x0all.assign(F.N, 0.0);
+    for (int k = 0; k < B; ++k)
+      if (x0s[k]) {
+        has_x0 = true;
+        std::copy(x0s[k], x0s[k] + (F.noff[k + 1] - F.noff[k]), x0all.begin() + F.noff[k]);
+      }
+  }
+  std::vector<int> rit(B, 0);
+  std::vector<unsigned char> on64(B, fp32 ? 0 : 1), on32(B, fp32 ? 1 : 0);
+  E64.init(x0all, has_x0);
+  upload(E64, on64, sigma, lamA, lamQ, rit);
+  if (fp32) {
+    H->e32->init(x0all, has_x0);
+    upload(*H->e32, on32, sigma, lamA, lamQ, rit);
+  }
+  std::vector<RI> ri(B);
+  for (int k = 0; k < B; ++k) ri[k].best_sigma = sigma[k];
+  std::vector<Res> R(B);
+  std::vector<int> status(B, -1), phase(B, fp32 ? 0 : 1), flag(B, 0);
+  std::vector<int64_t> it_end(B, 0), it_fp32(B, 0), it4(B, 0), it6(B, 0);
+  std::vector<double> t_end(B, 0), tm4(B, 0), tm6(B, 0), best32(B, kInf);
+  std::vector<int> stall32(B, 0);
+  std::vector<Pend> pend_cur(B), pend_last(B);
+  const double polish_tol = p.polish_tol > 0 ? p.polish_tol : 10.0 * p.stoptol;
+  int active = B;
+  auto on_print = [&](int64_t it) {
+    return p.print_frequency == -1 ? std::fmod((double)it, print_step(it)) == 0.0 : it % p.print_frequency == 0;
+  };
+  // M-norm from the slots (compute_M_norm!, m > 0, Q not diagonal)
+  auto mnorm_val = [&](const double* s, double s8, const Pend& pm) {
+    const double sg = pm.sigma;
+    double M2 = (1.0 / sg) * s[0];
+    M2 -= 2.0 * s[1];
+    double M1 = sg * pm.lamA * s8;
+    M1 -= 2.0 * sg * s[2];
+    M2 += 2.0 * s[3];
+    const double M3 = (sg * sg) / (1.0 + sg * pm.lamQ) * s[5];
+    M1 += sg * pm.lamQ * s[7];
+    M2 += std::max(M1, 0.0);
+    return std::sqrt(std::max(M2, 0.0) + std::max(M3, 0.0));
+  };
+  // compute_residuals! from the slots of engine E (operator Q: no scaling)
+  auto eval_res = [&](int k, int64_t iter, const std::vector<double>& rn, const std::vector<double>& rm) {
+    const double* r = &rn[(size_t)k * 8];
+    const double* q = &rm[(size_t)k * 3];
+    Res& X = R[k];
+    X.pobj = (r[0] + 0.5 * r[1]) + F.obj_constant[k];
+    X.dobj = (-0.5 * r[1] + r[2]) + F.obj_constant[k];
+    X.dobj += q[0];
+    X.gap = std::fabs(X.pobj - X.dobj) / (1.0 + std::max(std::fabs(X.pobj), std::fabs(X.dobj)));
+    X.err_Rd = r[4] / (1.0 + std::max(std::max(F.norm_c_org[k], r[5]), r[6]));
+    X.err_Rp = q[1] / (1.0 + std::max(F.norm_b_org[k], q[2]));
+    if (iter == 0) X.err_Rp = std::max(X.err_Rp, r[7]);
+    X.KKT = std::max(std::max(X.err_Rp, X.err_Rd), X.gap);
+  };
+  std::vector<unsigned char> fm(B, 0);
+  bool force = false;
+  std::vector<unsigned char> force_mask(B, 0);
+  for (int64_t iter = 0; iter <= p.max_iter && active > 0; ++iter) {
+    const bool print_yes = on_print(iter) || iter == p.max_iter;
+    if (iter % p.check_iter == 0 || print_yes || force) {
+      force = false;
+      std::vector<double> rn64, rm64, rn32, rm32, mc64, mm64c, ml64, mm64l, mc32, mm32c, ml32, mm32l;
+      auto gather = [&](auto& E, std::vector<double>& rn, std::vector<double>& rm, std::vector<double>& mc,
+                        std::vector<double>& mmc, std::vector<double>& ml, std::vector<double>& mml) {
+        E.residuals(E.on);
+        rn = read(E, E.out_rn, (int64_t)B * 8);
+        rm = read(E, E.out_rm, (int64_t)B * 3);
+        mc = read(E, E.out_mn_cur, (int64_t)B * 8);
+        mmc = read(E, E.out_mm_cur, (int64_t)B);
+        ml = read(E, E.out_mn_last, (int64_t)B * 8);
+        mml = read(E, E.out_mm_last, (int64_t)B);
+      };
+      gather(E64, rn64, rm64, mc64, mm64c, ml64, mm64l);
+      if (fp32) gather(*H->e32, rn32, rm32, mc32, mm32c, ml32, mm32l);
+      std::vector<unsigned char> sw(B, 0);
+      bool any_sw = false;
+      for (int k = 0; k < B; ++k) {
+        if (status[k] >= 0) continue;
+        const bool in64 = phase[k] == 1;
+        if (pend_cur[k].on) {
+          ri[k].current_gap = mnorm_val(&(in64 ? mc64 : mc32)[(size_t)k * 8], (in64 ? mm64c : mm32c)[k], pend_cur[k]);
+          pend_cur[k].on = false;
+        }
+        if (pend_last[k].on) {
+          ri[k].last_gap = mnorm_val(&(in64 ? ml64 : ml32)[(size_t)k * 8], (in64 ? mm64l : mm32l)[k], pend_last[k]);
+          pend_last[k].on = false;
+        }
+        eval_res(k, iter, in64 ? rn64 : rn32, in64 ? rm64 : rm32);
+        if (!in64) {
+          bool go = R[k].KKT < polish_tol;
+          if (R[k].KKT < 0.9 * best32[k]) {
+            best32[k] = R[k].KKT;
+            stall32[k] = 0;
+          } else if (++stall32[k] >= kStallChecks && iter >= kStallMinIter) {
+            go = true;
+          }
+          if (go) {
+            sw[k] = 1;
+            any_sw = true;
+          }
+        }
+      }
+      if (any_sw) {  // hand the switching instances to the FP64 engine and re-evaluate there
+        Engine<float>& E32 = *H->e32;
+        HPRQP_CUDA(cudaMemcpyAsync(E64.mask, sw.data(), B, cudaMemcpyHostToDevice, H->st));
+        const int *in = E64.inst_n, *im = E64.inst_m;
+        const unsigned char* mk = E64.mask;
+        auto cn = [&](double* d, const float* s_) { E64.each(E64.N, CopyMasked<double, float>{d, s_, in, mk}); };
+        auto cm_ = [&](double* d, const float* s_) { E64.each(E64.M, CopyMasked<double, float>{d, s_, im, mk}); };
+        cn(E64.x, E32.x); cn(E64.x_hat, E32.x_hat); cn(E64.x_bar, E32.x_bar); cn(E64.dx, E32.dx);
+        cn(E64.w, E32.w); cn(E64.w_bar, E32.w_bar); cn(E64.dw, E32.dw); cn(E64.z_bar, E32.z_bar);
+        cn(E64.Qw, E32.Qw); cn(E64.Qw_bar, E32.Qw_bar); cn(E64.ATy, E32.ATy); cn(E64.ATy_bar, E32.ATy_bar);
+        cn(E64.ATdy, E32.ATdy); cn(E64.tempv, E32.tempv);
+        cm_(E64.y, E32.y); cm_(E64.y_bar, E32.y_bar); cm_(E64.dy, E32.dy); cm_(E64.s, E32.s);
+        for (double* d : {E64.last_x, E64.last_w, E64.last_ATy}) {
+          const double* s_ = d == E64.last_x ? E32.last_x : d == E64.last_w ? E32.last_w : E32.last_ATy;
+          E64.each(E64.N, CopyMasked<double, double>{d, s_, in, mk});
+        }
+        E64.each(E64.M, CopyMasked<double, double>{E64.last_y, E32.last_y, im, mk});
+        for (int k = 0; k < B; ++k)
+          if (sw[k]) {
+            phase[k] = 1;
+            on64[k] = 1;
+            on32[k] = 0;
+            it_fp32[k] = iter;
+          }
+        upload(E64, on64, sigma, lamA, lamQ, rit);
+        upload(E32, on32, sigma, lamA, lamQ, rit);
+        E64.residuals(E64.mask);
+        const std::vector<double> rn = read(E64, E64.out_rn, (int64_t)B * 8);
+        const std::vector<double> rm = read(E64, E64.out_rm, (int64_t)B * 3);
+        for (int k = 0; k < B; ++k)
+          if (sw[k]) eval_res(k, iter, rn, rm);
+      }
+      for (int k = 0; k < B; ++k)
+        if (status[k] < 0 && (!std::isfinite(R[k].KKT) || !std::isfinite(R[k].pobj) || !std::isfinite(R[k].dobj)))
+          status[k] = HPRQP_STATUS_NUMERICAL_ERROR;
+    }
+    // check_break, check_restart per instance (src/algorithm.jl:441-492, 558-576)
+    bool finished_now = false;
+    for (int k = 0; k < B; ++k) {
+      flag[k] = 0;
+      if (status[k] >= 0) {
+        if (it_end[k] == 0 && t_end[k] == 0) {  // NUMERICAL_ERROR just now
+          it_end[k] = iter;
+          t_end[k] = now_s() - t0;
+          (phase[k] == 1 ? on64 : on32)[k] = 0;
+          --active;
+          finished_now = true;
+        }
+        continue;
+      }
+      if (R[k].KKT < p.stoptol) status[k] = HPRQP_STATUS_OPTIMAL;
+      else if (iter == p.max_iter) status[k] = HPRQP_STATUS_MAX_ITER;
+      else if (now_s() - t0 > p.time_limit) status[k] = HPRQP_STATUS_TIME_LIMIT;
+      RI& r = ri[k];
+      if (r.first) {
+        if (iter == p.check_iter) {
+          r.first = false;
+          flag[k] = 1;
+          r.weighted = r.current_gap;
+          r.best_gap = r.current_gap;
+          r.best_sigma = sigma[k];
+        }
+      } else if (iter % p.check_iter == 0) {
+        if (r.current_gap < 0) r.current_gap = 1e-6;
+        if (r.current_gap <= 0.2 * r.last_gap) flag[k] = 1;
+        if (r.current_gap <= 0.8 * r.last_gap && r.current_gap > r.save_gap) flag[k] = 2;
+        const double fct = (r.current_gap / r.weighted > 1e-1) ? 0.5 : 0.2;
+        if (r.inner >= fct * iter) flag[k] = 3;
+        if (r.best_gap > r.current_gap) {
+          r.best_gap = r.current_gap;
+          r.best_sigma = sigma[k];
+        }
+        r.save_gap = r.current_gap;
+      }
+      if (status[k] >= 0) {
+        finished_now = true;
+        it_end[k] = iter;
+        t_end[k] = now_s() - t0;
+        (phase[k] == 1 ? on64 : on32)[k] = 0;
+        --active;
+        flag[k] = 0;
+      }
+    }
+    // update_sigma! (src/algorithm.jl:323-423, m > 0, Q not diagonal: golden search)
+    bool any_flag = false;
+    for (int k = 0; k < B; ++k) any_flag |= flag[k] > 0;
+    if (any_flag) {
+      auto upd = [&](auto& E, int ph) {
+        bool any = false;
+        for (int k = 0; k < B; ++k) {
+          fm[k] = flag[k] > 0 && phase[k] == ph;
+          any |= fm[k] != 0;
+        }
+        if (!any) return;
+        HPRQP_CUDA(cudaMemcpyAsync(E.mask, fm.data(), B, cudaMemcpyHostToDevice, H->st));
+        if (!p.sigma_fixed) {
+          E.sigma_stats(E.mask);
+          const std::vector<double> sn = read(E, E.out_sn, (int64_t)B * 5);
+          const std::vector<double> sm = read(E, E.out_sm, (int64_t)B);
+          for (int k = 0; k < B; ++k) {
+            if (!fm[k]) continue;
+            const double* s = &sn[(size_t)k * 5];
+            double a = lamA[k] * sm[k] - 2 * s[1];
+            a += lamQ[k] * s[3];
+            const double c = s[4], d = lamQ[k];
+            a = std::max(a, 1e-12);
+            const double b = std::max(s[0], 1e-12);
+            const double est = golden(a, b, c, d, 1e-12, 1e12, 1e-13);
+            const RI& r = ri[k];
+            const double fct = std::exp(-0.05 * (r.current_gap / r.best_gap));
+            const double temp1 = std::max(std::min(R[k].err_Rd, R[k].err_Rp), std::min(R[k].gap, r.current_gap));
+            const double cand = std::exp(fct * std::log(est) + (1 - fct) * std::log(r.best_sigma));
+            double kappa;
+            if (temp1 > 9e-10) kappa = 1.0;
+            else if (temp1 > 5e-10) kappa = std::min(std::max(std::sqrt(R[k].err_Rd / R[k].err_Rp), 1e-2), 100.0);
+            else kappa = std::min(std::max(R[k].err_Rd / R[k].err_Rp, 1e-2), 100.0);
+            sigma[k] = kappa * cand;
+          }
+        }
+        E.restart(E.mask);  // do_restart! (src/algorithm.jl:522-555)
+      };
+      upd(E64, 1);
+      if (fp32) upd(*H->e32, 0);
+      for (int k = 0; k < B; ++k)
+        if (flag[k] > 0) {
+          ri[k].last_gap = ri[k].current_gap;
+          ri[k].save_gap = kInf;
+          ri[k].times++;
+          ri[k].inner = 0;
+          rit[k] = (int)iter;
+        }
+    }
+    for (int k = 0; k < B; ++k) {
+      if (status[k] >= 0) continue;
+      if (R[k].KKT < 1e-4 && it4[k] == 0 && tm4[k] == 0) { it4[k] = iter; tm4[k] = now_s() - t0; }
+      if (R[k].KKT < 1e-6 && it6[k] == 0 && tm6[k] == 0) { it6[k] = iter; tm6[k] = now_s() - t0; }
+    }
+    if (active == 0) break;
+    if (any_flag || finished_now) {
+      upload(E64, on64, sigma, lamA, lamQ, rit);
+      if (fp32) upload(*H->e32, on32, sigma, lamA, lamQ, rit);
+    }
+    const int64_t next = iter + 1;
+    const bool to_check = (next % p.check_iter == 0) || any_flag || on_print(next);
+    bool any64 = false, any32 = false;
+    for (int k = 0; k < B; ++k)
+      if (status[k] < 0) (phase[k] == 1 ? any64 : any32) = true;
+    if (any64) E64.step(to_check, (int)iter);
+    if (any32) H->e32->step(to_check, (int)iter);
+    if (any_flag) {
+      auto last = [&](auto& E, int ph) {
+        bool any = false;
+        for (int k = 0; k < B; ++k) {
+          fm[k] = flag[k] > 0 && phase[k] == ph && status[k] < 0;
+          any |= fm[k] != 0;
+        }
+        if (!any) return;
+        HPRQP_CUDA(cudaMemcpyAsync(E.mask, fm.data(), B, cudaMemcpyHostToDevice, H->st));
+        E.mnorm(E.out_mn_last, E.out_mm_last, E.mask);
+      };
+      last(E64, 1);
+      if (fp32) last(*H->e32, 0);
+      for (int k = 0; k < B; ++k)
+        if (flag[k] > 0 && status[k] < 0) pend_last[k] = Pend{true, sigma[k], lamA[k], lamQ[k]};
+    }
+    if ((iter + 1) % p.check_iter == 0) {
+      if (any64) E64.mnorm(E64.out_mn_cur, E64.out_mm_cur, E64.on);
+      if (any32) H->e32->mnorm(H->e32->out_mn_cur, H->e32->out_mm_cur, H->e32->on);
+      for (int k = 0; k < B; ++k)
+        if (status[k] < 0) pend_cur[k] = Pend{true, sigma[k], lamA[k], lamQ[k]};
+    }
+    for (int k = 0; k < B; ++k)
+      if (status[k] < 0) ri[k].inner++;
+  }
+  HPRQP_CUDA(cudaStreamSynchronize(H->st));
+  const double t_all = now_s() - t0;
+  if (const char* tv = std::getenv("HPRQP_TIMING"))
+    if (tv[0] == '1')
+      std::fprintf(stderr, "qp batch solve: engines %.3f s, power %.3f s, loop %.3f s\n", t_engines, power_time,
+                   t_all - power_time);
+  const int64_t launches = E64.launches + (H->e32 ? H->e32->launches : 0);
+  std::vector<double> x64(F.N), x32(fp32 ? F.N : 0);
+  HPRQP_CUDA(cudaMemcpy(x64.data(), E64.x_bar, sizeof(double) * F.N, cudaMemcpyDeviceToHost));
+  if (fp32) {
+    std::vector<float> xf(F.N);
+    HPRQP_CUDA(cudaMemcpy(xf.data(), H->e32->x_bar, sizeof(float) * F.N, cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < F.N; ++i) x32[i] = xf[i];
+  }
+  for (int k = 0; k < B; ++k) {
+    hprqp_result& r = res[k];
+    std::memset(&r, 0, sizeof(r));
+    r.iter = it_end[k];
+    r.time = t_end[k] > 0 ? t_end[k] : t_all;
+    r.power_time = power_time;
+    r.primal_obj = R[k].pobj;
+    r.dual_obj = R[k].dobj;
+    r.residuals = R[k].KKT;
+    r.gap = R[k].gap;
+    r.err_Rp = R[k].err_Rp;
+    r.err_Rd = R[k].err_Rd;
+    r.status = status[k] < 0 ? HPRQP_STATUS_MAX_ITER : status[k];
+    r.sigma = sigma[k];
+    r.lambda_max_A = lamA[k];
+    r.lambda_max_Q = lamQ[k];
+    r.restarts = ri[k].times;
+    r.iter_fp32 = it_fp32[k] ? it_fp32[k] : (fp32 ? it_end[k] : 0);
+    r.iter_4 = it4[k] ? it4[k] : it_end[k];
+    r.iter_6 = it6[k] ? it6[k] : it_end[k];
+    r.time_4 = tm4[k] > 0 ? tm4[k] : r.time;
+    r.time_6 = tm6[k] > 0 ? tm6[k] : r.time;
+    r.gpu_launches = launches;
+    r.device_time = t_all;
+    if (xs && xs[k]) {
+      const std::vector<double>& src = phase[k] == 1 ? x64 : x32;
+      std::memcpy(xs[k], &src[F.noff[k]], sizeof(double) * (F.noff[k + 1] - F.noff[k]));
+    }
+  }
+  E64.launches = 0;
+  if (H->e32) H->e32->launches = 0;
+}
+
+}  // namespace bqp
+}  // namespace hprqp

@@ -1,13 +1,18 @@
 /*
- * hprqp_batch.h — batched HPR solves of a LASSO family in one launch
- * sequence (libhprqp).  Every instance is a LASSO problem as built by the
- * reference's build_from_Ab_lambda (src/utils.jl:1222-1267): Q = A_k' A_k,
- * c_k = -A_k' b_k, no constraints (m = 0), lambda_k.  The instances are
- * concatenated block-diagonally and each HPR pass is one kernel over all of
- * them; converged instances drop out through a per-instance mask.  Each
- * instance follows the reference's control logic on its own (restarts,
- * sigma, stopping), so its result is the one hprqp_solve would return.
- * No counterpart in the reference (which solves one model per call).
+ * hprqp_batch.h — batched HPR solves in one launch sequence (libhprqp), for
+ * two families:
+ *  - LASSO problems as built by the reference's build_from_Ab_lambda
+ *    (src/utils.jl:1222-1267): Q = A_k' A_k, c_k = -A_k' b_k, no
+ *    constraints (m = 0), lambda_k;
+ *  - QAP relaxations as built by build_from_ABST (src/utils.jl:1133-1180):
+ *    x = vec(X_k), doubly-stochastic rows, X_k >= 0,
+ *    Q_k(X) = 2 (A_k X B_k - S_k X - X T_k), instances of uneven size.
+ * The instances are concatenated block-diagonally and each HPR pass is one
+ * kernel over all of them; converged instances drop out through a
+ * per-instance mask.  Each instance follows the reference's control logic
+ * on its own (restarts, sigma, stopping), so its result is the one
+ * hprqp_solve would return up to rounding.  No counterpart in the reference
+ * (which solves one model per call).
  */
 #ifndef HPRQP_BATCH_H
 #define HPRQP_BATCH_H
@@ -26,6 +31,10 @@ int hprqp_batch_create(hprqp_batch_handle* h, int32_t device);
 
 /* Copy `count` LASSO problems (Q_kind = HPRQP_Q_LASSO, m = 0). */
 int hprqp_batch_load_lasso(hprqp_batch_handle h, int32_t count, const hprqp_problem* problems);
+
+/* Copy `count` QAP relaxations (Q_kind = HPRQP_Q_QAP, m = 2 qap_n); replaces
+ * whatever the handle held.  hprqp_batch_solve then solves this family. */
+int hprqp_batch_load_qap(hprqp_batch_handle h, int32_t count, const hprqp_problem* problems);
 
 /* Solve all instances.  initial_x: NULL or `count` pointers (entries may be
  * NULL) to length-n_k warm starts; sigma0: NULL or `count` initial sigmas
