@@ -37,6 +37,7 @@
 #include "batch_qp.h"
 #include "host_setup.h"
 #include "kernels.cuh"
+#include "tcgen05.cuh"
 
 namespace hprqp {
 namespace bqp {
@@ -346,6 +347,141 @@ __global__ void __launch_bounds__(256) k_qap_out(const int* qn, const int64_t* o
   }
 }
 
+// FP32 phase: the whole Q operator of one instance (n_k <= 128) in one CTA
+// on the tensor cores, 3xTF32 with FP32 accumulation in TMEM:
+//   phase 1: acc1 = A_k X, acc2 = S_k X        (K = n_k in chunks of 32)
+//   phase 2: acc3 = TMP B_k + (-X) T_k, TMP = acc1 read back from TMEM
+//   Y = 2 acc3 - 2 acc2
+// Operands are split into TF32 hi/lo and staged K-major (tcgen05.cuh);
+// rows and columns beyond n_k are zero.  Every mbarrier wait is bounded;
+// on a timeout the CTA raises g_bqp_err, frees its TMEM and returns.
+__device__ int g_bqp_err = 0;
+constexpr int kQapTcSmem = 8 * tc::kOpBytes + 1024;
+constexpr uint32_t kQapTcCols = 512;  // acc1, acc2, acc3 (128 columns each), power of two
+
+__global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const int64_t* off, const unsigned char* on,
+                                                         const float* __restrict__ QA, const float* __restrict__ QB,
+                                                         const float* __restrict__ QS, const float* __restrict__ QT,
+                                                         const float* X, float* Y) {
+  using namespace tc;
+  const int k = blockIdx.x;
+  if (!on[k]) return;  // the whole CTA
+  const int n = qn[k];
+  if (n > kTile) {
+    if (threadIdx.x == 0) atomicExch(&g_bqp_err, 2);
+    return;
+  }
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char *sAh = sm, *sAl = sm + kOpBytes, *sSh = sm + 2 * kOpBytes, *sSl = sm + 3 * kOpBytes;
+  unsigned char *sBh = sm + 4 * kOpBytes, *sBl = sm + 5 * kOpBytes, *sTh = sm + 6 * kOpBytes,
+                *sTl = sm + 7 * kOpBytes;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int64_t o = off[k];
+  const float *Ak = QA + o, *Bk = QB + o, *Sk = QS + o, *Tk = QT + o, *Xk = X + o;
+  float* Yk = Y + o;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
+                 "r"(kQapTcCols));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar)), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tm = tmem_base, acc1 = tm, acc2 = tm + 128, acc3 = tm + 256;
+  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  uint32_t parity = 0;
+  // phase 1
+  for (int k0 = 0; k0 < n; k0 += kChunk) {
+    for (int e = tid; e < kTile * kChunk; e += kThreads) {
+      const int r = e & (kTile - 1), c = e >> 7, l = k0 + c;  // A operands: (row r, k = l), column-major source
+      const bool in = r < n && l < n;
+      put_split(sAh, sAl, kmaj_off(r, c), in ? Ak[r + (int64_t)l * n] : 0.0f);
+      put_split(sSh, sSl, kmaj_off(r, c), in ? Sk[r + (int64_t)l * n] : 0.0f);
+    }
+    for (int e = tid; e < kTile * kChunk; e += kThreads) {
+      const int c = e & (kChunk - 1), j = e >> 5, l = k0 + c;  // B operand X(l, j): row j, k = l
+      put_split(sBh, sBl, kmaj_off(j, c), (j < n && l < n) ? Xk[l + (int64_t)j * n] : 0.0f);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      mma_chunk_3x(acc1, smem_u32(sAh), smem_u32(sAl), smem_u32(sBh), smem_u32(sBl), k0 == 0);
+      mma_chunk_3x(acc2, smem_u32(sSh), smem_u32(sSl), smem_u32(sBh), smem_u32(sBl), k0 == 0);
+      mma_commit(&bar);
+    }
+    if (!mbar_wait(&bar, parity)) s_fail = 1;
+    parity ^= 1u;
+    __syncthreads();
+    if (s_fail) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // phase 2
+  const int row = warp * 32 + (tid & 31);
+  for (int k0 = 0; k0 < n && !s_fail; k0 += kChunk) {
+    uint32_t v[32];
+    tmem_ld32(acc1 + lane_base + (uint32_t)k0, v);  // TMP(row, k0 .. k0+31)
+#pragma unroll
+    for (int c = 0; c < kChunk; ++c)
+      put_split(sAh, sAl, kmaj_off(row, c), (row < n && k0 + c < n) ? __uint_as_float(v[c]) : 0.0f);
+    for (int e = tid; e < kTile * kChunk; e += kThreads) {
+      const int r = e & (kTile - 1), c = e >> 7, l = k0 + c;  // -X(r, l) as an A operand
+      put_split(sSh, sSl, kmaj_off(r, c), (r < n && l < n) ? -Xk[r + (int64_t)l * n] : 0.0f);
+    }
+    for (int e = tid; e < kTile * kChunk; e += kThreads) {
+      const int c = e & (kChunk - 1), j = e >> 5, l = k0 + c;  // B_k(l, j), T_k(l, j): row j, k = l
+      const bool in = j < n && l < n;
+      put_split(sBh, sBl, kmaj_off(j, c), in ? Bk[l + (int64_t)j * n] : 0.0f);
+      put_split(sTh, sTl, kmaj_off(j, c), in ? Tk[l + (int64_t)j * n] : 0.0f);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      mma_chunk_3x(acc3, smem_u32(sAh), smem_u32(sAl), smem_u32(sBh), smem_u32(sBl), k0 == 0);
+      mma_chunk_3x(acc3, smem_u32(sSh), smem_u32(sSl), smem_u32(sTh), smem_u32(sTl), false);
+      mma_commit(&bar);
+    }
+    if (!mbar_wait(&bar, parity)) s_fail = 1;
+    parity ^= 1u;
+    __syncthreads();
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!s_fail) {
+    for (int c0 = 0; c0 < kTile; c0 += 32) {
+      uint32_t a3[32], a2[32];
+      tmem_ld32(acc3 + lane_base + (uint32_t)c0, a3);
+      tmem_ld32(acc2 + lane_base + (uint32_t)c0, a2);
+      if (row < n) {
+#pragma unroll
+        for (int q = 0; q < 32; ++q) {
+          const int j = c0 + q;
+          if (j < n) Yk[row + (int64_t)j * n] = 2.0f * __uint_as_float(a3[q]) - 2.0f * __uint_as_float(a2[q]);
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(&g_bqp_err, 1);
+    mbar_wait(&bar, parity ^ 1u);  // give MMAs still in flight a bounded chance to drain
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tm), "r"(kQapTcCols));
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
@@ -574,14 +710,37 @@ struct Engine {
     for (double** o : {&out_rn, &out_rm, &out_mn_cur, &out_mn_last, &out_mm_cur, &out_mm_last, &out_sn, &out_sm,
                        &out_tmp})
       *o = mem.alloc<double>((int64_t)B * kMaxK);
+    if constexpr (std::is_same<V, float>::value) {
+      const char* e = std::getenv("HPRQP_QAP_TC");
+      use_tc = nmax <= tc::kTile && !(e && e[0] == '0');
+      if (use_tc)
+        HPRQP_CUDA(cudaFuncSetAttribute(k_qap_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kQapTcSmem));
+    }
+  }
+  // true (and the flag cleared) when a tensor-core operator launch gave up
+  bool tc_failed() {
+    int v = 0;
+    const int zero = 0;
+    HPRQP_CUDA(cudaMemcpyFromSymbolAsync(&v, g_bqp_err, sizeof(int), 0, cudaMemcpyDeviceToHost, st));
+    HPRQP_CUDA(cudaStreamSynchronize(st));
+    if (v) HPRQP_CUDA(cudaMemcpyToSymbolAsync(g_bqp_err, &zero, sizeof(int), 0, cudaMemcpyHostToDevice, st));
+    return v != 0;
   }
 
   void check() {
     launches++;
     HPRQP_LAUNCH_CHECK();
   }
+  bool use_tc = false;  // FP32 engine, every n_k <= 128: the tensor-core operator
   // Q operator for the instances in `mk`: yout = Q_k(xin)
   void qmap(const V* xin, V* yout, const unsigned char* mk) {
+    if constexpr (std::is_same<V, float>::value) {
+      if (use_tc) {
+        k_qap_tc<<<B, tc::kThreads, kQapTcSmem, st>>>(qn, off, mk, QA, QB, QS, QT, xin, yout);
+        check();
+        return;
+      }
+    }
     const dim3 g(B, (nmax + kQapCols - 1) / kQapCols);
     k_qap_tmp<V><<<g, 256, 0, st>>>(qn, off, mk, QA, xin, qtmp);
     check();
@@ -1199,6 +1358,7 @@ void solve(QpBatch* H, const hprqp_params& p, const double* const* x0s, const do
       if (status[k] < 0) ri[k].inner++;
   }
   HPRQP_CUDA(cudaStreamSynchronize(H->st));
+  if (fp32 && H->e32->tc_failed()) throw Error(HPRQP_E_CUDA, "QAP tensor-core operator: a bounded wait gave up");
   const double t_all = now_s() - t0;
   if (const char* tv = std::getenv("HPRQP_TIMING"))
     if (tv[0] == '1')

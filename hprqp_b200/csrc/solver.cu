@@ -561,9 +561,11 @@ static void back_to_back(Common& cm, int np, F one_iteration, double* ms) {
   HPRQP_CUDA(cudaGraphGetNodes(g, nullptr, &nn));
   std::vector<cudaGraphNode_t> nodes(nn);
   HPRQP_CUDA(cudaGraphGetNodes(g, nodes.data(), &nn));
-  HPRQP_CUDA(cudaGraphGetEdges(g, nullptr, nullptr, &ne));
+  // programmatic (PDL) edges carry edge data: the _v2 query returns them
+  HPRQP_CUDA(cudaGraphGetEdges_v2(g, nullptr, nullptr, nullptr, &ne));
   std::vector<cudaGraphNode_t> from(ne), to(ne);
-  if (ne) HPRQP_CUDA(cudaGraphGetEdges(g, from.data(), to.data(), &ne));
+  std::vector<cudaGraphEdgeData> edata(ne);
+  if (ne) HPRQP_CUDA(cudaGraphGetEdges_v2(g, from.data(), to.data(), edata.data(), &ne));
   // topological order (Kahn), kernel nodes only
   std::vector<int> indeg(nn, 0);
   auto idx = [&](cudaGraphNode_t x) { return (int)(std::find(nodes.begin(), nodes.end(), x) - nodes.begin()); };

@@ -27,84 +27,14 @@
 
 #include "common.cuh"
 #include "tc_gemm.h"
+#include "tcgen05.cuh"
 
 namespace hprqp {
 namespace tc {
 
-constexpr int kTile = 128;    // M and N of one CTA tile (one MMA: M = 128, N = 128)
-constexpr int kChunk = 32;    // K elements staged per round
-constexpr int kThreads = 128;
-constexpr int kOpBytes = kTile * kChunk * 4;      // one split half of one operand chunk: 16 KiB
 constexpr int kSmemBytes = 4 * kOpBytes + 1024;   // A hi/lo, B hi/lo, + alignment slack
-constexpr unsigned long long kWaitNs = 1000000000ull;
 
 __device__ int g_tc_err = 0;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-__device__ __forceinline__ uint32_t to_tf32(float a) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(a));
-  return r;
-}
-
-// byte offset of element (row r, k) in a K-major no-swizzle chunk of 128 rows
-// x 32 k: core matrix (k/4, r/8) of 8 rows x 16 bytes; K-adjacent core
-// matrices are kLbo apart, row-group-adjacent ones 128 bytes apart.
-constexpr uint32_t kSbo = 128;
-constexpr uint32_t kLbo = (kTile / 8) * 128;  // 2048
-__device__ __forceinline__ uint32_t kmaj_off(int r, int k) {
-  return (uint32_t)((k >> 2) * kLbo + (r >> 3) * kSbo + (r & 7) * 16 + (k & 3) * 4);
-}
-
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((addr >> 4) & 0x3FFF);
-  d |= (uint64_t)((kLbo >> 4) & 0x3FFF) << 16;
-  d |= (uint64_t)((kSbo >> 4) & 0x3FFF) << 32;
-  d |= (uint64_t)1 << 46;  // descriptor version (sm_100)
-  // base offset 0, LBO mode 0, layout type 0 (no swizzle)
-  return d;
-}
-
-// kind::tf32, D = F32, A = B = TF32, both K-major, M = 128, N = 128
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(kTile >> 3) << 17) |
-                            ((uint32_t)(kTile >> 4) << 24);
-
-__device__ __forceinline__ void mma_tf32(uint32_t dtm, uint64_t ad, uint64_t bd, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtm),
-      "l"(ad), "l"(bd), "r"(kIdesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t a = smem_u32(bar);
-  unsigned long long t0 = 0;
-  for (uint32_t it = 0;; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred P1;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
-        "selp.b32 %0, 1, 0, P1;\n\t}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    if (it == 0) t0 = t;
-    else if (t - t0 > kWaitNs || it > (1u << 26)) return false;
-  }
-}
 
 __global__ void __launch_bounds__(kThreads) k_gemm_3xtf32(int N, float alpha, const float* __restrict__ A,
                                                            const float* __restrict__ B, float beta, float* C) {
