@@ -401,15 +401,28 @@ __global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const in
   uint32_t parity = 0;
   // phase 1
   for (int k0 = 0; k0 < n; k0 += kChunk) {
-    for (int e = tid; e < kTile * kChunk; e += kThreads) {
-      const int r = e & (kTile - 1), c = e >> 7, l = k0 + c;  // A operands: (row r, k = l), column-major source
-      const bool in = r < n && l < n;
-      put_split(sAh, sAl, kmaj_off(r, c), in ? Ak[r + (int64_t)l * n] : 0.0f);
-      put_split(sSh, sSl, kmaj_off(r, c), in ? Sk[r + (int64_t)l * n] : 0.0f);
+    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+      const int r = e & (kTile - 1), c = (e >> 7) * 4;  // A operands: (row r, k = k0 + c .. +3), column-major source
+      float a[4], b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int l = k0 + c + q;
+        const bool in = r < n && l < n;
+        a[q] = in ? Ak[r + (int64_t)l * n] : 0.0f;
+        b[q] = in ? Sk[r + (int64_t)l * n] : 0.0f;
+      }
+      put_split4(sAh, sAl, kmaj_off(r, c), a[0], a[1], a[2], a[3]);
+      put_split4(sSh, sSl, kmaj_off(r, c), b[0], b[1], b[2], b[3]);
     }
-    for (int e = tid; e < kTile * kChunk; e += kThreads) {
-      const int c = e & (kChunk - 1), j = e >> 5, l = k0 + c;  // B operand X(l, j): row j, k = l
-      put_split(sBh, sBl, kmaj_off(j, c), (j < n && l < n) ? Xk[l + (int64_t)j * n] : 0.0f);
+    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+      const int c = (e & (kChunk / 4 - 1)) * 4, j = e >> 3;  // B operand X(l, j): row j, k = l
+      float x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int l = k0 + c + q;
+        x[q] = (j < n && l < n) ? Xk[l + (int64_t)j * n] : 0.0f;
+      }
+      put_split4(sBh, sBl, kmaj_off(j, c), x[0], x[1], x[2], x[3]);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -431,17 +444,34 @@ __global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const in
     uint32_t v[32];
     tmem_ld32(acc1 + lane_base + (uint32_t)k0, v);  // TMP(row, k0 .. k0+31)
 #pragma unroll
-    for (int c = 0; c < kChunk; ++c)
-      put_split(sAh, sAl, kmaj_off(row, c), (row < n && k0 + c < n) ? __uint_as_float(v[c]) : 0.0f);
-    for (int e = tid; e < kTile * kChunk; e += kThreads) {
-      const int r = e & (kTile - 1), c = e >> 7, l = k0 + c;  // -X(r, l) as an A operand
-      put_split(sSh, sSl, kmaj_off(r, c), (r < n && l < n) ? -Xk[r + (int64_t)l * n] : 0.0f);
+    for (int c = 0; c < kChunk; c += 4) {
+      float t[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) t[q] = (row < n && k0 + c + q < n) ? __uint_as_float(v[c + q]) : 0.0f;
+      put_split4(sAh, sAl, kmaj_off(row, c), t[0], t[1], t[2], t[3]);
     }
-    for (int e = tid; e < kTile * kChunk; e += kThreads) {
-      const int c = e & (kChunk - 1), j = e >> 5, l = k0 + c;  // B_k(l, j), T_k(l, j): row j, k = l
-      const bool in = j < n && l < n;
-      put_split(sBh, sBl, kmaj_off(j, c), in ? Bk[l + (int64_t)j * n] : 0.0f);
-      put_split(sTh, sTl, kmaj_off(j, c), in ? Tk[l + (int64_t)j * n] : 0.0f);
+    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+      const int r = e & (kTile - 1), c = (e >> 7) * 4;  // -X(r, l) as an A operand
+      float x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int l = k0 + c + q;
+        x[q] = (r < n && l < n) ? -Xk[r + (int64_t)l * n] : 0.0f;
+      }
+      put_split4(sSh, sSl, kmaj_off(r, c), x[0], x[1], x[2], x[3]);
+    }
+    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+      const int c = (e & (kChunk / 4 - 1)) * 4, j = e >> 3;  // B_k(l, j), T_k(l, j): row j, k = l
+      float b[4], t[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int l = k0 + c + q;
+        const bool in = j < n && l < n;
+        b[q] = in ? Bk[l + (int64_t)j * n] : 0.0f;
+        t[q] = in ? Tk[l + (int64_t)j * n] : 0.0f;
+      }
+      put_split4(sBh, sBl, kmaj_off(j, c), b[0], b[1], b[2], b[3]);
+      put_split4(sTh, sTl, kmaj_off(j, c), t[0], t[1], t[2], t[3]);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");

@@ -229,9 +229,16 @@ template <typename V>
 static V* upload(Common& cm, DeviceMem& mem, const std::vector<double>& h, int64_t len) {
   V* d = mem.alloc<V>(len);
   if (len > 0) {
-    std::vector<V> t(h.begin(), h.begin() + len);
-    cm.to_dev(d, t.data(), sizeof(V) * len);
-    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+    if constexpr (std::is_same<V, double>::value) {
+      cm.to_dev(d, h.data(), sizeof(V) * len);
+      HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+    } else {
+      std::vector<V> t(len);
+#pragma omp parallel for schedule(static) num_threads(host_threads(len))
+      for (int64_t i = 0; i < len; ++i) t[i] = (V)h[i];
+      cm.to_dev(d, t.data(), sizeof(V) * len);
+      HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+    }
   }
   return d;
 }
@@ -269,6 +276,26 @@ void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode) {
 
 // ELL copy of a CSR matrix: only for short rows (width <= 16) whose padding
 // stays within 25% of the nonzeros.
+// Scatter of the device CSR into a padded copy: row r's entry k goes to
+// base(r) + k * stride (ELL: base = r, stride = rows; SELL-32: base =
+// sptr[r / 32] + r % 32, stride = 32).  The padding was zeroed beforehand.
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_pad_copy(int rows, const int* __restrict__ ptr, const int* __restrict__ col,
+                                                     const V* __restrict__ val, const int* __restrict__ sptr,
+                                                     int stride, int* __restrict__ pcol, V* __restrict__ pval) {
+  const int r = blockIdx.x * kBlock + threadIdx.x;
+  if (r >= rows) return;
+  const int64_t base = sptr ? (int64_t)sptr[r >> 5] + (r & 31) : (int64_t)r;
+  const int b = ptr[r], e = ptr[r + 1];
+  for (int k = b; k < e; ++k) {
+    const int64_t j = base + (int64_t)(k - b) * stride;
+    pcol[j] = col[k];
+    pval[j] = val[k];
+  }
+}
+
+// ELL copy of a CSR matrix, built on the device from its CSR: only for
+// short rows (width <= 16) whose padding stays within 25% of the nonzeros.
 template <typename V>
 void Engine<V>::build_ell(const HCsr& h, DCsr<V>& d) {
   d.ell_w = 0;
@@ -277,22 +304,20 @@ void Engine<V>::build_ell(const HCsr& h, DCsr<V>& d) {
   for (int64_t r = 0; r < h.rows; ++r) w = std::max(w, h.ptr[r + 1] - h.ptr[r]);
   const int64_t total = (int64_t)w * h.rows;
   if (w > 16 || total > (int64_t)(1.25 * h.nnz()) + 64 || total > INT32_MAX) return;
-  std::vector<int> ecol(total, 0);
-  std::vector<double> evalv(total, 0.0);
-  for (int64_t r = 0; r < h.rows; ++r)
-    for (int k = h.ptr[r]; k < h.ptr[r + 1]; ++k) {
-      const int64_t j = (int64_t)(k - h.ptr[r]) * h.rows + r;
-      ecol[j] = h.col[k];
-      evalv[j] = h.val[k];
-    }
   int* dc = mem.alloc<int>(total);
-  cm.to_dev(dc, ecol.data(), sizeof(int) * total);
+  V* dv = mem.alloc<V>(total);
+  HPRQP_CUDA(cudaMemsetAsync(dc, 0, sizeof(int) * total, cm.stream));
+  HPRQP_CUDA(cudaMemsetAsync(dv, 0, sizeof(V) * total, cm.stream));
+  k_pad_copy<V><<<(int)((h.rows + kBlock - 1) / kBlock), kBlock, 0, cm.stream>>>((int)h.rows, d.ptr, d.col, d.val,
+                                                                                  nullptr, (int)h.rows, dc, dv);
+  HPRQP_LAUNCH_CHECK();
   d.ecol = dc;
-  d.evalv = upload<V>(cm, mem, evalv, total);
+  d.evalv = dv;
   d.ell_w = w;
 }
 
-// SELL-32 copy of a CSR matrix; skipped when padding would exceed 50%.
+// SELL-32 copy of a CSR matrix, built on the device from its CSR; skipped
+// when padding would exceed 50%.
 template <typename V>
 void Engine<V>::build_sell(const HCsr& h, DCsr<V>& d) {
   d.sell_len = 0;
@@ -306,23 +331,19 @@ void Engine<V>::build_sell(const HCsr& h, DCsr<V>& d) {
   }
   const int64_t total = sptr[ns];
   if (total > (int64_t)(1.5 * h.nnz()) + 64 || total > INT32_MAX) return;
-  std::vector<int> scol(total, 0);
-  std::vector<double> sval(total, 0.0);
-  for (int64_t r = 0; r < h.rows; ++r) {
-    const int64_t base = sptr[r / 32] + (r % 32);
-    for (int k = h.ptr[r]; k < h.ptr[r + 1]; ++k) {
-      const int64_t j = base + 32 * (int64_t)(k - h.ptr[r]);
-      scol[j] = h.col[k];
-      sval[j] = h.val[k];
-    }
-  }
   int* dsp = mem.alloc<int>(ns + 1);
   int* dsc = mem.alloc<int>(total);
+  V* dsv = mem.alloc<V>(total);
   cm.to_dev(dsp, sptr.data(), sizeof(int) * (ns + 1));
-  cm.to_dev(dsc, scol.data(), sizeof(int) * total);
+  HPRQP_CUDA(cudaMemsetAsync(dsc, 0, sizeof(int) * total, cm.stream));
+  HPRQP_CUDA(cudaMemsetAsync(dsv, 0, sizeof(V) * total, cm.stream));
+  k_pad_copy<V><<<(int)((h.rows + kBlock - 1) / kBlock), kBlock, 0, cm.stream>>>((int)h.rows, d.ptr, d.col, d.val,
+                                                                                  dsp, 32, dsc, dsv);
+  HPRQP_LAUNCH_CHECK();
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));  // sptr staging buffer
   d.sptr = dsp;
   d.scol = dsc;
-  d.sval = upload<V>(cm, mem, sval, total);
+  d.sval = dsv;
   d.sell_len = total;
 }
 

@@ -69,27 +69,23 @@ __global__ void __launch_bounds__(kThreads) k_gemm_3xtf32(int N, float alpha, co
   bool first = true;
   for (int k0 = 0; k0 < N; k0 += kChunk) {
     // stage A[i0 + r, k0 + k] and B[k0 + k, j0 + c] (zero outside the matrix)
-    for (int e = tid; e < kTile * kChunk; e += kThreads) {
-      // A is column-major: consecutive threads take consecutive rows
-      const int r = e & (kTile - 1), k = e >> 7;
+    // A is column-major: consecutive threads take consecutive rows, 4 k each
+    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+      const int r = e & (kTile - 1), k = (e >> 7) * 4;
       const int gi = i0 + r, gk = k0 + k;
-      const float a = (gi < N && gk < N) ? __ldg(A + (size_t)gk * N + gi) : 0.0f;
-      const uint32_t ah = to_tf32(a);
-      const uint32_t al = to_tf32(a - __uint_as_float(ah));
-      const uint32_t off = kmaj_off(r, k);
-      *(uint32_t*)(sAh + off) = ah;
-      *(uint32_t*)(sAl + off) = al;
+      float a[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) a[q] = (gi < N && gk + q < N) ? __ldg(A + (size_t)(gk + q) * N + gi) : 0.0f;
+      put_split4(sAh, sAl, kmaj_off(r, k), a[0], a[1], a[2], a[3]);
     }
-    for (int e = tid; e < kTile * kChunk; e += kThreads) {
-      // B[k, j] with k contiguous in memory: consecutive threads take consecutive k
-      const int k = e & (kChunk - 1), c = e >> 5;
+    // B[k, j] with k contiguous in memory: 4 consecutive k of one column each
+    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+      const int k = (e & (kChunk / 4 - 1)) * 4, c = e >> 3;
       const int gk = k0 + k, gj = j0 + c;
-      const float b = (gk < N && gj < N) ? __ldg(B + (size_t)gj * N + gk) : 0.0f;
-      const uint32_t bh = to_tf32(b);
-      const uint32_t bl = to_tf32(b - __uint_as_float(bh));
-      const uint32_t off = kmaj_off(c, k);
-      *(uint32_t*)(sBh + off) = bh;
-      *(uint32_t*)(sBl + off) = bl;
+      float b[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) b[q] = (gk + q < N && gj < N) ? __ldg(B + (size_t)gj * N + gk + q) : 0.0f;
+      put_split4(sBh, sBl, kmaj_off(c, k), b[0], b[1], b[2], b[3]);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();

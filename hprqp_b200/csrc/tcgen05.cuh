@@ -92,6 +92,24 @@ __device__ __forceinline__ void put_split(unsigned char* hi, unsigned char* lo, 
   *(uint32_t*)(lo + off) = to_tf32(a - __uint_as_float(h));
 }
 
+// the same for 4 consecutive k of one row (off 16-byte aligned): one
+// 16-byte store per half, so a warp writing 32 consecutive rows fills 512
+// contiguous bytes without bank conflicts
+__device__ __forceinline__ void put_split4(unsigned char* hi, unsigned char* lo, uint32_t off, float a0, float a1,
+                                           float a2, float a3) {
+  uint4 h, l;
+  h.x = to_tf32(a0);
+  h.y = to_tf32(a1);
+  h.z = to_tf32(a2);
+  h.w = to_tf32(a3);
+  l.x = to_tf32(a0 - __uint_as_float(h.x));
+  l.y = to_tf32(a1 - __uint_as_float(h.y));
+  l.z = to_tf32(a2 - __uint_as_float(h.z));
+  l.w = to_tf32(a3 - __uint_as_float(h.w));
+  *(uint4*)(hi + off) = h;
+  *(uint4*)(lo + off) = l;
+}
+
 // 3xTF32 product of one staged K chunk into the accumulator at TMEM column
 // `dtm`: D (+)= Alo*Bhi + Ahi*Blo + Ahi*Bhi for the chunk's 4 k-steps.
 // `first` starts the accumulation (D = ...) with the chunk's first MMA.
