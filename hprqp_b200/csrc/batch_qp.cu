@@ -359,7 +359,9 @@ __device__ int g_bqp_err = 0;
 constexpr int kQapTcSmem = 8 * tc::kOpBytes + 1024;
 constexpr uint32_t kQapTcCols = 512;  // acc1, acc2, acc3 (128 columns each), power of two
 
-__global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const int64_t* off, const unsigned char* on,
+constexpr int kQapTcThreads = 256;  // 8 warps: two warp groups share the TMEM lanes by column halves
+
+__global__ void __launch_bounds__(kQapTcThreads) k_qap_tc(const int* qn, const int64_t* off, const unsigned char* on,
                                                          const float* __restrict__ QA, const float* __restrict__ QB,
                                                          const float* __restrict__ QS, const float* __restrict__ QT,
                                                          const float* X, float* Y) {
@@ -397,11 +399,12 @@ __global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const in
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tm = tmem_base, acc1 = tm, acc2 = tm + 128, acc3 = tm + 256;
-  const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+  const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;  // warp w reads TMEM lanes 32 (w % 4) ..
+  const int half = warp >> 2;                                      // ... and column half w / 4
   uint32_t parity = 0;
   // phase 1
   for (int k0 = 0; k0 < n; k0 += kChunk) {
-    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
       const int r = e & (kTile - 1), c = (e >> 7) * 4;  // A operands: (row r, k = k0 + c .. +3), column-major source
       float a[4], b[4];
 #pragma unroll
@@ -414,7 +417,7 @@ __global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const in
       put_split4(sAh, sAl, kmaj_off(r, c), a[0], a[1], a[2], a[3]);
       put_split4(sSh, sSl, kmaj_off(r, c), b[0], b[1], b[2], b[3]);
     }
-    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
       const int c = (e & (kChunk / 4 - 1)) * 4, j = e >> 3;  // B operand X(l, j): row j, k = l
       float x[4];
 #pragma unroll
@@ -439,18 +442,19 @@ __global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const in
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   // phase 2
-  const int row = warp * 32 + (tid & 31);
+  const int row = (warp & 3) * 32 + (tid & 31);
   for (int k0 = 0; k0 < n && !s_fail; k0 += kChunk) {
-    uint32_t v[32];
-    tmem_ld32(acc1 + lane_base + (uint32_t)k0, v);  // TMP(row, k0 .. k0+31)
+    uint32_t v[16];
+    const int cb = half * 16;  // this warp group's 16 of the chunk's 32 columns
+    tmem_ld16(acc1 + lane_base + (uint32_t)(k0 + cb), v);  // TMP(row, k0 + cb .. +15)
 #pragma unroll
-    for (int c = 0; c < kChunk; c += 4) {
+    for (int c = 0; c < 16; c += 4) {
       float t[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) t[q] = (row < n && k0 + c + q < n) ? __uint_as_float(v[c + q]) : 0.0f;
-      put_split4(sAh, sAl, kmaj_off(row, c), t[0], t[1], t[2], t[3]);
+      for (int q = 0; q < 4; ++q) t[q] = (row < n && k0 + cb + c + q < n) ? __uint_as_float(v[c + q]) : 0.0f;
+      put_split4(sAh, sAl, kmaj_off(row, cb + c), t[0], t[1], t[2], t[3]);
     }
-    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
       const int r = e & (kTile - 1), c = (e >> 7) * 4;  // -X(r, l) as an A operand
       float x[4];
 #pragma unroll
@@ -460,7 +464,7 @@ __global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const in
       }
       put_split4(sSh, sSl, kmaj_off(r, c), x[0], x[1], x[2], x[3]);
     }
-    for (int e = tid; e < kTile * kChunk / 4; e += kThreads) {
+    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
       const int c = (e & (kChunk / 4 - 1)) * 4, j = e >> 3;  // B_k(l, j), T_k(l, j): row j, k = l
       float b[4], t[4];
 #pragma unroll
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(tc::kThreads) k_qap_tc(const int* qn, const in
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   if (!s_fail) {
-    for (int c0 = 0; c0 < kTile; c0 += 32) {
+    for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
       uint32_t a3[32], a2[32];
       tmem_ld32(acc3 + lane_base + (uint32_t)c0, a3);
       tmem_ld32(acc2 + lane_base + (uint32_t)c0, a2);
@@ -766,7 +770,7 @@ struct Engine {
   void qmap(const V* xin, V* yout, const unsigned char* mk) {
     if constexpr (std::is_same<V, float>::value) {
       if (use_tc) {
-        k_qap_tc<<<B, tc::kThreads, kQapTcSmem, st>>>(qn, off, mk, QA, QB, QS, QT, xin, yout);
+        k_qap_tc<<<B, kQapTcThreads, kQapTcSmem, st>>>(qn, off, mk, QA, QB, QS, QT, xin, yout);
         check();
         return;
       }
