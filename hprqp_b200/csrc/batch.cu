@@ -317,7 +317,7 @@ struct BEngine {
   int B;
   int64_t N, R;
   DCsr<V> L, LT;
-  int tprL = 8;
+  int tprL = 8, tprLT = 4;
   V *x, *x_hat, *x_bar, *dx, *w, *w_bar, *dw, *z_bar, *c, *ltemp, *Qv, *pz, *pq;
   double *last_x, *last_w;
   int *inst_n, *inst_r;
@@ -404,32 +404,63 @@ struct BEngine {
     tn.inst_tiles = up(it);
     partials = mem.alloc<double>((int64_t)tn.count * kMaxK);
     for (double** o : {&out_res, &out_mn_cur, &out_mn_last, &out_sig, &out_tmp}) *o = mem.alloc<double>((int64_t)B * kMaxK);
+    autotune();
   }
 
   template <typename Epi>
-  void rows_L(const V* xin, const Epi& e, const unsigned char* mask) {
-    const Inst I{inst_r, mask};
-    const CsrSrc<V, V> s{L.ptr, L.col, L.val, xin};
-    const long long threads = (long long)R * tprL;
+  void rows_csr(const DCsr<V>& M, const int* inst, int tpr, const V* xin, const Epi& e, const unsigned char* mask) {
+    const Inst I{inst, mask};
+    const CsrSrc<V, V> s{M.ptr, M.col, M.val, xin};
+    const long long threads = (long long)M.rows * tpr;
     const int grid = (int)((threads + kBlock - 1) / kBlock);
-    switch (tprL) {
-      case 2: k_rows<2, V><<<grid, kBlock, 0, st>>>((int)R, I, s, e); break;
-      case 4: k_rows<4, V><<<grid, kBlock, 0, st>>>((int)R, I, s, e); break;
-      case 8: k_rows<8, V><<<grid, kBlock, 0, st>>>((int)R, I, s, e); break;
-      case 16: k_rows<16, V><<<grid, kBlock, 0, st>>>((int)R, I, s, e); break;
-      default: k_rows<32, V><<<grid, kBlock, 0, st>>>((int)R, I, s, e); break;
+    switch (tpr) {
+      case 1: k_rows<1, V><<<grid, kBlock, 0, st>>>(M.rows, I, s, e); break;
+      case 2: k_rows<2, V><<<grid, kBlock, 0, st>>>(M.rows, I, s, e); break;
+      case 4: k_rows<4, V><<<grid, kBlock, 0, st>>>(M.rows, I, s, e); break;
+      case 8: k_rows<8, V><<<grid, kBlock, 0, st>>>(M.rows, I, s, e); break;
+      case 16: k_rows<16, V><<<grid, kBlock, 0, st>>>(M.rows, I, s, e); break;
+      default: k_rows<32, V><<<grid, kBlock, 0, st>>>(M.rows, I, s, e); break;
     }
     launches++;
     HPRQP_LAUNCH_CHECK();
   }
   template <typename Epi>
-  void rows_LT(const V* xin, const Epi& e) {
-    const Inst I{inst_n, on};
-    const CsrSrc<V, V> s{LT.ptr, LT.col, LT.val, xin};
-    const int grid = (int)((N * 4 + kBlock - 1) / kBlock);
-    k_rows<4, V><<<grid, kBlock, 0, st>>>((int)N, I, s, e);
-    launches++;
-    HPRQP_LAUNCH_CHECK();
+  void rows_L(const V* xin, const Epi& e, const unsigned char* mask) { rows_csr(L, inst_r, tprL, xin, e, mask); }
+  template <typename Epi>
+  void rows_LT(const V* xin, const Epi& e) { rows_csr(LT, inst_n, tprLT, xin, e, on); }
+  // Row-schedule autotuner for this instance class: threads per row of the
+  // A_d and A_d' products, the fastest of 3 timed rounds of 3 launches each
+  // (all instances active, plain products into scratch).
+  void autotune() {
+    unsigned char* all = mem.alloc<unsigned char>(B);
+    HPRQP_CUDA(cudaMemset(all, 1, B));
+    cudaEvent_t a, b;
+    HPRQP_CUDA(cudaEventCreate(&a));
+    HPRQP_CUDA(cudaEventCreate(&b));
+    auto tune = [&](const DCsr<V>& M, const int* inst, const V* xin, V* out, std::initializer_list<int> cands) {
+      float best = 1e30f;
+      int bt = *cands.begin();
+      for (int t : cands) {
+        rows_csr(M, inst, t, xin, EpiStoreB<V>{out, nullptr}, all);
+        float tb = 1e30f;
+        for (int r = 0; r < 3; ++r) {
+          HPRQP_CUDA(cudaEventRecord(a, st));
+          for (int q = 0; q < 3; ++q) rows_csr(M, inst, t, xin, EpiStoreB<V>{out, nullptr}, all);
+          HPRQP_CUDA(cudaEventRecord(b, st));
+          HPRQP_CUDA(cudaEventSynchronize(b));
+          float ms = 0;
+          HPRQP_CUDA(cudaEventElapsedTime(&ms, a, b));
+          tb = std::min(tb, ms);
+        }
+        if (tb < best) { best = tb; bt = t; }
+      }
+      return bt;
+    };
+    tprL = tune(L, inst_r, pz, ltemp, {2, 4, 8, 16, 32});
+    tprLT = tune(LT, inst_n, ltemp, Qv, {1, 2, 4, 8, 16});
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    launches = 0;
   }
   // segmented reduction with the A_d' product as the row source, then fold
   template <int K, unsigned MM, typename Epi, typename Fin = NoFinB>

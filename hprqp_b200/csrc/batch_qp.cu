@@ -744,6 +744,36 @@ struct Engine {
     for (double** o : {&out_rn, &out_rm, &out_mn_cur, &out_mn_last, &out_mm_cur, &out_mm_last, &out_sn, &out_sm,
                        &out_tmp})
       *o = mem.alloc<double>((int64_t)B * kMaxK);
+    // row-schedule autotuner for the A rows (n_k entries each): threads per
+    // row, the fastest of 3 timed rounds of 3 launches
+    {
+      unsigned char* all = mem.alloc<unsigned char>(B);
+      HPRQP_CUDA(cudaMemset(all, 1, B));
+      cudaEvent_t a, b;
+      HPRQP_CUDA(cudaEventCreate(&a));
+      HPRQP_CUDA(cudaEventCreate(&b));
+      float best = 1e30f;
+      for (int t : {4, 8, 16, 32}) {
+        rows_A_t(t, x, Plain<EpiStore<V>>{{y, 1.0}}, all);
+        float tb = 1e30f;
+        for (int r = 0; r < 3; ++r) {
+          HPRQP_CUDA(cudaEventRecord(a, st));
+          for (int q = 0; q < 3; ++q) rows_A_t(t, x, Plain<EpiStore<V>>{{y, 1.0}}, all);
+          HPRQP_CUDA(cudaEventRecord(b, st));
+          HPRQP_CUDA(cudaEventSynchronize(b));
+          float ms = 0;
+          HPRQP_CUDA(cudaEventElapsedTime(&ms, a, b));
+          tb = std::min(tb, ms);
+        }
+        if (tb < best) {
+          best = tb;
+          tprA = t;
+        }
+      }
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+      launches = 0;
+    }
     if constexpr (std::is_same<V, float>::value) {
       const char* e = std::getenv("HPRQP_QAP_TC");
       use_tc = nmax <= tc::kTile && !(e && e[0] == '0');
@@ -791,11 +821,13 @@ struct Engine {
     rows_n(CsrSrc<V, V>{AT.ptr, AT.col, AT.val, xin}, e, mk);
   }
   template <typename Epi>
-  void rows_A(const V* xin, const Epi& e, const unsigned char* mk) {
+  void rows_A(const V* xin, const Epi& e, const unsigned char* mk) { rows_A_t(tprA, xin, e, mk); }
+  template <typename Epi>
+  void rows_A_t(int t, const V* xin, const Epi& e, const unsigned char* mk) {
     const Gate G{inst_m, mk};
     const CsrSrc<V, V> src{A.ptr, A.col, A.val, xin};
-    const int grid = (int)((M * tprA + kBlock - 1) / kBlock);
-    switch (tprA) {
+    const int grid = (int)((M * t + kBlock - 1) / kBlock);
+    switch (t) {
       case 2: k_rows<2, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;
       case 4: k_rows<4, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;
       case 8: k_rows<8, V><<<grid, kBlock, 0, st>>>((int)M, G, src, e); break;

@@ -358,7 +358,12 @@ void Engine<V>::mat_rows(const DCsr<V>& M, const V* xin, const Epi& e) {
 // Fused product + reduction on M's format (FP64 accumulation).
 template <int K, unsigned MM, typename V, typename Epi, typename Fin = NoFin>
 static void mat_reduce(Common& cm, const DCsr<V>& M, const V* xin, const Epi& e, double* out, const Fin& fin = Fin()) {
-  if (M.ell) reduce<K, MM, double>(cm, 1, M.rows, EllSrc<V, V>{M.ecol, M.evalv, xin, M.rows, M.ell_w}, e, out, fin);
+  if (M.ell) {  // 4 rows per thread in flight
+    const int grid = reduce_grid(M.rows, 1, cm.reduce_cap);
+    launch(cm, k_ell_reduce<4, K, MM, double, V, Epi, Fin>, grid, kBlock, M.rows,
+           EllSrc<V, V>{M.ecol, M.evalv, xin, M.rows, M.ell_w}, e, cm.rws, out, fin);
+    return;
+  }
   else if (M.sell) reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
   else reduce<K, MM, double>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, e, out, fin);
 }
@@ -1025,6 +1030,17 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   }
   if (cm.pow_persistent && !is_qap && power_persistent(ca.on, cq.on, tol, max_it, lamA_out, lamQ_out, itA, itQ))
     return;
+  // the chained steps use ELL wherever the matrix has an ELL copy: its
+  // reduction keeps 4 rows per thread in flight (k_ell_reduce)
+  auto ellp = [&](const DCsr<V>& M) {
+    DCsr<V> d = M;
+    if (cm.pow_prefer_ell && d.ell_w > 0) {
+      d.ell = true;
+      d.sell = false;
+    }
+    return d;
+  };
+  const DCsr<V> pA = ellp(A), pAT = ellp(AT), pQ = ellp(Q), pL = ellp(L), pLT = ellp(LT);
   auto step = [&](const Chain& c, cudaStream_t st, int k) {
     use(c, st);
     V* zc = (k & 1) ? c.z1 : c.z0;
@@ -1032,17 +1048,17 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     double* zz = c.scal + 2;
     const PowerFin fin{c.log, k};
     if (c.which == 0) {  // A A' (power_iteration_A)
-      mat_rows(AT, zc, EpiStoreInvNorm<V>{c.t, zz});
-      mat_reduce<3, 0u>(cm, A, c.t, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
+      mat_rows(pAT, zc, EpiStoreInvNorm<V>{c.t, zz});
+      mat_reduce<3, 0u>(cm, pA, c.t, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
     } else if (is_lasso) {
-      mat_rows(L, zc, EpiStoreInvNorm<V>{ltemp2, zz});
-      mat_reduce<3, 0u>(cm, LT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
+      mat_rows(pL, zc, EpiStoreInvNorm<V>{ltemp2, zz});
+      mat_reduce<3, 0u>(cm, pLT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
     } else if (is_qap) {
       elem(cm, n, ScaleInvNorm<V>{c.t, zc, zz});
       qap_apply(c.t, zn);
       reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
     } else {
-      mat_reduce<3, 0u>(cm, Q, zc, EpiPowerFused<V>{zc, zn, zz, true}, c.scal + 1, fin);
+      mat_reduce<3, 0u>(cm, pQ, zc, EpiPowerFused<V>{zc, zn, zz, true}, c.scal + 1, fin);
     }
     restore();
   };

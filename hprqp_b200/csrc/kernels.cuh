@@ -210,6 +210,41 @@ __global__ void __launch_bounds__(kBlock) k_row_reduce(int nrows, Src src, Epi e
   grid_finish<K, MaxMask, Fin>(r, ws, out, fin);
 }
 
+// The same fused product + reduction for an ELL matrix with R rows per
+// thread in flight (rows r0 + q * stride, so a warp's loads stay
+// coalesced): the col -> x gathers of R rows overlap instead of running one
+// row after another as in the grid-stride loop above.
+template <int R, int K, unsigned MaxMask, typename Acc, typename V, typename Epi, typename Fin = NoFin>
+__global__ void __launch_bounds__(kBlock) k_ell_reduce(int nrows, EllSrc<V, V> src, Epi epi, ReduceWs ws,
+                                                       double* out, Fin fin = Fin()) {
+  pdl_enter();
+  double r[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) r[k] = 0.0;
+  const int stride = (int)(gridDim.x * kBlock);
+  for (int r0 = (int)(blockIdx.x * kBlock + threadIdx.x); r0 < nrows; r0 += R * stride) {
+    Acc acc[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) acc[q] = Acc(0);
+    for (int k = 0; k < src.w; ++k) {
+      const int* c = src.col + (size_t)k * src.rows;
+      const V* v = src.val + (size_t)k * src.rows;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int row = r0 + q * stride;
+        if (row < nrows) acc[q] = fma((Acc)__ldg(v + row), (Acc)__ldg(src.x + __ldg(c + row)), acc[q]);
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int row = r0 + q * stride;
+      if (row < nrows) epi(row, acc[q], r);
+    }
+  }
+  block_reduce<K, MaxMask>(r);
+  grid_finish<K, MaxMask, Fin>(r, ws, out, fin);
+}
+
 // ---------------------------------------------------------------------------
 // Epilogues of the iteration passes
 // ---------------------------------------------------------------------------
