@@ -47,7 +47,6 @@ const double kInf = std::numeric_limits<double>::infinity();
 constexpr int kTileRows = 1024;  // rows per reduction tile
 constexpr int kMaxK = 8;         // reduction slots
 constexpr int kPowWin = 16;      // power steps between host checks
-constexpr int kQapCols = 16;     // output columns per CTA of the Q-operator kernels
 constexpr int kStallChecks = 3;  // FP32 phase: evaluations without a 10% KKT gain before the switch
 constexpr int kStallMinIter = 300;
 
@@ -293,32 +292,94 @@ __global__ void k_each(int64_t len, F f) {
   if (i < len) f(i);
 }
 
-// Q operator, stage 1: TMP_k = A_k X_k for every active instance
-// (blockIdx.x = instance, blockIdx.y = block of kQapCols output columns).
-// Sums run over l in increasing order, accumulated in V.
+// Q operator on the CUDA cores, shared-memory tiled: one CTA computes a
+// 64 x 64 tile of one instance's output (blockIdx.x = instance,
+// blockIdx.y = tile), each thread a 4 x 4 block, with the K dimension
+// staged 16 at a time.  Every sum runs over l in increasing order (one FMA
+// per term, accumulated in V).
+//   stage 1: TMP_k = A_k X_k
+//   stage 2: Y_k = 2 TMP_k B_k - 2 S_k X_k - 2 X_k T_k, composed in the order
+//            of the single-instance operator (Y = 2 TMP B; Y += -2 S X;
+//            Y += -2 X T)
+constexpr int kQT = 64;   // output tile
+constexpr int kQK = 16;   // K chunk
+constexpr int kQMaxTiles = 4;  // tiles per side: n_k <= 256 on this path
+
+template <typename V, int P>
+__device__ __forceinline__ void qap_tile_products(int n, int i0, int j0, const V* const (&L)[P], const V* const (&R)[P],
+                                                  V (&acc)[P][4][4]) {
+  __shared__ V Ls[P][kQK][kQT];
+  __shared__ V Rs[P][kQK][kQT];
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+#pragma unroll
+  for (int p = 0; p < P; ++p)
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[p][a][b] = V(0);
+  for (int l0 = 0; l0 < n; l0 += kQK) {
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+#pragma unroll
+      for (int q = 0; q < (kQT * kQK) / 256; ++q) {
+        const int e = tid + 256 * q;
+        {  // left operand L(i, l), column-major: consecutive threads take consecutive i
+          const int ii = e & (kQT - 1), ll = e >> 6;
+          const int gi = i0 + ii, gl = l0 + ll;
+          Ls[p][ll][ii] = (gi < n && gl < n) ? L[p][gi + (int64_t)gl * n] : V(0);
+        }
+        {  // right operand R(l, j): consecutive threads take consecutive l
+          const int ll = e & (kQK - 1), jj = e >> 4;
+          const int gl = l0 + ll, gj = j0 + jj;
+          Rs[p][ll][jj] = (gl < n && gj < n) ? R[p][gl + (int64_t)gj * n] : V(0);
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ll = 0; ll < kQK; ++ll) {
+#pragma unroll
+      for (int p = 0; p < P; ++p) {
+        V a[4], b[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          a[q] = Ls[p][ll][ty * 4 + q];
+          b[q] = Rs[p][ll][tx * 4 + q];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) acc[p][u][v] = fma(a[u], b[v], acc[p][u][v]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
 template <typename V>
 __global__ void __launch_bounds__(256) k_qap_tmp(const int* qn, const int64_t* off, const unsigned char* on,
                                                  const V* __restrict__ QA, const V* X, V* TMP) {
   const int k = blockIdx.x;
   if (!on[k]) return;
   const int n = qn[k];
-  const int j0 = blockIdx.y * kQapCols;
-  if (j0 >= n) return;
+  const int nt = (n + kQT - 1) / kQT;
+  if ((int)blockIdx.y >= nt * nt) return;
+  const int i0 = (blockIdx.y % nt) * kQT, j0 = (blockIdx.y / nt) * kQT;
   const int64_t o = off[k];
-  const V* Ak = QA + o;
-  const V* Xk = X + o;
-  V* Tk = TMP + o;
-  const int jn = min(kQapCols, n - j0);
-  for (int e = threadIdx.x; e < n * jn; e += blockDim.x) {
-    const int i = e % n, j = j0 + e / n;
-    V s = V(0);
-    for (int l = 0; l < n; ++l) s = fma(Ak[i + (int64_t)l * n], Xk[l + (int64_t)j * n], s);
-    Tk[i + (int64_t)j * n] = s;
-  }
+  const V* const L[1] = {QA + o};
+  const V* const R[1] = {X + o};
+  V acc[1][4][4];
+  qap_tile_products<V, 1>(n, i0, j0, L, R, acc);
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+      if (i < n && j < n) TMP[o + i + (int64_t)j * n] = acc[0][u][v];
+    }
 }
 
-// stage 2: Y_k = 2 TMP_k B_k - 2 S_k X_k - 2 X_k T_k, in the order of the
-// single-instance operator (Y = 2 TMP B; Y += -2 S X; Y += -2 X T)
 template <typename V>
 __global__ void __launch_bounds__(256) k_qap_out(const int* qn, const int64_t* off, const unsigned char* on,
                                                  const V* __restrict__ QB, const V* __restrict__ QS,
@@ -326,25 +387,27 @@ __global__ void __launch_bounds__(256) k_qap_out(const int* qn, const int64_t* o
   const int k = blockIdx.x;
   if (!on[k]) return;
   const int n = qn[k];
-  const int j0 = blockIdx.y * kQapCols;
-  if (j0 >= n) return;
+  const int nt = (n + kQT - 1) / kQT;
+  if ((int)blockIdx.y >= nt * nt) return;
+  const int i0 = (blockIdx.y % nt) * kQT, j0 = (blockIdx.y / nt) * kQT;
   const int64_t o = off[k];
-  const V *Bk = QB + o, *Sk = QS + o, *Tk = QT + o, *Xk = X + o, *Pk = TMP + o;
-  V* Yk = Y + o;
-  const int jn = min(kQapCols, n - j0);
-  for (int e = threadIdx.x; e < n * jn; e += blockDim.x) {
-    const int i = e % n, j = j0 + e / n;
-    V a = V(0), b = V(0), c = V(0);
-    for (int l = 0; l < n; ++l) {
-      a = fma(Pk[i + (int64_t)l * n], Bk[l + (int64_t)j * n], a);
-      b = fma(Sk[i + (int64_t)l * n], Xk[l + (int64_t)j * n], b);
-      c = fma(Xk[i + (int64_t)l * n], Tk[l + (int64_t)j * n], c);
+  const V* const L[3] = {TMP + o, QS + o, X + o};
+  const V* const R[3] = {QB + o, X + o, QT + o};
+  V acc[3][4][4];
+  qap_tile_products<V, 3>(n, i0, j0, L, R, acc);
+  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+      if (i < n && j < n) {
+        V y = V(2) * acc[0][u][v];
+        y = fma(V(-2), acc[1][u][v], y);
+        y = fma(V(-2), acc[2][u][v], y);
+        Y[o + i + (int64_t)j * n] = y;
+      }
     }
-    V y = V(2) * a;
-    y = fma(V(-2), b, y);
-    y = fma(V(-2), c, y);
-    Yk[i + (int64_t)j * n] = y;
-  }
 }
 
 // FP32 phase: the whole Q operator of one instance (n_k <= 128) in one CTA
@@ -702,6 +765,7 @@ struct Engine {
   }
 
   Engine(const Family& F, cudaStream_t s_) : st(s_), B(F.B), N(F.N), M(F.M), nmax(F.nmax) {
+    if (nmax > kQT * kQMaxTiles) throw Error(HPRQP_E_ARG, "QP batch: QAP instances are limited to n <= 256");
     upload_csr(F.A, A);
     upload_csr(F.AT, AT);
     const double avg = F.M ? (double)F.A.nnz() / F.M : 1.0;
@@ -805,7 +869,8 @@ struct Engine {
         return;
       }
     }
-    const dim3 g(B, (nmax + kQapCols - 1) / kQapCols);
+    const int nt = (nmax + kQT - 1) / kQT;
+    const dim3 g(B, nt * nt);
     k_qap_tmp<V><<<g, 256, 0, st>>>(qn, off, mk, QA, xin, qtmp);
     check();
     k_qap_out<V><<<g, 256, 0, st>>>(qn, off, mk, QB, QS, QT, xin, qtmp, yout);
