@@ -205,13 +205,9 @@ def run_ours(args):
         td.init_process_group("nccl", timeout=timedelta(seconds=600))
         dist = td
 
-    def barrier_max(v):
-        if dist is None:
-            return v
-        import torch
-        t = torch.tensor([float(v)], device=f"cuda:{local_rank}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    def barrier_max(v):  # the job's time is the slowest rank's
+        from hprqp_b200.dist import max_over_ranks
+        return max_over_ranks(v, device=f"cuda:{local_rank}") if dist is not None else v
 
     from hprqp_b200 import HPRQP_parameters, Solver
     from hprqp_b200 import workloads as W
