@@ -47,7 +47,7 @@ void Common::init() {
   const char* rc = std::getenv("HPRQP_REDUCE_CAP");
   if (rc) reduce_cap = std::max(1, std::min(std::atoi(rc), kReduceGridLimit));
   const char* pel = std::getenv("HPRQP_POWER_ELL");
-  pow_prefer_ell = !(pel && pel[0] == '0');
+  pow_prefer_ell = pel && pel[0] == '1';
   const char* pc = std::getenv("HPRQP_POWER_CTAS_PER_SM");
   if (pc) pow_ctas_per_sm = std::atoi(pc);
 }
@@ -1030,8 +1030,9 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   }
   if (cm.pow_persistent && !is_qap && power_persistent(ca.on, cq.on, tol, max_it, lamA_out, lamQ_out, itA, itQ))
     return;
-  // the chained steps use ELL wherever the matrix has an ELL copy: its
-  // reduction keeps 4 rows per thread in flight (k_ell_reduce)
+  // HPRQP_POWER_ELL=1: the chained steps use ELL wherever the matrix has an
+  // ELL copy (its reduction keeps 4 rows per thread in flight); measured
+  // slower than the autotuned formats on the 700x700 grid (107 vs 97 ms)
   auto ellp = [&](const DCsr<V>& M) {
     DCsr<V> d = M;
     if (cm.pow_prefer_ell && d.ell_w > 0) {

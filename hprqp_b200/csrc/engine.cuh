@@ -74,7 +74,7 @@ struct Common {  // per-handle resources shared by the engines
   // the 700x700 grid (99 vs 112 ms); HPRQP_POWER_PERSISTENT=1 selects it
   bool pow_persistent = false;
   int reduce_cap = kMaxReduceGrid;  // CTAs of a grid-stride reduction (HPRQP_REDUCE_CAP)
-  bool pow_prefer_ell = true;
+  bool pow_prefer_ell = false;  // HPRQP_POWER_ELL=1: power sweeps on ELL copies
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;
   void init();
