@@ -378,6 +378,16 @@ void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& o) 
       for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], S.val.data() + S.ptr[i]);
       Q = std::move(S);
     }
+    finish_sparse(o, n);
+  }
+  int64_t nfree = 0;
+  for (int64_t i = 0; i < n; ++i) nfree += (hp.l[i] == -kInf && hp.u[i] == kInf);
+  o.noC = nfree > 0.8 * n;
+}
+
+void finish_sparse(Prepared& o, int64_t n) {
+  {
+    const HCsr& Q = o.Q;
     o.norm_b = norm_b_of(o.AL, o.AU, false);
     o.norm_c = norm2(o.c);
     // check_Q_diagonal on the scaled Q (src/utils.jl:827-855)
@@ -398,9 +408,15 @@ void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& o) 
     }
     o.Q_maxval = Q.nnz() ? *std::max_element(Q.val.begin(), Q.val.end()) : 0.0;
   }
-  int64_t nfree = 0;
-  for (int64_t i = 0; i < n; ++i) nfree += (hp.l[i] == -kInf && hp.u[i] == kInf);
-  o.noC = nfree > 0.8 * n;
 }
+
+void finish_common(const HostProblem& hp, Prepared& o) {
+  int64_t nfree = 0;
+  for (int64_t i = 0; i < hp.n; ++i) nfree += (hp.l[i] == -kInf && hp.u[i] == kInf);
+  o.noC = nfree > 0.8 * hp.n;
+}
+
+double norm_b_inf_org(const std::vector<double>& AL, const std::vector<double>& AU) { return norm_b_of(AL, AU, true); }
+double norm_inf(const std::vector<double>& v) { return norminf(v); }
 
 }  // namespace hprqp

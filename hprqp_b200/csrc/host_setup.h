@@ -11,6 +11,7 @@
 // scaled arrays are then uploaded to HBM.
 #pragma once
 
+#include <cuda_runtime.h>
 #include <stdint.h>
 
 #include <string>
@@ -57,6 +58,15 @@ struct Prepared {  // scaled problem + scaling info (Scaling_info_cpu)
 void load_problem(const hprqp_problem* pr, HostProblem& hp);
 // scaling! + check_Q_diagonal + the noC rule (src/algorithm.jl:1969-1974).
 void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& out);
+// The same for a sparse Q with the matrix scaling on the GPU (scale.cu):
+// bitwise the host result, with the scaled arrays copied back into `out`.
+void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared& out, cudaStream_t st);
+// the tails shared by both: norms, check_Q_diagonal and Q_maxval on the
+// scaled sparse Q; the noC rule
+void finish_sparse(Prepared& o, int64_t n);
+void finish_common(const HostProblem& hp, Prepared& o);
+double norm_b_inf_org(const std::vector<double>& AL, const std::vector<double>& AU);
+double norm_inf(const std::vector<double>& v);
 HCsr transpose(const HCsr& A);
 // Host threads for a row-parallel loop over `work` items: 1 below ~64k
 // items (a parallel region costs more than it saves there), else at most

@@ -1,0 +1,257 @@
+// scale.cu — scaling! for a sparse Q on the GPU (src/utils.jl:350-804, CPU
+// branch: 10 Ruiz passes on [Q; A], one Pock-Chambolle pass, Q symmetrised
+// afterwards).  The same arithmetic as the host restatement in
+// host_setup.cpp, expression by expression, so the result is bitwise the
+// host one: column maxima and sums are row sweeps of the transposes A' and
+// Q' (kept scaled side by side with A and Q), maxima are exact in any
+// order, sums run along each row in stored order, and the factors are
+// sqrt / reciprocal / multiply in the host's order.  The symmetrised
+// pattern and its index maps come from the host (the pattern does not
+// change under scaling); the values are merged on the device.  The scaled
+// arrays are copied back into the host Prepared record, from which the
+// engines upload their copies as before.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "common.cuh"
+#include "host_setup.h"
+
+namespace hprqp {
+namespace {
+
+constexpr int kT = 256;
+
+// per-row max |v| (mode 0) or sum |v| (mode 1), in stored order
+__global__ void k_row_abs(int rows, const int* __restrict__ ptr, const double* __restrict__ val, int mode,
+                          double* __restrict__ out) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i >= rows) return;
+  double x = 0.0;
+  for (int k = ptr[i]; k < ptr[i + 1]; ++k) x = mode == 0 ? fmax(x, fabs(val[k])) : x + fabs(val[k]);
+  out[i] = x;
+}
+
+// column factors: t = sqrt(max(ca, cq)) (Ruiz) or sqrt(ca + cq) (Pock-Chambolle),
+// 1 where that is 0; the running norm *= t; tinv = 1 / t
+__global__ void k_col_factors(int n, const double* ca, const double* cq, int mode, double* t, double* tinv,
+                              double* norm) {
+  const int j = blockIdx.x * kT + threadIdx.x;
+  if (j >= n) return;
+  double v = mode == 0 ? sqrt(fmax(ca[j], cq[j])) : sqrt(ca[j] + cq[j]);
+  if (v == 0.0) v = 1.0;
+  t[j] = v;
+  tinv[j] = 1.0 / v;
+  norm[j] *= v;
+}
+__global__ void k_row_factors(int m, const double* ra, double* t, double* tinv, double* norm) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i >= m) return;
+  double v = sqrt(ra[i]);
+  if (v == 0.0) v = 1.0;
+  t[i] = v;
+  tinv[i] = 1.0 / v;
+  norm[i] *= v;
+}
+
+// M <- diag(1/dr) M diag(1/dc): v = (1/dr_i) v, then v (1/dc_j); on the
+// transpose (trans = 1) row j, column i of the same entry
+__global__ void k_scale(int rows, const int* __restrict__ ptr, const int* __restrict__ col, double* val,
+                        const double* __restrict__ rinv, const double* __restrict__ cinv, int trans) {
+  const int r = blockIdx.x * kT + threadIdx.x;
+  if (r >= rows) return;
+  for (int k = ptr[r]; k < ptr[r + 1]; ++k) {
+    double v = val[k];
+    const int c = col[k];
+    if (trans) {
+      v = rinv[c] * v;
+      v = v * cinv[r];
+    } else {
+      v = rinv[r] * v;
+      v = v * cinv[c];
+    }
+    val[k] = v;
+  }
+}
+
+__global__ void k_scale_n(int n, const double* tc, double* c, double* l, double* u) {
+  const int j = blockIdx.x * kT + threadIdx.x;
+  if (j >= n) return;
+  c[j] /= tc[j];
+  l[j] *= tc[j];
+  u[j] *= tc[j];
+}
+__global__ void k_scale_m(int m, const double* tr, double* AL, double* AU) {
+  const int i = blockIdx.x * kT + threadIdx.x;
+  if (i >= m) return;
+  AL[i] /= tr[i];
+  AU[i] /= tr[i];
+}
+
+// S = (Q + Q') / 2 on the merged pattern: ia / ib index Q / Q' values (-1: absent)
+__global__ void k_sym(int nnz, const int* ia, const int* ib, const double* qv, const double* qtv, double* sv) {
+  const int p = blockIdx.x * kT + threadIdx.x;
+  if (p >= nnz) return;
+  const int a = ia[p], b = ib[p];
+  const double v = (a >= 0 && b >= 0) ? qv[a] + qtv[b] : (a >= 0 ? qv[a] : qtv[b]);
+  sv[p] = v / 2.0;
+}
+
+struct DevBuf {  // cudaMalloc'ed scratch freed at scope exit
+  std::vector<void*> p;
+  template <typename T>
+  T* get(int64_t n) {
+    void* q = nullptr;
+    HPRQP_CUDA(cudaMalloc(&q, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    p.push_back(q);
+    return (T*)q;
+  }
+  ~DevBuf() {
+    for (void* q : p) cudaFree(q);
+  }
+};
+
+inline int blocks(int64_t n) { return (int)((std::max<int64_t>(n, 1) + kT - 1) / kT); }
+
+}  // namespace
+
+void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared& o, cudaStream_t st) {
+  if (hp.Q_kind != HPRQP_Q_SPARSE) {
+    prepare_problem(hp, p, o);
+    return;
+  }
+  const int64_t n = hp.n, m = hp.m;
+  o = Prepared();
+  o.ruiz = p.use_Ruiz_scaling;
+  o.pc = p.use_Pock_Chambolle_scaling;
+  o.A = hp.A;
+  o.AT = hp.AT;
+  o.c = hp.c;
+  o.AL = hp.AL;
+  o.AU = hp.AU;
+  o.l = hp.l;
+  o.u = hp.u;
+  o.row_norm.assign(m, 1.0);
+  o.col_norm.assign(n, 1.0);
+  o.norm_b_org = m > 0 ? norm_b_inf_org(o.AL, o.AU) : 0.0;
+  o.norm_c_org = norm_inf(o.c);
+  const HCsr &Q = hp.Q, &QT = hp.QT;
+  // merged pattern of Q + Q' with index maps (the values come later)
+  std::vector<int> len(n, 0);
+  auto merge = [&](int64_t i, int* cols, int* ia, int* ib) {
+    int a = Q.ptr[i], b = QT.ptr[i], cnt = 0;
+    const int ae = Q.ptr[i + 1], be = QT.ptr[i + 1];
+    while (a < ae || b < be) {
+      const int ca = a < ae ? Q.col[a] : INT32_MAX;
+      const int cb = b < be ? QT.col[b] : INT32_MAX;
+      int xa = -1, xb = -1, cc;
+      if (ca == cb) { xa = a++; xb = b++; cc = ca; }
+      else if (ca < cb) { xa = a++; cc = ca; }
+      else { xb = b++; cc = cb; }
+      if (cols) {
+        cols[cnt] = cc;
+        ia[cnt] = xa;
+        ib[cnt] = xb;
+      }
+      ++cnt;
+    }
+    return cnt;
+  };
+#pragma omp parallel for schedule(static) num_threads(host_threads(n))
+  for (int64_t i = 0; i < n; ++i) len[i] = merge(i, nullptr, nullptr, nullptr);
+  HCsr& S = o.Q;
+  S.rows = S.cols = n;
+  S.ptr.assign(n + 1, 0);
+  for (int64_t i = 0; i < n; ++i) S.ptr[i + 1] = S.ptr[i] + len[i];
+  const int64_t nnzS = S.ptr[n];
+  S.col.resize(nnzS);
+  S.val.resize(nnzS);
+  std::vector<int> ia(nnzS), ib(nnzS);
+#pragma omp parallel for schedule(static) num_threads(host_threads(n))
+  for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], ia.data() + S.ptr[i], ib.data() + S.ptr[i]);
+
+  // device copies
+  DevBuf d;
+  auto up = [&](auto* dst, const auto& v) {
+    if (!v.empty())
+      HPRQP_CUDA(cudaMemcpyAsync(dst, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice, st));
+  };
+  struct DM {
+    int rows = 0;
+    int* ptr = nullptr;
+    int* col = nullptr;
+    double* val = nullptr;
+  };
+  auto dev_csr = [&](const HCsr& h) {
+    DM x;
+    x.rows = (int)h.rows;
+    x.ptr = d.get<int>(h.rows + 1);
+    x.col = d.get<int>(h.nnz());
+    x.val = d.get<double>(h.nnz());
+    up(x.ptr, h.ptr);
+    up(x.col, h.col);
+    up(x.val, h.val);
+    return x;
+  };
+  const DM dA = dev_csr(hp.A), dAT = dev_csr(hp.AT), dQ = dev_csr(Q), dQT = dev_csr(QT);
+  double *c = d.get<double>(n), *l = d.get<double>(n), *u = d.get<double>(n), *cn = d.get<double>(n);
+  double *AL = d.get<double>(m), *AU = d.get<double>(m), *rn = d.get<double>(m);
+  double *ca = d.get<double>(n), *cq = d.get<double>(n), *tc = d.get<double>(n), *tci = d.get<double>(n);
+  double *ra = d.get<double>(m), *tr = d.get<double>(m), *tri = d.get<double>(m);
+  up(c, o.c);
+  up(l, o.l);
+  up(u, o.u);
+  up(cn, o.col_norm);
+  up(AL, o.AL);
+  up(AU, o.AU);
+  up(rn, o.row_norm);
+  auto pass = [&](int mode) {  // one Ruiz (0) or Pock-Chambolle (1) pass
+    k_row_abs<<<blocks(n), kT, 0, st>>>((int)n, dAT.ptr, dAT.val, mode, ca);
+    k_row_abs<<<blocks(n), kT, 0, st>>>((int)n, dQT.ptr, dQT.val, mode, cq);
+    k_col_factors<<<blocks(n), kT, 0, st>>>((int)n, ca, cq, mode, tc, tci, cn);
+    if (m > 0) {
+      k_row_abs<<<blocks(m), kT, 0, st>>>((int)m, dA.ptr, dA.val, mode, ra);
+      k_row_factors<<<blocks(m), kT, 0, st>>>((int)m, ra, tr, tri, rn);
+    }
+    k_scale<<<blocks(n), kT, 0, st>>>((int)n, dQ.ptr, dQ.col, dQ.val, tci, tci, 0);
+    k_scale<<<blocks(n), kT, 0, st>>>((int)n, dQT.ptr, dQT.col, dQT.val, tci, tci, 1);
+    if (m > 0) {
+      k_scale<<<blocks(m), kT, 0, st>>>((int)m, dA.ptr, dA.col, dA.val, tri, tci, 0);
+      k_scale<<<blocks(n), kT, 0, st>>>((int)n, dAT.ptr, dAT.col, dAT.val, tri, tci, 1);
+      k_scale_m<<<blocks(m), kT, 0, st>>>((int)m, tr, AL, AU);
+    }
+    k_scale_n<<<blocks(n), kT, 0, st>>>((int)n, tc, c, l, u);
+    HPRQP_LAUNCH_CHECK();
+  };
+  if (p.use_Ruiz_scaling)
+    for (int k = 0; k < 10; ++k) pass(0);
+  if (p.use_Pock_Chambolle_scaling) pass(1);
+  int* dia = d.get<int>(nnzS);
+  int* dib = d.get<int>(nnzS);
+  double* sv = d.get<double>(nnzS);
+  up(dia, ia);
+  up(dib, ib);
+  k_sym<<<blocks(nnzS), kT, 0, st>>>((int)nnzS, dia, dib, dQ.val, dQT.val, sv);
+  HPRQP_LAUNCH_CHECK();
+  auto down = [&](std::vector<double>& dst, const double* src) {
+    if (!dst.empty())
+      HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
+  };
+  down(o.A.val, dA.val);
+  down(o.AT.val, dAT.val);
+  down(S.val, sv);
+  down(o.c, c);
+  down(o.l, l);
+  down(o.u, u);
+  down(o.col_norm, cn);
+  down(o.AL, AL);
+  down(o.AU, AU);
+  down(o.row_norm, rn);
+  HPRQP_CUDA(cudaStreamSynchronize(st));
+  finish_sparse(o, n);
+  finish_common(hp, o);
+}
+
+}  // namespace hprqp

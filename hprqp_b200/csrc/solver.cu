@@ -11,6 +11,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -375,7 +376,14 @@ static void prepare(Handle& H, const hprqp_params& p) {
   const double t = now_s();
   H.e64.reset();
   H.e32.reset();
-  prepare_problem(H.hp, p, H.pp);
+  // scaling on the GPU for large sparse problems (bitwise the host result);
+  // HPRQP_HOST_SCALING=1 keeps it on the host
+  const char* hs = std::getenv("HPRQP_HOST_SCALING");
+  const int64_t work = H.hp.A.nnz() + H.hp.Q.nnz();
+  if (H.hp.Q_kind == HPRQP_Q_SPARSE && work >= 100000 && !(hs && hs[0] == '1'))
+    prepare_problem_gpu(H.hp, p, H.pp, H.cm->stream);
+  else
+    prepare_problem(H.hp, p, H.pp);
   if (H.hp.Q_kind == HPRQP_Q_LASSO) H.path = PATH_LASSO;
   else if (H.hp.Q_kind == HPRQP_Q_QAP || H.pp.Q.nnz() > 0) H.path = H.pp.noC ? PATH_NOC : PATH_QP;
   else H.path = PATH_LP;
