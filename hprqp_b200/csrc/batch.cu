@@ -268,6 +268,13 @@ struct ZzFin {
   __device__ void operator()(int, const double (&)[K]) const {}
 };
 
+template <typename V>
+struct CastVal {  // dst[i] = (V) src[i]
+  V* dst;
+  const double* src;
+  __device__ __forceinline__ void operator()(int i) const { dst[i] = (V)src[i]; }
+};
+
 template <typename F>
 __global__ void k_each(int len, F f) {
   pdl_enter();
@@ -281,10 +288,15 @@ __global__ void k_each(int len, F f) {
 struct Mem {
   std::vector<void*> blocks;
   template <typename T>
-  T* alloc(int64_t n) {
+  T* alloc(int64_t n) {  // zeroed
+    T* p = alloc_raw<T>(n);
+    HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    return p;
+  }
+  template <typename T>
+  T* alloc_raw(int64_t n) {  // for buffers that are written in full right away
     void* p = nullptr;
     HPRQP_CUDA(cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
-    HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
     blocks.push_back(p);
     return (T*)p;
   }
@@ -330,13 +342,29 @@ struct BEngine {
   Tiles tn;
   int64_t launches = 0;
 
-  void upload_csr(const HCsr& h, DCsr<V>& d) {
+  // A CSR on the device.  With `from` (the FP64 engine's copy of the same
+  // matrix) the pattern arrays are shared and the values cast on the device,
+  // so the FP32 engine moves nothing across PCIe.
+  void upload_csr(const HCsr& h, DCsr<V>& d, const DCsr<double>* from = nullptr) {
     d.rows = (int)h.rows;
     d.cols = (int)h.cols;
     d.nnz = h.nnz();
-    int* p = mem.alloc<int>(h.rows + 1);
-    int* cc = mem.alloc<int>(d.nnz);
-    V* v = mem.alloc<V>(d.nnz);
+    V* v = mem.alloc_raw<V>(d.nnz);
+    if (from) {
+      d.ptr = from->ptr;
+      d.col = from->col;
+      const double* src = from->val;
+      if (d.nnz) {
+        k_each<<<(int)((d.nnz + kBlock - 1) / kBlock), kBlock, 0, st>>>((int)d.nnz,
+                                                                        CastVal<V>{v, src});
+        HPRQP_LAUNCH_CHECK();
+        HPRQP_CUDA(cudaStreamSynchronize(st));
+      }
+      d.val = v;
+      return;
+    }
+    int* p = mem.alloc_raw<int>(h.rows + 1);
+    int* cc = mem.alloc_raw<int>(d.nnz);
     HPRQP_CUDA(cudaMemcpy(p, h.ptr.data(), sizeof(int) * (h.rows + 1), cudaMemcpyHostToDevice));
     if (d.nnz) HPRQP_CUDA(cudaMemcpy(cc, h.col.data(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice));
     if (d.nnz) {
@@ -360,9 +388,10 @@ struct BEngine {
     return d;
   }
 
-  BEngine(const Family& F, cudaStream_t s) : st(s), B(F.B), N(F.N), R(F.R) {
-    upload_csr(F.L, L);
-    upload_csr(F.LT, LT);
+  BEngine(const Family& F, cudaStream_t s, const DCsr<double>* L64 = nullptr, const DCsr<double>* LT64 = nullptr)
+      : st(s), B(F.B), N(F.N), R(F.R) {
+    upload_csr(F.L, L, L64);
+    upload_csr(F.LT, LT, LT64);
     const double avg = F.R ? (double)F.L.nnz() / F.R : 1.0;
     tprL = avg > 48 ? 32 : avg > 24 ? 16 : avg > 12 ? 8 : avg > 6 ? 4 : 2;
     for (V** p : {&x, &x_hat, &x_bar, &dx, &w, &w_bar, &dw, &z_bar, &Qv, &pz, &pq}) *p = mem.alloc<V>(N);
@@ -668,7 +697,7 @@ static void build_family(int count, const hprqp_problem* probs, Family& F) {
   for (int k = 0; k < count; ++k) {
     try {
       load_problem(&probs[k], hps[k]);
-      LTs[k] = transpose(hps[k].L);
+      LTs[k] = std::move(hps[k].LT);
     } catch (const Error& e) {
       codes[k] = e.code;
       errs[k] = e.what();
@@ -771,7 +800,7 @@ static void solve(Handle& H, const hprqp_params& p, const double* const* x0s, co
   const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
   const double tc0 = now_s();
   if (!H.e64) H.e64 = std::make_unique<BEngine<double>>(F, H.st);
-  if (fp32 && !H.e32) H.e32 = std::make_unique<BEngine<float>>(F, H.st);
+  if (fp32 && !H.e32) H.e32 = std::make_unique<BEngine<float>>(F, H.st, &H.e64->L, &H.e64->LT);
   const double t_engines = now_s() - tc0;
   BEngine<double>& E64 = *H.e64;
   const double t0 = now_s();

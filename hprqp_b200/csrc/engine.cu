@@ -459,7 +459,7 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   if (is_lasso) {
     ltemp = mem.alloc<V>(hp.L.rows);
     upload_csr(hp.L, L, tpr_Q);
-    upload_csr(transpose(hp.L), LT, tpr_Q);
+    upload_csr(hp.LT, LT, tpr_Q);
   }
   if (is_qap) {
     const int64_t N2 = hp.qn * hp.qn;

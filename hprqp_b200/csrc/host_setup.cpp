@@ -258,6 +258,7 @@ void load_problem(const hprqp_problem* pr, HostProblem& hp) {
   } else if (h.Q_kind == HPRQP_Q_LASSO) {
     if (pr->lasso_m <= 0 || pr->lasso_m > INT32_MAX) throw Error(HPRQP_E_ARG, "LASSO: bad lasso_m");
     h.L = csc_to_csr(pr->lasso_m, h.n, pr->L_colptr, pr->L_rowval, pr->L_nzval, base, "LASSO data matrix");
+    if (!csc_as_transpose(pr->lasso_m, h.n, pr->L_colptr, pr->L_rowval, pr->L_nzval, base, h.LT)) h.LT = transpose(h.L);
   } else if (h.Q_kind == HPRQP_Q_QAP) {
     const int64_t N = pr->qap_n;
     if (N <= 0 || N * N != h.n) throw Error(HPRQP_E_ARG, "QAP: n must equal qap_n^2");

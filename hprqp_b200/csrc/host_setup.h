@@ -37,7 +37,8 @@ struct HostProblem {  // the loaded, unscaled problem
   std::vector<double> c, AL, AU, l, u;
   double obj_constant = 0.0, lambda = 0.0;
   HCsr Q;  // n x n (sparse kind)
-  HCsr L;  // lasso data, lasso_m x n
+  HCsr L;   // lasso data, lasso_m x n
+  HCsr LT;  // its transpose (the caller's CSC read as CSR)
   int64_t qn = 0;
   std::vector<double> qA, qB, qS, qT;  // column-major qn x qn
   bool loaded = false;
