@@ -175,11 +175,22 @@ __device__ __forceinline__ void grid_finish(double (&r)[K], ReduceWs ws, double*
   double acc[K];
 #pragma unroll
   for (int k = 0; k < K; ++k) acc[k] = 0.0;
-  for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock) {
+  // the partials are read in batches of kFold CTAs per thread, all loads of
+  // a batch issued before any is consumed; they are still combined in
+  // increasing CTA order, so the result does not depend on the batching
+  constexpr int kFold = 4;
+  for (int b0 = threadIdx.x; b0 < (int)gridDim.x; b0 += kFold * kBlock) {
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-      const double v = __ldcg(ws.partials + (size_t)b * K + k);
-      acc[k] = ((MaxMask >> k) & 1u) ? fmax(acc[k], v) : acc[k] + v;
+      double v[kFold];
+#pragma unroll
+      for (int q = 0; q < kFold; ++q) {
+        const int b = b0 + q * kBlock;
+        v[q] = b < (int)gridDim.x ? __ldcg(ws.partials + (size_t)b * K + k) : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q < kFold; ++q)
+        if (b0 + q * kBlock < (int)gridDim.x) acc[k] = ((MaxMask >> k) & 1u) ? fmax(acc[k], v[q]) : acc[k] + v[q];
     }
   }
   block_reduce<K, MaxMask>(acc);

@@ -19,7 +19,9 @@ def trace(model, host):
     try:
         s = Solver().load(model)
         xt, yt, wt = s.set_trace(30)
-        r = s.solve(HPRQP_parameters(verbose=False, max_iter=30))
+        # a pinned row schedule: the autotuner may pick different ones in
+        # two runs, and schedules sum rows in different orders
+        r = s.solve(HPRQP_parameters(verbose=False, max_iter=30, spmv_mode_Q=1, spmv_mode_A=1))
         s.close()
     finally:
         os.environ.pop("HPRQP_HOST_SCALING", None)
