@@ -1025,7 +1025,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     cm.to_dev(c->z0, zv.data(), sizeof(V) * c->len);
     HPRQP_CUDA(cudaStreamSynchronize(main));
     use(*c, main);
-    reduce<1, 0u, double>(cm, 1, c->len, ZeroSrc{}, EpiSumSq<V>{c->z0}, c->scal + 2);
+    reduce<1, 0u, double>(cm, 1, c->len, ZeroSrc{}, EpiSumSq<V>{c->z0}, c->scal + 2, InvNormFin{c->scal + 4});
     restore();
   }
   if (cm.pow_persistent && !is_qap && power_persistent(ca.on, cq.on, tol, max_it, lamA_out, lamQ_out, itA, itQ))
@@ -1047,19 +1047,21 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     V* zc = (k & 1) ? c.z1 : c.z0;
     V* zn = (k & 1) ? c.z0 : c.z1;
     double* zz = c.scal + 2;
-    const PowerFin fin{c.log, k};
+    // 1/||z|| is formed once per step (PowerFin / InvNormFin) into scal + 4
+    const double* inv = c.scal + 4;
+    const PowerFin fin{c.log, k, c.scal + 4};
     if (c.which == 0) {  // A A' (power_iteration_A)
-      mat_rows(pAT, zc, EpiStoreInvNorm<V>{c.t, zz});
-      mat_reduce<3, 0u>(cm, pA, c.t, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
+      mat_rows(pAT, zc, EpiStoreInvNorm<V>{c.t, zz, inv});
+      mat_reduce<3, 0u>(cm, pA, c.t, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
     } else if (is_lasso) {
-      mat_rows(pL, zc, EpiStoreInvNorm<V>{ltemp2, zz});
-      mat_reduce<3, 0u>(cm, pLT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
+      mat_rows(pL, zc, EpiStoreInvNorm<V>{ltemp2, zz, inv});
+      mat_reduce<3, 0u>(cm, pLT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
     } else if (is_qap) {
       elem(cm, n, ScaleInvNorm<V>{c.t, zc, zz});
       qap_apply(c.t, zn);
-      reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false}, c.scal + 1, fin);
+      reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
     } else {
-      mat_reduce<3, 0u>(cm, pQ, zc, EpiPowerFused<V>{zc, zn, zz, true}, c.scal + 1, fin);
+      mat_reduce<3, 0u>(cm, pQ, zc, EpiPowerFused<V>{zc, zn, zz, true, inv}, c.scal + 1, fin);
     }
     restore();
   };

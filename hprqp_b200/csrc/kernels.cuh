@@ -578,9 +578,10 @@ struct EpiPowerFused {
   V* zn;
   const double* zz;
   bool scale_acc;
+  const double* inv_norm = nullptr;  // 1/||z_cur|| formed once by the previous step, or null
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc, double (&r)[3]) const {
-    const double inv = 1.0 / sqrt(*zz);
+    const double inv = inv_norm ? *inv_norm : 1.0 / sqrt(*zz);
     const double v = scale_acc ? (double)acc * inv : (double)acc;
     zn[i] = (V)v;
     const double q = (double)zc[i] * inv;
@@ -595,20 +596,33 @@ template <typename V>
 struct EpiStoreInvNorm {
   V* y;
   const double* zz;
+  const double* inv_norm = nullptr;  // 1/||x|| formed once, or null
   template <typename A>
-  __device__ __forceinline__ void operator()(int i, A acc) const { y[i] = (V)((double)acc / sqrt(*zz)); }
+  __device__ __forceinline__ void operator()(int i, A acc) const {
+    y[i] = inv_norm ? (V)((double)acc * *inv_norm) : (V)((double)acc / sqrt(*zz));
+  }
 };
 
 // Last-CTA step of a power iteration: log (lambda, err) for iteration k.
 struct PowerFin {
   double* log;
   int k;
+  double* inv_out = nullptr;  // also store 1/||z_next|| for the next step's rows
   __device__ __forceinline__ void operator()(const double (&a)[3]) const {
     const double lam = a[0], zz = a[1], qq = a[2];
     const double rr = fmax(zz - 2.0 * lam * lam + lam * lam * qq, 0.0);
     log[2 * k] = lam;
     log[2 * k + 1] = sqrt(rr) / (sqrt(zz) + lam);
+    if (inv_out) *inv_out = 1.0 / sqrt(zz);
   }
+  template <int K>
+  __device__ __forceinline__ void operator()(const double (&)[K]) const {}
+};
+
+// 1/sqrt of a reduced sum of squares (the start vector's norm)
+struct InvNormFin {
+  double* inv_out;
+  __device__ __forceinline__ void operator()(const double (&a)[1]) const { *inv_out = 1.0 / sqrt(a[0]); }
   template <int K>
   __device__ __forceinline__ void operator()(const double (&)[K]) const {}
 };
