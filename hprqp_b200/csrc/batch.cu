@@ -313,11 +313,30 @@ struct Tiles {  // reduction tiles over a concatenated row space
   int count = 0;
 };
 
+// A host CSR in plain arrays, left uninitialised at allocation: the batch
+// intake fills them in parallel, one instance block per thread, so the
+// first touch of the pages is parallel too.
+struct FlatCsr {
+  int64_t rows = 0, cols = 0, nz = 0;
+  std::unique_ptr<int[]> ptr, col;
+  std::unique_ptr<double[]> val;
+  void alloc(int64_t r, int64_t c, int64_t z) {
+    rows = r;
+    cols = c;
+    nz = z;
+    ptr.reset(new int[r + 1]);
+    col.reset(new int[std::max<int64_t>(z, 1)]);
+    val.reset(new double[std::max<int64_t>(z, 1)]);
+    ptr[0] = 0;
+  }
+  int64_t nnz() const { return nz; }
+};
+
 struct Family {  // host copy of the batch
   int B = 0;
   int64_t N = 0, R = 0;                 // total columns (variables), total data rows
   std::vector<int64_t> noff, roff;      // [B+1]
-  HCsr L, LT;                           // block diagonal
+  FlatCsr L, LT;                        // block diagonal
   std::vector<double> c, lam;
   std::vector<double> obj_constant, norm_c_org;
 };
@@ -345,7 +364,7 @@ struct BEngine {
   // A CSR on the device.  With `from` (the FP64 engine's copy of the same
   // matrix) the pattern arrays are shared and the values cast on the device,
   // so the FP32 engine moves nothing across PCIe.
-  void upload_csr(const HCsr& h, DCsr<V>& d, const DCsr<double>* from = nullptr) {
+  void upload_csr(const FlatCsr& h, DCsr<V>& d, const DCsr<double>* from = nullptr) {
     d.rows = (int)h.rows;
     d.cols = (int)h.cols;
     d.nnz = h.nnz();
@@ -365,11 +384,11 @@ struct BEngine {
     }
     int* p = mem.alloc_raw<int>(h.rows + 1);
     int* cc = mem.alloc_raw<int>(d.nnz);
-    HPRQP_CUDA(cudaMemcpy(p, h.ptr.data(), sizeof(int) * (h.rows + 1), cudaMemcpyHostToDevice));
-    if (d.nnz) HPRQP_CUDA(cudaMemcpy(cc, h.col.data(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice));
+    HPRQP_CUDA(cudaMemcpy(p, h.ptr.get(), sizeof(int) * (h.rows + 1), cudaMemcpyHostToDevice));
+    if (d.nnz) HPRQP_CUDA(cudaMemcpy(cc, h.col.get(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice));
     if (d.nnz) {
       if constexpr (std::is_same<V, double>::value) {
-        HPRQP_CUDA(cudaMemcpy(v, h.val.data(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
+        HPRQP_CUDA(cudaMemcpy(v, h.val.get(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
       } else {
         std::vector<V> vv(d.nnz);
 #pragma omp parallel for schedule(static) num_threads(host_threads(d.nnz))
@@ -679,25 +698,116 @@ struct CopyMasked {
   }
 };
 
+// The family intake: offsets from the callers' CSC column pointers, then
+// one parallel pass per instance that validates its arrays and writes its
+// blocks of the concatenated A_d (CSR, by a counting sort of the CSC, which
+// keeps the columns of a row in increasing order as load_problem does) and
+// A_d' (the CSC read as CSR) in place.  An instance whose row indices are
+// not sorted within a column goes through load_problem + transpose instead.
 static void build_family(int count, const hprqp_problem* probs, Family& F) {
   if (count <= 0 || !probs) throw Error(HPRQP_E_ARG, "empty batch");
   F = Family();
   F.B = count;
   F.noff.assign(count + 1, 0);
   F.roff.assign(count + 1, 0);
-  for (int k = 0; k < count; ++k)
-    if (probs[k].Q_kind != HPRQP_Q_LASSO || probs[k].m != 0)
+  std::vector<int64_t> zoff(count + 1, 0);
+  for (int k = 0; k < count; ++k) {
+    const hprqp_problem& p = probs[k];
+    if (p.Q_kind != HPRQP_Q_LASSO || p.m != 0)
       throw Error(HPRQP_E_ARG, "batch: every instance must be a LASSO problem (m = 0)");
-  // per-instance intake and transpose, in parallel (instances are independent)
-  std::vector<HostProblem> hps(count);
-  std::vector<HCsr> LTs(count);
+    if (p.n <= 0 || p.n > INT32_MAX || p.lasso_m <= 0 || p.lasso_m > INT32_MAX || !p.L_colptr ||
+        (p.index_base != 0 && p.index_base != 1))
+      throw Error(HPRQP_E_ARG, "batch instance " + std::to_string(k) + ": bad sizes or data matrix");
+    const int64_t z = (int64_t)p.L_colptr[p.n] - p.index_base;
+    if (z < 0) throw Error(HPRQP_E_ARG, "batch instance " + std::to_string(k) + ": bad nnz");
+    F.noff[k + 1] = F.noff[k] + p.n;
+    F.roff[k + 1] = F.roff[k] + p.lasso_m;
+    zoff[k + 1] = zoff[k] + z;
+  }
+  F.N = F.noff[count];
+  F.R = F.roff[count];
+  if (F.N > INT32_MAX || F.R > INT32_MAX || zoff[count] > INT32_MAX) throw Error(HPRQP_E_ARG, "batch too large");
+  F.L.alloc(F.R, F.N, zoff[count]);
+  F.LT.alloc(F.N, F.R, zoff[count]);
+  F.c.resize(F.N);
+  F.lam.resize(count);
+  F.obj_constant.resize(count);
+  F.norm_c_org.resize(count);
   std::vector<int> codes(count, 0);
   std::vector<std::string> errs(count);
-#pragma omp parallel for schedule(dynamic, 1) num_threads(host_threads((int64_t)count * 4096))
+#pragma omp parallel for schedule(dynamic, 1) num_threads(host_threads(zoff[count]))
   for (int k = 0; k < count; ++k) {
     try {
-      load_problem(&probs[k], hps[k]);
-      LTs[k] = std::move(hps[k].LT);
+      const hprqp_problem& p = probs[k];
+      const int base = p.index_base;
+      const int64_t n = p.n, mk = p.lasso_m, z0 = zoff[k], no = F.noff[k], ro = F.roff[k];
+      const int32_t *cp = p.L_colptr, *rv = p.L_rowval;
+      const double* nz = p.L_nzval;
+      const int64_t z = zoff[k + 1] - z0;
+      if (z > 0 && (!rv || !nz)) throw Error(HPRQP_E_ARG, "null rowval/nzval");
+      if (cp[0] != base) throw Error(HPRQP_E_ARG, "colptr[0] != index_base");
+      bool sorted = true;
+      for (int64_t j = 0; j < n; ++j) {
+        if (cp[j + 1] < cp[j]) throw Error(HPRQP_E_ARG, "colptr not monotone");
+        for (int64_t q = cp[j] - base; q < cp[j + 1] - base; ++q) {
+          const int64_t r = (int64_t)rv[q] - base;
+          if (r < 0 || r >= mk) throw Error(HPRQP_E_ARG, "row index out of range");
+          if (!std::isfinite(nz[q])) throw Error(HPRQP_E_ARG, "LASSO data matrix contains NaN or Inf values.");
+          if (q > cp[j] - base && rv[q] <= rv[q - 1]) sorted = false;
+        }
+      }
+      int* Lp = F.L.ptr.get();
+      int* Lc = F.L.col.get();
+      double* Lv = F.L.val.get();
+      int* Tp = F.LT.ptr.get();
+      int* Tc = F.LT.col.get();
+      double* Tv = F.LT.val.get();
+      if (sorted) {
+        // A_d' block: the CSC read as CSR, shifted by (noff, roff)
+        for (int64_t j = 0; j < n; ++j) Tp[no + j + 1] = (int)(z0 + (cp[j + 1] - base));
+        for (int64_t q = 0; q < z; ++q) {
+          Tc[z0 + q] = (int)(rv[q] - base + ro);
+          Tv[z0 + q] = nz[q];
+        }
+        // A_d block: counting sort of the CSC by row
+        std::vector<int> pos(mk + 1, 0);
+        for (int64_t q = 0; q < z; ++q) pos[rv[q] - base + 1]++;
+        for (int64_t r = 0; r < mk; ++r) pos[r + 1] += pos[r];
+        for (int64_t r = 0; r < mk; ++r) Lp[ro + r + 1] = (int)(z0 + pos[r + 1]);
+        for (int64_t j = 0; j < n; ++j)
+          for (int64_t q = cp[j] - base; q < cp[j + 1] - base; ++q) {
+            const int r = rv[q] - base;
+            const int64_t at = z0 + pos[r]++;
+            Lc[at] = (int)(j + no);
+            Lv[at] = nz[q];
+          }
+      } else {
+        HostProblem hp;
+        load_problem(&p, hp);
+        const HCsr& Lk = hp.L;
+        const HCsr Tk = transpose(Lk);
+        for (int64_t r = 0; r < Lk.rows; ++r) Lp[ro + r + 1] = (int)(z0 + Lk.ptr[r + 1]);
+        for (int64_t q = 0; q < Lk.nnz(); ++q) {
+          Lc[z0 + q] = (int)(Lk.col[q] + no);
+          Lv[z0 + q] = Lk.val[q];
+        }
+        for (int64_t r = 0; r < Tk.rows; ++r) Tp[no + r + 1] = (int)(z0 + Tk.ptr[r + 1]);
+        for (int64_t q = 0; q < Tk.nnz(); ++q) {
+          Tc[z0 + q] = (int)(Tk.col[q] + ro);
+          Tv[z0 + q] = Tk.val[q];
+        }
+      }
+      if (n > 0 && !p.c) throw Error(HPRQP_E_ARG, "c vector: null pointer");
+      double nc = 0.0;
+      for (int64_t j = 0; j < n; ++j) {
+        const double v = p.c[j];
+        if (!std::isfinite(v)) throw Error(HPRQP_E_ARG, "c vector contains NaN or Inf values.");
+        F.c[no + j] = v;
+        nc = std::max(nc, std::fabs(v));
+      }
+      F.norm_c_org[k] = nc;
+      F.lam[k] = p.lambda;
+      F.obj_constant[k] = p.obj_constant;
     } catch (const Error& e) {
       codes[k] = e.code;
       errs[k] = e.what();
@@ -705,50 +815,6 @@ static void build_family(int count, const hprqp_problem* probs, Family& F) {
   }
   for (int k = 0; k < count; ++k)
     if (codes[k]) throw Error(codes[k], "batch instance " + std::to_string(k) + ": " + errs[k]);
-  std::vector<int64_t> zoff(count + 1, 0);  // nonzero offsets
-  for (int k = 0; k < count; ++k) {
-    const HostProblem& hp = hps[k];
-    F.noff[k + 1] = F.noff[k] + hp.n;
-    F.roff[k + 1] = F.roff[k] + hp.L.rows;
-    zoff[k + 1] = zoff[k] + hp.L.nnz();
-    F.lam.push_back(hp.lambda);
-    F.obj_constant.push_back(hp.obj_constant);
-    double nc = 0;
-    for (double v : hp.c) nc = std::max(nc, std::fabs(v));
-    F.norm_c_org.push_back(nc);
-  }
-  F.N = F.noff[count];
-  F.R = F.roff[count];
-  if (F.N > INT32_MAX || F.R > INT32_MAX || zoff[count] > INT32_MAX) throw Error(HPRQP_E_ARG, "batch too large");
-  F.c.resize(F.N);
-  HCsr& L = F.L;
-  HCsr& LT = F.LT;
-  L.rows = LT.cols = F.R;
-  L.cols = LT.rows = F.N;
-  L.ptr.assign(F.R + 1, 0);
-  LT.ptr.assign(F.N + 1, 0);
-  L.col.resize(zoff[count]);
-  L.val.resize(zoff[count]);
-  LT.col.resize(zoff[count]);
-  LT.val.resize(zoff[count]);
-  // block-diagonal concatenation: block k shifted by (roff[k], noff[k])
-#pragma omp parallel for schedule(dynamic, 1) num_threads(host_threads(zoff[count]))
-  for (int k = 0; k < count; ++k) {
-    const HCsr& Lk = hps[k].L;
-    const HCsr& Tk = LTs[k];
-    const int64_t z = zoff[k];
-    for (int64_t r = 0; r < Lk.rows; ++r) L.ptr[F.roff[k] + r + 1] = (int)(z + Lk.ptr[r + 1]);
-    for (int64_t q = 0; q < Lk.nnz(); ++q) {
-      L.col[z + q] = (int)(Lk.col[q] + F.noff[k]);
-      L.val[z + q] = Lk.val[q];
-    }
-    for (int64_t r = 0; r < Tk.rows; ++r) LT.ptr[F.noff[k] + r + 1] = (int)(z + Tk.ptr[r + 1]);
-    for (int64_t q = 0; q < Tk.nnz(); ++q) {
-      LT.col[z + q] = (int)(Tk.col[q] + F.roff[k]);
-      LT.val[z + q] = Tk.val[q];
-    }
-    std::copy(hps[k].c.begin(), hps[k].c.end(), F.c.begin() + F.noff[k]);
-  }
 }
 
 template <typename V>
