@@ -120,7 +120,7 @@ struct EpiLassoB {
 
 // Segmented reduction over tiles: each CTA owns one tile (instance, rows
 // [b, e)); Epi(i, k, acc, r) adds to K slots (MaxMask selects max).
-template <int K, unsigned MM, typename V, typename Src, typename Epi>
+template <int K, unsigned MM, typename V, int TPR = 1, typename Src, typename Epi>
 __global__ void __launch_bounds__(kBlock) k_seg(const int* tile_inst, const int* tile_begin, const int* tile_end,
                                                 Inst I, Src src, Epi epi, double* partials) {
   pdl_enter();
@@ -129,10 +129,11 @@ __global__ void __launch_bounds__(kBlock) k_seg(const int* tile_inst, const int*
   double r[K];
 #pragma unroll
   for (int j = 0; j < K; ++j) r[j] = 0.0;
-  if (I.on[k]) {
-    for (int i = tile_begin[t] + threadIdx.x; i < tile_end[t]; i += kBlock) {
-      const double acc = src.template dot<1, double>(i, 0);
-      epi(i, k, acc, r);
+  if (I.on[k]) {  // TPR threads per row (the row schedule of the source matrix)
+    const int lane = threadIdx.x & (TPR - 1);
+    for (int i = tile_begin[t] + (int)threadIdx.x / TPR; i < tile_end[t]; i += kBlock / TPR) {
+      const double acc = src.template dot<TPR, double>(i, lane);
+      if (lane == 0) epi(i, k, acc, r);
     }
   }
   block_reduce<K, MM>(r);
@@ -514,8 +515,14 @@ struct BEngine {
   template <int K, unsigned MM, typename Epi, typename Fin = NoFinB>
   void seg_LT(const V* xin, const Epi& e, const unsigned char* mask, double* dst, const Fin& fin = Fin()) {
     const Inst I{inst_n, mask};
-    k_seg<K, MM, V><<<tn.count, kBlock, 0, st>>>(tn.inst, tn.begin, tn.end, I, CsrSrc<V, V>{LT.ptr, LT.col, LT.val, xin},
-                                               e, partials);
+    const CsrSrc<V, V> src{LT.ptr, LT.col, LT.val, xin};
+    switch (tprLT) {
+      case 1: k_seg<K, MM, V, 1><<<tn.count, kBlock, 0, st>>>(tn.inst, tn.begin, tn.end, I, src, e, partials); break;
+      case 2: k_seg<K, MM, V, 2><<<tn.count, kBlock, 0, st>>>(tn.inst, tn.begin, tn.end, I, src, e, partials); break;
+      case 4: k_seg<K, MM, V, 4><<<tn.count, kBlock, 0, st>>>(tn.inst, tn.begin, tn.end, I, src, e, partials); break;
+      case 8: k_seg<K, MM, V, 8><<<tn.count, kBlock, 0, st>>>(tn.inst, tn.begin, tn.end, I, src, e, partials); break;
+      default: k_seg<K, MM, V, 16><<<tn.count, kBlock, 0, st>>>(tn.inst, tn.begin, tn.end, I, src, e, partials); break;
+    }
     k_fold<K, MM><<<(B + 7) / 8, 256, 0, st>>>(B, tn.inst_tiles, mask, partials, dst, fin);
     launches += 2;
     HPRQP_LAUNCH_CHECK();
