@@ -44,6 +44,8 @@ void Common::init() {
   pow_persistent = pe && pe[0] == '1';
   const char* tq = std::getenv("HPRQP_QAP_TC");
   tc_qap = !(tq && tq[0] == '0');
+  const char* ps = std::getenv("HPRQP_POWER_SPLIT");
+  pow_split = ps && ps[0] == '1';
   const char* rc = std::getenv("HPRQP_REDUCE_CAP");
   if (rc) reduce_cap = std::max(1, std::min(std::atoi(rc), kReduceGridLimit));
   const char* pel = std::getenv("HPRQP_POWER_ELL");
@@ -1050,18 +1052,40 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     // 1/||z|| is formed once per step (PowerFin / InvNormFin) into scal + 4
     const double* inv = c.scal + 4;
     const PowerFin fin{c.log, k, c.scal + 4};
+    // HPRQP_POWER_SPLIT=1: the last product of a step as a plain row pass
+    // (one row per thread, no reduction) and the three dots as a separate
+    // streaming reduction over (z, z_next)
+    auto dots = [&](int64_t len) {
+      reduce<3, 0u, double>(cm, 1, len, VecSrc<V>{zn}, EpiPowerFused<V>{zc, nullptr, zz, false, inv}, c.scal + 1,
+                            fin);
+    };
     if (c.which == 0) {  // A A' (power_iteration_A)
       mat_rows(pAT, zc, EpiStoreInvNorm<V>{c.t, zz, inv});
-      mat_reduce<3, 0u>(cm, pA, c.t, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
+      if (cm.pow_split) {
+        mat_rows(pA, c.t, EpiStore<V>{zn, 1.0});
+        dots(m);
+      } else {
+        mat_reduce<3, 0u>(cm, pA, c.t, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
+      }
     } else if (is_lasso) {
       mat_rows(pL, zc, EpiStoreInvNorm<V>{ltemp2, zz, inv});
-      mat_reduce<3, 0u>(cm, pLT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
+      if (cm.pow_split) {
+        mat_rows(pLT, ltemp2, EpiStore<V>{zn, 1.0});
+        dots(n);
+      } else {
+        mat_reduce<3, 0u>(cm, pLT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
+      }
     } else if (is_qap) {
       elem(cm, n, ScaleInvNorm<V>{c.t, zc, zz});
       qap_apply(c.t, zn);
       reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
     } else {
-      mat_reduce<3, 0u>(cm, pQ, zc, EpiPowerFused<V>{zc, zn, zz, true, inv}, c.scal + 1, fin);
+      if (cm.pow_split) {
+        mat_rows(pQ, zc, EpiStoreInvNorm<V>{zn, zz, inv});
+        dots(n);
+      } else {
+        mat_reduce<3, 0u>(cm, pQ, zc, EpiPowerFused<V>{zc, zn, zz, true, inv}, c.scal + 1, fin);
+      }
     }
     restore();
   };

@@ -75,6 +75,7 @@ struct Common {  // per-handle resources shared by the engines
   bool pow_persistent = false;
   int reduce_cap = kMaxReduceGrid;  // CTAs of a grid-stride reduction (HPRQP_REDUCE_CAP)
   bool pow_prefer_ell = false;  // HPRQP_POWER_ELL=1: power sweeps on ELL copies
+  bool pow_split = false;       // HPRQP_POWER_SPLIT=1: product pass + separate dot reduction
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;
   void init();

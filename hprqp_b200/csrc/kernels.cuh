@@ -583,7 +583,7 @@ struct EpiPowerFused {
   __device__ __forceinline__ void operator()(int i, A acc, double (&r)[3]) const {
     const double inv = inv_norm ? *inv_norm : 1.0 / sqrt(*zz);
     const double v = scale_acc ? (double)acc * inv : (double)acc;
-    zn[i] = (V)v;
+    if (zn) zn[i] = (V)v;
     const double q = (double)zc[i] * inv;
     r[0] += q * v;
     r[1] += v * v;
