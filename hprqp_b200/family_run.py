@@ -47,7 +47,7 @@ def _learn(a, train, out, log):
     log(f"labels: {len(pairs)} in {out['label_s']:.1f} s")
 
     t = time.perf_counter()
-    ws = learned.WarmStart.fit(pairs, epochs=a.epochs, lr=1e-3, width=a.width, batch=256)
+    ws = learned.WarmStart.fit(pairs, epochs=a.epochs, lr=a.lr, width=a.width, batch=256)
     out["train_s"] = time.perf_counter() - t
     out["loss_first"], out["loss_last"] = float(ws.history[0]), float(ws.history[-1])
     log(f"trained in {out['train_s']:.1f} s, loss {ws.history[0]:.4f} -> {ws.history[-1]:.4f}")
@@ -63,6 +63,7 @@ def main(argv=None):
     ap.add_argument("--n", type=int, default=10000)
     ap.add_argument("--density", type=float, default=0.01)
     ap.add_argument("--epochs", type=int, default=150)
+    ap.add_argument("--lr", type=float, default=1e-3)
     ap.add_argument("--width", type=int, default=512)
     ap.add_argument("--label-tol", type=float, default=1e-8)
     ap.add_argument("--tol", type=float, default=1e-6)
@@ -101,6 +102,8 @@ def main(argv=None):
                            solve_s=sc * sum(r.device_time for r in ref), power_s=sc * sum(r.power_time for r in ref))
     log(f"seq fp64: {t_seq:.2f} s")
 
+    sol = {}
+
     def batched(tag, precision, x0=None, sg=None, extra_s=0.0):
         res, solve_s, power_s, max_it = [], 0.0, 0.0, 0
         t0 = time.perf_counter()
@@ -117,6 +120,7 @@ def main(argv=None):
         ok = all(r.status == "OPTIMAL" for r in res)
         obj = max(_rel(r.primal_obj, q.primal_obj) for r, q in zip(res, ref))
         kkt = max(max(r.residuals, 0.0) for r in res)
+        sol[tag] = [r.x for r in res]
         out[tag] = dict(s=dt, solve_s=solve_s, power_s=power_s, max_iter=max_it,
                         iters=float(np.mean([r.iter for r in res])), all_optimal=ok,
                         max_rel_obj_vs_seq=obj, max_kkt=kkt, speedup_vs_seq=t_seq / dt)
@@ -136,6 +140,10 @@ def main(argv=None):
     x0, sg = np.concatenate(x0), np.concatenate(sg)
     t_prop = time.perf_counter() - t
     out["propose_s"] = t_prop
+    # how close the proposals are to the solutions (the FP64 batch's)
+    out["x0_rel_err_mean"] = float(np.mean([np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)
+                                            for a, b in zip(x0, sol["batch_fp64"])]))
+    out["x0_zero_rel_err"] = 1.0
     batched("batch_learned", "fp32_polish", x0=x0, extra_s=t_prop)
     batched("batch_learned_sigma", "fp32_polish", x0=x0, sg=sg, extra_s=t_prop)
     print(json.dumps(out), flush=True)
