@@ -270,6 +270,16 @@ def run_ours(args):
                 "kernel": best["kernel"], "algorithmic_bytes_per_launch": best["bytes"],
                 "ms_per_launch": best["ms"], "peak_source": peak_kind,
                 "share_of_iteration": round(best["share"], 3)}
+    # the power method is the larger part of a solve: its aggregate bandwidth (algorithmic bytes of
+    # all its steps over its CUDA-event-bracketed time inside the timed solves)
+    rp = results[args.precision][-1]
+    roof_power = None
+    if rp.power_bytes > 0 and head["power_s"] > 0:
+        ach_p = rp.power_bytes / head["power_s"] / 1e9
+        roof_power = {"bound": "hbm", "achieved": round(ach_p, 1), "peak": peak, "unit": "GB/s",
+                      "frac": round(ach_p / peak, 4), "steps_A": rp.power_iter_A, "steps_Q": rp.power_iter_Q,
+                      "algorithmic_bytes": rp.power_bytes, "seconds": head["power_s"],
+                      "share_of_solve": round(head["power_s"] / head["value"], 3) if head["value"] else None}
     # end to end through the public API from host buffers (load -> solve -> x,y,z,w on the host)
     e2e_t, h2d, d2h, setup = [], 0, 0, 0.0
     for _ in range(max(1, min(args.steps, 3))):
@@ -315,7 +325,7 @@ def run_ours(args):
                                                    if st64["ms_per_iter"] else None),
                        "ms_per_plain_iteration": st64["ms_per_iter"]},
         "speedup_vs_plain_fp64": fp64["value"] / head["value"] if head["value"] else None,
-        "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "roofline": roof, "roofline_power_method": roof_power, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": head["launches"],
     }
     if rank == 0:

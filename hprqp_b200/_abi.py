@@ -66,6 +66,7 @@ class Result(C.Structure):
         ("sigma", C.c_double), ("lambda_max_A", C.c_double), ("lambda_max_Q", C.c_double),
         ("restarts", C.c_int64), ("iter_fp32", C.c_int64), ("gpu_launches", C.c_int64),
         ("device_time", C.c_double), ("h2d_bytes", C.c_int64), ("d2h_bytes", C.c_int64),
+        ("power_iter_A", C.c_int64), ("power_iter_Q", C.c_int64), ("power_bytes", C.c_double),
     ]
 
 

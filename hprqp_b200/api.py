@@ -122,6 +122,9 @@ class HPRQP_results:
     gpu_launches: int = 0
     Q_is_diag: bool = False
     device_time: float = 0.0
+    power_iter_A: int = 0
+    power_iter_Q: int = 0
+    power_bytes: float = 0.0
     h2d_bytes: int = 0
     d2h_bytes: int = 0
 

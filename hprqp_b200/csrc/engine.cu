@@ -643,6 +643,19 @@ void Engine<V>::step(bool full, double h1, double h2) {
   }
 }
 
+// One power step streams the matrices once, gathers the input vector once,
+// writes the intermediate and the next iterate and reads the current one in
+// the fused dots (counted once each, at the storage size).
+template <typename V>
+double Engine<V>::power_step_bytes(int which) const {
+  const double v = sizeof(V);
+  auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
+  if (which == 0) return m > 0 ? csr(AT) + csr(A) + 2.0 * n * v + 3.0 * m * v : 0.0;
+  if (is_qap) return 0.0;
+  if (is_lasso) return csr(L) + csr(LT) + 2.0 * L.rows * v + 3.0 * n * v;
+  return csr(Q) + 2.0 * n * v;
+}
+
 // Name, algorithmic HBM bytes (plain iteration) and schedule of pass k.
 // CSR stream = nnz (sizeof(V) + 4) + 4 (rows + 1); every distinct vector is
 // counted once per pass at its storage size (FP64 anchors stay 8 bytes);

@@ -161,6 +161,9 @@ class Engine {
     return path == PATH_QP ? (m > 0 ? 4 : 2) : path == PATH_NOC ? (m > 0 ? 3 : 2) : path == PATH_LP ? (m > 0 ? 2 : 1) : 2;
   }
   void pass_info(int k, const char** name, double* bytes, int* tpr) const;
+  // algorithmic HBM bytes of one power-method step of chain `which`
+  // (0 = A A', 1 = Q or the LASSO operator); 0 for the QAP operator
+  double power_step_bytes(int which) const;
 
  private:
   DeviceMem mem;

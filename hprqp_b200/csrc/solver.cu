@@ -399,7 +399,8 @@ static void prepare(Handle& H, const hprqp_params& p) {
 // src/unified_operations.jl:703-718): the power methods for A A' and Q run
 // together, in the precision of the first phase (their 1e-4 stopping test is
 // far above FP32 rounding).
-static void estimate_lambdas(Handle& H, const hprqp_params& p, bool fp32, double* lamA, double* lamQ) {
+static void estimate_lambdas(Handle& H, const hprqp_params& p, bool fp32, double* lamA, double* lamQ,
+                             int64_t* itA_out = nullptr, int64_t* itQ_out = nullptr, double* bytes_out = nullptr) {
   const Prepared& pp = H.pp;
   const bool needA = H.hp.m > 0 && !(p.lambda_max_A_override > 0);
   const bool opQ = H.hp.Q_kind != HPRQP_Q_SPARSE || (pp.Q.nnz() > 0 && !pp.Q_is_diag);
@@ -409,6 +410,14 @@ static void estimate_lambdas(Handle& H, const hprqp_params& p, bool fp32, double
   if (needA || needQ) {
     if (fp32) H.e32->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
     else H.e64->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
+  }
+  if (!needA) ia = 0;
+  if (!needQ) iq = 0;
+  if (itA_out) *itA_out = ia;
+  if (itQ_out) *itQ_out = iq;
+  if (bytes_out) {
+    if (fp32) *bytes_out = ia * H.e32->power_step_bytes(0) + iq * H.e32->power_step_bytes(1);
+    else *bytes_out = ia * H.e64->power_step_bytes(0) + iq * H.e64->power_step_bytes(1);
   }
   *lamA = H.hp.m > 0 ? (needA ? a * p.eig_factor : p.lambda_max_A_override) : 0.0;
   if (opQ) *lamQ = needQ ? q * p.eig_factor : p.lambda_max_Q_override;
@@ -451,7 +460,9 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   // The power method runs in the precision of the first phase: its 1e-4
   // stopping test is far above FP32 rounding.
   const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
-  estimate_lambdas(H, p, fp32, &lamA, &lamQ);
+  int64_t pitA = 0, pitQ = 0;
+  double pbytes = 0.0;
+  estimate_lambdas(H, p, fp32, &lamA, &lamQ, &pitA, &pitQ, &pbytes);
   const double power_time = now_s() - L.t0;
   // sigma of allocate_workspace (src/algorithm.jl:838-851)
   double sigma0 = p.sigma > 0 ? p.sigma : 1.0;
@@ -536,6 +547,9 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   res->iter_fp32 = iter_fp32;
   res->gpu_launches = cm.launches - launches0;
   res->device_time = dev_ms * 1e-3;
+  res->power_iter_A = pitA;
+  res->power_iter_Q = pitQ;
+  res->power_bytes = pbytes;
   res->h2d_bytes = cm.h2d - H.h2d_at_solve_start;
   res->d2h_bytes = cm.d2h - d2h0;
   (void)h2d0;

@@ -164,6 +164,8 @@ typedef struct hprqp_result {
     int64_t gpu_launches;            /* kernels launched by this solve              */
     double  device_time;             /* CUDA-event time of the same span as `time`  */
     int64_t h2d_bytes, d2h_bytes;    /* host<->device bytes moved by this call      */
+    int64_t power_iter_A, power_iter_Q; /* power-method steps of the two chains     */
+    double  power_bytes;             /* algorithmic HBM bytes of those steps         */
 } hprqp_result;
 
 /* Per-pass timing of the hot loop (hprqp_profile_iterations). */

@@ -89,6 +89,7 @@ mutable struct CResult
     sigma::Float64; lambda_max_A::Float64; lambda_max_Q::Float64
     restarts::Int64; iter_fp32::Int64; gpu_launches::Int64
     device_time::Float64; h2d_bytes::Int64; d2h_bytes::Int64
+    power_iter_A::Int64; power_iter_Q::Int64; power_bytes::Float64
     CResult() = new()
 end
 
