@@ -39,7 +39,7 @@ void Common::init() {
   const char* e = std::getenv("HPRQP_PDL");
   pdl = !(e && e[0] == '0');
   pow_part = mem.alloc<double>(2 * 2 * kPowMaxGrid * 3);
-  pow_bar = mem.alloc<unsigned>(4);
+  pow_bar = mem.alloc<unsigned>(64);  // [0] arrivals, [1] status, [32] released phase
   const char* pe = std::getenv("HPRQP_POWER_PERSISTENT");
   pow_persistent = pe && pe[0] == '1';
   const char* tq = std::getenv("HPRQP_QAP_TC");
@@ -963,7 +963,7 @@ bool Engine<V>::power_persistent(bool onA, bool onQ, double tol, int max_it, dou
   pa.bar = cm.pow_bar;
   pa.status = reinterpret_cast<int*>(cm.pow_bar + 1);
   pa.out = cm.d_scal + S_POWLOG;
-  HPRQP_CUDA(cudaMemsetAsync(cm.pow_bar, 0, 2 * sizeof(unsigned), cm.stream));
+  HPRQP_CUDA(cudaMemsetAsync(cm.pow_bar, 0, 64 * sizeof(unsigned), cm.stream));
   cudaLaunchConfig_t cfg{};
   cfg.gridDim = dim3((unsigned)grid);
   cfg.blockDim = dim3((unsigned)kPowBlock);
@@ -1035,10 +1035,17 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   };
   for (Chain* c : {&ca, &cq}) {
     if (!c->on) continue;
-    std::vector<double> z0 = power_start_vector(c->len);
-    std::vector<V> zv(z0.begin(), z0.end());
-    cm.to_dev(c->z0, zv.data(), sizeof(V) * c->len);
-    HPRQP_CUDA(cudaStreamSynchronize(main));
+    // the start vector depends only on its length: generated and uploaded
+    // once per engine, then copied on the device for every later solve
+    V*& keep = c->which == 0 ? start_A : start_Q;
+    if (!keep) {
+      std::vector<double> z0 = power_start_vector(c->len);
+      std::vector<V> zv(z0.begin(), z0.end());
+      keep = mem.alloc<V>(c->len);
+      cm.to_dev(keep, zv.data(), sizeof(V) * c->len);
+      HPRQP_CUDA(cudaStreamSynchronize(main));
+    }
+    HPRQP_CUDA(cudaMemcpyAsync(c->z0, keep, sizeof(V) * c->len, cudaMemcpyDeviceToDevice, main));
     use(*c, main);
     reduce<1, 0u, double>(cm, 1, c->len, ZeroSrc{}, EpiSumSq<V>{c->z0}, c->scal + 2, InvNormFin{c->scal + 4});
     restore();

@@ -48,7 +48,7 @@ struct PowArgs {
   double tol;
   int max_it;
   double* partials;  // [2 (phase parity)][2 (chain)][gridDim.x][3]
-  unsigned* bar;     // barrier arrivals (zeroed before the launch)
+  unsigned* bar;     // barrier arrivals; bar[32] the released phase (both zeroed before the launch)
   int* status;       // 0, or 1 once a barrier wait gave up
   double* out;       // [c*4 + 0] lambda, [c*4 + 1] stop step (or -1), [c*4 + 2] steps; [8] status
 };
@@ -65,27 +65,38 @@ __device__ __forceinline__ unsigned pow_ld_acquire(const unsigned* p) {
   return v;
 }
 
-// Grid barrier: arrivals count up monotonically (target = gridDim.x * phase
-// number), so it needs no reset between phases.  Returns false when this
-// CTA gave up (time or poll limit, or another CTA's abort).
-__device__ __forceinline__ bool pow_barrier(unsigned* bar, unsigned target, int* status) {
+// Grid barrier: arrivals count up monotonically on `bar` (target = gridDim.x
+// * phase number, so it needs no reset between phases); the CTA whose
+// arrival completes the phase publishes the phase number on `flag` (its own
+// 128-byte line), and the others poll that flag with a backoff instead of
+// the counter the arrivals are still updating.  Returns false when this CTA
+// gave up (time or poll limit, or another CTA's abort).
+__device__ __forceinline__ bool pow_barrier(unsigned* bar, unsigned* flag, unsigned phase_no, unsigned target,
+                                            int* status) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
     __threadfence();
-    atomicAdd(bar, 1u);
+    const unsigned prev = atomicAdd(bar, 1u);
     int ok = 1;
-    const unsigned long long t0 = pow_clock_ns();
-    for (unsigned polls = 0;; ++polls) {
-      if (pow_ld_acquire(bar) >= target) break;
-      if ((polls & 255u) == 255u) {
-        if (*(volatile int*)status != 0 || pow_clock_ns() - t0 > kPowBarrierNs || polls > kPowMaxPolls) {
-          atomicExch(status, 1);
-          ok = 0;
-          break;
+    if (prev == target - 1u) {
+      __threadfence();  // every arrival (and the partials fenced before it) precedes the release
+      asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(flag), "r"(phase_no) : "memory");
+    } else {
+      const unsigned long long t0 = pow_clock_ns();
+      unsigned backoff = 32;
+      for (unsigned polls = 0;; ++polls) {
+        if (pow_ld_acquire(flag) >= phase_no) break;
+        if ((polls & 63u) == 63u) {
+          if (*(volatile int*)status != 0 || pow_clock_ns() - t0 > kPowBarrierNs || polls > kPowMaxPolls) {
+            atomicExch(status, 1);
+            ok = 0;
+            break;
+          }
         }
+        __nanosleep(backoff);
+        if (backoff < 256) backoff <<= 1;
       }
-      __nanosleep(32);
     }
     __threadfence();
     s_ok = ok;
@@ -272,7 +283,7 @@ __global__ void __launch_bounds__(kPowBlock, 2) k_power_persistent(PowArgs<V> a)
         for (int k = 0; k < 3; ++k) part[((size_t)c * G + blockIdx.x) * 3 + k] = r[c][k];
       }
     }
-    if (!pow_barrier(a.bar, (unsigned)G * (phase + 1u), a.status)) {
+    if (!pow_barrier(a.bar, a.bar + 32, phase + 1u, (unsigned)G * (phase + 1u), a.status)) {
       ok = false;
       break;
     }
