@@ -12,7 +12,8 @@ from batched plain-HPR solves to 1e-8; held-out instances are then solved to
   batch_fp64    one batched solve, plain FP64
   batch_fp32    one batched solve, FP32 storage + FP64 polish
   batch_learned as batch_fp32, started from the network's x0 (proposal time
-                included); batch_learned_sigma also takes its sigma0
+                included); batch_learned_sigma also takes its sigma0;
+                batch_learned_sigma_only takes sigma0 alone
 
 Every solve must end OPTIMAL with the objective within 1e-6 (relative) of
 the sequential FP64 solve.  Prints one JSON line.
@@ -146,6 +147,7 @@ def main(argv=None):
     out["x0_zero_rel_err"] = 1.0
     batched("batch_learned", "fp32_polish", x0=x0, extra_s=t_prop)
     batched("batch_learned_sigma", "fp32_polish", x0=x0, sg=sg, extra_s=t_prop)
+    batched("batch_learned_sigma_only", "fp32_polish", sg=sg, extra_s=t_prop)
     print(json.dumps(out), flush=True)
 
 
