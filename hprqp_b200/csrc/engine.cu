@@ -516,11 +516,12 @@ void Engine<V>::qap_apply(const V* xin, V* yout) {
   const int N = (int)std::lround(std::sqrt((double)n));
   if constexpr (std::is_same<V, float>::value) {
     if (cm.tc_qap) {
-      gemm_3xtf32(N, 1.0f, qA, xin, 0.0f, qTmp, cm.stream);
-      gemm_3xtf32(N, 2.0f, qTmp, qB, 0.0f, yout, cm.stream);
-      gemm_3xtf32(N, -2.0f, qS, xin, 1.0f, yout, cm.stream);
-      gemm_3xtf32(N, -2.0f, xin, qT, 1.0f, yout, cm.stream);
-      cm.launches += 4;
+      if (!qws) qws = mem.alloc<float>(gemm_3xtf32_ws_floats(N));
+      gemm_3xtf32_ws(N, 1.0f, qA, xin, 0.0f, qTmp, qws, cm.stream);
+      gemm_3xtf32_ws(N, 2.0f, qTmp, qB, 0.0f, yout, qws, cm.stream);
+      gemm_3xtf32_ws(N, -2.0f, qS, xin, 1.0f, yout, qws, cm.stream);
+      gemm_3xtf32_ws(N, -2.0f, xin, qT, 1.0f, yout, qws, cm.stream);
+      cm.launches += 12;
       return;
     }
   }

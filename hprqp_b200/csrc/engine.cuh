@@ -123,6 +123,7 @@ class Engine {
 
   DCsr<V> A, AT, Q, L, LT;
   V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;
+  float* qws = nullptr;  // TF32 operand images of the tensor-core QAP products
 
   void reset_state();
   void set_sigma(double s);  // + diagonal factors (unified_update_Q_factors!)
