@@ -17,7 +17,8 @@ LIB_PATH = os.path.join(HERE, "libhprqp.so")
 # Every entry point declared in include/hprqp.h
 EXPORTS = ("hprqp_abi_info", "hprqp_default_params", "hprqp_create", "hprqp_load", "hprqp_prepare",
            "hprqp_solve", "hprqp_set_trace", "hprqp_profile_iterations", "hprqp_get_pass_stats",
-           "hprqp_power_lambda_noalloc", "hprqp_gemm_3xtf32", "hprqp_last_error", "hprqp_destroy")
+           "hprqp_power_lambda_noalloc", "hprqp_gemm_3xtf32", "hprqp_gemm_3xtf32_ws_floats",
+           "hprqp_gemm_3xtf32_ws", "hprqp_last_error", "hprqp_destroy")
 
 _lib = None
 
@@ -61,6 +62,10 @@ def load():
     L.hprqp_power_lambda_noalloc.restype = C.c_int
     L.hprqp_gemm_3xtf32.argtypes = [C.c_int32, C.c_float, vp, vp, C.c_float, vp, vp]
     L.hprqp_gemm_3xtf32.restype = C.c_int
+    L.hprqp_gemm_3xtf32_ws_floats.argtypes = [C.c_int32]
+    L.hprqp_gemm_3xtf32_ws_floats.restype = C.c_int64
+    L.hprqp_gemm_3xtf32_ws.argtypes = [C.c_int32, C.c_float, vp, vp, C.c_float, vp, vp, vp]
+    L.hprqp_gemm_3xtf32_ws.restype = C.c_int
     L.hprqp_last_error.argtypes = [vp]
     L.hprqp_last_error.restype = C.c_char_p
     L.hprqp_destroy.argtypes = [vp]

@@ -363,6 +363,23 @@ bool gemm_3xtf32_failed(cudaStream_t st) {
 // ---------------------------------------------------------------------------
 // C ABI (include/hprqp.h)
 // ---------------------------------------------------------------------------
+extern "C" int64_t hprqp_gemm_3xtf32_ws_floats(int32_t n) { return n > 0 ? hprqp::gemm_3xtf32_ws_floats(n) : 0; }
+
+extern "C" int hprqp_gemm_3xtf32_ws(int32_t n, float alpha, const float* A, const float* B, float beta, float* C,
+                                    float* ws, void* stream) {
+  try {
+    if (n < 0 || (n > 0 && (!A || !B || !C || !ws))) return -1;
+    const cudaStream_t st = (cudaStream_t)stream;
+    hprqp::gemm_3xtf32_ws(n, alpha, A, B, beta, C, ws, st);
+    return 0;
+  } catch (const hprqp::Error& e) {
+    std::fprintf(stderr, "hprqp_gemm_3xtf32_ws: %s\n", e.what());
+    return e.code;
+  } catch (...) {
+    return -2;
+  }
+}
+
 extern "C" int hprqp_gemm_3xtf32(int32_t n, float alpha, const float* A, const float* B, float beta, float* C,
                                  void* stream) {
   try {

@@ -9,9 +9,11 @@
                    the oracle) so no power-method launches precede the passes.
 --mode solve:      one full solve to 1e-6 (power method included).
 --mode gemm:       the 3xTF32 tensor-core GEMM of the FP32 QAP operator on
-                   --n x --n FP32 matrices (--iters timed launches after 3
-                   warm-up launches); reports time and TFLOP/s (2 n^3 per
-                   product; the tensor pipe executes 3x that).
+                   --n x --n FP32 matrices with a preallocated workspace
+                   (--iters timed calls after 3 warm-up calls, each call =
+                   the two TF32 image splits + the GEMM); reports time and
+                   TFLOP/s (2 n^3 per product; the tensor pipe executes 3x
+                   that).
 Prints one JSON line with the per-pass CUDA-event times.
 """
 import argparse
@@ -71,9 +73,10 @@ def _gemm(n, iters):
     L = load()
     g = torch.Generator(device="cuda").manual_seed(0)
     A, B, Cm = (torch.randn(n * n, device="cuda", generator=g) for _ in range(3))
+    ws = torch.empty(int(L.hprqp_gemm_3xtf32_ws_floats(n)), device="cuda", dtype=torch.float32)
     st = torch.cuda.current_stream()
-    call = lambda: L.hprqp_gemm_3xtf32(n, C.c_float(1.0), A.data_ptr(), B.data_ptr(), C.c_float(0.0),
-                                       Cm.data_ptr(), C.c_void_p(st.cuda_stream))
+    call = lambda: L.hprqp_gemm_3xtf32_ws(n, C.c_float(1.0), A.data_ptr(), B.data_ptr(), C.c_float(0.0),
+                                          Cm.data_ptr(), ws.data_ptr(), C.c_void_p(st.cuda_stream))
     for _ in range(3):
         assert call() == 0
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -84,6 +87,8 @@ def _gemm(n, iters):
         e1.record(st)
         torch.cuda.synchronize()
         ms.append(e0.elapsed_time(e1))
+    assert L.hprqp_gemm_3xtf32(8, C.c_float(1.0), A.data_ptr(), B.data_ptr(), C.c_float(0.0), Cm.data_ptr(),
+                               C.c_void_p(st.cuda_stream)) == 0  # also reports a timed-out wait of the runs above
     ms.sort()
     t = ms[len(ms) // 2] / 1e3
     return dict(n=n, ms=t * 1e3, tflops=2.0 * n ** 3 / t / 1e12, tensor_tflops=6.0 * n ** 3 / t / 1e12)

@@ -282,6 +282,15 @@ int hprqp_power_lambda_noalloc(int64_t m, int64_t n,
 int hprqp_gemm_3xtf32(int32_t n, float alpha, const float* A, const float* B, float beta, float* C,
                       void* stream);
 
+/* The same product with a caller-owned workspace `ws` of
+ * hprqp_gemm_3xtf32_ws_floats(n) floats (device memory) that holds the
+ * operands pre-split into TF32 hi/lo images; enqueued on `stream` without
+ * synchronising (a timed-out internal wait is reported by the next
+ * hprqp_gemm_3xtf32 call). */
+int64_t hprqp_gemm_3xtf32_ws_floats(int32_t n);
+int hprqp_gemm_3xtf32_ws(int32_t n, float alpha, const float* A, const float* B, float beta, float* C, float* ws,
+                         void* stream);
+
 /* Text of the last error on this handle ("" if none); valid until the next
  * call on the handle.  h may be NULL for errors from hprqp_create. */
 const char* hprqp_last_error(hprqp_handle h);
