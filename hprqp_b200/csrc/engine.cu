@@ -50,6 +50,8 @@ void Common::init() {
   if (rc) reduce_cap = std::max(1, std::min(std::atoi(rc), kReduceGridLimit));
   const char* pel = std::getenv("HPRQP_POWER_ELL");
   pow_prefer_ell = pel && pel[0] == '1';
+  const char* pg = std::getenv("HPRQP_POWER_GRAM");
+  if (pg) pow_gram = pg[0] == '0' ? 0 : 1;
   const char* pc = std::getenv("HPRQP_POWER_CTAS_PER_SM");
   if (pc) pow_ctas_per_sm = std::atoi(pc);
 }
@@ -358,16 +360,18 @@ void Engine<V>::mat_rows(const DCsr<V>& M, const V* xin, const Epi& e) {
 }
 
 // Fused product + reduction on M's format (FP64 accumulation).
-template <int K, unsigned MM, typename V, typename Epi, typename Fin = NoFin>
-static void mat_reduce(Common& cm, const DCsr<V>& M, const V* xin, const Epi& e, double* out, const Fin& fin = Fin()) {
+// (The input vector may be wider than the matrix values: the Gram chain
+// keeps its FP64 state under an FP32 Gram matrix.)
+template <int K, unsigned MM, typename V, typename X, typename Epi, typename Fin = NoFin>
+static void mat_reduce(Common& cm, const DCsr<V>& M, const X* xin, const Epi& e, double* out, const Fin& fin = Fin()) {
   if (M.ell) {  // 4 rows per thread in flight
     const int grid = reduce_grid(M.rows, 1, cm.reduce_cap);
-    launch(cm, k_ell_reduce<4, K, MM, double, V, Epi, Fin>, grid, kBlock, M.rows,
-           EllSrc<V, V>{M.ecol, M.evalv, xin, M.rows, M.ell_w}, e, cm.rws, out, fin);
+    launch(cm, k_ell_reduce<4, K, MM, double, V, X, Epi, Fin>, grid, kBlock, M.rows,
+           EllSrc<V, X>{M.ecol, M.evalv, xin, M.rows, M.ell_w}, e, cm.rws, out, fin);
     return;
   }
-  else if (M.sell) reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, V>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
-  else reduce<K, MM, double>(cm, M.tpr, M.rows, CsrSrc<V, V>{M.ptr, M.col, M.val, xin}, e, out, fin);
+  else if (M.sell) reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, X>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
+  else reduce<K, MM, double>(cm, M.tpr, M.rows, CsrSrc<V, X>{M.ptr, M.col, M.val, xin}, e, out, fin);
 }
 
 // Row-schedule autotuner: time the plain product for each threads-per-row
@@ -414,8 +418,94 @@ int Engine<V>::autotune(DCsr<V>& d) {
   return best_t;
 }
 
+// Values of the Gram matrix G = A'A: G_pj = sum over the rows r of A with
+// entries in both columns p and j of A_rp A_rj, in increasing r (a merge of
+// rows p and j of A'), FP64 sums rounded once to V.  G_jp runs the same
+// merge with the factors swapped, so G is exactly symmetric.  Row p's entry
+// t goes to out[base(p) + t * stride] (CSR: base = ptr[p], stride 1; ELL:
+// base = p, stride = rows; SELL-32: base = sptr[p / 32] + p % 32, stride 32).
 template <typename V>
-Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int path_, int tpr_Q, int tpr_A)
+__global__ void __launch_bounds__(kBlock) k_gram_vals(int rows, const int* __restrict__ tptr,
+                                                      const int* __restrict__ tcol, const V* __restrict__ tval,
+                                                      const int* __restrict__ gptr, const int* __restrict__ gcol,
+                                                      int layout, const int* __restrict__ sptr, V* __restrict__ out) {
+  const int p = blockIdx.x * kBlock + threadIdx.x;
+  if (p >= rows) return;
+  const int b1 = tptr[p], e1 = tptr[p + 1];
+  const int gb = gptr[p], ge = gptr[p + 1];
+  const int64_t base = layout == 0 ? (int64_t)gb : layout == 1 ? (int64_t)p : (int64_t)sptr[p >> 5] + (p & 31);
+  const int64_t stride = layout == 0 ? 1 : layout == 1 ? (int64_t)rows : 32;
+  for (int k = gb; k < ge; ++k) {
+    const int j = gcol[k];
+    int a = b1, b = tptr[j];
+    const int e2 = tptr[j + 1];
+    double acc = 0.0;
+    while (a < e1 && b < e2) {
+      const int ra = tcol[a], rb = tcol[b];
+      if (ra == rb) {
+        acc += (double)tval[a] * (double)tval[b];
+        ++a;
+        ++b;
+      } else if (ra < rb) {
+        ++a;
+      } else {
+        ++b;
+      }
+    }
+    out[base + (int64_t)(k - gb) * stride] = (V)acc;
+  }
+}
+
+// Values of G into the format its products use (the padding of ELL / SELL
+// copies stays zero from their construction)
+template <typename V>
+void Engine<V>::gram_values() {
+  const int layout = G.ell ? 1 : G.sell ? 2 : 0;
+  V* out = const_cast<V*>(G.ell ? G.evalv : G.sell ? G.sval : G.val);
+  k_gram_vals<V><<<(G.rows + kBlock - 1) / kBlock, kBlock, 0, cm.stream>>>(G.rows, AT.ptr, AT.col, AT.val, G.ptr,
+                                                                            G.col, layout, G.sptr, out);
+  HPRQP_LAUNCH_CHECK();
+  cm.launches++;
+}
+
+// The A A' chain's Gram matrix: pattern on the host (gram_pattern), values on
+// the device, then the ELL / SELL-32 copies and the row-schedule autotuner
+// as for the problem's own matrices.  Skipped (the chain then runs its two
+// products per step) for LASSO and QAP operators, when disabled, when the
+// product work exceeds its bound, or, in the automatic mode, when A'A has
+// more than 3 nnz(A) entries.
+template <typename V>
+void Engine<V>::build_gram(const Prepared& pp) {
+  gram = false;
+  if (m <= 0 || is_qap || is_lasso || cm.pow_gram == 0 || pp.A.nnz() == 0) return;
+  const bool force = cm.pow_gram == 1;
+  const int64_t nnzA = pp.A.nnz();
+  HCsr h;
+  if (!gram_pattern(pp.A, pp.AT, (force ? 64 : 6) * nnzA, h)) return;
+  if (!force && h.nnz() > 3 * nnzA) return;
+  G = DCsr<V>();
+  G.rows = G.cols = (int)n;
+  G.nnz = h.nnz();
+  int* ptr = mem.alloc<int>(n + 1);
+  int* col = mem.alloc<int>(G.nnz);
+  cm.to_dev(ptr, h.ptr.data(), sizeof(int) * (n + 1));
+  cm.to_dev(col, h.col.data(), sizeof(int) * G.nnz);
+  G.ptr = ptr;
+  G.col = col;
+  G.val = mem.alloc<V>(G.nnz);
+  gu0 = mem.alloc<double>(n);
+  gu1 = mem.alloc<double>(n);
+  gram_values();  // CSR values, copied into the padded formats next
+  build_sell(h, G);
+  build_ell(h, G);
+  G.tpr = autotune(G);
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+  gram = true;
+}
+
+template <typename V>
+Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int path_, int tpr_Q, int tpr_A,
+                  bool power_engine)
     : cm(c_) {
   n = hp.n;
   m = hp.m;
@@ -471,6 +561,7 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
     qT = upload<V>(cm, mem, hp.qT, N2);
     qTmp = mem.alloc<V>(N2);
   }
+  if (power_engine) build_gram(pp);
   reset_state();
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
 }
@@ -651,6 +742,7 @@ template <typename V>
 double Engine<V>::power_step_bytes(int which) const {
   const double v = sizeof(V);
   auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
+  if (which == 0 && gram) return csr(G) + 2.0 * n * 8.0;  // FP64 state
   if (which == 0) return m > 0 ? csr(AT) + csr(A) + 2.0 * n * v + 3.0 * m * v : 0.0;
   if (is_qap) return 0.0;
   if (is_lasso) return csr(L) + csr(LT) + 2.0 * L.rows * v + 3.0 * n * v;
@@ -1065,6 +1157,14 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     return d;
   };
   const DCsr<V> pA = ellp(A), pAT = ellp(AT), pQ = ellp(Q), pL = ellp(L), pLT = ellp(LT);
+  // A A' on the Gram matrix: G's values for this solve, u_0 = A' z_0 (the
+  // chain's n-space state; 1/||z_0|| is already in scal + 4), then one
+  // sweep of G per step
+  const bool use_gram = gram && ca.on;
+  if (use_gram) {
+    gram_values();
+    mat_rows(pAT, pz, EpiStore<double>{gu0, 1.0});
+  }
   auto step = [&](const Chain& c, cudaStream_t st, int k) {
     use(c, st);
     V* zc = (k & 1) ? c.z1 : c.z0;
@@ -1080,7 +1180,11 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
       reduce<3, 0u, double>(cm, 1, len, VecSrc<V>{zn}, EpiPowerFused<V>{zc, nullptr, zz, false, inv}, c.scal + 1,
                             fin);
     };
-    if (c.which == 0) {  // A A' (power_iteration_A)
+    if (c.which == 0 && use_gram) {  // u ping-pongs between gu0 and gu1
+      const double* uc = (k & 1) ? gu1 : gu0;
+      double* un = (k & 1) ? gu0 : gu1;
+      mat_reduce<2, 0u>(cm, G, uc, EpiGramPower<double>{uc, un, inv}, c.scal + 1, GramPowerFin{c.log, k, c.scal + 4});
+    } else if (c.which == 0) {  // A A' (power_iteration_A)
       mat_rows(pAT, zc, EpiStoreInvNorm<V>{c.t, zz, inv});
       if (cm.pow_split) {
         mat_rows(pA, c.t, EpiStore<V>{zn, 1.0});

@@ -76,6 +76,10 @@ struct Common {  // per-handle resources shared by the engines
   int reduce_cap = kMaxReduceGrid;  // CTAs of a grid-stride reduction (HPRQP_REDUCE_CAP)
   bool pow_prefer_ell = false;  // HPRQP_POWER_ELL=1: power sweeps on ELL copies
   bool pow_split = false;       // HPRQP_POWER_SPLIT=1: product pass + separate dot reduction
+  // A A' chain on the Gram matrix A'A (HPRQP_POWER_GRAM): -1 = when A'A has
+  // at most 3 nnz(A) entries, 0 = never, 1 = whenever its product work
+  // (sum of squared row lengths of A) stays within 64 nnz(A)
+  int pow_gram = -1;
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;
   void init();
@@ -102,7 +106,10 @@ struct PendingMnorm {
 template <typename V>
 class Engine {
  public:
-  Engine(Common& cm, const HostProblem& hp, const Prepared& pp, int path, int tpr_mode_Q, int tpr_mode_A);
+  // power_engine: this engine runs the power method (it then builds the
+  // Gram matrix of the A A' chain where that applies)
+  Engine(Common& cm, const HostProblem& hp, const Prepared& pp, int path, int tpr_mode_Q, int tpr_mode_A,
+         bool power_engine = true);
   int64_t n, m;
   int path;
   bool Q_is_diag, has_Q_sparse, is_qap, is_lasso;
@@ -122,6 +129,11 @@ class Engine {
   V *pz, *pq, *pt;                    // power method vectors
 
   DCsr<V> A, AT, Q, L, LT;
+  // Gram matrix G = A'A (n x n) of the A A' power chain; its values are
+  // formed on the device at every power method (gram_values)
+  DCsr<V> G;
+  bool gram = false;
+  double *gu0 = nullptr, *gu1 = nullptr;  // the Gram chain's state u_k (FP64 in both engines)
   V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;
   float* qws = nullptr;  // TF32 operand images of the tensor-core QAP products
 
@@ -175,6 +187,8 @@ class Engine {
   void build_sell(const HCsr& h, DCsr<V>& d);
   void build_ell(const HCsr& h, DCsr<V>& d);
   void qap_apply(const V* xin, V* yout);
+  void build_gram(const Prepared& pp);
+  void gram_values();
 };
 
 }  // namespace hprqp

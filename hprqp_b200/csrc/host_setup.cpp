@@ -193,6 +193,61 @@ HCsr transpose(const HCsr& A) {
   return T;
 }
 
+bool gram_pattern(const HCsr& A, const HCsr& AT, int64_t max_work, HCsr& G) {
+  G = HCsr();
+  const int64_t n = AT.rows, m = A.rows;
+  if (n <= 0 || m <= 0 || A.nnz() == 0) return false;
+  int64_t work = 0;
+  for (int64_t r = 0; r < m; ++r) {
+    const int64_t len = A.ptr[r + 1] - A.ptr[r];
+    work += len * len;
+  }
+  if (work > max_work) return false;
+  bool sorted = true;
+#pragma omp parallel for schedule(static) reduction(&& : sorted) num_threads(host_threads(n))
+  for (int64_t p = 0; p < n; ++p)
+    for (int k = AT.ptr[p] + 1; k < AT.ptr[p + 1]; ++k) sorted = sorted && AT.col[k - 1] < AT.col[k];
+  if (!sorted) return false;
+  std::vector<int> len(n, 0);
+  // pass 0 counts, pass 1 writes; a per-thread marker array dedupes
+  for (int pass = 0; pass < 2; ++pass) {
+#pragma omp parallel num_threads(host_threads(n))
+    {
+      std::vector<int> mark(n, -1), list;
+#pragma omp for schedule(static)
+      for (int64_t p = 0; p < n; ++p) {
+        list.clear();
+        for (int k = AT.ptr[p]; k < AT.ptr[p + 1]; ++k) {
+          const int r = AT.col[k];
+          for (int t = A.ptr[r]; t < A.ptr[r + 1]; ++t) {
+            const int j = A.col[t];
+            if (mark[j] != (int)p) {
+              mark[j] = (int)p;
+              list.push_back(j);
+            }
+          }
+        }
+        if (pass == 0) {
+          len[p] = (int)list.size();
+        } else {
+          std::sort(list.begin(), list.end());
+          std::copy(list.begin(), list.end(), G.col.begin() + G.ptr[p]);
+        }
+      }
+    }
+    if (pass == 0) {
+      int64_t total = 0;
+      for (int64_t p = 0; p < n; ++p) total += len[p];
+      if (total > std::numeric_limits<int>::max()) return false;  // int row pointers
+      G.rows = G.cols = n;
+      G.ptr.assign(n + 1, 0);
+      for (int64_t p = 0; p < n; ++p) G.ptr[p + 1] = G.ptr[p] + len[p];
+      G.col.resize(total);
+    }
+  }
+  return true;
+}
+
 void StartVectorStream::fill(double* out, int64_t count) {
   auto next = [this]() {
     uint64_t v = (s += 0x9E3779B97F4A7C15ULL);

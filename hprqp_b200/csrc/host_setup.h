@@ -25,7 +25,7 @@ struct HCsr {
   int64_t rows = 0, cols = 0;
   std::vector<int> ptr, col;
   std::vector<double> val;
-  int64_t nnz() const { return (int64_t)val.size(); }
+  int64_t nnz() const { return (int64_t)col.size(); }
 };
 
 struct HostProblem {  // the loaded, unscaled problem
@@ -69,6 +69,14 @@ void finish_common(const HostProblem& hp, Prepared& o);
 double norm_b_inf_org(const std::vector<double>& AL, const std::vector<double>& AU);
 double norm_inf(const std::vector<double>& v);
 HCsr transpose(const HCsr& A);
+// Pattern of the Gram matrix G = A'A (n x n) from A (CSR) and A' (CSR of
+// the transpose): row p holds the columns of every row of A that has an
+// entry in column p, sorted and without repeats.  Only ptr and col are
+// filled (the values are formed on the device).  Returns false, leaving G
+// empty, when A' has a row that is not strictly increasing (the device
+// merge needs sorted rows) or when the product's work, sum over the rows of
+// A of their length squared, exceeds max_work.
+bool gram_pattern(const HCsr& A, const HCsr& AT, int64_t max_work, HCsr& G);
 // Host threads for a row-parallel loop over `work` items: 1 below ~64k
 // items (a parallel region costs more than it saves there), else at most
 // 16 (the loops are memory-bound; more threads only add wake-up cost).

@@ -225,8 +225,8 @@ __global__ void __launch_bounds__(kBlock) k_row_reduce(int nrows, Src src, Epi e
 // thread in flight (rows r0 + q * stride, so a warp's loads stay
 // coalesced): the col -> x gathers of R rows overlap instead of running one
 // row after another as in the grid-stride loop above.
-template <int R, int K, unsigned MaxMask, typename Acc, typename V, typename Epi, typename Fin = NoFin>
-__global__ void __launch_bounds__(kBlock) k_ell_reduce(int nrows, EllSrc<V, V> src, Epi epi, ReduceWs ws,
+template <int R, int K, unsigned MaxMask, typename Acc, typename V, typename X, typename Epi, typename Fin = NoFin>
+__global__ void __launch_bounds__(kBlock) k_ell_reduce(int nrows, EllSrc<V, X> src, Epi epi, ReduceWs ws,
                                                        double* out, Fin fin = Fin()) {
   pdl_enter();
   double r[K];
@@ -614,6 +614,49 @@ struct PowerFin {
     log[2 * k] = lam;
     log[2 * k + 1] = sqrt(rr) / (sqrt(zz) + lam);
     if (inv_out) *inv_out = 1.0 / sqrt(zz);
+  }
+  template <int K>
+  __device__ __forceinline__ void operator()(const double (&)[K]) const {}
+};
+
+// The A A' power step carried in n-space on the Gram matrix G = A'A.  With
+// q_k = z_k / ||z_k|| the reference's iterate, w_k = A' q_k, and
+// u_k = G w_{k-1} kept unnormalised (w_k = u_k / ||z_k||):
+//   z_{k+1} = A w_k,  lambda_k = q_k . z_{k+1} = ||w_k||^2,
+//   ||z_{k+1}||^2 = w_k . G w_k,  ||z_{k+1} - lambda_k q_k||^2 = ||z_{k+1}||^2 - lambda_k^2,
+// i.e. the same (lambda, err) sequence with one sweep of G per step.
+// Row i: u_{k+1,i} = (G u_k)_i / ||z_k||; sums 0: w.u_{k+1}, 1: w.w.  The
+// state is kept in FP64 whatever G's type: ||z||^2 - lambda^2 cancels to
+// ~4e-8 lambda^2 at the 1e-4 stopping test, and FP32 rounding of u would
+// move that difference by several per cent (the stop by up to ~100 steps).
+template <typename V>
+struct EpiGramPower {
+  const V* uc;
+  V* un;
+  const double* inv_norm;  // 1 / ||z_k||
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, double (&r)[2]) const {
+    const double s = *inv_norm;
+    const double v = (double)acc * s;
+    un[i] = (V)v;
+    const double w = (double)uc[i] * s;
+    r[0] += w * v;
+    r[1] += w * w;
+  }
+};
+
+// Last-CTA step of a Gram power step: log (lambda, err) for iteration k and
+// store 1/||z_{k+1}|| for the next step's rows
+struct GramPowerFin {
+  double* log;
+  int k;
+  double* inv_out;
+  __device__ __forceinline__ void operator()(const double (&a)[2]) const {
+    const double zz = a[0], lam = a[1];
+    const double rr = fmax(zz - lam * lam, 0.0);
+    log[2 * k] = lam;
+    log[2 * k + 1] = sqrt(rr) / (sqrt(zz) + lam);
+    *inv_out = 1.0 / sqrt(zz);
   }
   template <int K>
   __device__ __forceinline__ void operator()(const double (&)[K]) const {}

@@ -370,7 +370,7 @@ static void prepare(Handle& H, const hprqp_params& p) {
   if (H.prepared && std::memcmp(key, H.key, sizeof(key)) == 0) {
     // same scaling and schedule: only add the FP32 engine if it is missing
     if (p.precision == HPRQP_PRECISION_FP32_POLISH && !H.e32)
-      H.e32 = std::make_unique<Engine<float>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A);
+      H.e32 = std::make_unique<Engine<float>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A, true);
     return;
   }
   const double t = now_s();
@@ -387,9 +387,12 @@ static void prepare(Handle& H, const hprqp_params& p) {
   if (H.hp.Q_kind == HPRQP_Q_LASSO) H.path = PATH_LASSO;
   else if (H.hp.Q_kind == HPRQP_Q_QAP || H.pp.Q.nnz() > 0) H.path = H.pp.noC ? PATH_NOC : PATH_QP;
   else H.path = PATH_LP;
-  H.e64 = std::make_unique<Engine<double>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A);
-  if (p.precision == HPRQP_PRECISION_FP32_POLISH)
-    H.e32 = std::make_unique<Engine<float>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A);
+  // the power method runs on the first phase's engine: only that one builds
+  // the Gram matrix of the A A' chain
+  const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
+  H.e64 = std::make_unique<Engine<double>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A, !fp32);
+  if (fp32)
+    H.e32 = std::make_unique<Engine<float>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A, true);
   std::memcpy(H.key, key, sizeof(key));
   H.prepared = true;
   H.setup_time = now_s() - t;

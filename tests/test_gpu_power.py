@@ -69,3 +69,34 @@ def test_persistent_kernel_matches_launch_chain():
     for k in CASES:
         for a, b in zip(out["1"][k], out["0"][k]):
             assert abs(a - b) <= 1e-10 * max(abs(b), 1e-300), (k, a, b)
+
+
+def _lambdas_with_env(env_over, precision):
+    code = ("import json; from hprqp_b200 import HPRQP_parameters, Solver; from tests.test_gpu_power import CASES\n"
+            "out = {}\n"
+            "for k, (fn, pt) in CASES.items():\n"
+            "    s = Solver(0).load(fn())\n"
+            f"    r = s.solve(HPRQP_parameters(verbose=False, problem_type=pt, max_iter=0, precision='{precision}'))\n"
+            "    s.close()\n"
+            "    out[k] = [r.lambda_max_A, r.power_iter_A, r.lambda_max_Q, r.power_iter_Q]\n"
+            "print(json.dumps(out))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, **env_over)
+    r = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-10), ("fp32_polish", 1e-6)])
+def test_gram_chain_matches_two_product_chain(precision, rtol):
+    """The A A' chain on the Gram matrix A'A (forced on every case) runs the
+    reference's iteration in n-space: same stopping step and the same lambda
+    to rounding as the chain of two products per step."""
+    on = _lambdas_with_env({"HPRQP_POWER_GRAM": "1"}, precision)
+    off = _lambdas_with_env({"HPRQP_POWER_GRAM": "0"}, precision)
+    for k in CASES:
+        lam1, it1, lq1, iq1 = on[k]
+        lam0, it0, lq0, iq0 = off[k]
+        assert it1 == it0, (k, it1, it0)
+        assert abs(lam1 - lam0) <= rtol * max(abs(lam0), 1e-300), (k, lam1, lam0)
+        assert (lq1, iq1) == (lq0, iq0), k  # the Q chain is untouched
