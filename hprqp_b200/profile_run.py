@@ -58,7 +58,7 @@ def main(argv=None):
             p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr in ("sell", "ell") else int(a.tpr)
         r = s.solve(p)
         out = dict(status=r.status, iter=r.iter, iter_fp32=r.iter_fp32, time=r.time, device_time=r.device_time,
-                   power_time=r.power_time, kkt=r.residuals, launches=r.gpu_launches, passes=s.pass_stats())
+                   power_time=r.power_time, power_iter=[r.power_iter_A, r.power_iter_Q], kkt=r.residuals, launches=r.gpu_launches, passes=s.pass_stats())
     s.close()
     print(json.dumps(out))
     return 0
