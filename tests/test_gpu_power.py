@@ -99,4 +99,7 @@ def test_gram_chain_matches_two_product_chain(precision, rtol):
         lam0, it0, lq0, iq0 = off[k]
         assert it1 == it0, (k, it1, it0)
         assert abs(lam1 - lam0) <= rtol * max(abs(lam0), 1e-300), (k, lam1, lam0)
-        assert (lq1, iq1) == (lq0, iq0), k  # the Q chain is untouched
+        # the Q chain is the same code either way (its row schedule is
+        # autotuned per process, so only to rounding)
+        assert iq1 == iq0, (k, iq1, iq0)
+        assert abs(lq1 - lq0) <= rtol * max(abs(lq0), 1e-300), (k, lq1, lq0)
