@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <cstdlib>
@@ -418,6 +419,10 @@ int Engine<V>::autotune(DCsr<V>& d) {
   return best_t;
 }
 
+static double wall_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 // Values of the Gram matrix G = A'A: G_pj = sum over the rows r of A with
 // entries in both columns p and j of A_rp A_rj, in increasing r (a merge of
 // rows p and j of A'), FP64 sums rounded once to V.  G_jp runs the same
@@ -480,8 +485,10 @@ void Engine<V>::build_gram(const Prepared& pp) {
   if (m <= 0 || is_qap || is_lasso || cm.pow_gram == 0 || pp.A.nnz() == 0) return;
   const bool force = cm.pow_gram == 1;
   const int64_t nnzA = pp.A.nnz();
+  const double t0 = wall_s();
   HCsr h;
   if (!gram_pattern(pp.A, pp.AT, (force ? 64 : 6) * nnzA, h)) return;
+  const double t_pat = wall_s();
   if (!force && h.nnz() > 3 * nnzA) return;
   G = DCsr<V>();
   G.rows = G.cols = (int)n;
@@ -501,6 +508,11 @@ void Engine<V>::build_gram(const Prepared& pp) {
   G.tpr = autotune(G);
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   gram = true;
+  if (const char* tv = std::getenv("HPRQP_TIMING"))
+    if (tv[0] == '1')
+      std::fprintf(stderr, "[hprqp] Gram matrix A'A: %lld entries (A: %lld), pattern %.3f s, total %.3f s, %s\n",
+                   (long long)G.nnz, (long long)nnzA, t_pat - t0, wall_s() - t0,
+                   G.ell ? "ELL" : G.sell ? "SELL-32" : "CSR");
 }
 
 template <typename V>

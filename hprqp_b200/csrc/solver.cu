@@ -390,12 +390,18 @@ static void prepare(Handle& H, const hprqp_params& p) {
   // the power method runs on the first phase's engine: only that one builds
   // the Gram matrix of the A A' chain
   const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
+  const double t_scaled = now_s();
   H.e64 = std::make_unique<Engine<double>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A, !fp32);
+  const double t_e64 = now_s();
   if (fp32)
     H.e32 = std::make_unique<Engine<float>>(*H.cm, H.hp, H.pp, H.path, p.spmv_mode_Q, p.spmv_mode_A, true);
   std::memcpy(H.key, key, sizeof(key));
   H.prepared = true;
   H.setup_time = now_s() - t;
+  if (const char* tv = std::getenv("HPRQP_TIMING"))
+    if (tv[0] == '1')
+      std::fprintf(stderr, "[hprqp] setup: scaling %.3f s, FP64 engine %.3f s, FP32 engine %.3f s\n", t_scaled - t,
+                   t_e64 - t_scaled, now_s() - t_e64);
 }
 
 // estimate_eigenvalues + compute_lambda_max_Q (src/algorithm.jl:1407-1440,
