@@ -51,6 +51,8 @@ void Common::init() {
   if (rc) reduce_cap = std::max(1, std::min(std::atoi(rc), kReduceGridLimit));
   const char* pel = std::getenv("HPRQP_POWER_ELL");
   pow_prefer_ell = pel && pel[0] == '1';
+  const char* ep = std::getenv("HPRQP_EPI_PREFETCH");
+  if (ep) epi_prefetch = std::max(0, std::min(std::atoi(ep), 2));
   const char* pg = std::getenv("HPRQP_POWER_GRAM");
   if (pg) pow_gram = pg[0] == '0' ? 0 : 1;
   const char* pc = std::getenv("HPRQP_POWER_CTAS_PER_SM");
@@ -93,7 +95,7 @@ template <int TPR, typename Acc, typename Src, typename Epi>
 static void rows_t(Common& cm, int nrows, const Src& src, const Epi& epi) {
   const long long threads = (long long)nrows * TPR;
   const int grid = (int)((threads + kBlock - 1) / kBlock);
-  launch(cm, k_row_pass<TPR, Acc, Src, Epi>, grid, kBlock, nrows, src, epi);
+  launch(cm, k_row_pass<TPR, Acc, Src, Epi>, grid, kBlock, nrows, src, epi, cm.epi_prefetch);
 }
 
 template <typename Acc, typename Src, typename Epi>

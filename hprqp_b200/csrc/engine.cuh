@@ -80,6 +80,9 @@ struct Common {  // per-handle resources shared by the engines
   // at most 3 nnz(A) entries, 0 = never, 1 = whenever its product work
   // (sum of squared row lengths of A) stays within 64 nnz(A)
   int pow_gram = -1;
+  // pass epilogues prefetch their row operands before the product
+  // (HPRQP_EPI_PREFETCH: 0 off, 1 into L1, 2 into L2)
+  int epi_prefetch = 1;
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;
   void init();

@@ -15,6 +15,9 @@
 // results are deterministic and stay on the device.
 #pragma once
 
+#include <type_traits>
+#include <utility>
+
 #include "common.cuh"
 
 namespace hprqp {
@@ -91,13 +94,33 @@ __device__ __forceinline__ double clampd(double v, double lo, double hi) { retur
 // ---------------------------------------------------------------------------
 // Generic row kernels
 // ---------------------------------------------------------------------------
+// Epilogue operand prefetch: an epilogue may declare prefetch(i, level)
+// naming the vectors its row i reads; level 1 = into L1, 2 = into L2.
+template <typename E, typename = void>
+struct HasPrefetch : std::false_type {};
+template <typename E>
+struct HasPrefetch<E, std::void_t<decltype(std::declval<const E&>().prefetch(0, 1))>> : std::true_type {};
+
+__device__ __forceinline__ void pf_line(const void* p, int level) {
+  if (level == 1) asm volatile("prefetch.global.L1 [%0];" ::"l"(p));
+  else asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+template <typename... P>
+__device__ __forceinline__ void pf_rows(int i, int level, const P*... p) {
+  (pf_line(p + i, level), ...);
+}
+
 template <int TPR, typename Acc, typename Src, typename Epi>
-__global__ void __launch_bounds__(kBlock) k_row_pass(int nrows, Src src, Epi epi) {
+__global__ void __launch_bounds__(kBlock) k_row_pass(int nrows, Src src, Epi epi, int pf = 0) {
   pdl_enter();
   const long long g = (long long)blockIdx.x * kBlock + threadIdx.x;
   const int row = (int)(g / TPR);
   if (row >= nrows) return;  // whole row groups leave together
   const int lane = threadIdx.x & (TPR - 1);
+  // the epilogue's own operands do not depend on the row's product: ask for
+  // them before the dependent col -> x gathers, so their latency overlaps
+  if constexpr (HasPrefetch<Epi>::value)
+    if (pf && lane == 0) epi.prefetch(row, pf);
   const Acc acc = src.template dot<TPR, Acc>(row, lane);
   if (lane == 0) epi(row, acc);
 }
@@ -276,6 +299,10 @@ struct EpiZxw1 {
   const V *ATy, *c, *l, *u, *w, *fact1, *fact2;
   const double* last_x;
   double sigma, f1s, f2s, h1, h2;
+  __device__ __forceinline__ void prefetch(int i, int lv) const {
+    pf_rows(i, lv, x, w, ATy, c, l, u, last_x);
+    if (Diag) pf_rows(i, lv, fact1, fact2);
+  }
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
     const double qw = (double)acc;
@@ -304,6 +331,7 @@ struct EpiTempv {
   V* tempv;
   const V *x_hat, *Qw;
   double sigma;
+  __device__ __forceinline__ void prefetch(int i, int lv) const { pf_rows(i, lv, x_hat, Qw); }
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
     tempv[i] = (V)((double)x_hat[i] + sigma * ((double)Qw[i] - (double)acc));
@@ -320,6 +348,7 @@ struct EpiY {
   const V *AL, *AU;
   const double* last_y;
   double f1, f2, h1, h2;
+  __device__ __forceinline__ void prefetch(int i, int lv) const { pf_rows(i, lv, (const V*)y, AL, AU, last_y); }
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
     const double yi = y[i];
@@ -344,6 +373,10 @@ struct EpiW2 {
   const V* fact;
   const double *last_w, *last_ATy;
   double fs, h1, h2;
+  __device__ __forceinline__ void prefetch(int i, int lv) const {
+    pf_rows(i, lv, (const V*)w, (const V*)ATy, (const V*)w_bar, last_w, last_ATy);
+    if (Diag) pf_rows(i, lv, fact);
+  }
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
     const double atyb = (double)acc;
