@@ -51,6 +51,8 @@ void Common::init() {
   if (rc) reduce_cap = std::max(1, std::min(std::atoi(rc), kReduceGridLimit));
   const char* pel = std::getenv("HPRQP_POWER_ELL");
   pow_prefer_ell = pel && pel[0] == '1';
+  const char* at = std::getenv("HPRQP_AUTOTUNE");
+  autotune = !(at && at[0] == '0');
   const char* ep = std::getenv("HPRQP_EPI_PREFETCH");
   if (ep) epi_prefetch = std::max(0, std::min(std::atoi(ep), 2));
   const char* pg = std::getenv("HPRQP_POWER_GRAM");
@@ -384,6 +386,14 @@ template <typename V>
 int Engine<V>::autotune(DCsr<V>& d) {
   if (d.rows <= 0 || d.nnz == 0) return 1;
   const double avg = (double)d.nnz / d.rows;
+  if (!cm.autotune) {  // fixed rule: ELL, else SELL-32, else threads per row by mean row length
+    d.ell = d.ell_w > 0;
+    d.sell = !d.ell && d.sell_len > 0;
+    if (d.ell || d.sell) return 1;
+    int t = 1;
+    while (t < 32 && avg >= 4.0 * t) t *= 2;
+    return t;
+  }
   cudaEvent_t e0, e1;
   HPRQP_CUDA(cudaEventCreate(&e0));
   HPRQP_CUDA(cudaEventCreate(&e1));

@@ -83,6 +83,10 @@ struct Common {  // per-handle resources shared by the engines
   // pass epilogues prefetch their row operands before the product
   // (HPRQP_EPI_PREFETCH: 0 off, 1 into L1, 2 into L2)
   int epi_prefetch = 1;
+  // row-schedule autotuner (timed); HPRQP_AUTOTUNE=0 applies a fixed rule
+  // instead, e.g. under a profiler, whose serialisation makes the timings
+  // meaningless
+  bool autotune = true;
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
   DeviceMem mem;
   void init();
