@@ -215,7 +215,10 @@ def run_ours(args):
     nnzA, nnzQ = model.A.nnz, model.Q.Q.nnz
     solver = Solver(local_rank).load(model)
     modes = [args.precision] + (["fp64"] if args.precision != "fp64" else [])
-    params = {mode: HPRQP_parameters(verbose=False, precision=mode, profile_passes=True) for mode in modes}
+    # the timed solves run exactly as a user's do (no per-pass events); the per-pass
+    # statistics come from separate profiled solves after the timed region
+    params = {mode: HPRQP_parameters(verbose=False, precision=mode, profile_passes=False) for mode in modes}
+    prof_params = {mode: HPRQP_parameters(verbose=False, precision=mode, profile_passes=True) for mode in modes}
     for mode in modes:
         solver.prepare(params[mode])       # setup (scaling + upload) outside the timed region
     for _ in range(args.warmup):
@@ -232,15 +235,16 @@ def run_ours(args):
         for _ in range(args.steps):
             r = solver.solve(params[mode])
             results[mode].append(r)
-        stats[mode] = solver.pass_stats()
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    # the same solves without the per-pass events, to show they do not skew the value
-    unprof = {}
+    # outside the timed region: one solve per mode with CUDA events around every pass (the
+    # per-pass roofline), and whole plain iterations timed back to back (the iteration roofline)
+    with_events, iteration = {}, {}
     for mode in modes:
-        q = HPRQP_parameters(verbose=False, precision=mode, profile_passes=False)
-        unprof[mode] = barrier_max(statistics.mean(solver.solve(q).device_time for _ in range(args.steps)))
+        with_events[mode] = barrier_max(solver.solve(prof_params[mode]).device_time)
+        stats[mode] = solver.pass_stats()
+        iteration[mode] = solver.profile_iterations(params[mode], 50)
 
     def summarize(rs):
         dev = barrier_max(statistics.mean(r.device_time for r in rs))
@@ -272,6 +276,17 @@ def run_ours(args):
                 "share_of_iteration": round(best["share"], 3)}
     # the power method is the larger part of a solve: its aggregate bandwidth (algorithmic bytes of
     # all its steps over its CUDA-event-bracketed time inside the timed solves)
+    # whole plain iterations: algorithmic bytes of the four fused passes over the CUDA-event time of
+    # 50 iterations launched back to back exactly as the solve launches them
+    roof_iter = {}
+    for mode in modes:
+        it = iteration[mode]
+        if it["ms_per_iter"]:
+            ach_i = it["bytes_per_iter"] / (it["ms_per_iter"] * 1e-3) / 1e9
+            roof_iter["fp32" if mode == "fp32_polish" else "fp64"] = {
+                "bound": "hbm", "achieved": round(ach_i, 1), "peak": peak, "unit": "GB/s",
+                "frac": round(ach_i / peak, 4), "bytes_per_iteration": it["bytes_per_iter"],
+                "ms_per_iteration": it["ms_per_iter"], "peak_source": peak_kind}
     rp = results[args.precision][-1]
     roof_power = None
     if rp.power_bytes > 0 and head["power_s"] > 0:
@@ -290,7 +305,8 @@ def run_ours(args):
         e2e_t.append(time.perf_counter() - t)
         h2d, d2h = r.h2d_bytes, r.d2h_bytes
         setup = r.setup_time
-    e2e = {"value": barrier_max(statistics.mean(e2e_t)), "unit": "s", "h2d_bytes_per_step": h2d,
+    e2e = {"value": barrier_max(statistics.median(e2e_t)), "unit": "s", "statistic": "median",
+           "samples_s": [round(t, 4) for t in e2e_t], "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "setup_s_last": setup,
            "note": "hprqp_load + hprqp_solve from host arrays (host-side scaling, upload, solve, solution copy-back)"}
     cpu = None
@@ -303,7 +319,6 @@ def run_ours(args):
                "sample": f"oracle power method in full + {args.cpu_sample_iters} HPR iterations, extrapolated "
                          f"to {iters} iterations (FP64 iteration count to 1e-6)", **det}
     fp64 = summ.get("fp64", head)
-    st64 = stats[args.precision]["fp64"]
     loop_s = max(fp64["value"] - fp64["power_s"], 1e-9)
     line = {
         "metric": METRIC, "value": round(head["value"], 6), "unit": "s", "n_gpus": world, "steps": args.steps,
@@ -315,17 +330,14 @@ def run_ours(args):
                    "n": model.n, "m": model.m, "nnz_A": nnzA, "nnz_Q": nnzQ, "stoptol": 1e-6,
                    "precision": args.precision, "parallelism": f"replicas x{world}",
                    "l2": "inputs larger than L2 (>= 168 MB streamed per iteration vs 126 MB L2)"},
-        "value_without_pass_events": unprof[args.precision],
+        "value_with_pass_events": with_events[args.precision],
         "status": head["status"], "kkt": head["kkt"], "iters": head["iters"], "iters_fp32": head["iter_fp32"],
         "power_method_s": head["power_s"],
-        "plain_fp64": {"time_s": fp64["value"], "time_s_without_pass_events": unprof.get("fp64"),
+        "plain_fp64": {"time_s": fp64["value"], "time_s_with_pass_events": with_events.get("fp64"),
                        "iters": fp64["iters"], "power_method_s": fp64["power_s"],
-                       "iters_per_s": fp64["iters"] / loop_s,
-                       "hbm_gbs_plain_iteration": (st64["bytes_per_iter"] / (st64["ms_per_iter"] * 1e-3) / 1e9
-                                                   if st64["ms_per_iter"] else None),
-                       "ms_per_plain_iteration": st64["ms_per_iter"]},
+                       "iters_per_s": fp64["iters"] / loop_s},
         "speedup_vs_plain_fp64": fp64["value"] / head["value"] if head["value"] else None,
-        "roofline": roof, "roofline_power_method": roof_power, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        "roofline": roof, "roofline_iteration": roof_iter, "roofline_power_method": roof_power, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": head["launches"],
     }
     if rank == 0:

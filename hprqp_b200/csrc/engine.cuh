@@ -81,8 +81,10 @@ struct Common {  // per-handle resources shared by the engines
   // (sum of squared row lengths of A) stays within 64 nnz(A)
   int pow_gram = -1;
   // pass epilogues prefetch their row operands before the product
-  // (HPRQP_EPI_PREFETCH: 0 off, 1 into L1, 2 into L2)
-  int epi_prefetch = 1;
+  // (HPRQP_EPI_PREFETCH: 0 off, 1 into L1, 2 into L2); measured no faster
+  // on the 700x700 grid (FP32 iteration 40.3 vs 40.3 us, FP64 50.3 vs
+  // 48.4 us), so off by default
+  int epi_prefetch = 0;
   // row-schedule autotuner (timed); HPRQP_AUTOTUNE=0 applies a fixed rule
   // instead, e.g. under a profiler, whose serialisation makes the timings
   // meaningless
