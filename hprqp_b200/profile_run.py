@@ -8,6 +8,9 @@
                    injected (--lam-A/--lam-Q, defaults for the 700x700 grid from
                    the oracle) so no power-method launches precede the passes.
 --mode solve:      one full solve to 1e-6 (power method included).
+--mode power:      the power method alone (max_iter = 0): both chains, the
+                   A A' chain alone and the Q chain alone (the other's
+                   lambda given as --lam-Q / --lam-A), median of 5 solves.
 --mode gemm:       the 3xTF32 tensor-core GEMM of the FP32 QAP operator on
                    --n x --n FP32 matrices with a preallocated workspace
                    (--iters timed calls after 3 warm-up calls, each call =
@@ -29,7 +32,7 @@ def main(argv=None):
     ap.add_argument("--grid", type=int, default=700)
     ap.add_argument("--workload", default="grid", choices=["grid", "random_qp", "lasso"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32_polish"])
-    ap.add_argument("--mode", default="iterations", choices=["iterations", "solve", "gemm"])
+    ap.add_argument("--mode", default="iterations", choices=["iterations", "solve", "gemm", "power"])
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--lam-A", type=float, default=0.44866094653915195)
@@ -46,6 +49,23 @@ def main(argv=None):
     else:
         model, ptype = W.lasso(), "LASSO"
     s = Solver(0).load(model)
+    if a.mode == "power":
+        # the power method alone (max_iter = 0): both chains, then each chain with the other's
+        # lambda given, median of 5 solves each
+        out = {}
+        for tag, over in (("both", {}), ("A_only", {"lambda_max_Q_override": a.lam_Q}),
+                          ("Q_only", {"lambda_max_A_override": a.lam_A})):
+            p = HPRQP_parameters(verbose=False, precision=a.precision, problem_type=ptype, max_iter=0, **over)
+            ts, r = [], None
+            for _ in range(6):
+                r = s.solve(p)
+                ts.append(r.power_time)
+            ts = sorted(ts[1:])
+            out[tag] = dict(power_ms=ts[len(ts) // 2] * 1e3, steps=[r.power_iter_A, r.power_iter_Q],
+                            lam=[r.lambda_max_A, r.lambda_max_Q])
+        s.close()
+        print(json.dumps(out))
+        return 0
     if a.mode == "iterations":
         p = HPRQP_parameters(verbose=False, precision=a.precision, problem_type=ptype,
                              lambda_max_A_override=a.lam_A, lambda_max_Q_override=a.lam_Q)
