@@ -296,17 +296,22 @@ def run_ours(args):
                       "algorithmic_bytes": rp.power_bytes, "seconds": head["power_s"],
                       "share_of_solve": round(head["power_s"] / head["value"], 3) if head["value"] else None}
     # end to end through the public API from host buffers (load -> solve -> x,y,z,w on the host)
-    e2e_t, h2d, d2h, setup = [], 0, 0, 0.0
+    e2e_t, h2d, d2h, setup, parts = [], 0, 0, 0.0, []
     for _ in range(max(1, min(args.steps, 3))):
         t = time.perf_counter()
         s2 = Solver(local_rank).load(model)
+        t1 = time.perf_counter()
         r = s2.solve(HPRQP_parameters(verbose=False, precision=args.precision))
+        t2 = time.perf_counter()
         s2.close()
         e2e_t.append(time.perf_counter() - t)
         h2d, d2h = r.h2d_bytes, r.d2h_bytes
         setup = r.setup_time
+        parts.append({"load_s": round(t1 - t, 4), "solve_call_s": round(t2 - t1, 4),
+                      "setup_s": round(r.setup_time, 4), "solve_s": round(r.time, 4),
+                      "close_s": round(e2e_t[-1] - (t2 - t), 4)})
     e2e = {"value": barrier_max(statistics.median(e2e_t)), "unit": "s", "statistic": "median",
-           "samples_s": [round(t, 4) for t in e2e_t], "h2d_bytes_per_step": h2d,
+           "samples_s": [round(t, 4) for t in e2e_t], "parts": parts, "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "setup_s_last": setup,
            "note": "hprqp_load + hprqp_solve from host arrays (host-side scaling, upload, solve, solution copy-back)"}
     cpu = None
