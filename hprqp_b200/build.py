@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libhprqp.so")
-SOURCES = ["engine.cu", "solver.cu", "host_setup.cpp", "noalloc.cu", "mlp.cu", "batch.cu", "batch_qp.cu", "tc_gemm.cu", "scale.cu"]
+SOURCES = ["engine.cu", "solver.cu", "host_setup.cpp", "pool.cpp", "noalloc.cu", "mlp.cu", "batch.cu", "batch_qp.cu", "tc_gemm.cu", "scale.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

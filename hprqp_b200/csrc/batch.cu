@@ -29,6 +29,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "pool.h"
 #include "../../include/hprqp.h"
 #include "../../include/hprqp_batch.h"
 #include "batch_qp.h"
@@ -286,8 +287,7 @@ __global__ void k_each(int len, F f) {
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-struct Mem {
-  std::vector<void*> blocks;
+struct Mem : PoolBlocks {  // blocks of the library's device memory pool
   template <typename T>
   T* alloc(int64_t n) {  // zeroed
     T* p = alloc_raw<T>(n);
@@ -296,13 +296,7 @@ struct Mem {
   }
   template <typename T>
   T* alloc_raw(int64_t n) {  // for buffers that are written in full right away
-    void* p = nullptr;
-    HPRQP_CUDA(cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
-    blocks.push_back(p);
-    return (T*)p;
-  }
-  ~Mem() {
-    for (void* p : blocks) cudaFree(p);
+    return (T*)get(sizeof(T) * (size_t)std::max<int64_t>(n, 1));
   }
 };
 

@@ -34,6 +34,7 @@
 #include <type_traits>
 #include <vector>
 
+#include "pool.h"
 #include "batch_qp.h"
 #include "host_setup.h"
 #include "kernels.cuh"
@@ -582,18 +583,12 @@ __global__ void __launch_bounds__(kQapTcThreads) k_qap_tc(const int* qn, const i
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-struct Mem {
-  std::vector<void*> blocks;
+struct Mem : PoolBlocks {  // zeroed blocks of the library's device memory pool
   template <typename T>
   T* alloc(int64_t n) {
-    void* p = nullptr;
-    HPRQP_CUDA(cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    void* p = get(sizeof(T) * (size_t)std::max<int64_t>(n, 1));
     HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
-    blocks.push_back(p);
     return (T*)p;
-  }
-  ~Mem() {
-    for (void* p : blocks) cudaFree(p);
   }
 };
 

@@ -15,6 +15,7 @@
 #include <memory>
 #include <vector>
 
+#include "pool.h"
 #include "host_setup.h"
 #include "kernels.cuh"
 
@@ -38,20 +39,9 @@ enum Slot {
   kNumSlots = S_POWLOG_Q + 2 * kPowChunk,
 };
 
-struct DeviceMem {  // owns cudaMalloc'ed blocks
-  std::vector<void*> blocks;
-  void* get(size_t bytes) {
-    void* p = nullptr;
-    if (bytes == 0) bytes = 16;
-    HPRQP_CUDA(cudaMalloc(&p, bytes));
-    blocks.push_back(p);
-    return p;
-  }
+struct DeviceMem : PoolBlocks {  // owns blocks of the library's device memory pool
   template <typename T>
   T* alloc(int64_t count) { return (T*)get(sizeof(T) * (size_t)(count > 0 ? count : 1)); }
-  ~DeviceMem() {
-    for (void* p : blocks) cudaFree(p);
-  }
 };
 
 struct Common {  // per-handle resources shared by the engines

@@ -21,6 +21,7 @@
 #include <string>
 #include <vector>
 
+#include "pool.h"
 #include "../../include/hprqp.h"
 #include "../../include/hprqp_mlp.h"
 #include "common.cuh"
@@ -162,18 +163,16 @@ struct Net {
   float *Z1 = nullptr, *Z2 = nullptr, *Y = nullptr, *T = nullptr, *dYf = nullptr, *dH2 = nullptr, *dH1 = nullptr;
   double* sq = nullptr;
   int64_t step = 0;
-  std::vector<void*> blocks;
+  PoolBlocks mem;  // blocks of the library's device memory pool
   std::string err;
   template <typename T>
   T* alloc(int64_t n) {
-    void* p = nullptr;
-    HPRQP_CUDA(cudaMalloc(&p, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    void* p = mem.get(sizeof(T) * (size_t)std::max<int64_t>(n, 1));
     HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
-    blocks.push_back(p);
     return (T*)p;
   }
   ~Net() {
-    for (void* p : blocks) cudaFree(p);
+    pool_free(mem.blocks, mem.dev);
     if (st) cudaStreamDestroy(st);
   }
 };

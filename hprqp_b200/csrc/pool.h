@@ -1,0 +1,35 @@
+// pool.h — device memory of the library's engines and batches.
+//
+// Every device block the library owns comes from one stream-ordered memory
+// pool per GPU (cudaMemPoolCreate), whose release threshold keeps freed
+// memory mapped for the process: a handle that is destroyed and a new one
+// built for the next problem (the load -> solve -> destroy cycle of a caller
+// that solves many problems) reuse the physical pages instead of paying
+// cudaMalloc / cudaFree (page mapping, unmapping and an implicit device
+// synchronisation) for every block.  The pool keeps at most
+// HPRQP_POOL_KEEP_MB megabytes (default 8192) reserved once its blocks are
+// free; beyond that it returns memory to the driver.
+#pragma once
+
+#include <cstddef>
+#include <vector>
+
+namespace hprqp {
+
+// A block of `bytes` (at least 16) on the current device, usable on any
+// stream once this returns.  Throws Error(HPRQP_E_CUDA) when out of memory.
+void* pool_alloc(size_t bytes);
+
+// Return blocks allocated on device `dev`.  Waits for the device first (no
+// kernel of ours may still use them), never throws; clears the list.
+void pool_free(std::vector<void*>& blocks, int dev);
+
+// Owner of a list of pool blocks of one device, freed together.
+struct PoolBlocks {
+  std::vector<void*> blocks;
+  int dev = -1;
+  void* get(size_t bytes);
+  ~PoolBlocks() { pool_free(blocks, dev); }
+};
+
+}  // namespace hprqp

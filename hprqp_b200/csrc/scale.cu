@@ -16,6 +16,7 @@
 #include <cmath>
 #include <vector>
 
+#include "pool.h"
 #include "common.cuh"
 #include "host_setup.h"
 
@@ -99,17 +100,10 @@ __global__ void k_sym(int nnz, const int* ia, const int* ib, const double* qv, c
   sv[p] = v / 2.0;
 }
 
-struct DevBuf {  // cudaMalloc'ed scratch freed at scope exit
-  std::vector<void*> p;
+struct DevBuf : PoolBlocks {  // pool scratch freed at scope exit
   template <typename T>
-  T* get(int64_t n) {
-    void* q = nullptr;
-    HPRQP_CUDA(cudaMalloc(&q, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
-    p.push_back(q);
-    return (T*)q;
-  }
-  ~DevBuf() {
-    for (void* q : p) cudaFree(q);
+  T* take(int64_t n) {
+    return (T*)PoolBlocks::get(sizeof(T) * (size_t)std::max<int64_t>(n, 1));
   }
 };
 
@@ -187,19 +181,19 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   auto dev_csr = [&](const HCsr& h) {
     DM x;
     x.rows = (int)h.rows;
-    x.ptr = d.get<int>(h.rows + 1);
-    x.col = d.get<int>(h.nnz());
-    x.val = d.get<double>(h.nnz());
+    x.ptr = d.take<int>(h.rows + 1);
+    x.col = d.take<int>(h.nnz());
+    x.val = d.take<double>(h.nnz());
     up(x.ptr, h.ptr);
     up(x.col, h.col);
     up(x.val, h.val);
     return x;
   };
   const DM dA = dev_csr(hp.A), dAT = dev_csr(hp.AT), dQ = dev_csr(Q), dQT = dev_csr(QT);
-  double *c = d.get<double>(n), *l = d.get<double>(n), *u = d.get<double>(n), *cn = d.get<double>(n);
-  double *AL = d.get<double>(m), *AU = d.get<double>(m), *rn = d.get<double>(m);
-  double *ca = d.get<double>(n), *cq = d.get<double>(n), *tc = d.get<double>(n), *tci = d.get<double>(n);
-  double *ra = d.get<double>(m), *tr = d.get<double>(m), *tri = d.get<double>(m);
+  double *c = d.take<double>(n), *l = d.take<double>(n), *u = d.take<double>(n), *cn = d.take<double>(n);
+  double *AL = d.take<double>(m), *AU = d.take<double>(m), *rn = d.take<double>(m);
+  double *ca = d.take<double>(n), *cq = d.take<double>(n), *tc = d.take<double>(n), *tci = d.take<double>(n);
+  double *ra = d.take<double>(m), *tr = d.take<double>(m), *tri = d.take<double>(m);
   up(c, o.c);
   up(l, o.l);
   up(u, o.u);
@@ -228,9 +222,9 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   if (p.use_Ruiz_scaling)
     for (int k = 0; k < 10; ++k) pass(0);
   if (p.use_Pock_Chambolle_scaling) pass(1);
-  int* dia = d.get<int>(nnzS);
-  int* dib = d.get<int>(nnzS);
-  double* sv = d.get<double>(nnzS);
+  int* dia = d.take<int>(nnzS);
+  int* dib = d.take<int>(nnzS);
+  double* sv = d.take<double>(nnzS);
   up(dia, ia);
   up(dib, ib);
   k_sym<<<blocks(nnzS), kT, 0, st>>>((int)nnzS, dia, dib, dQ.val, dQT.val, sv);

@@ -852,10 +852,15 @@ const char* hprqp_last_error(hprqp_handle h) { return h ? h->err.c_str() : hprqp
 int hprqp_destroy(hprqp_handle h) {
   if (!h) return HPRQP_OK;
   cudaSetDevice(h->device);
+  const double t0 = hprqp::now_s();
   if (h->cm && h->cm->stream) cudaStreamSynchronize(h->cm->stream);
   h->e32.reset();
   h->e64.reset();
+  const double t1 = hprqp::now_s();
   delete h;
+  if (const char* tv = std::getenv("HPRQP_TIMING"))
+    if (tv[0] == '1')
+      std::fprintf(stderr, "[hprqp] destroy: engines %.3f s, handle %.3f s\n", t1 - t0, hprqp::now_s() - t1);
   return HPRQP_OK;
 }
 

@@ -30,6 +30,7 @@
 #include <algorithm>
 #include <mutex>
 
+#include "pool.h"
 #include "common.cuh"
 #include "tc_gemm.h"
 #include "tcgen05.cuh"
@@ -385,17 +386,11 @@ extern "C" int hprqp_gemm_3xtf32(int32_t n, float alpha, const float* A, const f
   try {
     if (n < 0 || (n > 0 && (!A || !B || !C))) return -1;
     const cudaStream_t st = (cudaStream_t)stream;
-    float* ws = nullptr;
     const int64_t wf = hprqp::gemm_3xtf32_ws_floats(n);
-    HPRQP_CUDA(cudaMalloc(&ws, sizeof(float) * (size_t)std::max<int64_t>(wf, 1)));
-    try {
-      hprqp::gemm_3xtf32_ws(n, alpha, A, B, beta, C, ws, st);
-    } catch (...) {
-      cudaFree(ws);
-      throw;
-    }
+    hprqp::PoolBlocks tmp;  // the TF32 operand images, returned to the pool on exit
+    float* ws = (float*)tmp.get(sizeof(float) * (size_t)std::max<int64_t>(wf, 1));
+    hprqp::gemm_3xtf32_ws(n, alpha, A, B, beta, C, ws, st);
     const bool failed = hprqp::gemm_3xtf32_failed(st);  // synchronises the stream
-    cudaFree(ws);
     return failed ? -2 : 0;
   } catch (const hprqp::Error& e) {
     std::fprintf(stderr, "hprqp_gemm_3xtf32: %s\n", e.what());
