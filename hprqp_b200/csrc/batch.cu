@@ -628,12 +628,14 @@ static std::vector<double> read(BEngine<V>& E, const double* d, int64_t count) {
 template <typename V>
 static std::vector<double> power_batch(BEngine<V>& E, const Family& F, double tol, int max_it) {
   const int B = F.B;
-  std::vector<V> z0(E.N);
-  for (int k = 0; k < B; ++k) {
-    std::vector<double> v = power_start_vector(F.noff[k + 1] - F.noff[k]);
-    for (size_t i = 0; i < v.size(); ++i) z0[F.noff[k] + i] = (V)v[i];
+  {  // every instance's start vector, generated in place
+    PoolBlocks tmp;
+    int64_t* off = (int64_t*)tmp.get(sizeof(int64_t) * (B + 1));
+    HPRQP_CUDA(cudaMemcpyAsync(off, F.noff.data(), sizeof(int64_t) * (B + 1), cudaMemcpyHostToDevice, E.st));
+    k_start_vector_seg<V><<<(int)((E.N + kBlock - 1) / kBlock), kBlock, 0, E.st>>>(B, off, E.N, E.pz);
+    HPRQP_LAUNCH_CHECK();
+    HPRQP_CUDA(cudaStreamSynchronize(E.st));
   }
-  HPRQP_CUDA(cudaMemcpy(E.pz, z0.data(), sizeof(V) * E.N, cudaMemcpyHostToDevice));
   std::vector<unsigned char> act(B, 1);
   HPRQP_CUDA(cudaMemcpy(E.on_pw, act.data(), B, cudaMemcpyHostToDevice));
   E.template seg_plain<1, 0u>(EpiSumSqB<V>{E.pz}, E.on_pw, E.out_tmp, ZzFin{E.zz});

@@ -1028,16 +1028,14 @@ template <typename V>
 static void power_batch(Engine<V>& E, const Family& F, double tol, int max_it, std::vector<double>& lamA,
                         std::vector<double>& lamQ) {
   const int B = F.B;
-  std::vector<double> za(E.M), zq(E.N);
-  for (int k = 0; k < B; ++k) {
-    const std::vector<double> a = power_start_vector(F.moff[k + 1] - F.moff[k]);
-    const std::vector<double> q = power_start_vector(F.noff[k + 1] - F.noff[k]);
-    std::copy(a.begin(), a.end(), za.begin() + F.moff[k]);
-    std::copy(q.begin(), q.end(), zq.begin() + F.noff[k]);
-  }
-  std::vector<V> va(za.begin(), za.end()), vq(zq.begin(), zq.end());
-  HPRQP_CUDA(cudaMemcpyAsync(E.pz, va.data(), sizeof(V) * E.M, cudaMemcpyHostToDevice, E.st));
-  HPRQP_CUDA(cudaMemcpyAsync(E.pz2, vq.data(), sizeof(V) * E.N, cudaMemcpyHostToDevice, E.st));
+  PoolBlocks tmp;  // every instance's two start vectors, generated in place
+  int64_t* offs = (int64_t*)tmp.get(sizeof(int64_t) * 2 * (B + 1));
+  HPRQP_CUDA(cudaMemcpyAsync(offs, F.moff.data(), sizeof(int64_t) * (B + 1), cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaMemcpyAsync(offs + B + 1, F.noff.data(), sizeof(int64_t) * (B + 1), cudaMemcpyHostToDevice, E.st));
+  if (E.M > 0)
+    k_start_vector_seg<V><<<(int)((E.M + kBlock - 1) / kBlock), kBlock, 0, E.st>>>(B, offs, E.M, E.pz);
+  k_start_vector_seg<V><<<(int)((E.N + kBlock - 1) / kBlock), kBlock, 0, E.st>>>(B, offs + B + 1, E.N, E.pz2);
+  HPRQP_LAUNCH_CHECK();
   std::vector<unsigned char> onA(B, 1), onQ(B, 1);
   HPRQP_CUDA(cudaMemcpyAsync(E.maskA, onA.data(), B, cudaMemcpyHostToDevice, E.st));
   HPRQP_CUDA(cudaMemcpyAsync(E.maskQ, onQ.data(), B, cudaMemcpyHostToDevice, E.st));

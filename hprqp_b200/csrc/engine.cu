@@ -1152,17 +1152,10 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   };
   for (Chain* c : {&ca, &cq}) {
     if (!c->on) continue;
-    // the start vector depends only on its length: generated and uploaded
-    // once per engine, then copied on the device for every later solve
-    V*& keep = c->which == 0 ? start_A : start_Q;
-    if (!keep) {
-      std::vector<double> z0 = power_start_vector(c->len);
-      std::vector<V> zv(z0.begin(), z0.end());
-      keep = mem.alloc<V>(c->len);
-      cm.to_dev(keep, zv.data(), sizeof(V) * c->len);
-      HPRQP_CUDA(cudaStreamSynchronize(main));
-    }
-    HPRQP_CUDA(cudaMemcpyAsync(c->z0, keep, sizeof(V) * c->len, cudaMemcpyDeviceToDevice, main));
+    // the start vector (power_start_vector's stream) generated in place
+    k_start_vector<V><<<(int)((c->len + kBlock - 1) / kBlock), kBlock, 0, main>>>(c->len, c->z0);
+    HPRQP_LAUNCH_CHECK();
+    cm.launches++;
     use(*c, main);
     reduce<1, 0u, double>(cm, 1, c->len, ZeroSrc{}, EpiSumSq<V>{c->z0}, c->scal + 2, InvNormFin{c->scal + 4});
     restore();

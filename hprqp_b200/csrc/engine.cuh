@@ -154,7 +154,6 @@ class Engine {
   bool power_persistent(bool onA, bool onQ, double tol, int max_it, double* lamA_out, double* lamQ_out,
                         int64_t* itA, int64_t* itQ);
   V *pz2 = nullptr, *pq2 = nullptr, *pt2 = nullptr;  // Q chain vectors
-  V *start_A = nullptr, *start_Q = nullptr;          // power-method start vectors (device)
   template <typename W>
   void import_state(const Engine<W>& o);  // precision switch (FP32 -> FP64)
 

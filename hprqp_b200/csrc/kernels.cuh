@@ -695,6 +695,49 @@ struct GramPowerFin {
   __device__ __forceinline__ void operator()(const double (&)[K]) const {}
 };
 
+// The power method's start vector on the device: element i takes outputs 2i
+// and 2i + 1 of the splitmix64 stream from state 1 (output k mixes
+// 1 + (k + 1) * 0x9E3779B97F4A7C15, so every element is independent) through
+// Box-Muller, plus 1e-8: the host power_start_vector values up to the last
+// bit of log / cos / sqrt.
+__device__ __forceinline__ uint64_t splitmix_at(uint64_t k) {
+  uint64_t v = 1ull + (k + 1ull) * 0x9E3779B97F4A7C15ULL;
+  v = (v ^ (v >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  v = (v ^ (v >> 27)) * 0x94D049BB133111EBULL;
+  return v ^ (v >> 31);
+}
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_start_vector(int64_t len, V* __restrict__ out) {
+  const int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (i >= len) return;
+  const double u1 = ((double)(splitmix_at(2 * (uint64_t)i) >> 11) + 1.0) * 0x1.0p-53;
+  const double u2 = (double)(splitmix_at(2 * (uint64_t)i + 1) >> 11) * 0x1.0p-53;
+  out[i] = (V)(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2) + 1e-8);
+}
+
+// The same for B instances concatenated at offsets off[0..B] (instance k's
+// own stream in [off[k], off[k+1]); zeros past off[B])
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_start_vector_seg(int B, const int64_t* __restrict__ off, int64_t total,
+                                                             V* __restrict__ out) {
+  const int64_t j = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (j >= total) return;
+  if (j >= off[B]) {
+    out[j] = (V)0;
+    return;
+  }
+  int lo = 0, hi = B;  // off[lo] <= j < off[hi]
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (off[mid] <= j) lo = mid;
+    else hi = mid;
+  }
+  const uint64_t i = (uint64_t)(j - off[lo]);
+  const double u1 = ((double)(splitmix_at(2 * i) >> 11) + 1.0) * 0x1.0p-53;
+  const double u2 = (double)(splitmix_at(2 * i + 1) >> 11) * 0x1.0p-53;
+  out[j] = (V)(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2) + 1e-8);
+}
+
 // 1/sqrt of a reduced sum of squares (the start vector's norm)
 struct InvNormFin {
   double* inv_out;
