@@ -492,7 +492,7 @@ void Engine<V>::gram_values() {
 // product work exceeds its bound, or, in the automatic mode, when A'A has
 // more than 3 nnz(A) entries.
 template <typename V>
-void Engine<V>::build_gram(const Prepared& pp) {
+void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
   gram = false;
   if (m <= 0 || is_qap || is_lasso || cm.pow_gram == 0 || pp.A.nnz() == 0) return;
   const bool force = cm.pow_gram == 1;
@@ -517,7 +517,17 @@ void Engine<V>::build_gram(const Prepared& pp) {
   gram_values();  // CSR values, copied into the padded formats next
   build_sell(h, G);
   build_ell(h, G);
-  G.tpr = autotune(G);
+  if (tpr_mode == 7 && G.sell_len > 0) {  // A's schedule pinned by the caller: G follows it
+    G.sell = true;
+    G.tpr = 1;
+  } else if (tpr_mode == 8 && G.ell_w > 0) {
+    G.ell = true;
+    G.tpr = 1;
+  } else if (tpr_mode > 0 && tpr_mode < 7) {
+    G.tpr = 1 << std::min(tpr_mode - 1, 5);
+  } else {
+    G.tpr = autotune(G);
+  }
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   gram = true;
   if (const char* tv = std::getenv("HPRQP_TIMING"))
@@ -585,7 +595,7 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
     qT = upload<V>(cm, mem, hp.qT, N2);
     qTmp = mem.alloc<V>(N2);
   }
-  if (power_engine) build_gram(pp);
+  if (power_engine) build_gram(pp, tpr_A);
   reset_state();
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
 }
