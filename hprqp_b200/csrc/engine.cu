@@ -23,8 +23,6 @@ namespace hprqp {
 void Common::init() {
   HPRQP_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   HPRQP_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
-  if (cublasCreate(&cublas) != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cublasCreate failed");
-  cublasSetStream(cublas, stream);
   d_scal = mem.alloc<double>(kNumSlots);
   HPRQP_CUDA(cudaMemset(d_scal, 0, sizeof(double) * kNumSlots));
   HPRQP_CUDA(cudaMallocHost(&h_scal, sizeof(double) * kNumSlots));
@@ -653,10 +651,11 @@ void Engine<V>::qap_apply(const V* xin, V* yout) {
   auto ck = [](cublasStatus_t s) {
     if (s != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cuBLAS GEMM failed");
   };
-  ck(gemm<V>(cm.cublas, N, 1.0, qA, xin, 0.0, qTmp));
-  ck(gemm<V>(cm.cublas, N, 2.0, qTmp, qB, 0.0, yout));
-  ck(gemm<V>(cm.cublas, N, -2.0, qS, xin, 1.0, yout));
-  ck(gemm<V>(cm.cublas, N, -2.0, xin, qT, 1.0, yout));
+  cublasHandle_t hb = cm.blas();
+  ck(gemm<V>(hb, N, 1.0, qA, xin, 0.0, qTmp));
+  ck(gemm<V>(hb, N, 2.0, qTmp, qB, 0.0, yout));
+  ck(gemm<V>(hb, N, -2.0, qS, xin, 1.0, yout));
+  ck(gemm<V>(hb, N, -2.0, xin, qT, 1.0, yout));
   cm.launches += 4;
 }
 

@@ -47,7 +47,14 @@ struct DeviceMem : PoolBlocks {  // owns blocks of the library's device memory p
 struct Common {  // per-handle resources shared by the engines
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;  // second chain of the power method
-  cublasHandle_t cublas = nullptr;
+  cublasHandle_t cublas = nullptr;  // created on first use (the dense QAP operator)
+  cublasHandle_t blas() {
+    if (!cublas) {
+      if (cublasCreate(&cublas) != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cublasCreate failed");
+      cublasSetStream(cublas, stream);
+    }
+    return cublas;
+  }
   double* d_scal = nullptr;
   double* h_scal = nullptr;  // pinned mirror
   ReduceWs rws{}, rws2{};
