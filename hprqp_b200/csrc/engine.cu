@@ -523,6 +523,9 @@ void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
     G.tpr = 1;
   } else if (tpr_mode > 0 && tpr_mode < 7) {
     G.tpr = 1 << std::min(tpr_mode - 1, 5);
+  } else if (cm.pow_prefer_ell && G.ell_w > 0) {  // HPRQP_POWER_ELL=1
+    G.ell = true;
+    G.tpr = 1;
   } else {
     G.tpr = autotune(G);
   }
