@@ -25,35 +25,6 @@ namespace hprqp {
 // ---------------------------------------------------------------------------
 // Row sources: what the per-row accumulator is
 // ---------------------------------------------------------------------------
-
-// A short row (len <= kShortRow entries at base + k * stride) with every
-// load issued before any is used: all col / val loads, then all x gathers,
-// then the FMAs in entry order, so the sum is the plain loop's bit for bit
-// while the row costs two dependent memory latencies instead of two per
-// group of unrolled entries.  The sparse rows of the engine's matrices are
-// mostly this short, and their sweeps are bound by these latencies.
-constexpr int kShortRow = 8;
-template <typename Acc, typename V, typename X>
-__device__ __forceinline__ Acc dot_short(int len, int64_t base, int64_t stride, const int* __restrict__ col,
-                                         const V* __restrict__ val, const X* __restrict__ x) {
-  int c[kShortRow];
-  Acc v[kShortRow], xv[kShortRow];
-#pragma unroll
-  for (int k = 0; k < kShortRow; ++k)
-    if (k < len) {
-      c[k] = __ldg(col + base + k * stride);
-      v[k] = (Acc)__ldg(val + base + k * stride);
-    }
-#pragma unroll
-  for (int k = 0; k < kShortRow; ++k)
-    if (k < len) xv[k] = (Acc)__ldg(x + c[k]);
-  Acc s = Acc(0);
-#pragma unroll
-  for (int k = 0; k < kShortRow; ++k)
-    if (k < len) s = fma(v[k], xv[k], s);
-  return s;
-}
-
 template <typename V, typename X>
 struct CsrSrc {  // (M x)_row with M in CSR
   const int* __restrict__ ptr;
@@ -63,7 +34,6 @@ struct CsrSrc {  // (M x)_row with M in CSR
   template <int TPR, typename Acc>
   __device__ __forceinline__ Acc dot(int row, int lane) const {
     const int b = __ldg(ptr + row), e = __ldg(ptr + row + 1);
-    if (TPR == 1 && e - b <= kShortRow) return dot_short<Acc>(e - b, b, 1, col, val, x);
     Acc s = Acc(0);
 #pragma unroll 4
     for (int k = b + lane; k < e; k += TPR) s = fma((Acc)__ldg(val + k), (Acc)__ldg(x + __ldg(col + k)), s);
@@ -82,7 +52,6 @@ struct SellSrc {  // (M x)_row with M in SELL-32, one thread per row
   __device__ __forceinline__ Acc dot(int row, int) const {
     const int len = __ldg(ptr + row + 1) - __ldg(ptr + row);
     const int base = __ldg(sptr + (row >> 5)) + (row & 31);
-    if (len <= kShortRow) return dot_short<Acc>(len, base, 32, col, val, x);
     Acc s = Acc(0);
 #pragma unroll 4
     for (int k = 0; k < len; ++k)
@@ -99,7 +68,6 @@ struct EllSrc {  // (M x)_row with M in ELL (width w, column-major), one thread 
   int rows, w;
   template <int TPR, typename Acc>
   __device__ __forceinline__ Acc dot(int row, int) const {
-    if (w <= kShortRow) return dot_short<Acc>(w, row, rows, col, val, x);
     Acc s = Acc(0);
     const int* c = col + row;
     const V* v = val + row;
@@ -291,9 +259,15 @@ __global__ void __launch_bounds__(kBlock) k_ell_reduce(int nrows, EllSrc<V, X> s
   for (int r0 = (int)(blockIdx.x * kBlock + threadIdx.x); r0 < nrows; r0 += R * stride) {
     Acc acc[R];
 #pragma unroll
-    for (int q = 0; q < R; ++q) {
-      const int row = r0 + q * stride;
-      acc[q] = row < nrows ? src.template dot<1, Acc>(row, 0) : Acc(0);
+    for (int q = 0; q < R; ++q) acc[q] = Acc(0);
+    for (int k = 0; k < src.w; ++k) {
+      const int* c = src.col + (size_t)k * src.rows;
+      const V* v = src.val + (size_t)k * src.rows;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int row = r0 + q * stride;
+        if (row < nrows) acc[q] = fma((Acc)__ldg(v + row), (Acc)__ldg(src.x + __ldg(c + row)), acc[q]);
+      }
     }
 #pragma unroll
     for (int q = 0; q < R; ++q) {
