@@ -56,6 +56,8 @@ def main(argv=None):
         for tag, over in (("both", {}), ("A_only", {"lambda_max_Q_override": a.lam_Q}),
                           ("Q_only", {"lambda_max_A_override": a.lam_A})):
             p = HPRQP_parameters(verbose=False, precision=a.precision, problem_type=ptype, max_iter=0, **over)
+            if a.tpr != "0":
+                p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr in ("sell", "ell") else int(a.tpr)
             ts, r = [], None
             for _ in range(6):
                 r = s.solve(p)
