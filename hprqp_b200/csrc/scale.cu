@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
+#include <cstdlib>
 #include <cmath>
 #include <vector>
 
@@ -116,6 +118,12 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
     prepare_problem(hp, p, o);
     return;
   }
+  const char* tv = std::getenv("HPRQP_TIMING");
+  const bool timing = tv && tv[0] == '1';
+  auto wall = [] { return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count(); };
+  double tm[8];
+  int nt = 0;
+  tm[nt++] = wall();
   const int64_t n = hp.n, m = hp.m;
   o = Prepared();
   o.ruiz = p.use_Ruiz_scaling;
@@ -166,6 +174,7 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
 #pragma omp parallel for schedule(static) num_threads(host_threads(n))
   for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], ia.data() + S.ptr[i], ib.data() + S.ptr[i]);
 
+  tm[nt++] = wall();  // merged pattern
   // device copies
   DevBuf d;
   auto up = [&](auto* dst, const auto& v) {
@@ -201,6 +210,8 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   up(AL, o.AL);
   up(AU, o.AU);
   up(rn, o.row_norm);
+  HPRQP_CUDA(cudaStreamSynchronize(st));
+  tm[nt++] = wall();  // uploads
   auto pass = [&](int mode) {  // one Ruiz (0) or Pock-Chambolle (1) pass
     k_row_abs<<<blocks(n), kT, 0, st>>>((int)n, dAT.ptr, dAT.val, mode, ca);
     k_row_abs<<<blocks(n), kT, 0, st>>>((int)n, dQT.ptr, dQT.val, mode, cq);
@@ -229,6 +240,8 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   up(dib, ib);
   k_sym<<<blocks(nnzS), kT, 0, st>>>((int)nnzS, dia, dib, dQ.val, dQT.val, sv);
   HPRQP_LAUNCH_CHECK();
+  HPRQP_CUDA(cudaStreamSynchronize(st));
+  tm[nt++] = wall();  // scaling kernels
   auto down = [&](std::vector<double>& dst, const double* src) {
     if (!dst.empty())
       HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
@@ -244,8 +257,13 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   down(o.AU, AU);
   down(o.row_norm, rn);
   HPRQP_CUDA(cudaStreamSynchronize(st));
+  tm[nt++] = wall();  // downloads
   finish_sparse(o, n);
   finish_common(hp, o);
+  tm[nt++] = wall();
+  if (timing)
+    std::fprintf(stderr, "[hprqp] scaling: pattern %.3f, uploads %.3f, kernels %.3f, downloads %.3f, finish %.3f s\n",
+                 tm[1] - tm[0], tm[2] - tm[1], tm[3] - tm[2], tm[4] - tm[3], tm[5] - tm[4]);
 }
 
 }  // namespace hprqp
