@@ -93,11 +93,13 @@ __global__ void k_scale_m(int m, const double* tr, double* AL, double* AU) {
   AU[i] /= tr[i];
 }
 
-// S = (Q + Q') / 2 on the merged pattern: ia / ib index Q / Q' values (-1: absent)
+// S = (Q + Q') / 2 on the merged pattern: ia / ib index Q / Q' values (-1:
+// absent); both null when Q's pattern is symmetric (entry p of S is entry p
+// of Q and of Q')
 __global__ void k_sym(int nnz, const int* ia, const int* ib, const double* qv, const double* qtv, double* sv) {
   const int p = blockIdx.x * kT + threadIdx.x;
   if (p >= nnz) return;
-  const int a = ia[p], b = ib[p];
+  const int a = ia ? ia[p] : p, b = ib ? ib[p] : p;
   const double v = (a >= 0 && b >= 0) ? qv[a] + qtv[b] : (a >= 0 ? qv[a] : qtv[b]);
   sv[p] = v / 2.0;
 }
@@ -140,8 +142,10 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   o.norm_b_org = m > 0 ? norm_b_inf_org(o.AL, o.AU) : 0.0;
   o.norm_c_org = norm_inf(o.c);
   const HCsr &Q = hp.Q, &QT = hp.QT;
-  // merged pattern of Q + Q' with index maps (the values come later)
-  std::vector<int> len(n, 0);
+  // merged pattern of Q + Q' with index maps (the values come later); a
+  // structurally symmetric Q (the common case) is its own merged pattern
+  const bool sym_pattern = Q.ptr == QT.ptr && Q.col == QT.col;
+  std::vector<int> len(sym_pattern ? 0 : n, 0);
   auto merge = [&](int64_t i, int* cols, int* ia, int* ib) {
     int a = Q.ptr[i], b = QT.ptr[i], cnt = 0;
     const int ae = Q.ptr[i + 1], be = QT.ptr[i + 1];
@@ -161,18 +165,25 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
     }
     return cnt;
   };
-#pragma omp parallel for schedule(static) num_threads(host_threads(n))
-  for (int64_t i = 0; i < n; ++i) len[i] = merge(i, nullptr, nullptr, nullptr);
   HCsr& S = o.Q;
   S.rows = S.cols = n;
-  S.ptr.assign(n + 1, 0);
-  for (int64_t i = 0; i < n; ++i) S.ptr[i + 1] = S.ptr[i] + len[i];
-  const int64_t nnzS = S.ptr[n];
-  S.col.resize(nnzS);
-  S.val.resize(nnzS);
-  std::vector<int> ia(nnzS), ib(nnzS);
+  std::vector<int> ia, ib;
+  if (sym_pattern) {
+    S.ptr = Q.ptr;
+    S.col = Q.col;
+  } else {
 #pragma omp parallel for schedule(static) num_threads(host_threads(n))
-  for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], ia.data() + S.ptr[i], ib.data() + S.ptr[i]);
+    for (int64_t i = 0; i < n; ++i) len[i] = merge(i, nullptr, nullptr, nullptr);
+    S.ptr.assign(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) S.ptr[i + 1] = S.ptr[i] + len[i];
+    S.col.resize(S.ptr[n]);
+    ia.resize(S.ptr[n]);
+    ib.resize(S.ptr[n]);
+#pragma omp parallel for schedule(static) num_threads(host_threads(n))
+    for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], ia.data() + S.ptr[i], ib.data() + S.ptr[i]);
+  }
+  const int64_t nnzS = S.ptr[n];
+  S.val.resize(nnzS);
 
   tm[nt++] = wall();  // merged pattern
   // device copies
@@ -233,11 +244,13 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   if (p.use_Ruiz_scaling)
     for (int k = 0; k < 10; ++k) pass(0);
   if (p.use_Pock_Chambolle_scaling) pass(1);
-  int* dia = d.take<int>(nnzS);
-  int* dib = d.take<int>(nnzS);
+  int* dia = sym_pattern ? nullptr : d.take<int>(nnzS);
+  int* dib = sym_pattern ? nullptr : d.take<int>(nnzS);
   double* sv = d.take<double>(nnzS);
-  up(dia, ia);
-  up(dib, ib);
+  if (!sym_pattern) {
+    up(dia, ia);
+    up(dib, ib);
+  }
   k_sym<<<blocks(nnzS), kT, 0, st>>>((int)nnzS, dia, dib, dQ.val, dQT.val, sv);
   HPRQP_LAUNCH_CHECK();
   HPRQP_CUDA(cudaStreamSynchronize(st));

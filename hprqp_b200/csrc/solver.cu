@@ -857,10 +857,16 @@ int hprqp_destroy(hprqp_handle h) {
   h->e32.reset();
   h->e64.reset();
   const double t1 = hprqp::now_s();
+  h->cm.reset();
+  const double t2 = hprqp::now_s();
+  h->hp = hprqp::HostProblem();
+  h->pp = hprqp::Prepared();
+  const double t3 = hprqp::now_s();
   delete h;
   if (const char* tv = std::getenv("HPRQP_TIMING"))
     if (tv[0] == '1')
-      std::fprintf(stderr, "[hprqp] destroy: engines %.3f s, handle %.3f s\n", t1 - t0, hprqp::now_s() - t1);
+      std::fprintf(stderr, "[hprqp] destroy: engines %.3f s, device resources %.3f s, host arrays %.3f s, rest %.3f s\n",
+                   t1 - t0, t2 - t1, t3 - t2, hprqp::now_s() - t3);
   return HPRQP_OK;
 }
 
