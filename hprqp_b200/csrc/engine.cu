@@ -17,6 +17,10 @@
 namespace hprqp {
 
 
+static double wall_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
 // ---------------------------------------------------------------------------
 // Common
 // ---------------------------------------------------------------------------
@@ -60,10 +64,18 @@ void Common::init() {
 }
 
 Common::~Common() {
+  const double t0 = wall_s();
   if (h_scal) cudaFreeHost(h_scal);
+  const double t1 = wall_s();
   if (cublas) cublasDestroy(cublas);
   if (stream) cudaStreamDestroy(stream);
   if (stream2) cudaStreamDestroy(stream2);
+  const double t2 = wall_s();
+  pool_free(mem.blocks, mem.dev);
+  if (const char* tv = std::getenv("HPRQP_TIMING"))
+    if (tv[0] == '1')
+      std::fprintf(stderr, "[hprqp] handle resources: pinned %.3f s, streams %.3f s, device blocks %.3f s\n", t1 - t0,
+                   t2 - t1, wall_s() - t2);
 }
 
 void Common::sync_read(int first, int count) {
@@ -250,18 +262,37 @@ static V* upload(Common& cm, DeviceMem& mem, const std::vector<double>& h, int64
   return d;
 }
 
+// A vector of the scaled problem: copied (FP64) or cast (FP32) from the
+// GPU scaling's device copy when there is one, else uploaded from the host.
 template <typename V>
-void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode) {
+V* Engine<V>::vec_in(const std::vector<double>& h, const double* dsrc, int64_t len) {
+  if (!dsrc || len <= 0) return upload<V>(cm, mem, h, len);
+  V* d = mem.alloc<V>(len);
+  if constexpr (std::is_same<V, double>::value)
+    HPRQP_CUDA(cudaMemcpyAsync(d, dsrc, sizeof(double) * len, cudaMemcpyDeviceToDevice, cm.stream));
+  else
+    elem(cm, len, CastCopy<V, double>{d, dsrc});
+  return d;
+}
+
+template <typename V>
+void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode, const DevCsrView* dsrc) {
   d.rows = (int)h.rows;
   d.cols = (int)h.cols;
   d.nnz = h.nnz();
   int* ptr = mem.alloc<int>(h.rows + 1);
   int* col = mem.alloc<int>(d.nnz);
-  cm.to_dev(ptr, h.ptr.data(), sizeof(int) * (h.rows + 1));
-  cm.to_dev(col, h.col.data(), sizeof(int) * d.nnz);
+  if (dsrc && dsrc->ptr) {  // the pattern is the host one; the copy is on the device already
+    HPRQP_CUDA(cudaMemcpyAsync(ptr, dsrc->ptr, sizeof(int) * (h.rows + 1), cudaMemcpyDeviceToDevice, cm.stream));
+    if (d.nnz)
+      HPRQP_CUDA(cudaMemcpyAsync(col, dsrc->col, sizeof(int) * d.nnz, cudaMemcpyDeviceToDevice, cm.stream));
+  } else {
+    cm.to_dev(ptr, h.ptr.data(), sizeof(int) * (h.rows + 1));
+    cm.to_dev(col, h.col.data(), sizeof(int) * d.nnz);
+  }
   d.ptr = ptr;
   d.col = col;
-  d.val = upload<V>(cm, mem, h.val, d.nnz);
+  d.val = vec_in(h.val, dsrc ? dsrc->val : nullptr, d.nnz);
   d.sell = false;
   d.ell = false;
   if (tpr_mode == 7) {  // SELL-32 requested
@@ -429,9 +460,6 @@ int Engine<V>::autotune(DCsr<V>& d) {
   return best_t;
 }
 
-static double wall_s() {
-  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
-}
 
 // Values of the Gram matrix G = A'A: G_pj = sum over the rows r of A with
 // entries in both columns p and j of A_rp A_rj, in increasing r (a merge of
@@ -572,17 +600,18 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   pq2 = mem.alloc<V>(n);
   pt2 = mem.alloc<V>(n);
   ltemp2 = is_lasso ? mem.alloc<V>(hp.L.rows) : nullptr;
-  c = upload<V>(cm, mem, pp.c, n);
-  l = upload<V>(cm, mem, pp.l, n);
-  u = upload<V>(cm, mem, pp.u, n);
-  col_norm = upload<V>(cm, mem, pp.col_norm, n);
+  const DevScaled* ds = pp.dev.get();  // the GPU scaling's device copy, if any
+  c = vec_in(pp.c, ds ? ds->c : nullptr, n);
+  l = vec_in(pp.l, ds ? ds->l : nullptr, n);
+  u = vec_in(pp.u, ds ? ds->u : nullptr, n);
+  col_norm = vec_in(pp.col_norm, ds ? ds->col_norm : nullptr, n);
   diag_Q = upload<V>(cm, mem, pp.diag_Q, n);
-  AL = upload<V>(cm, mem, pp.AL, m);
-  AU = upload<V>(cm, mem, pp.AU, m);
-  row_norm = upload<V>(cm, mem, pp.row_norm, m);
-  upload_csr(pp.A, A, tpr_A);
-  upload_csr(pp.AT, AT, tpr_A);
-  if (has_Q_sparse) upload_csr(pp.Q, Q, tpr_Q);
+  AL = vec_in(pp.AL, ds ? ds->AL : nullptr, m);
+  AU = vec_in(pp.AU, ds ? ds->AU : nullptr, m);
+  row_norm = vec_in(pp.row_norm, ds ? ds->row_norm : nullptr, m);
+  upload_csr(pp.A, A, tpr_A, ds ? &ds->A : nullptr);
+  upload_csr(pp.AT, AT, tpr_A, ds ? &ds->AT : nullptr);
+  if (has_Q_sparse) upload_csr(pp.Q, Q, tpr_Q, ds ? &ds->Q : nullptr);
   if (is_lasso) {
     ltemp = mem.alloc<V>(hp.L.rows);
     upload_csr(hp.L, L, tpr_Q);

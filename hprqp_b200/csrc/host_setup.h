@@ -14,10 +14,12 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <memory>
 #include <string>
 #include <vector>
 
 #include "../../include/hprqp.h"
+#include "pool.h"
 
 namespace hprqp {
 
@@ -44,7 +46,23 @@ struct HostProblem {  // the loaded, unscaled problem
   bool loaded = false;
 };
 
+// Device copies of the scaled problem left by the GPU scaling: the engines
+// copy from them on the device (FP64) or cast them there (FP32) instead of
+// uploading the host arrays a second time.
+struct DevCsrView {
+  const int* ptr = nullptr;
+  const int* col = nullptr;
+  const double* val = nullptr;
+};
+struct DevScaled {
+  PoolBlocks mem;  // owns every array below
+  DevCsrView A, AT, Q;
+  const double *c = nullptr, *l = nullptr, *u = nullptr, *AL = nullptr, *AU = nullptr;
+  const double *row_norm = nullptr, *col_norm = nullptr;
+};
+
 struct Prepared {  // scaled problem + scaling info (Scaling_info_cpu)
+  std::shared_ptr<DevScaled> dev;  // set by the GPU scaling, null after host scaling
   HCsr A, AT, Q;
   std::vector<double> c, AL, AU, l, u, row_norm, col_norm, diag_Q;
   double norm_b = 0, norm_c = 0, norm_b_org = 0, norm_c_org = 0;

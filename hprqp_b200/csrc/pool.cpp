@@ -38,7 +38,7 @@ DevPool* pool_of(int dev) {
     d.pool = nullptr;
     return nullptr;
   }
-  uint64_t keep = 8192ull << 20;
+  uint64_t keep = ~0ull;  // keep everything; an allocation that fails trims and retries
   if (const char* e = std::getenv("HPRQP_POOL_KEEP_MB")) keep = (uint64_t)std::strtoull(e, nullptr, 10) << 20;
   cudaMemPoolSetAttribute(d.pool, cudaMemPoolAttrReleaseThreshold, &keep);
   if (cudaStreamCreateWithFlags(&d.st, cudaStreamNonBlocking) != cudaSuccess) {
@@ -58,7 +58,14 @@ void* pool_alloc(size_t bytes) {
   DevPool* d = pool_of(dev);
   if (!d) throw Error(HPRQP_E_CUDA, "cannot create the device memory pool");
   void* p = nullptr;
-  HPRQP_CUDA(cudaMallocFromPoolAsync(&p, bytes < 16 ? 16 : bytes, d->pool, d->st));
+  const size_t b = bytes < 16 ? 16 : bytes;
+  if (cudaMallocFromPoolAsync(&p, b, d->pool, d->st) != cudaSuccess) {
+    // out of memory: return the pool's unused reserve to the driver, then retry once
+    cudaGetLastError();
+    cudaStreamSynchronize(d->st);
+    cudaMemPoolTrimTo(d->pool, 0);
+    HPRQP_CUDA(cudaMallocFromPoolAsync(&p, b, d->pool, d->st));
+  }
   HPRQP_CUDA(cudaStreamSynchronize(d->st));
   return p;
 }

@@ -6,9 +6,10 @@
 // built for the next problem (the load -> solve -> destroy cycle of a caller
 // that solves many problems) reuse the physical pages instead of paying
 // cudaMalloc / cudaFree (page mapping, unmapping and an implicit device
-// synchronisation) for every block.  The pool keeps at most
-// HPRQP_POOL_KEEP_MB megabytes (default 8192) reserved once its blocks are
-// free; beyond that it returns memory to the driver.
+// synchronisation) for every block.  The pool keeps what it has reserved
+// (at most the peak of the blocks in use at once); an allocation that finds
+// the device full first returns the pool's unused reserve to the driver and
+// retries.  HPRQP_POOL_KEEP_MB caps the reserve kept across frees instead.
 #pragma once
 
 #include <cstddef>

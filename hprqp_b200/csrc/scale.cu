@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cstdlib>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "pool.h"
@@ -186,7 +187,9 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   S.val.resize(nnzS);
 
   tm[nt++] = wall();  // merged pattern
-  // device copies
+  // device copies: what the engines copy from afterwards lives in ds->mem,
+  // the scaling's scratch in d
+  auto ds = std::make_shared<DevScaled>();
   DevBuf d;
   auto up = [&](auto* dst, const auto& v) {
     if (!v.empty())
@@ -198,20 +201,27 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
     int* col = nullptr;
     double* val = nullptr;
   };
-  auto dev_csr = [&](const HCsr& h) {
+  auto keep = [&](auto* type_tag, int64_t len) {  // an array the engines copy from
+    using T = std::remove_pointer_t<decltype(type_tag)>;
+    return (T*)ds->mem.get(sizeof(T) * (size_t)std::max<int64_t>(len, 1));
+  };
+  auto dev_csr = [&](const HCsr& h, bool kept) {
     DM x;
     x.rows = (int)h.rows;
-    x.ptr = d.take<int>(h.rows + 1);
-    x.col = d.take<int>(h.nnz());
-    x.val = d.take<double>(h.nnz());
+    x.ptr = kept ? keep((int*)nullptr, h.rows + 1) : d.take<int>(h.rows + 1);
+    x.col = kept ? keep((int*)nullptr, h.nnz()) : d.take<int>(h.nnz());
+    x.val = kept ? keep((double*)nullptr, h.nnz()) : d.take<double>(h.nnz());
     up(x.ptr, h.ptr);
     up(x.col, h.col);
     up(x.val, h.val);
     return x;
   };
-  const DM dA = dev_csr(hp.A), dAT = dev_csr(hp.AT), dQ = dev_csr(Q), dQT = dev_csr(QT);
-  double *c = d.take<double>(n), *l = d.take<double>(n), *u = d.take<double>(n), *cn = d.take<double>(n);
-  double *AL = d.take<double>(m), *AU = d.take<double>(m), *rn = d.take<double>(m);
+  // Q's pattern is kept when it is also S's (the symmetric case)
+  const DM dA = dev_csr(hp.A, true), dAT = dev_csr(hp.AT, true), dQ = dev_csr(Q, sym_pattern),
+           dQT = dev_csr(QT, false);
+  double *c = keep((double*)nullptr, n), *l = keep((double*)nullptr, n), *u = keep((double*)nullptr, n);
+  double* cn = keep((double*)nullptr, n);
+  double *AL = keep((double*)nullptr, m), *AU = keep((double*)nullptr, m), *rn = keep((double*)nullptr, m);
   double *ca = d.take<double>(n), *cq = d.take<double>(n), *tc = d.take<double>(n), *tci = d.take<double>(n);
   double *ra = d.take<double>(m), *tr = d.take<double>(m), *tri = d.take<double>(m);
   up(c, o.c);
@@ -246,7 +256,7 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   if (p.use_Pock_Chambolle_scaling) pass(1);
   int* dia = sym_pattern ? nullptr : d.take<int>(nnzS);
   int* dib = sym_pattern ? nullptr : d.take<int>(nnzS);
-  double* sv = d.take<double>(nnzS);
+  double* sv = keep((double*)nullptr, nnzS);
   if (!sym_pattern) {
     up(dia, ia);
     up(dib, ib);
@@ -269,7 +279,28 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   down(o.AL, AL);
   down(o.AU, AU);
   down(o.row_norm, rn);
+  // S's pattern on the device (Q's when that is symmetric)
+  const int *sptr = dQ.ptr, *scol = dQ.col;
+  if (!sym_pattern) {
+    int* p2 = keep((int*)nullptr, n + 1);
+    int* c2 = keep((int*)nullptr, nnzS);
+    up(p2, S.ptr);
+    up(c2, S.col);
+    sptr = p2;
+    scol = c2;
+  }
   HPRQP_CUDA(cudaStreamSynchronize(st));
+  ds->A = DevCsrView{dA.ptr, dA.col, dA.val};
+  ds->AT = DevCsrView{dAT.ptr, dAT.col, dAT.val};
+  ds->Q = DevCsrView{sptr, scol, sv};
+  ds->c = c;
+  ds->l = l;
+  ds->u = u;
+  ds->AL = AL;
+  ds->AU = AU;
+  ds->row_norm = rn;
+  ds->col_norm = cn;
+  o.dev = ds;
   tm[nt++] = wall();  // downloads
   finish_sparse(o, n);
   finish_common(hp, o);
