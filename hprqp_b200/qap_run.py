@@ -9,6 +9,7 @@ solve must end OPTIMAL with the objective within 1e-6 (FP64) / 1e-5 (FP32 +
 polish) of the single FP64 solve.  Prints one JSON line.
 
     python -m hprqp_b200.qap_run --count 256 --nmin 30 --nmax 128 --seq-sample 16
+    python -m hprqp_b200.qap_run --only batch_fp32      # one batched path alone
 """
 from __future__ import annotations
 
@@ -32,6 +33,8 @@ def main(argv=None):
     ap.add_argument("--tol", type=float, default=1e-6)
     ap.add_argument("--seq-sample", type=int, default=16,
                     help="time the sequential FP64 baseline on this many instances and scale (0 = all)")
+    ap.add_argument("--only", default="all", choices=["all", "batch_fp64", "batch_fp32"],
+                    help="one batched path alone, without the sequential baseline (for profilers)")
     a = ap.parse_args(argv)
 
     def log(*x):
@@ -44,6 +47,15 @@ def main(argv=None):
     out = dict(workload=f"qap_batch_{a.count}_n{a.nmin}-{a.nmax}", count=a.count, tol=a.tol,
                n_mean=float(np.mean(sizes)))
     base = dict(verbose=False, stoptol=a.tol, problem_type="QAP")
+    if a.only != "all":
+        prec = "fp64" if a.only == "batch_fp64" else "fp32_polish"
+        t = time.perf_counter()
+        res = solve_batch(models, HPRQP_parameters(**base, precision=prec))
+        out[a.only] = dict(s=time.perf_counter() - t, solve_s=res[0].device_time,
+                           iters=float(np.mean([r.iter for r in res])),
+                           all_optimal=all(r.status == "OPTIMAL" for r in res))
+        print(json.dumps(out), flush=True)
+        return
     idx = list(range(a.count)) if not a.seq_sample else list(range(0, a.count, max(1, a.count // a.seq_sample)))
     t = time.perf_counter()
     ref = {}
