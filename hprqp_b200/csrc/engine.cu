@@ -398,13 +398,17 @@ void Engine<V>::mat_rows(const DCsr<V>& M, const V* xin, const Epi& e) {
 // keeps its FP64 state under an FP32 Gram matrix.)
 template <int K, unsigned MM, typename V, typename X, typename Epi, typename Fin = NoFin>
 static void mat_reduce(Common& cm, const DCsr<V>& M, const X* xin, const Epi& e, double* out, const Fin& fin = Fin()) {
-  if (M.ell) {  // 4 rows per thread in flight
+  // An ELL copy serves the plain passes; the reductions measured faster on
+  // SELL-32 or CSR (the ELL reduction's rows in flight cost registers and
+  // occupancy), except when HPRQP_POWER_ELL=1 asks for it
+  if (M.ell && cm.pow_prefer_ell) {  // 4 rows per thread in flight
     const int grid = reduce_grid(M.rows, 1, cm.reduce_cap);
     launch(cm, k_ell_reduce<4, K, MM, double, V, X, Epi, Fin>, grid, kBlock, M.rows,
            EllSrc<V, X>{M.ecol, M.evalv, xin, M.rows, M.ell_w}, e, cm.rws, out, fin);
     return;
   }
-  else if (M.sell) reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, X>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
+  if (M.sell || (M.ell && M.sell_len > 0))
+    reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, X>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
   else reduce<K, MM, double>(cm, M.tpr, M.rows, CsrSrc<V, X>{M.ptr, M.col, M.val, xin}, e, out, fin);
 }
 
@@ -542,7 +546,7 @@ void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
   gu1 = mem.alloc<double>(n);
   gram_values();  // CSR values, copied into the padded formats next
   build_sell(h, G);
-  build_ell(h, G);
+  if (cm.pow_prefer_ell) build_ell(h, G);  // G only feeds reductions, which run on SELL-32 or CSR
   if (tpr_mode == 7 && G.sell_len > 0) {  // A's schedule pinned by the caller: G follows it
     G.sell = true;
     G.tpr = 1;
