@@ -547,11 +547,8 @@ void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
   gram_values();  // CSR values, copied into the padded formats next
   build_sell(h, G);
   if (cm.pow_prefer_ell) build_ell(h, G);  // G only feeds reductions, which run on SELL-32 or CSR
-  if (tpr_mode == 7 && G.sell_len > 0) {  // A's schedule pinned by the caller: G follows it
-    G.sell = true;
-    G.tpr = 1;
-  } else if (tpr_mode == 8 && G.ell_w > 0) {
-    G.ell = true;
+  if (tpr_mode == 7 || tpr_mode == 8) {  // A's schedule pinned by the caller: G follows it (SELL for ELL)
+    G.sell = G.sell_len > 0;
     G.tpr = 1;
   } else if (tpr_mode > 0 && tpr_mode < 7) {
     G.tpr = 1 << std::min(tpr_mode - 1, 5);
