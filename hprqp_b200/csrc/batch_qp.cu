@@ -295,119 +295,105 @@ __global__ void k_each(int64_t len, F f) {
 
 // Q operator on the CUDA cores, shared-memory tiled: one CTA computes a
 // 64 x 64 tile of one instance's output (blockIdx.x = instance,
-// blockIdx.y = tile), each thread a 4 x 4 block, with the K dimension
-// staged 16 at a time.  Every sum runs over l in increasing order (one FMA
-// per term, accumulated in V).
-//   stage 1: TMP_k = A_k X_k
-//   stage 2: Y_k = 2 TMP_k B_k - 2 S_k X_k - 2 X_k T_k, composed in the order
-//            of the single-instance operator (Y = 2 TMP B; Y += -2 S X;
-//            Y += -2 X T)
+// blockIdx.y = tile), each thread a 4 x 4 block.  The products of one
+// output are one GEMM over the segments of a concatenated K dimension,
+//   TMP_k = A_k X_k                                   (one segment)
+//   Y_k / 2 = TMP_k B_k + (-S_k) X_k + (-X_k) T_k     (three segments),
+// staged 16 at a time (each segment padded to a multiple of 16 with zeros),
+// into ONE accumulator per output: 32 registers of FP64 accumulators keep
+// three CTAs of 256 threads resident per SM.  The next chunk's operands are
+// loaded into registers while the current one is multiplied.  Sums run
+// over the segments in order and over l in increasing order within each.
 constexpr int kQT = 64;   // output tile
 constexpr int kQK = 16;   // K chunk
 constexpr int kQMaxTiles = 4;  // tiles per side: n_k <= 256 on this path
 
-template <typename V, int P>
-__device__ __forceinline__ void qap_tile_products(int n, int i0, int j0, const V* const (&L)[P], const V* const (&R)[P],
-                                                  V (&acc)[P][4][4]) {
-  __shared__ V Ls[P][kQK][kQT];
-  __shared__ V Rs[P][kQK][kQT];
+template <typename V, int NS>
+struct QapSegs {  // segment s: L[s] (i, l) * sign[s] times R[s] (l, j), column-major n_k x n_k each
+  const V* L[NS];
+  const V* R[NS];
+  V sign[NS];
+};
+
+template <typename V, int NS>
+__global__ void __launch_bounds__(256, 3) k_qap_gemm(const int* qn, const int64_t* off, const unsigned char* on,
+                                                  QapSegs<V, NS> sg, V out_scale, V* Y) {
+  __shared__ V Ls[kQK][kQT];
+  __shared__ V Rs[kQK][kQT];
+  const int k = blockIdx.x;
+  if (!on[k]) return;
+  const int n = qn[k];
+  const int nt = (n + kQT - 1) / kQT;
+  if ((int)blockIdx.y >= nt * nt) return;
+  const int i0 = (blockIdx.y % nt) * kQT, j0 = (blockIdx.y / nt) * kQT;
+  const int64_t o = off[k];
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
+  const int nch = (n + kQK - 1) / kQK;  // chunks per segment
+  const int total = NS * nch;
+  // this thread's 4 + 4 staging slots (64 x 16 tiles, 256 threads)
+  V lv[4], rv[4];
+  auto fetch = [&](int c) {
+    const int sgi = c / nch, l0 = (c - sgi * nch) * kQK;
+    // a select instead of an indexed read keeps the segment table out of local memory
+    const V* Lp = sg.L[0];
+    const V* Rp = sg.R[0];
+    V sgn = sg.sign[0];
 #pragma unroll
-  for (int p = 0; p < P; ++p)
-#pragma unroll
-    for (int a = 0; a < 4; ++a)
-#pragma unroll
-      for (int b = 0; b < 4; ++b) acc[p][a][b] = V(0);
-  for (int l0 = 0; l0 < n; l0 += kQK) {
-#pragma unroll
-    for (int p = 0; p < P; ++p) {
-#pragma unroll
-      for (int q = 0; q < (kQT * kQK) / 256; ++q) {
-        const int e = tid + 256 * q;
-        {  // left operand L(i, l), column-major: consecutive threads take consecutive i
-          const int ii = e & (kQT - 1), ll = e >> 6;
-          const int gi = i0 + ii, gl = l0 + ll;
-          Ls[p][ll][ii] = (gi < n && gl < n) ? L[p][gi + (int64_t)gl * n] : V(0);
-        }
-        {  // right operand R(l, j): consecutive threads take consecutive l
-          const int ll = e & (kQK - 1), jj = e >> 4;
-          const int gl = l0 + ll, gj = j0 + jj;
-          Rs[p][ll][jj] = (gl < n && gj < n) ? R[p][gl + (int64_t)gj * n] : V(0);
-        }
+    for (int t = 1; t < NS; ++t)
+      if (sgi == t) {
+        Lp = sg.L[t];
+        Rp = sg.R[t];
+        sgn = sg.sign[t];
       }
+    Lp += o;
+    Rp += o;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;
+      const int ii = e & (kQT - 1), ll = e >> 6;  // L(i, l): consecutive threads, consecutive i
+      const int gi = i0 + ii, gl = l0 + ll;
+      lv[q] = (gi < n && gl < n) ? sgn * Lp[gi + (int64_t)gl * n] : V(0);
+      const int rl = e & (kQK - 1), jj = e >> 4;  // R(l, j): consecutive threads, consecutive l
+      const int rgl = l0 + rl, gj = j0 + jj;
+      rv[q] = (rgl < n && gj < n) ? Rp[rgl + (int64_t)gj * n] : V(0);
+    }
+  };
+  V acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = V(0);
+  fetch(0);
+  for (int c = 0; c < total; ++c) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + 256 * q;
+      Ls[e >> 6][e & (kQT - 1)] = lv[q];
+      Rs[e & (kQK - 1)][e >> 4] = rv[q];
     }
     __syncthreads();
+    if (c + 1 < total) fetch(c + 1);  // in flight during the FMAs below
 #pragma unroll
     for (int ll = 0; ll < kQK; ++ll) {
+      V a[4], b[4];
 #pragma unroll
-      for (int p = 0; p < P; ++p) {
-        V a[4], b[4];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          a[q] = Ls[p][ll][ty * 4 + q];
-          b[q] = Rs[p][ll][tx * 4 + q];
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-          for (int v = 0; v < 4; ++v) acc[p][u][v] = fma(a[u], b[v], acc[p][u][v]);
+      for (int q = 0; q < 4; ++q) {
+        a[q] = Ls[ll][ty * 4 + q];
+        b[q] = Rs[ll][tx * 4 + q];
       }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
     }
     __syncthreads();
   }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(256) k_qap_tmp(const int* qn, const int64_t* off, const unsigned char* on,
-                                                 const V* __restrict__ QA, const V* X, V* TMP) {
-  const int k = blockIdx.x;
-  if (!on[k]) return;
-  const int n = qn[k];
-  const int nt = (n + kQT - 1) / kQT;
-  if ((int)blockIdx.y >= nt * nt) return;
-  const int i0 = (blockIdx.y % nt) * kQT, j0 = (blockIdx.y / nt) * kQT;
-  const int64_t o = off[k];
-  const V* const L[1] = {QA + o};
-  const V* const R[1] = {X + o};
-  V acc[1][4][4];
-  qap_tile_products<V, 1>(n, i0, j0, L, R, acc);
-  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
 #pragma unroll
   for (int u = 0; u < 4; ++u)
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
-      if (i < n && j < n) TMP[o + i + (int64_t)j * n] = acc[0][u][v];
-    }
-}
-
-template <typename V>
-__global__ void __launch_bounds__(256) k_qap_out(const int* qn, const int64_t* off, const unsigned char* on,
-                                                 const V* __restrict__ QB, const V* __restrict__ QS,
-                                                 const V* __restrict__ QT, const V* X, const V* TMP, V* Y) {
-  const int k = blockIdx.x;
-  if (!on[k]) return;
-  const int n = qn[k];
-  const int nt = (n + kQT - 1) / kQT;
-  if ((int)blockIdx.y >= nt * nt) return;
-  const int i0 = (blockIdx.y % nt) * kQT, j0 = (blockIdx.y / nt) * kQT;
-  const int64_t o = off[k];
-  const V* const L[3] = {TMP + o, QS + o, X + o};
-  const V* const R[3] = {QB + o, X + o, QT + o};
-  V acc[3][4][4];
-  qap_tile_products<V, 3>(n, i0, j0, L, R, acc);
-  const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
-#pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
-      if (i < n && j < n) {
-        V y = V(2) * acc[0][u][v];
-        y = fma(V(-2), acc[1][u][v], y);
-        y = fma(V(-2), acc[2][u][v], y);
-        Y[o + i + (int64_t)j * n] = y;
-      }
+      if (i < n && j < n) Y[o + i + (int64_t)j * n] = out_scale * acc[u][v];
     }
 }
 
@@ -866,9 +852,11 @@ struct Engine {
     }
     const int nt = (nmax + kQT - 1) / kQT;
     const dim3 g(B, nt * nt);
-    k_qap_tmp<V><<<g, 256, 0, st>>>(qn, off, mk, QA, xin, qtmp);
+    const QapSegs<V, 1> s1{{QA}, {xin}, {V(1)}};
+    k_qap_gemm<V, 1><<<g, 256, 0, st>>>(qn, off, mk, s1, V(1), qtmp);
     check();
-    k_qap_out<V><<<g, 256, 0, st>>>(qn, off, mk, QB, QS, QT, xin, qtmp, yout);
+    const QapSegs<V, 3> s3{{qtmp, QS, xin}, {QB, xin, QT}, {V(1), V(-1), V(-1)}};
+    k_qap_gemm<V, 3><<<g, 256, 0, st>>>(qn, off, mk, s3, V(2), yout);
     check();
   }
   template <typename Src, typename Epi>
