@@ -315,11 +315,19 @@ struct QapSegs {  // segment s: L[s] (i, l) * sign[s] times R[s] (l, j), column-
   V sign[NS];
 };
 
+// Shared layout: L tile as Ls[l][i], R tile as Rs[l][j] with rows padded
+// to kQT + 2 elements (stores of consecutive l land in different banks;
+// rows stay 16-byte aligned).  Thread (ty, tx) owns rows {2ty, 2ty+1,
+// 32+2ty, 32+2ty+1} and the same four columns from tx, so each operand
+// pair is one 16-byte load and a warp's loads of R cover 16 consecutive
+// pairs: no bank conflicts.
+constexpr int kQRow = kQT + 2;
+
 template <typename V, int NS>
 __global__ void __launch_bounds__(256, 3) k_qap_gemm(const int* qn, const int64_t* off, const unsigned char* on,
-                                                  QapSegs<V, NS> sg, V out_scale, V* Y) {
-  __shared__ V Ls[kQK][kQT];
-  __shared__ V Rs[kQK][kQT];
+                                                     QapSegs<V, NS> sg, V out_scale, V* Y) {
+  __shared__ __align__(16) V Ls[kQK][kQT];
+  __shared__ __align__(16) V Rs[kQK][kQRow];
   const int k = blockIdx.x;
   if (!on[k]) return;
   const int n = qn[k];
@@ -377,9 +385,23 @@ __global__ void __launch_bounds__(256, 3) k_qap_gemm(const int* qn, const int64_
     for (int ll = 0; ll < kQK; ++ll) {
       V a[4], b[4];
 #pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        a[q] = Ls[ll][ty * 4 + q];
-        b[q] = Rs[ll][tx * 4 + q];
+      for (int h = 0; h < 2; ++h) {
+        // elements 2ty, 2ty+1 (h = 0) and 32+2ty, 32+2ty+1 (h = 1): one 16-byte load each
+        if constexpr (sizeof(V) == 8) {
+          const double2 av = *reinterpret_cast<const double2*>(&Ls[ll][32 * h + 2 * ty]);
+          const double2 bv = *reinterpret_cast<const double2*>(&Rs[ll][32 * h + 2 * tx]);
+          a[2 * h] = av.x;
+          a[2 * h + 1] = av.y;
+          b[2 * h] = bv.x;
+          b[2 * h + 1] = bv.y;
+        } else {
+          const float2 av = *reinterpret_cast<const float2*>(&Ls[ll][32 * h + 2 * ty]);
+          const float2 bv = *reinterpret_cast<const float2*>(&Rs[ll][32 * h + 2 * tx]);
+          a[2 * h] = av.x;
+          a[2 * h + 1] = av.y;
+          b[2 * h] = bv.x;
+          b[2 * h + 1] = bv.y;
+        }
       }
 #pragma unroll
       for (int u = 0; u < 4; ++u)
@@ -392,7 +414,7 @@ __global__ void __launch_bounds__(256, 3) k_qap_gemm(const int* qn, const int64_
   for (int u = 0; u < 4; ++u)
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
-      const int i = i0 + ty * 4 + u, j = j0 + tx * 4 + v;
+      const int i = i0 + 32 * (u >> 1) + 2 * ty + (u & 1), j = j0 + 32 * (v >> 1) + 2 * tx + (v & 1);
       if (i < n && j < n) Y[o + i + (int64_t)j * n] = out_scale * acc[u][v];
     }
 }
