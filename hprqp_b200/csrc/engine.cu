@@ -503,6 +503,59 @@ __global__ void __launch_bounds__(kBlock) k_gram_vals(int rows, const int* __res
   }
 }
 
+// G only feeds the power step (a fused product + two dot products + the
+// last CTA's fold), so its schedule is chosen by timing that step itself:
+// SELL-32 and CSR with 1, 2, 4 or 8 threads per row, each the best of 3
+// rounds of 8 chained steps on a unit start.
+template <typename V>
+void Engine<V>::autotune_gram() {
+  double* inv = cm.d_scal + S_POW + 5;
+  double* lg = cm.d_scal + S_POWLOG;
+  double* u0 = gu0;
+  const int64_t nn = n;
+  elem(cm, nn, [=] __device__(int i) { u0[i] = 1.0; });
+  elem(cm, 1, [=] __device__(int) { *inv = 1.0; });
+  auto step = [&](int k) {
+    const double* uc = (k & 1) ? gu1 : gu0;
+    double* un = (k & 1) ? gu0 : gu1;
+    mat_reduce<2, 0u>(cm, G, uc, EpiGramPower<double>{uc, un, inv}, cm.d_scal + S_POW + 6,
+                      GramPowerFin{lg, k & 31, inv});
+  };
+  cudaEvent_t e0, e1;
+  HPRQP_CUDA(cudaEventCreate(&e0));
+  HPRQP_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  int best_t = 1;
+  bool best_sell = false;
+  const double avg = (double)G.nnz / std::max(G.rows, 1);
+  for (int t : {-1, 1, 2, 4, 8}) {
+    if (t == -1 && G.sell_len == 0) continue;
+    if (t == 8 && avg < 8) continue;
+    G.sell = t == -1;
+    G.tpr = t < 0 ? 1 : t;
+    for (int k = 0; k < 2; ++k) step(k);
+    float tb = 1e30f;
+    for (int round = 0; round < 3; ++round) {
+      HPRQP_CUDA(cudaEventRecord(e0, cm.stream));
+      for (int k = 0; k < 8; ++k) step(k);
+      HPRQP_CUDA(cudaEventRecord(e1, cm.stream));
+      HPRQP_CUDA(cudaEventSynchronize(e1));
+      float ms = 0;
+      HPRQP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      tb = std::min(tb, ms);
+    }
+    if (tb < best) {
+      best = tb;
+      best_t = G.tpr;
+      best_sell = G.sell;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  G.sell = best_sell;
+  G.tpr = best_t;
+}
+
 // Values of G into the format its products use (the padding of ELL / SELL
 // copies stays zero from their construction)
 template <typename V>
@@ -555,8 +608,11 @@ void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
   } else if (cm.pow_prefer_ell && G.ell_w > 0) {  // HPRQP_POWER_ELL=1
     G.ell = true;
     G.tpr = 1;
+  } else if (!cm.autotune) {
+    G.sell = G.sell_len > 0;
+    G.tpr = 1;
   } else {
-    G.tpr = autotune(G);
+    autotune_gram();
   }
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   gram = true;

@@ -139,6 +139,7 @@ class Engine {
   // formed on the device at every power method (gram_values)
   DCsr<V> G;
   bool gram = false;
+  void autotune_gram();  // (public: it launches device lambdas)
   double *gu0 = nullptr, *gu1 = nullptr;  // the Gram chain's state u_k (FP64 in both engines)
   V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;
   float* qws = nullptr;  // TF32 operand images of the tensor-core QAP products
