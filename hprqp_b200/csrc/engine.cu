@@ -508,31 +508,21 @@ __global__ void __launch_bounds__(kBlock) k_gram_vals(int rows, const int* __res
 // SELL-32 and CSR with 1, 2, 4 or 8 threads per row, each the best of 3
 // rounds of 8 chained steps on a unit start.
 template <typename V>
-void Engine<V>::autotune_gram() {
-  double* inv = cm.d_scal + S_POW + 5;
-  double* lg = cm.d_scal + S_POWLOG;
-  double* u0 = gu0;
-  const int64_t nn = n;
-  elem(cm, nn, [=] __device__(int i) { u0[i] = 1.0; });
-  elem(cm, 1, [=] __device__(int) { *inv = 1.0; });
-  auto step = [&](int k) {
-    const double* uc = (k & 1) ? gu1 : gu0;
-    double* un = (k & 1) ? gu0 : gu1;
-    mat_reduce<2, 0u>(cm, G, uc, EpiGramPower<double>{uc, un, inv}, cm.d_scal + S_POW + 6,
-                      GramPowerFin{lg, k & 31, inv});
-  };
+template <typename Step>
+void Engine<V>::tune_reduce(DCsr<V>& M, Step step) {
   cudaEvent_t e0, e1;
   HPRQP_CUDA(cudaEventCreate(&e0));
   HPRQP_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = 1;
   bool best_sell = false;
-  const double avg = (double)G.nnz / std::max(G.rows, 1);
+  const double avg = (double)M.nnz / std::max(M.rows, 1);
+  M.ell = false;
   for (int t : {-1, 1, 2, 4, 8}) {
-    if (t == -1 && G.sell_len == 0) continue;
+    if (t == -1 && M.sell_len == 0) continue;
     if (t == 8 && avg < 8) continue;
-    G.sell = t == -1;
-    G.tpr = t < 0 ? 1 : t;
+    M.sell = t == -1;
+    M.tpr = t < 0 ? 1 : t;
     for (int k = 0; k < 2; ++k) step(k);
     float tb = 1e30f;
     for (int round = 0; round < 3; ++round) {
@@ -546,14 +536,54 @@ void Engine<V>::autotune_gram() {
     }
     if (tb < best) {
       best = tb;
-      best_t = G.tpr;
-      best_sell = G.sell;
+      best_t = M.tpr;
+      best_sell = M.sell;
     }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  G.sell = best_sell;
-  G.tpr = best_t;
+  M.sell = best_sell;
+  M.tpr = best_t;
+}
+
+template <typename V>
+void Engine<V>::autotune_gram() {
+  double* inv = cm.d_scal + S_POW + 5;
+  double* lg = cm.d_scal + S_POWLOG;
+  double* u0 = gu0;
+  const int64_t nn = n;
+  elem(cm, nn, [=] __device__(int i) { u0[i] = 1.0; });
+  elem(cm, 1, [=] __device__(int) { *inv = 1.0; });
+  tune_reduce(G, [&](int k) {
+    const double* uc = (k & 1) ? gu1 : gu0;
+    double* un = (k & 1) ? gu0 : gu1;
+    mat_reduce<2, 0u>(cm, G, uc, EpiGramPower<double>{uc, un, inv}, cm.d_scal + S_POW + 6,
+                      GramPowerFin{lg, k & 31, inv});
+  });
+}
+
+// The sparse Q's power step runs on its own copy of Q's schedule, chosen by
+// timing that step (Q's own schedule is chosen for the iteration's passes).
+template <typename V>
+void Engine<V>::autotune_power_Q() {
+  Qp = Q;
+  if (!has_Q_sparse || Q.nnz == 0 || !cm.autotune || cm.pow_prefer_ell) return;
+  double* inv = cm.d_scal + S_POW_Q + 5;
+  double* zz = cm.d_scal + S_POW_Q + 4;
+  double* lg = cm.d_scal + S_POWLOG_Q;
+  V* z0 = pz2;
+  const int64_t nn = n;
+  elem(cm, nn, [=] __device__(int i) { z0[i] = (V)1.0; });
+  elem(cm, 1, [=] __device__(int) {
+    *inv = 1.0;
+    *zz = 1.0;
+  });
+  tune_reduce(Qp, [&](int k) {
+    V* zc = (k & 1) ? pq2 : pz2;
+    V* zn = (k & 1) ? pz2 : pq2;
+    mat_reduce<3, 0u>(cm, Qp, zc, EpiPowerFused<V>{zc, zn, zz, true, inv}, cm.d_scal + S_POW_Q + 1,
+                      PowerFin{lg, k & 31, inv});
+  });
 }
 
 // Values of G into the format its products use (the padding of ELL / SELL
@@ -683,6 +713,8 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
     qTmp = mem.alloc<V>(N2);
   }
   if (power_engine) build_gram(pp, tpr_A);
+  if (power_engine && tpr_Q <= 0) autotune_power_Q();
+  else Qp = Q;
   reset_state();
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
 }
@@ -1271,7 +1303,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     }
     return d;
   };
-  const DCsr<V> pA = ellp(A), pAT = ellp(AT), pQ = ellp(Q), pL = ellp(L), pLT = ellp(LT);
+  const DCsr<V> pA = ellp(A), pAT = ellp(AT), pQ = ellp(Qp.rows ? Qp : Q), pL = ellp(L), pLT = ellp(LT);
   // A A' on the Gram matrix: G's values for this solve, u_0 = A' z_0 (the
   // chain's n-space state; 1/||z_0|| is already in scal + 4), then one
   // sweep of G per step

@@ -140,6 +140,10 @@ class Engine {
   DCsr<V> G;
   bool gram = false;
   void autotune_gram();  // (public: it launches device lambdas)
+  void autotune_power_Q();
+  template <typename Step>
+  void tune_reduce(DCsr<V>& M, Step step);
+  DCsr<V> Qp;  // Q under the schedule of its power step
   double *gu0 = nullptr, *gu1 = nullptr;  // the Gram chain's state u_k (FP64 in both engines)
   V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;
   float* qws = nullptr;  // TF32 operand images of the tensor-core QAP products
