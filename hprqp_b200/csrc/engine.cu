@@ -562,6 +562,19 @@ void Engine<V>::autotune_gram() {
   });
 }
 
+// What the power method needs beyond the iteration's matrices (the Gram
+// matrix, the power schedule of Q): built once, by the constructor of the
+// engine that runs the power method, or on the first power method of the
+// other engine (a handle prepared for one precision and then solved in the
+// other).
+template <typename V>
+void Engine<V>::power_setup(const Prepared& pp, int tpr_A, int tpr_Q) {
+  if (power_ready) return;
+  power_ready = true;
+  build_gram(pp, tpr_A);
+  if (tpr_Q <= 0) autotune_power_Q();
+}
+
 // The sparse Q's power step runs on its own copy of Q's schedule, chosen by
 // timing that step (Q's own schedule is chosen for the iteration's passes).
 template <typename V>
@@ -712,9 +725,8 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
     qT = upload<V>(cm, mem, hp.qT, N2);
     qTmp = mem.alloc<V>(N2);
   }
-  if (power_engine) build_gram(pp, tpr_A);
-  if (power_engine && tpr_Q <= 0) autotune_power_Q();
-  else Qp = Q;
+  Qp = Q;
+  if (power_engine) power_setup(pp, tpr_A, tpr_Q);
   reset_state();
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
 }

@@ -144,6 +144,8 @@ class Engine {
   template <typename Step>
   void tune_reduce(DCsr<V>& M, Step step);
   DCsr<V> Qp;  // Q under the schedule of its power step
+  bool power_ready = false;
+  void power_setup(const Prepared& pp, int tpr_A, int tpr_Q);
   double *gu0 = nullptr, *gu1 = nullptr;  // the Gram chain's state u_k (FP64 in both engines)
   V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;
   float* qws = nullptr;  // TF32 operand images of the tensor-core QAP products

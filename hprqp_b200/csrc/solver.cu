@@ -417,8 +417,13 @@ static void estimate_lambdas(Handle& H, const hprqp_params& p, bool fp32, double
   double a = 0.0, q = 0.0;
   int64_t ia = 0, iq = 0;
   if (needA || needQ) {
-    if (fp32) H.e32->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
-    else H.e64->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
+    if (fp32) {
+      H.e32->power_setup(pp, p.spmv_mode_A, p.spmv_mode_Q);
+      H.e32->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
+    } else {
+      H.e64->power_setup(pp, p.spmv_mode_A, p.spmv_mode_Q);
+      H.e64->power_both(needA, needQ, 1e-4, 5000, &a, &q, &ia, &iq);
+    }
   }
   if (!needA) ia = 0;
   if (!needQ) iq = 0;
