@@ -53,6 +53,8 @@ void Common::init() {
   if (rc) reduce_cap = std::max(1, std::min(std::atoi(rc), kReduceGridLimit));
   const char* pel = std::getenv("HPRQP_POWER_ELL");
   pow_prefer_ell = pel && pel[0] == '1';
+  const char* cf = std::getenv("HPRQP_POWER_CHUNK_FOLD");
+  pow_chunk_fold = !(cf && cf[0] == '0');
   const char* at = std::getenv("HPRQP_AUTOTUNE");
   autotune = !(at && at[0] == '0');
   const char* ep = std::getenv("HPRQP_EPI_PREFETCH");
@@ -88,9 +90,9 @@ void Common::sync_read(int first, int count) {
 // all are launched with programmatic stream serialisation.
 // ---------------------------------------------------------------------------
 template <typename... KArgs, typename... Args>
-static void launch(Common& cm, void (*kernel)(KArgs...), int grid, int block, Args... args) {
+static void launch(Common& cm, void (*kernel)(KArgs...), dim3 grid, int block, Args... args) {
   cudaLaunchConfig_t cfg{};
-  cfg.gridDim = dim3((unsigned)grid);
+  cfg.gridDim = grid;
   cfg.blockDim = dim3((unsigned)block);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = cm.stream;
@@ -410,6 +412,34 @@ static void mat_reduce(Common& cm, const DCsr<V>& M, const X* xin, const Epi& e,
   if (M.sell || (M.ell && M.sell_len > 0))
     reduce<K, MM, double>(cm, 1, M.rows, SellSrc<V, X>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, out, fin);
   else reduce<K, MM, double>(cm, M.tpr, M.rows, CsrSrc<V, X>{M.ptr, M.col, M.val, xin}, e, out, fin);
+}
+
+// CTAs of a partials-only pass over M (the fold needs the count)
+template <typename V>
+static int partials_grid(const Common& cm, const DCsr<V>& M) {
+  const bool sell = M.sell || (M.ell && M.sell_len > 0);
+  return reduce_grid(M.rows, sell ? 1 : M.tpr, cm.reduce_cap);
+}
+
+// Fused product + per-CTA sums, no fold (the power steps of a chunk)
+template <int K, typename V, typename X, typename Epi>
+static void mat_partials(Common& cm, const DCsr<V>& M, const X* xin, const Epi& e, double* partials) {
+  const int grid = partials_grid(cm, M);
+  if (M.sell || (M.ell && M.sell_len > 0)) {
+    launch(cm, k_row_partials<1, K, double, SellSrc<V, X>, Epi>, grid, kBlock, M.rows,
+           SellSrc<V, X>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, partials);
+    return;
+  }
+  switch (M.tpr) {
+#define HPRQP_PARTIALS(T)                                                                                      \
+  case T:                                                                                                      \
+    launch(cm, k_row_partials<T, K, double, CsrSrc<V, X>, Epi>, grid, kBlock, M.rows,                          \
+           CsrSrc<V, X>{M.ptr, M.col, M.val, xin}, e, partials);                                               \
+    break;
+    HPRQP_PARTIALS(1) HPRQP_PARTIALS(2) HPRQP_PARTIALS(4) HPRQP_PARTIALS(8) HPRQP_PARTIALS(16) HPRQP_PARTIALS(32)
+#undef HPRQP_PARTIALS
+    default: throw Error(HPRQP_E_ARG, "bad threads-per-row");
+  }
 }
 
 // Row-schedule autotuner: time the plain product for each threads-per-row
@@ -1320,10 +1350,49 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   // chain's n-space state; 1/||z_0|| is already in scal + 4), then one
   // sweep of G per step
   const bool use_gram = gram && ca.on;
+  // Chunk fold (HPRQP_POWER_CHUNK_FOLD, default on): the Gram chain and a
+  // sparse Q's chain run unnormalised, each step writing only its per-CTA
+  // sums; one fold per chunk gives every step's (lambda, err) and
+  // renormalises the state (kernels.cuh).  The other chains keep the
+  // per-step fold.
+  const bool cfA = cm.pow_chunk_fold && use_gram;
+  const bool cfQ = cm.pow_chunk_fold && cq.on && has_Q_sparse && !is_lasso && !is_qap;
+  const int nblkA = cfA ? partials_grid(cm, G) : 0, nblkQ = cfQ ? partials_grid(cm, pQ) : 0;
+  if ((cfA || cfQ) && !pow_cf_part) {
+    pow_cf_part = mem.alloc<double>((int64_t)2 * kPowChunk * kMaxReduceGrid * 3);
+    pow_cf_tot = mem.alloc<double>(2 * kPowChunk * 3);
+  }
+  // the unnormalised Q chain keeps an FP64 state: within a chunk it grows by
+  // about lambda^32, which FP32 cannot hold for lambda above ~15
+  if (cfQ) {
+    if (!gq0) {
+      gq0 = mem.alloc<double>(n);
+      gq1 = mem.alloc<double>(n);
+    }
+    k_start_vector<double><<<(int)((n + kBlock - 1) / kBlock), kBlock, 0, main>>>(n, gq0);
+    HPRQP_LAUNCH_CHECK();
+    cm.launches++;
+  }
   if (use_gram) {
     gram_values();
-    mat_rows(pAT, pz, EpiStore<double>{gu0, 1.0});
+    // u_0 = A' z_0 / ||z_0|| = w_0 (the chunk fold starts from a normalised state)
+    mat_rows(pAT, pz, EpiStoreInvNorm<double>{gu0, ca.scal + 2, ca.scal + 4});
   }
+  auto chunk_chain = [&](bool on, int kind, int nblk, double* log) {
+    PowChunkChain d{};
+    if (!on) return d;
+    d.kind = kind;
+    d.K = kind == 0 ? 2 : 3;
+    d.nblk = nblk;
+    d.steps = kPowChunk;
+    d.partials = pow_cf_part + (size_t)kind * kPowChunk * kMaxReduceGrid * 3;
+    d.totals = pow_cf_tot + kind * kPowChunk * 3;
+    d.log = log;
+    d.len = n;
+    if (kind == 0) d.state64 = gu0;
+    else d.stateQ64 = gq0;
+    return d;
+  };
   auto step = [&](const Chain& c, cudaStream_t st, int k) {
     use(c, st);
     V* zc = (k & 1) ? c.z1 : c.z0;
@@ -1339,7 +1408,16 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
       reduce<3, 0u, double>(cm, 1, len, VecSrc<V>{zn}, EpiPowerFused<V>{zc, nullptr, zz, false, inv}, c.scal + 1,
                             fin);
     };
-    if (c.which == 0 && use_gram) {  // u ping-pongs between gu0 and gu1
+    if (c.which == 0 && cfA) {  // chunk fold: partials of step k only
+      const double* uc = (k & 1) ? gu1 : gu0;
+      double* un = (k & 1) ? gu0 : gu1;
+      mat_partials<2>(cm, G, uc, EpiGramRaw{uc, un}, pow_cf_part + (size_t)k * nblkA * 2);
+    } else if (c.which == 1 && cfQ) {
+      const double* yc = (k & 1) ? gq1 : gq0;
+      double* yn = (k & 1) ? gq0 : gq1;
+      mat_partials<3>(cm, pQ, yc, EpiPowRaw<double>{yc, yn},
+                      pow_cf_part + (size_t)kPowChunk * kMaxReduceGrid * 3 + (size_t)k * nblkQ * 3);
+    } else if (c.which == 0 && use_gram) {  // u ping-pongs between gu0 and gu1
       const double* uc = (k & 1) ? gu1 : gu0;
       double* un = (k & 1) ? gu0 : gu1;
       mat_reduce<2, 0u>(cm, G, uc, EpiGramPower<double>{uc, un, inv}, c.scal + 1, GramPowerFin{c.log, k, c.scal + 4});
@@ -1394,8 +1472,16 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
       HPRQP_CUDA(cudaEventRecord(join, qst));
       HPRQP_CUDA(cudaStreamWaitEvent(main, join, 0));
     }
+    const PowChunkChain c0 = chunk_chain(doA && cfA, 0, nblkA, ca.log);
+    const PowChunkChain c1 = chunk_chain(doQ && cfQ, 1, nblkQ, cq.log);
+    if (c0.steps || c1.steps) {
+      launch(cm, k_pow_chunk_fold, dim3(kPowChunk, 2), kBlock, c0, c1);
+      const int g = (int)std::min<int64_t>(kMaxReduceGrid, (n + kBlock - 1) / kBlock);
+      launch(cm, k_pow_chunk_finish, dim3(g, 2), kBlock, c0, c1);
+    }
   };
   int it = 0;
+  bool cf_failed = false;
   while (it < max_it && ((ca.on && ca.found < 0) || (cq.on && cq.found < 0))) {
     const bool doA = ca.on && ca.found < 0, doQ = cq.on && cq.found < 0;
     const int gi = (doA ? 1 : 0) | (doQ ? 2 : 0);
@@ -1423,6 +1509,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
       if (!c->on || c->found >= 0) continue;
       const double* lg = cm.h_scal + (c->which == 0 ? S_POWLOG : S_POWLOG_Q);
       for (int k = 0; k < kPowChunk && it + k < max_it; ++k) {
+        if (std::isnan(lg[2 * k]) && (c->which == 0 ? cfA : cfQ)) cf_failed = true;
         c->lam = lg[2 * k];
         if (lg[2 * k + 1] < tol) {
           c->found = it + k + 1;
@@ -1431,11 +1518,23 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
       }
     }
     it += kPowChunk;
+    if (cf_failed) break;
   }
   for (auto& g : graphs)
     if (g) cudaGraphExecDestroy(g);
   cudaEventDestroy(fork);
   cudaEventDestroy(join);
+  if (cf_failed) {  // a chunk-fold state left FP64 range: the per-step fold instead
+    cm.pow_chunk_fold = false;
+    try {
+      power_both(want_A, want_Q, tol, max_it, lamA_out, lamQ_out, itA, itQ);
+    } catch (...) {
+      cm.pow_chunk_fold = true;
+      throw;
+    }
+    cm.pow_chunk_fold = true;
+    return;
+  }
   for (Chain* c : {&ca, &cq})
     if (c->on && c->found < 0)
       std::fprintf(stderr, "Power iteration (%s) did not converge within the specified tolerance.\n",

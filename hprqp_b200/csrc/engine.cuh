@@ -82,6 +82,8 @@ struct Common {  // per-handle resources shared by the engines
   // on the 700x700 grid (FP32 iteration 40.3 vs 40.3 us, FP64 50.3 vs
   // 48.4 us), so off by default
   int epi_prefetch = 0;
+  // power chains folded once per chunk (HPRQP_POWER_CHUNK_FOLD=0: per step)
+  bool pow_chunk_fold = true;
   // row-schedule autotuner (timed); HPRQP_AUTOTUNE=0 applies a fixed rule
   // instead, e.g. under a profiler, whose serialisation makes the timings
   // meaningless
@@ -145,6 +147,8 @@ class Engine {
   void tune_reduce(DCsr<V>& M, Step step);
   DCsr<V> Qp;  // Q under the schedule of its power step
   bool power_ready = false;
+  double *pow_cf_part = nullptr, *pow_cf_tot = nullptr;  // chunk-fold partials and totals
+  double *gq0 = nullptr, *gq1 = nullptr;                  // the chunk-fold Q chain's FP64 state
   void power_setup(const Prepared& pp, int tpr_A, int tpr_Q);
   double *gu0 = nullptr, *gu1 = nullptr;  // the Gram chain's state u_k (FP64 in both engines)
   V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;

@@ -738,6 +738,146 @@ __global__ void __launch_bounds__(kBlock) k_start_vector_seg(int B, const int64_
   out[j] = (V)(sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2) + 1e-8);
 }
 
+// ---------------------------------------------------------------------------
+// Power steps with the fold once per chunk.  The chains run unnormalised
+// (y_{k+1} = M y_k) and every step only writes its per-CTA dot products;
+// one fold per chunk of steps turns them into each step's (lambda, err)
+// with scale-invariant formulas and renormalises the state.
+//   Q chain (q_k = y_k / ||y_k||, z_{k+1} = Q q_k):
+//     a = y_k . y_{k+1}, b = y_k . y_k, c = y_{k+1} . y_{k+1}
+//     lambda_k = a / b, ||z_{k+1}||^2 = c / b, ||z_{k+1} - lambda q_k||^2 = c / b - lambda^2
+//   Gram chain (w_k = s_k u_k with s_0 = 1 at the chunk start, s_k = 1 / sqrt(a_{k-1})):
+//     a = u_k . u_{k+1}, b = u_k . u_k
+//     lambda_k = s_k^2 b, ||z_{k+1}||^2 = s_k^2 a
+// Both states are FP64 (an unnormalised chain grows or shrinks by about
+// lambda per step between renormalisations); b is taken from the stored
+// y_k, so each step's sums describe the same vectors and ||z||^2 >= lambda^2
+// holds up to FP64 rounding.  A total that is not finite and positive
+// (a state out of FP64 range) logs NaN, and the host then reruns the
+// method with the per-step fold.
+// ---------------------------------------------------------------------------
+template <int TPR, int K, typename Acc, typename Src, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_row_partials(int nrows, Src src, Epi epi, double* __restrict__ partials) {
+  pdl_enter();
+  double r[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) r[k] = 0.0;
+  const int lane = threadIdx.x & (TPR - 1);
+  const int rows_per_grid = (int)(gridDim.x * (kBlock / TPR));
+  for (int row = (int)((blockIdx.x * kBlock + threadIdx.x) / TPR); row < nrows; row += rows_per_grid) {
+    const Acc acc = src.template dot<TPR, Acc>(row, lane);
+    if (lane == 0) epi(row, acc, r);
+  }
+  block_reduce<K, 0u>(r);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) partials[(size_t)blockIdx.x * K + k] = r[k];
+  }
+}
+
+template <typename V>
+struct EpiPowRaw {  // Q chain: y_{k+1} = Q y_k; sums a, b, c
+  const V* yc;
+  V* yn;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, double (&r)[3]) const {
+    const double v = (double)acc;
+    yn[i] = (V)v;
+    const double y = (double)yc[i];
+    r[0] += y * v;
+    r[1] += y * y;
+    r[2] += v * v;
+  }
+};
+
+struct EpiGramRaw {  // Gram chain: u_{k+1} = G u_k; sums a, b
+  const double* uc;
+  double* un;
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, double (&r)[2]) const {
+    const double v = (double)acc;
+    un[i] = v;
+    const double u = uc[i];
+    r[0] += u * v;
+    r[1] += u * u;
+  }
+};
+
+// One chain's chunk of steps for the fold: its per-step partials
+// (steps x nblk x K), its totals (steps x K), its log (lambda, err per
+// step), the state to renormalise, and the kind (0 = Gram, 1 = Q).
+struct PowChunkChain {
+  const double* partials;
+  double* totals;
+  double* log;
+  int nblk, K, steps, kind;
+  double* state64;   // Gram state
+  double* stateQ64;  // Q state
+  int64_t len;
+  double* scale_out;  // the renormalisation factor of the chunk's last state
+};
+
+// Fold: CTA (step, chain) sums that step's per-CTA partials in CTA order.
+static __global__ void __launch_bounds__(kBlock) k_pow_chunk_fold(PowChunkChain c0, PowChunkChain c1) {
+  const PowChunkChain& c = blockIdx.y == 0 ? c0 : c1;
+  const int k = blockIdx.x;
+  if (k >= c.steps || c.nblk == 0) return;
+  double acc[3] = {0.0, 0.0, 0.0};
+  const double* p = c.partials + (size_t)k * c.nblk * c.K;
+  for (int b = threadIdx.x; b < c.nblk; b += kBlock)
+    for (int q = 0; q < c.K; ++q) acc[q] += __ldcg(p + (size_t)b * c.K + q);
+  block_reduce<3, 0u>(acc);
+  if (threadIdx.x == 0)
+    for (int q = 0; q < c.K; ++q) c.totals[k * 3 + q] = acc[q];
+}
+
+// The chunk's (lambda, err) recurrence (every CTA computes it from the
+// totals, CTA 0 writes the log) and the renormalisation of the last state.
+__device__ __forceinline__ double pow_chunk_recur(const PowChunkChain& c, bool write) {
+  double s2 = 1.0;  // s_k^2 of the Gram chain (1 at the chunk start)
+  double scale = 1.0;
+  for (int k = 0; k < c.steps; ++k) {
+    const double* t = c.totals + k * 3;
+    double lam, zz;
+    const bool ok = isfinite(t[0]) && isfinite(t[1]) && t[0] > 0.0 && t[1] > 0.0 &&
+                    (c.kind == 0 || (isfinite(t[2]) && t[2] > 0.0));
+    if (!ok) {
+      if (write) c.log[2 * k] = c.log[2 * k + 1] = nan("");
+      continue;
+    }
+    if (c.kind == 0) {
+      lam = s2 * t[1];
+      zz = s2 * t[0];
+      s2 = 1.0 / t[0];
+    } else {
+      lam = t[0] / t[1];
+      zz = t[2] / t[1];
+    }
+    if (write) {
+      c.log[2 * k] = lam;
+      c.log[2 * k + 1] = sqrt(fmax(zz - lam * lam, 0.0)) / (sqrt(zz) + lam);
+    }
+    if (k == c.steps - 1) scale = c.kind == 0 ? sqrt(s2) : 1.0 / sqrt(t[2]);
+  }
+  return scale;
+}
+
+static __global__ void __launch_bounds__(kBlock) k_pow_chunk_finish(PowChunkChain c0, PowChunkChain c1) {
+  const PowChunkChain& c = blockIdx.y == 0 ? c0 : c1;
+  if (c.steps == 0) return;
+  __shared__ double s_scale;
+  if (threadIdx.x == 0) {
+    s_scale = pow_chunk_recur(c, blockIdx.x == 0);
+    if (blockIdx.x == 0 && c.scale_out) *c.scale_out = s_scale;
+  }
+  __syncthreads();
+  const double sc = s_scale;
+  for (int64_t i = (int64_t)blockIdx.x * kBlock + threadIdx.x; i < c.len; i += (int64_t)gridDim.x * kBlock) {
+    if (c.state64) c.state64[i] *= sc;
+    if (c.stateQ64) c.stateQ64[i] *= sc;
+  }
+}
+
 // 1/sqrt of a reduced sum of squares (the start vector's norm)
 struct InvNormFin {
   double* inv_out;

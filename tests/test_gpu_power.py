@@ -103,3 +103,21 @@ def test_gram_chain_matches_two_product_chain(precision, rtol):
         # autotuned per process, so only to rounding)
         assert iq1 == iq0, (k, iq1, iq0)
         assert abs(lq1 - lq0) <= rtol * max(abs(lq0), 1e-300), (k, lq1, lq0)
+
+
+@pytest.mark.parametrize("precision,rtol", [("fp64", 1e-10), ("fp32_polish", 1e-5)])
+def test_chunk_fold_matches_per_step_fold(precision, rtol):
+    """The chains folded once per 32-step chunk (unnormalised FP64 states,
+    scale-invariant formulas) stop at the per-step fold's step with the same
+    lambda to rounding.  In FP32 the per-step Q chain keeps an FP32 state,
+    the chunk-fold one an FP64 state: the stop may move by a step or two."""
+    on = _lambdas_with_env({"HPRQP_POWER_CHUNK_FOLD": "1"}, precision)
+    off = _lambdas_with_env({"HPRQP_POWER_CHUNK_FOLD": "0"}, precision)
+    for k in CASES:
+        lam1, it1, lq1, iq1 = on[k]
+        lam0, it0, lq0, iq0 = off[k]
+        slack = 0 if precision == "fp64" else max(2, it0 // 100)
+        assert abs(it1 - it0) <= slack and abs(iq1 - iq0) <= max(slack, 0 if precision == "fp64" else 2 + iq0 // 100), \
+            (k, it1, it0, iq1, iq0)
+        assert abs(lam1 - lam0) <= rtol * max(abs(lam0), 1e-300), (k, lam1, lam0)
+        assert abs(lq1 - lq0) <= rtol * max(abs(lq0), 1e-300), (k, lq1, lq0)
