@@ -819,6 +819,7 @@ struct PowChunkChain {
 
 // Fold: CTA (step, chain) sums that step's per-CTA partials in CTA order.
 static __global__ void __launch_bounds__(kBlock) k_pow_chunk_fold(PowChunkChain c0, PowChunkChain c1) {
+  pdl_enter();  // the chunk's last steps must be complete
   const PowChunkChain& c = blockIdx.y == 0 ? c0 : c1;
   const int k = blockIdx.x;
   if (k >= c.steps || c.nblk == 0) return;
@@ -863,6 +864,7 @@ __device__ __forceinline__ double pow_chunk_recur(const PowChunkChain& c, bool w
 }
 
 static __global__ void __launch_bounds__(kBlock) k_pow_chunk_finish(PowChunkChain c0, PowChunkChain c1) {
+  pdl_enter();  // the fold must be complete
   const PowChunkChain& c = blockIdx.y == 0 ? c0 : c1;
   if (c.steps == 0) return;
   __shared__ double s_scale;
