@@ -1476,13 +1476,9 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     }
   };
   // both chunk-fold chains in one launch per step while both run, when each
-  // matrix is on SELL-32 or CSR with 1, 2 or 4 threads per row (HPRQP_POWER_DUAL=0:
-  // two streams)
-  auto sched = [](const DCsr<V>& M) {  // 0 = SELL-32, else CSR threads per row
-    return (M.sell || (M.ell && M.sell_len > 0)) ? 0 : M.tpr;
-  };
-  const int schA = cfA ? sched(G) : -1, schQ = cfQ ? sched(pQ) : -1;
-  const bool dual_ok = cm.pow_dual && cfA && cfQ && schA <= 4 && schQ <= 4;
+  // matrix has a one-thread-per-row schedule (HPRQP_POWER_DUAL=0: two streams)
+  auto one_tpr = [](const DCsr<V>& M) { return M.sell || (M.ell && M.sell_len > 0) || M.tpr == 1; };
+  const bool dual_ok = cm.pow_dual && cfA && cfQ && one_tpr(G) && one_tpr(pQ);
   auto dual_step = [&](int k) {
     const double* uc = (k & 1) ? gu1 : gu0;
     double* un = (k & 1) ? gu0 : gu1;
@@ -1490,40 +1486,25 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     double* yn = (k & 1) ? gq0 : gq1;
     double* pa = pow_cf_part + (size_t)k * nblkA * 2;
     double* pq = pow_cf_part + (size_t)kPowChunk * kMaxReduceGrid * 3 + (size_t)k * nblkQ * 3;
+    const bool sa = G.sell || (G.ell && G.sell_len > 0), sq = pQ.sell || (pQ.ell && pQ.sell_len > 0);
     const SellSrc<V, double> SA{G.sptr, G.ptr, G.scol, G.sval, uc}, SQ{pQ.sptr, pQ.ptr, pQ.scol, pQ.sval, yc};
     const CsrSrc<V, double> CA{G.ptr, G.col, G.val, uc}, CQ{pQ.ptr, pQ.col, pQ.val, yc};
     const EpiGramRaw ea{uc, un};
     const EpiPowRaw<double> eq{yc, yn};
     const dim3 grid(nblkA + nblkQ);
     const int nA = (int)n, nQ = (int)n;
-    auto with_q = [&](auto ta, const auto& srcA) {
-      constexpr int TA = decltype(ta)::value;
-      using SA_t = std::decay_t<decltype(srcA)>;
-      switch (schQ) {
-        case 0:
-          launch(cm, k_dual_partials<TA, SA_t, EpiGramRaw, 1, SellSrc<V, double>, EpiPowRaw<double>>, grid, kBlock, nA,
-                 srcA, ea, pa, nblkA, nQ, SQ, eq, pq);
-          break;
-        case 1:
-          launch(cm, k_dual_partials<TA, SA_t, EpiGramRaw, 1, CsrSrc<V, double>, EpiPowRaw<double>>, grid, kBlock, nA,
-                 srcA, ea, pa, nblkA, nQ, CQ, eq, pq);
-          break;
-        case 2:
-          launch(cm, k_dual_partials<TA, SA_t, EpiGramRaw, 2, CsrSrc<V, double>, EpiPowRaw<double>>, grid, kBlock, nA,
-                 srcA, ea, pa, nblkA, nQ, CQ, eq, pq);
-          break;
-        default:
-          launch(cm, k_dual_partials<TA, SA_t, EpiGramRaw, 4, CsrSrc<V, double>, EpiPowRaw<double>>, grid, kBlock, nA,
-                 srcA, ea, pa, nblkA, nQ, CQ, eq, pq);
-          break;
-      }
-    };
-    switch (schA) {
-      case 0: with_q(std::integral_constant<int, 1>{}, SA); break;
-      case 1: with_q(std::integral_constant<int, 1>{}, CA); break;
-      case 2: with_q(std::integral_constant<int, 2>{}, CA); break;
-      default: with_q(std::integral_constant<int, 4>{}, CA); break;
-    }
+    if (sa && sq)
+      launch(cm, k_dual_partials<SellSrc<V, double>, EpiGramRaw, SellSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
+             nA, SA, ea, pa, nblkA, nQ, SQ, eq, pq);
+    else if (sa)
+      launch(cm, k_dual_partials<SellSrc<V, double>, EpiGramRaw, CsrSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
+             nA, SA, ea, pa, nblkA, nQ, CQ, eq, pq);
+    else if (sq)
+      launch(cm, k_dual_partials<CsrSrc<V, double>, EpiGramRaw, SellSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
+             nA, CA, ea, pa, nblkA, nQ, SQ, eq, pq);
+    else
+      launch(cm, k_dual_partials<CsrSrc<V, double>, EpiGramRaw, CsrSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
+             nA, CA, ea, pa, nblkA, nQ, CQ, eq, pq);
   };
   auto issue_chunk = [&](bool doA, bool doQ) {
     if (doA && doQ && dual_ok) {

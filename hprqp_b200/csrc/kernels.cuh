@@ -779,17 +779,14 @@ __global__ void __launch_bounds__(kBlock) k_row_partials(int nrows, Src src, Epi
 // the rest sweep Q, each writing its chain's per-CTA sums (the same layout
 // as two separate k_row_partials launches).  One launch per step instead
 // of two concurrent ones that compete for the SMs.
-template <int TA, typename SrcA, typename EpiA, int TQ, typename SrcQ, typename EpiQ>
+template <typename SrcA, typename EpiA, typename SrcQ, typename EpiQ>
 __global__ void __launch_bounds__(kBlock) k_dual_partials(int nA, SrcA sa, EpiA ea, double* __restrict__ pa, int gA,
                                                           int nQ, SrcQ sq, EpiQ eq, double* __restrict__ pq) {
   pdl_enter();
   if ((int)blockIdx.x < gA) {
     double r[2] = {0.0, 0.0};
-    const int lane = threadIdx.x & (TA - 1);
-    for (int row = (int)((blockIdx.x * kBlock + threadIdx.x) / TA); row < nA; row += gA * (kBlock / TA)) {
-      const double acc = sa.template dot<TA, double>(row, lane);
-      if (lane == 0) ea(row, acc, r);
-    }
+    for (int row = (int)(blockIdx.x * kBlock + threadIdx.x); row < nA; row += gA * kBlock)
+      ea(row, sa.template dot<1, double>(row, 0), r);
     block_reduce<2, 0u>(r);
     if (threadIdx.x == 0) {
       pa[(size_t)blockIdx.x * 2] = r[0];
@@ -798,11 +795,8 @@ __global__ void __launch_bounds__(kBlock) k_dual_partials(int nA, SrcA sa, EpiA 
   } else {
     const int b = (int)blockIdx.x - gA, gQ = (int)gridDim.x - gA;
     double r[3] = {0.0, 0.0, 0.0};
-    const int lane = threadIdx.x & (TQ - 1);
-    for (int row = (b * kBlock + (int)threadIdx.x) / TQ; row < nQ; row += gQ * (kBlock / TQ)) {
-      const double acc = sq.template dot<TQ, double>(row, lane);
-      if (lane == 0) eq(row, acc, r);
-    }
+    for (int row = b * kBlock + (int)threadIdx.x; row < nQ; row += gQ * kBlock)
+      eq(row, sq.template dot<1, double>(row, 0), r);
     block_reduce<3, 0u>(r);
     if (threadIdx.x == 0) {
       pq[(size_t)b * 3] = r[0];
