@@ -1451,16 +1451,14 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     }
     restore();
   };
-  // a chunk = kPowChunk steps of every active chain (captured in a graph),
-  // then, for the chunk-fold chains, the fold
+  // one chunk = kPowChunk steps of every active chain; A on the main stream,
+  // Q forked onto the second stream when both run (captured in a graph)
   cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
   int64_t graph_launches[4] = {0, 0, 0, 0};
   cudaEvent_t fork = nullptr, join = nullptr;
   HPRQP_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   HPRQP_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
-  // one chunk of steps of the active chains: A on the main stream, Q forked
-  // onto the second stream when both run (captured in a graph)
-  auto issue_steps = [&](bool doA, bool doQ) {
+  auto issue_chunk = [&](bool doA, bool doQ) {
     const bool two = doA && doQ && qst != main;
     if (two) {
       HPRQP_CUDA(cudaEventRecord(fork, main));
@@ -1473,44 +1471,6 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     if (two) {
       HPRQP_CUDA(cudaEventRecord(join, qst));
       HPRQP_CUDA(cudaStreamWaitEvent(main, join, 0));
-    }
-  };
-  // both chunk-fold chains in one launch per step while both run, when each
-  // matrix has a one-thread-per-row schedule (HPRQP_POWER_DUAL=0: two streams)
-  auto one_tpr = [](const DCsr<V>& M) { return M.sell || (M.ell && M.sell_len > 0) || M.tpr == 1; };
-  const bool dual_ok = cm.pow_dual && cfA && cfQ && one_tpr(G) && one_tpr(pQ);
-  auto dual_step = [&](int k) {
-    const double* uc = (k & 1) ? gu1 : gu0;
-    double* un = (k & 1) ? gu0 : gu1;
-    const double* yc = (k & 1) ? gq1 : gq0;
-    double* yn = (k & 1) ? gq0 : gq1;
-    double* pa = pow_cf_part + (size_t)k * nblkA * 2;
-    double* pq = pow_cf_part + (size_t)kPowChunk * kMaxReduceGrid * 3 + (size_t)k * nblkQ * 3;
-    const bool sa = G.sell || (G.ell && G.sell_len > 0), sq = pQ.sell || (pQ.ell && pQ.sell_len > 0);
-    const SellSrc<V, double> SA{G.sptr, G.ptr, G.scol, G.sval, uc}, SQ{pQ.sptr, pQ.ptr, pQ.scol, pQ.sval, yc};
-    const CsrSrc<V, double> CA{G.ptr, G.col, G.val, uc}, CQ{pQ.ptr, pQ.col, pQ.val, yc};
-    const EpiGramRaw ea{uc, un};
-    const EpiPowRaw<double> eq{yc, yn};
-    const dim3 grid(nblkA + nblkQ);
-    const int nA = (int)n, nQ = (int)n;
-    if (sa && sq)
-      launch(cm, k_dual_partials<SellSrc<V, double>, EpiGramRaw, SellSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
-             nA, SA, ea, pa, nblkA, nQ, SQ, eq, pq);
-    else if (sa)
-      launch(cm, k_dual_partials<SellSrc<V, double>, EpiGramRaw, CsrSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
-             nA, SA, ea, pa, nblkA, nQ, CQ, eq, pq);
-    else if (sq)
-      launch(cm, k_dual_partials<CsrSrc<V, double>, EpiGramRaw, SellSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
-             nA, CA, ea, pa, nblkA, nQ, SQ, eq, pq);
-    else
-      launch(cm, k_dual_partials<CsrSrc<V, double>, EpiGramRaw, CsrSrc<V, double>, EpiPowRaw<double>>, grid, kBlock,
-             nA, CA, ea, pa, nblkA, nQ, CQ, eq, pq);
-  };
-  auto issue_chunk = [&](bool doA, bool doQ) {
-    if (doA && doQ && dual_ok) {
-      for (int k = 0; k < kPowChunk; ++k) dual_step(k);
-    } else {
-      issue_steps(doA, doQ);
     }
     const PowChunkChain c0 = chunk_chain(doA && cfA, 0, nblkA, ca.log);
     const PowChunkChain c1 = chunk_chain(doQ && cfQ, 1, nblkQ, cq.log);

@@ -84,7 +84,6 @@ struct Common {  // per-handle resources shared by the engines
   int epi_prefetch = 0;
   // power chains folded once per chunk (HPRQP_POWER_CHUNK_FOLD=0: per step)
   bool pow_chunk_fold = true;
-  bool pow_dual = true;  // both chunk-fold chains in one launch per step (HPRQP_POWER_DUAL=0: two streams)
   // row-schedule autotuner (timed); HPRQP_AUTOTUNE=0 applies a fixed rule
   // instead, e.g. under a profiler, whose serialisation makes the timings
   // meaningless

@@ -775,37 +775,6 @@ __global__ void __launch_bounds__(kBlock) k_row_partials(int nrows, Src src, Epi
   }
 }
 
-// Both chains' steps in one launch: CTAs [0, gA) sweep the Gram matrix,
-// the rest sweep Q, each writing its chain's per-CTA sums (the same layout
-// as two separate k_row_partials launches).  One launch per step instead
-// of two concurrent ones that compete for the SMs.
-template <typename SrcA, typename EpiA, typename SrcQ, typename EpiQ>
-__global__ void __launch_bounds__(kBlock) k_dual_partials(int nA, SrcA sa, EpiA ea, double* __restrict__ pa, int gA,
-                                                          int nQ, SrcQ sq, EpiQ eq, double* __restrict__ pq) {
-  pdl_enter();
-  if ((int)blockIdx.x < gA) {
-    double r[2] = {0.0, 0.0};
-    for (int row = (int)(blockIdx.x * kBlock + threadIdx.x); row < nA; row += gA * kBlock)
-      ea(row, sa.template dot<1, double>(row, 0), r);
-    block_reduce<2, 0u>(r);
-    if (threadIdx.x == 0) {
-      pa[(size_t)blockIdx.x * 2] = r[0];
-      pa[(size_t)blockIdx.x * 2 + 1] = r[1];
-    }
-  } else {
-    const int b = (int)blockIdx.x - gA, gQ = (int)gridDim.x - gA;
-    double r[3] = {0.0, 0.0, 0.0};
-    for (int row = b * kBlock + (int)threadIdx.x; row < nQ; row += gQ * kBlock)
-      eq(row, sq.template dot<1, double>(row, 0), r);
-    block_reduce<3, 0u>(r);
-    if (threadIdx.x == 0) {
-      pq[(size_t)b * 3] = r[0];
-      pq[(size_t)b * 3 + 1] = r[1];
-      pq[(size_t)b * 3 + 2] = r[2];
-    }
-  }
-}
-
 template <typename V>
 struct EpiPowRaw {  // Q chain: y_{k+1} = Q y_k; sums a, b, c
   const V* yc;
