@@ -63,7 +63,7 @@ struct DevScaled {
 
 struct Prepared {  // scaled problem + scaling info (Scaling_info_cpu)
   std::shared_ptr<DevScaled> dev;  // set by the GPU scaling, null after host scaling
-  HCsr A, AT, Q;
+  HCsr A, AT, Q;  // with `dev`, A and A' carry their patterns only (values on the device)
   std::vector<double> c, AL, AU, l, u, row_norm, col_norm, diag_Q;
   double norm_b = 0, norm_c = 0, norm_b_org = 0, norm_c_org = 0;
   double b_scale = 1.0, c_scale = 1.0;

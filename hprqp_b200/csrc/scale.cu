@@ -131,8 +131,19 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   o = Prepared();
   o.ruiz = p.use_Ruiz_scaling;
   o.pc = p.use_Pock_Chambolle_scaling;
-  o.A = hp.A;
-  o.AT = hp.AT;
+  // A and A' keep their scaled values on the device only (o.dev): the host
+  // records hold the patterns (the engines' formats and the Gram pattern
+  // are built from them)
+  auto pattern_of = [](const HCsr& h) {
+    HCsr x;
+    x.rows = h.rows;
+    x.cols = h.cols;
+    x.ptr = h.ptr;
+    x.col = h.col;
+    return x;
+  };
+  o.A = pattern_of(hp.A);
+  o.AT = pattern_of(hp.AT);
   o.c = hp.c;
   o.AL = hp.AL;
   o.AU = hp.AU;
@@ -269,8 +280,6 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
     if (!dst.empty())
       HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
   };
-  down(o.A.val, dA.val);
-  down(o.AT.val, dAT.val);
   down(S.val, sv);
   down(o.c, c);
   down(o.l, l);
