@@ -762,6 +762,12 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
 }
 
 template <typename V>
+Engine<V>::~Engine() {
+  for (auto& g : pow_exec)
+    if (g) cudaGraphExecDestroy(g);
+}
+
+template <typename V>
 void Engine<V>::reset_state() {
   V* nv[] = {x, x_hat, x_bar, dx, w, w_bar, dw, z_bar, Qw, Qw_bar, ATy, ATy_bar, ATdy, QATdy, dQw, Qx, tempv};
   for (V* p : nv) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(V) * n, cm.stream));
@@ -1453,8 +1459,20 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   };
   // one chunk = kPowChunk steps of every active chain; A on the main stream,
   // Q forked onto the second stream when both run (captured in a graph)
-  cudaGraphExec_t graphs[4] = {nullptr, nullptr, nullptr, nullptr};
-  int64_t graph_launches[4] = {0, 0, 0, 0};
+  // the instantiated chunk graphs are kept for the engine's later power
+  // methods: they depend only on the engine's buffers and on this key
+  const int key = (ca.on ? 1 : 0) | (cq.on ? 2 : 0) | (use_gram ? 4 : 0) | (cfA ? 8 : 0) | (cfQ ? 16 : 0) |
+                  (cm.pow_split ? 32 : 0) | (cm.pow_prefer_ell ? 64 : 0);
+  if (key != pow_exec_key) {
+    for (auto& g : pow_exec)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+    pow_exec_key = key;
+  }
+  cudaGraphExec_t* graphs = pow_exec;
+  int64_t* graph_launches = pow_exec_launches;
   cudaEvent_t fork = nullptr, join = nullptr;
   HPRQP_CUDA(cudaEventCreateWithFlags(&fork, cudaEventDisableTiming));
   HPRQP_CUDA(cudaEventCreateWithFlags(&join, cudaEventDisableTiming));
@@ -1520,8 +1538,6 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     it += kPowChunk;
     if (cf_failed) break;
   }
-  for (auto& g : graphs)
-    if (g) cudaGraphExecDestroy(g);
   cudaEventDestroy(fork);
   cudaEventDestroy(join);
   if (cf_failed) {  // a chunk-fold state left FP64 range: the per-step fold instead

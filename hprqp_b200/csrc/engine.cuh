@@ -147,6 +147,10 @@ class Engine {
   void tune_reduce(DCsr<V>& M, Step step);
   DCsr<V> Qp;  // Q under the schedule of its power step
   bool power_ready = false;
+  ~Engine();
+  cudaGraphExec_t pow_exec[4] = {nullptr, nullptr, nullptr, nullptr};  // power chunk graphs by active chains
+  int64_t pow_exec_launches[4] = {0, 0, 0, 0};
+  int pow_exec_key = -1;
   double *pow_cf_part = nullptr, *pow_cf_tot = nullptr;  // chunk-fold partials and totals
   double *gq0 = nullptr, *gq1 = nullptr;                  // the chunk-fold Q chain's FP64 state
   void power_setup(const Prepared& pp, int tpr_A, int tpr_Q);
