@@ -29,7 +29,7 @@ void Common::init() {
   HPRQP_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
   d_scal = mem.alloc<double>(kNumSlots);
   HPRQP_CUDA(cudaMemset(d_scal, 0, sizeof(double) * kNumSlots));
-  HPRQP_CUDA(cudaMallocHost(&h_scal, sizeof(double) * kNumSlots));
+  h_scal = (double*)pinned_take(sizeof(double) * kNumSlots);
   rws.partials = mem.alloc<double>((int64_t)kReduceGridLimit * 16);
   rws.counter = mem.alloc<unsigned>(4);
   HPRQP_CUDA(cudaMemset(rws.counter, 0, sizeof(unsigned) * 4));
@@ -67,7 +67,7 @@ void Common::init() {
 
 Common::~Common() {
   const double t0 = wall_s();
-  if (h_scal) cudaFreeHost(h_scal);
+  if (h_scal) pinned_give(h_scal, sizeof(double) * kNumSlots);
   const double t1 = wall_s();
   if (cublas) cublasDestroy(cublas);
   if (stream) cudaStreamDestroy(stream);

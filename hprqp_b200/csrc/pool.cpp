@@ -84,6 +84,32 @@ void pool_free(std::vector<void*>& blocks, int dev) {
   if (dev >= 0 && dev != cur && cur >= 0) cudaSetDevice(cur);
 }
 
+namespace {
+std::mutex g_pin_mu;
+std::vector<std::pair<size_t, void*>> g_pinned;  // free pinned buffers by size
+}  // namespace
+
+void* pinned_take(size_t bytes) {
+  {
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    for (size_t i = 0; i < g_pinned.size(); ++i)
+      if (g_pinned[i].first == bytes) {
+        void* p = g_pinned[i].second;
+        g_pinned.erase(g_pinned.begin() + (long)i);
+        return p;
+      }
+  }
+  void* p = nullptr;
+  HPRQP_CUDA(cudaMallocHost(&p, bytes));
+  return p;
+}
+
+void pinned_give(void* p, size_t bytes) {
+  if (!p) return;
+  std::lock_guard<std::mutex> lk(g_pin_mu);
+  g_pinned.emplace_back(bytes, p);
+}
+
 void* PoolBlocks::get(size_t bytes) {
   if (dev < 0) HPRQP_CUDA(cudaGetDevice(&dev));
   void* p = pool_alloc(bytes);

@@ -25,6 +25,12 @@ void* pool_alloc(size_t bytes);
 // kernel of ours may still use them), never throws; clears the list.
 void pool_free(std::vector<void*>& blocks, int dev);
 
+// Pinned host buffers, kept for the process once allocated: a handle's
+// scalar mirror is taken from this list and given back at destroy, since
+// cudaFreeHost synchronises the device and measured up to a second here.
+void* pinned_take(size_t bytes);
+void pinned_give(void* p, size_t bytes);
+
 // Owner of a list of pool blocks of one device, freed together.
 struct PoolBlocks {
   std::vector<void*> blocks;
