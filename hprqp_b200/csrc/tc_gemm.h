@@ -6,10 +6,8 @@
 
 namespace hprqp {
 
-// C = alpha * A * B + beta * C, N x N column-major FP32, on `st`.
-void gemm_3xtf32(int N, float alpha, const float* A, const float* B, float beta, float* C, cudaStream_t st);
-
-// The pipelined form: operands pre-split into TF32 hi/lo images in `ws`
+// C = alpha * A * B + beta * C, N x N column-major FP32, on `st`: the
+// operands are pre-split into TF32 hi/lo images in `ws`
 // (gemm_3xtf32_ws_floats(N) floats, caller-owned), then bulk-copied tiles.
 int64_t gemm_3xtf32_ws_floats(int N);
 void gemm_3xtf32_ws(int N, float alpha, const float* A, const float* B, float beta, float* C, float* ws,
