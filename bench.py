@@ -291,9 +291,16 @@ def run_ours(args):
     roof_power = None
     if rp.power_bytes > 0 and head["power_s"] > 0:
         ach_p = rp.power_bytes / head["power_s"] / 1e9
+        steps = max(rp.power_iter_A + rp.power_iter_Q, 1)
         roof_power = {"bound": "hbm", "achieved": round(ach_p, 1), "peak": peak, "unit": "GB/s",
-                      "frac": round(ach_p / peak, 4), "steps_A": rp.power_iter_A, "steps_Q": rp.power_iter_Q,
-                      "algorithmic_bytes": rp.power_bytes, "seconds": head["power_s"],
+                      "frac": round(ach_p / peak, 4),
+                      "kernel": "power steps: k_row_partials over G = A'A (A A' chain) and Q (Q chain), two streams",
+                      "traffic": ncu_traffic("power:gram step"),
+                      "traffic_note": "DRAM bytes of one Gram step launch (ncu, caches flushed); the algorithmic "
+                                      "bytes per step are algorithmic_bytes / (steps_A + steps_Q) on average",
+                      "steps_A": rp.power_iter_A, "steps_Q": rp.power_iter_Q,
+                      "algorithmic_bytes": rp.power_bytes, "algorithmic_bytes_per_step": rp.power_bytes / steps,
+                      "seconds": head["power_s"], "peak_source": peak_kind,
                       "share_of_solve": round(head["power_s"] / head["value"], 3) if head["value"] else None}
     # end to end through the public API from host buffers (load -> solve -> x,y,z,w on the host)
     e2e_t, h2d, d2h, setup, parts = [], 0, 0, 0.0, []
@@ -342,7 +349,12 @@ def run_ours(args):
                        "iters": fp64["iters"], "power_method_s": fp64["power_s"],
                        "iters_per_s": fp64["iters"] / loop_s},
         "speedup_vs_plain_fp64": fp64["value"] / head["value"] if head["value"] else None,
-        "roofline": roof, "roofline_iteration": roof_iter, "roofline_power_method": roof_power, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
+        # the dominant kernel by share of the solve: the power steps when they take more of it than
+        # the busiest pass (they do on the grid), else that pass
+        "roofline": (roof_power if roof_power and roof and roof_power["share_of_solve"] is not None
+                     and roof_power["share_of_solve"] > roof["share_of_iteration"] * (1 - roof_power["share_of_solve"])
+                     else roof),
+        "roofline_pass": roof, "roofline_iteration": roof_iter, "roofline_power_method": roof_power, "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks,
         "gpu_launches": head["launches"],
     }
     if rank == 0:
