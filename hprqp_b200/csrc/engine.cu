@@ -948,7 +948,8 @@ double Engine<V>::power_step_bytes(int which) const {
   if (which == 0) return m > 0 ? csr(AT) + csr(A) + 2.0 * n * v + 3.0 * m * v : 0.0;
   if (is_qap) return 0.0;
   if (is_lasso) return csr(L) + csr(LT) + 2.0 * L.rows * v + 3.0 * n * v;
-  return csr(Q) + 2.0 * n * v;
+  // the chunk-fold Q chain reads and writes an FP64 state
+  return csr(Q) + 2.0 * n * (cm.pow_chunk_fold ? 8.0 : v);
 }
 
 // Name, algorithmic HBM bytes (plain iteration) and schedule of pass k.
