@@ -121,3 +121,40 @@ def test_chunk_fold_matches_per_step_fold(precision, rtol):
             (k, it1, it0, iq1, iq0)
         assert abs(lam1 - lam0) <= rtol * max(abs(lam0), 1e-300), (k, lam1, lam0)
         assert abs(lq1 - lq0) <= rtol * max(abs(lq0), 1e-300), (k, lq1, lq0)
+
+
+def _huge_lambda_qp():
+    """A QP whose Q has lambda_max ~ 4e11 with scaling off: an unnormalised
+    chain leaves FP64 range within a 32-step chunk (4e11^32 > 1e308)."""
+    import numpy as np
+    import scipy.sparse as sp
+    from hprqp_b200 import build_from_QAbc
+    n, m = 3000, 500
+    rng = np.random.default_rng(5)
+    T = sp.diags([2.0 * np.ones(n), -np.ones(n - 1), -np.ones(n - 1)], [0, 1, -1])
+    Q = (1e11 * T).tocsc()
+    A = sp.random(m, n, density=0.002, random_state=6, format="csc")
+    return build_from_QAbc(Q, rng.standard_normal(n), A, -np.ones(m), np.ones(m), -np.ones(n), np.ones(n),
+                           verbose=False)
+
+
+def test_chunk_fold_falls_back_when_a_state_leaves_fp64_range():
+    code = ("import json; from hprqp_b200 import HPRQP_parameters, Solver; "
+            "from tests.test_gpu_power import _huge_lambda_qp\n"
+            "s = Solver(0).load(_huge_lambda_qp())\n"
+            "r = s.solve(HPRQP_parameters(verbose=False, max_iter=0, use_Ruiz_scaling=False, "
+            "use_Pock_Chambolle_scaling=False))\n"
+            "s.close()\n"
+            "print(json.dumps([r.lambda_max_Q, r.power_iter_Q, r.lambda_max_A, r.power_iter_A]))")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = {}
+    for flag in ("1", "0"):
+        env = dict(os.environ, HPRQP_POWER_CHUNK_FOLD=flag)
+        r = subprocess.run([sys.executable, "-c", code], cwd=root, env=env, capture_output=True, text=True,
+                           timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[flag] = json.loads(r.stdout.strip().splitlines()[-1])
+    lq1, iq1, la1, ia1 = out["1"]
+    lq0, iq0, la0, ia0 = out["0"]
+    assert lq0 > 1e11 and abs(lq1 - lq0) <= 1e-10 * lq0 and iq1 == iq0, (out["1"], out["0"])
+    assert abs(la1 - la0) <= 1e-10 * abs(la0) and ia1 == ia0
