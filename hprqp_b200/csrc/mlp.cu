@@ -9,11 +9,10 @@
 // Layout: every matrix is row-major with leading dimensions padded to
 // multiples of 64 (zero padding stays zero: padded inputs are zero, padded
 // weight rows/columns start at zero and receive zero gradient).  Products
-// run on the tensor cores through WMMA 16x16x16 BF16 fragments with FP32
-// accumulators; one warp owns a 32x32 output tile, a CTA of 4 warps 64x64.
+// run on the tcgen05 tensor cores (kind::f16, BF16 operands, FP32
+// accumulators in TMEM), one 128 x 128 output tile per CTA.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
-#include <mma.h>
 
 #include <cmath>
 #include <cstring>
@@ -25,60 +24,146 @@
 #include "../../include/hprqp.h"
 #include "../../include/hprqp_mlp.h"
 #include "common.cuh"
+#include "tcgen05.cuh"
 
 namespace hprqp {
 namespace mlp {
 
 using bf16 = __nv_bfloat16;
-using namespace nvcuda;
 
 constexpr int kTile = 64;
 inline int64_t pad64(int64_t v) { return (v + 63) / 64 * 64; }
 
-// C[M x N] (+)= opA(A) opB(B), fp32 out.  TA: A is stored K x M (row-major)
-// i.e. used transposed; TB: B is stored N x K (row-major) and used transposed.
-// All of M, N, K are multiples of 64; lda/ldb/ldc are the row strides.
+// C[M x N] = opA(A) opB(B), FP32 out, on the tcgen05 tensor cores
+// (kind::f16 with BF16 operands, FP32 accumulator in TMEM).  TA: A is
+// stored K x M (row-major), i.e. used transposed; TB: B is stored N x K
+// (row-major) and used transposed.  M, N, K are multiples of 64; lda, ldb,
+// ldc are row strides (multiples of 64).  One CTA of 128 threads computes a
+// 128 x 128 tile of C: per 64-wide K chunk the threads stage both operands
+// in the canonical K-major no-swizzle layout (8-row x 16-byte core
+// matrices: 8 BF16 of one row per 16 bytes; K-adjacent core matrices 2 KiB
+// apart, row-adjacent ones 128 bytes), one thread issues the chunk's four
+// MMAs (M = N = 128, K = 16) and commits them to an mbarrier, and the
+// epilogue reads the accumulator rows from TMEM (warp w: lanes 32w..).
+// Rows and columns of the tile beyond M or N are staged as zeros and not
+// stored.  Every mbarrier wait is bounded; on a timeout the CTA raises
+// g_mlp_tc_err, frees its TMEM and returns.
+__device__ int g_mlp_tc_err = 0;
+constexpr int kTcK = 64;                          // K elements per staged chunk
+constexpr int kTcOpBytes = tc::kTile * kTcK * 2;  // one operand chunk: 16 KiB
+constexpr int kTcSmem = 2 * kTcOpBytes + 1024;
+// kind::f16: D = F32, A = B = BF16 (the same type on both sides), K-major, M = N = 128
+constexpr uint32_t kIdescBf16 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(tc::kTile >> 3) << 17) |
+                                ((uint32_t)(tc::kTile >> 4) << 24);
+
+__device__ __forceinline__ uint32_t kmaj16_off(int r, int k) {  // element (r, k) of a 128 x 64 chunk
+  return (uint32_t)((k >> 3) * tc::kLbo + (r >> 3) * tc::kSbo + (r & 7) * 16 + (k & 7) * 2);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t dtm, uint64_t ad, uint64_t bd, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(dtm),
+      "l"(ad), "l"(bd), "r"(kIdescBf16), "r"(accumulate));
+}
+
+// 8 consecutive K elements of row `r` of an operand: contiguous (one 16-byte
+// load) when the operand is stored K-contiguous, else gathered with stride ld
+__device__ __forceinline__ uint4 load8(const bf16* base, bool kcontig, int64_t ld) {
+  if (kcontig) return *reinterpret_cast<const uint4*>(base);
+  uint4 v;
+  uint16_t* h = reinterpret_cast<uint16_t*>(&v);
+#pragma unroll
+  for (int q = 0; q < 8; ++q) h[q] = *reinterpret_cast<const uint16_t*>(base + q * ld);
+  return v;
+}
+
 template <bool TA, bool TB>
-__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const bf16* __restrict__ A, int lda,
-                                              const bf16* __restrict__ B, int ldb, float* __restrict__ C, int ldc,
-                                              bool accumulate) {
-  using LA = typename std::conditional<TA, wmma::col_major, wmma::row_major>::type;
-  using LB = typename std::conditional<TB, wmma::col_major, wmma::row_major>::type;
-  const int warp = threadIdx.x >> 5;
-  const int row0 = blockIdx.y * kTile + (warp >> 1) * 32;
-  const int col0 = blockIdx.x * kTile + (warp & 1) * 32;
-  if (row0 >= M || col0 >= N) return;
-  wmma::fragment<wmma::accumulator, 16, 16, 16, float> acc[2][2];
-#pragma unroll
-  for (int i = 0; i < 2; ++i)
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      if (accumulate) wmma::load_matrix_sync(acc[i][j], C + (size_t)(row0 + 16 * i) * ldc + col0 + 16 * j, ldc, wmma::mem_row_major);
-      else wmma::fill_fragment(acc[i][j], 0.0f);
-    }
-  for (int k = 0; k < K; k += 16) {
-    wmma::fragment<wmma::matrix_a, 16, 16, 16, bf16, LA> a[2];
-    wmma::fragment<wmma::matrix_b, 16, 16, 16, bf16, LB> b[2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const bf16* pa = TA ? A + (size_t)k * lda + row0 + 16 * i : A + (size_t)(row0 + 16 * i) * lda + k;
-      wmma::load_matrix_sync(a[i], pa, lda);
-    }
-#pragma unroll
-    for (int j = 0; j < 2; ++j) {
-      const bf16* pb = TB ? B + (size_t)(col0 + 16 * j) * ldb + k : B + (size_t)k * ldb + col0 + 16 * j;
-      wmma::load_matrix_sync(b[j], pb, ldb);
-    }
-#pragma unroll
-    for (int i = 0; i < 2; ++i)
-#pragma unroll
-      for (int j = 0; j < 2; ++j) wmma::mma_sync(acc[i][j], a[i], b[j], acc[i][j]);
+__global__ void __launch_bounds__(tc::kThreads) k_gemm(int M, int N, int K, const bf16* __restrict__ A, int lda,
+                                                       const bf16* __restrict__ B, int ldb, float* __restrict__ C,
+                                                       int ldc) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ uint32_t tmem_base;
+  __shared__ int s_fail;
+  unsigned char* sm = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char *sA = sm, *sB = sm + kTcOpBytes;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int m0 = blockIdx.y * tc::kTile, n0 = blockIdx.x * tc::kTile;
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc::smem_u32(&tmem_base)),
+                 "r"(128u));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(tc::smem_u32(&bar)), "r"(1u));
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_fail = 0;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t acc = tmem_base;
+  uint32_t parity = 0;
+  for (int k0 = 0; k0 < K; k0 += kTcK) {
+    // 128 rows x 8 groups of 8 K elements per operand: 8 pairs per thread
+    for (int e = tid; e < tc::kTile * (kTcK / 8); e += tc::kThreads) {
+      const int r = e & (tc::kTile - 1), g = e >> 7;
+      const int k = k0 + 8 * g;
+      const int m = m0 + r, n = n0 + r;
+      const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+      // opA(m, k): TA ? A[k][m] : A[m][k];  opB(k, n) as the N x K operand: TB ? B[n][k] : B[k][n]
+      const uint4 av = m < M ? (TA ? load8(A + (int64_t)k * lda + m, false, lda) : load8(A + (int64_t)m * lda + k, true, 1))
+                             : z;
+      const uint4 bv = n < N ? (TB ? load8(B + (int64_t)n * ldb + k, true, 1) : load8(B + (int64_t)k * ldb + n, false, ldb))
+                             : z;
+      *reinterpret_cast<uint4*>(sA + kmaj16_off(r, 8 * g)) = av;
+      *reinterpret_cast<uint4*>(sB + kmaj16_off(r, 8 * g)) = bv;
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
-  for (int i = 0; i < 2; ++i)
+      for (int s = 0; s < kTcK / 16; ++s) {
+        const uint32_t o = (uint32_t)s * 2 * tc::kLbo;  // K = 16 per MMA: two core matrices along K
+        mma_bf16(acc, tc::smem_desc(tc::smem_u32(sA) + o), tc::smem_desc(tc::smem_u32(sB) + o),
+                 (k0 == 0 && s == 0) ? 0u : 1u);
+      }
+      tc::mma_commit(&bar);
+    }
+    if (!tc::mbar_wait(&bar, parity)) s_fail = 1;
+    parity ^= 1u;
+    __syncthreads();
+    if (s_fail) break;
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (!s_fail) {
+    const int row = warp * 32 + (tid & 31);
+    const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+    for (int c0 = 0; c0 < tc::kTile; c0 += 32) {
+      uint32_t v[32];
+      tc::tmem_ld32(acc + lane_base + (uint32_t)c0, v);
+      const int m = m0 + row;
+      if (m < M) {
 #pragma unroll
-    for (int j = 0; j < 2; ++j)
-      wmma::store_matrix_sync(C + (size_t)(row0 + 16 * i) * ldc + col0 + 16 * j, acc[i][j], ldc, wmma::mem_row_major);
+        for (int q = 0; q < 32; ++q) {
+          const int n = n0 + c0 + q;
+          if (n < N) C[(int64_t)m * ldc + n] = __uint_as_float(v[q]);
+        }
+      }
+    }
+  } else if (tid == 0) {
+    atomicExch(&g_mlp_tc_err, 1);
+    tc::mbar_wait(&bar, parity ^ 1u);  // a bounded chance for MMAs in flight to drain
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(acc), "r"(128u));
+  }
 }
 
 // Z = Z + bias (per column); relu -> H (bf16); keeps Z for the ReLU mask.
@@ -177,13 +262,24 @@ struct Net {
   }
 };
 
+// C = opA(A) opB(B) (the callers never accumulate into C)
 static void gemm(Net& N, bool TA, bool TB, int M, int Ncols, int K, const bf16* A, int lda, const bf16* B, int ldb,
                  float* C, int ldc, bool acc) {
-  dim3 grid(Ncols / kTile, M / kTile);
-  if (!TA && TB) k_gemm<false, true><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
-  else if (!TA && !TB) k_gemm<false, false><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
-  else if (TA && !TB) k_gemm<true, false><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
-  else k_gemm<true, true><<<grid, 128, 0, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc, acc);
+  if (acc) throw Error(HPRQP_E_ARG, "mlp gemm: accumulation into C is not supported");
+  static bool ready[64][4] = {};
+  int dev = 0;
+  HPRQP_CUDA(cudaGetDevice(&dev));
+  const int v = (TA ? 2 : 0) | (TB ? 1 : 0);
+  if (dev < 64 && !ready[dev][v]) {
+    auto f = !TA && TB ? k_gemm<false, true> : !TA ? k_gemm<false, false> : !TB ? k_gemm<true, false> : k_gemm<true, true>;
+    HPRQP_CUDA(cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem));
+    ready[dev][v] = true;
+  }
+  const dim3 grid((Ncols + tc::kTile - 1) / tc::kTile, (M + tc::kTile - 1) / tc::kTile);
+  if (!TA && TB) k_gemm<false, true><<<grid, tc::kThreads, kTcSmem, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc);
+  else if (!TA && !TB) k_gemm<false, false><<<grid, tc::kThreads, kTcSmem, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc);
+  else if (TA && !TB) k_gemm<true, false><<<grid, tc::kThreads, kTcSmem, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc);
+  else k_gemm<true, true><<<grid, tc::kThreads, kTcSmem, N.st>>>(M, Ncols, K, A, lda, B, ldb, C, ldc);
   HPRQP_LAUNCH_CHECK();
 }
 
