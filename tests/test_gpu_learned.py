@@ -59,6 +59,27 @@ def test_mlp_gradients_match_numpy_oracle():
     net.close()
 
 
+def test_mlp_gradients_match_numpy_oracle_multi_tile():
+    """Shapes that take several 64-wide K chunks and several 128 x 128
+    output tiles (with partial ones) in every product of the network."""
+    rng = np.random.default_rng(4)
+    n_in, width, n_out, R = 300, 256, 130, 100
+    net = learned.MLP(n_in, n_out, width=width, batch=128, seed=5)
+    p = net.get_params()
+    p[:] = bf16(p)
+    net.set_params(p)
+    X = bf16(rng.standard_normal((R, n_in))).astype(np.float32)
+    T = rng.standard_normal((R, n_out)).astype(np.float32)
+    loss, g = net.gradients(X, T)
+    ref_loss, ref = numpy_grads(*[a.astype(np.float64) for a in net.unpack(p)], X.astype(np.float64),
+                                T.astype(np.float64))
+    assert abs(loss - ref_loss) <= 2e-3 * ref_loss
+    for got, want in zip(net.unpack(g), ref):
+        err = np.linalg.norm(got - want) / max(np.linalg.norm(want), 1e-12)
+        assert err < 3e-2, err
+    net.close()
+
+
 def test_mlp_training_reduces_loss():
     rng = np.random.default_rng(1)
     X = rng.standard_normal((512, 64)).astype(np.float32)
