@@ -171,23 +171,23 @@ template <typename V>
 struct EpiRestartN {
   V *x, *w, *ATy, *ATy_bar, *Qw;
   const V *x_bar, *w_bar, *Qw_bar;
-  double *last_x, *last_w, *last_ATy, *last_Qw;
+  V *last_x, *last_w, *last_ATy, *last_Qw;
   bool has_m, noC;
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
     const V xb = x_bar[i], wb = w_bar[i];
     x[i] = xb;
     w[i] = wb;
-    last_x[i] = (double)xb;
-    last_w[i] = (double)wb;
+    last_x[i] = xb;
+    last_w[i] = wb;
     if (has_m) {
       ATy_bar[i] = (V)acc;
-      last_ATy[i] = (double)(V)acc;
+      last_ATy[i] = (V)acc;
       ATy[i] = (V)acc;
     }
     if (noC) {
       Qw[i] = Qw_bar[i];
-      last_Qw[i] = (double)Qw_bar[i];
+      last_Qw[i] = Qw_bar[i];
     }
   }
 };
@@ -718,8 +718,8 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   for (V** p : nv) *p = mem.alloc<V>(n);
   V** mv[] = {&y, &y_bar, &dy, &s, &Ax};
   for (V** p : mv) *p = mem.alloc<V>(m);
-  for (double** p : {&last_x, &last_w, &last_ATy, &last_Qw}) *p = mem.alloc<double>(n);
-  last_y = mem.alloc<double>(m);
+  for (V** p : {&last_x, &last_w, &last_ATy, &last_Qw}) *p = mem.alloc<V>(n);
+  last_y = mem.alloc<V>(m);
   stage_n = mem.alloc<double>(n);
   stage_m = mem.alloc<double>(m);
   pz = mem.alloc<V>(mx);
@@ -774,8 +774,8 @@ void Engine<V>::reset_state() {
   V* mv[] = {y, y_bar, dy, s, Ax};
   for (V* p : mv)
     if (m) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(V) * m, cm.stream));
-  for (double* p : {last_x, last_w, last_ATy, last_Qw}) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(double) * n, cm.stream));
-  if (m) HPRQP_CUDA(cudaMemsetAsync(last_y, 0, sizeof(double) * m, cm.stream));
+  for (V* p : {last_x, last_w, last_ATy, last_Qw}) HPRQP_CUDA(cudaMemsetAsync(p, 0, sizeof(V) * n, cm.stream));
+  if (m) HPRQP_CUDA(cudaMemsetAsync(last_y, 0, sizeof(V) * m, cm.stream));
 }
 
 // ---------------------------------------------------------------------------
@@ -852,7 +852,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
     spmv(L, w, ltemp);
     mark();
     HPRQP_BOOL(full, F, {
-      EpiLasso<V, F> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, c, last_x, last_w, sigma, lasso_lam, f1s, f2s, h1, h2};
+      EpiLasso<V, F, V> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, c, last_x, last_w, sigma, lasso_lam, f1s, f2s, h1, h2};
       mat_rows(LT, ltemp, e);
     })
     mark();
@@ -860,7 +860,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
   }
   if (path == PATH_QP) {
     HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
-      EpiZxw1<V, F, D> e{Qw, x, x_hat, w_bar, dx, x_bar, z_bar, ATy, c, l, u, w, fact1, fact2, last_x,
+      EpiZxw1<V, F, D, V> e{Qw, x, x_hat, w_bar, dx, x_bar, z_bar, ATy, c, l, u, w, fact1, fact2, last_x,
                          sigma, f1s, f2s, h1, h2};
       if (is_qap) {
         qap_apply(w, Qw);
@@ -880,14 +880,14 @@ void Engine<V>::step(bool full, double h1, double h2) {
       }
       mark();
       HPRQP_BOOL(full, F, {
-        EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
+        EpiY<V, F, true, V> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
         mat_rows(A, tempv, ey);
       })
       mark();
     }
     const double fs = sigma / (1.0 + sigma * lamQ);
     HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
-      EpiW2<V, F, D> e{w, ATy, w_bar, dw, ATdy, ATy_bar, fact, last_w, last_ATy, fs, h1, h2};
+      EpiW2<V, F, D, V> e{w, ATy, w_bar, dw, ATdy, ATy_bar, fact, last_w, last_ATy, fs, h1, h2};
       if (m > 0) mat_rows(AT, y_bar, e);
       else rows<V>(cm, 1, n, ZeroSrc{}, e);
     }))
@@ -896,14 +896,14 @@ void Engine<V>::step(bool full, double h1, double h2) {
   }
   if (path == PATH_NOC) {
     HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
-      EpiZxwNoC<V, F, D> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, Qw, c, l, u, fact1, fact2, last_x, last_w,
+      EpiZxwNoC<V, F, D, V> e{x, x_hat, w_bar, w, dx, x_bar, z_bar, dw, Qw, c, l, u, fact1, fact2, last_x, last_w,
                            sigma, f1s, f2s, h1, h2};
       if (m > 0) mat_rows(AT, y, e);
       else rows<V>(cm, 1, n, ZeroSrc{}, e);
     }))
     mark();
     HPRQP_BOOL(full, F, {
-      EpiTempvNoC<V, F> e{Qw, tempv, Qw_bar, x_hat, last_Qw, sigma, h1, h2};
+      EpiTempvNoC<V, F, V> e{Qw, tempv, Qw_bar, x_hat, last_Qw, sigma, h1, h2};
       if (is_qap) {
         qap_apply(w_bar, Qw_bar);
         rows<V>(cm, 1, n, VecSrc<V>{Qw_bar}, e);
@@ -914,7 +914,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
     mark();
     if (m > 0) {
       HPRQP_BOOL(full, F, {
-        EpiY<V, F, true> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
+        EpiY<V, F, true, V> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
         mat_rows(A, tempv, ey);
       })
       mark();
@@ -923,14 +923,14 @@ void Engine<V>::step(bool full, double h1, double h2) {
   }
   // PATH_LP
   HPRQP_BOOL(full, F, {
-    EpiZxLP<V, F> e{x, x_hat, dx, x_bar, z_bar, c, l, u, last_x, sigma, h1, h2};
+    EpiZxLP<V, F, V> e{x, x_hat, dx, x_bar, z_bar, c, l, u, last_x, sigma, h1, h2};
     if (m > 0) mat_rows(AT, y, e);
     else rows<V>(cm, 1, n, ZeroSrc{}, e);
   })
   mark();
   if (m > 0) {
     HPRQP_BOOL(full, F, {
-      EpiY<V, F, false> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
+      EpiY<V, F, false, V> ey{y, y_bar, s, dy, AL, AU, last_y, fy1, fy2, h1, h2};
       mat_rows(A, x_hat, ey);
     })
     mark();
@@ -954,11 +954,11 @@ double Engine<V>::power_step_bytes(int which) const {
 
 // Name, algorithmic HBM bytes (plain iteration) and schedule of pass k.
 // CSR stream = nnz (sizeof(V) + 4) + 4 (rows + 1); every distinct vector is
-// counted once per pass at its storage size (FP64 anchors stay 8 bytes);
+// counted once per pass at its storage size (the anchors included);
 // the gathered input vector is counted once.
 template <typename V>
 void Engine<V>::pass_info(int k, const char** name, double* bytes, int* tpr) const {
-  const double v = sizeof(V), d = 8.0;
+  const double v = sizeof(V), d = sizeof(V);  // d: the Halpern anchors (storage type too)
   auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
   auto sched = [](const DCsr<V>& M) { return M.ell ? -1 : M.sell ? 0 : M.tpr; };  // 0 = SELL-32, -1 = ELL
   const double N = (double)n, M_ = (double)m;
@@ -1023,17 +1023,17 @@ void Engine<V>::sigma_stats_launch() {
   {
     V *dx_ = dx, *dw_ = dw, *ATdy_ = ATdy;
     const V *xb = x_bar, *wb = w_bar, *atyb = ATy_bar;
-    const double *lx = last_x, *lw = last_w, *laty = last_ATy;
+    const V *lx = last_x, *lw = last_w, *laty = last_ATy;
     const bool hm = m > 0;
     elem(cm, n, [=] __device__(int i) {
-      dx_[i] = (V)((double)xb[i] - lx[i]);
-      dw_[i] = (V)((double)wb[i] - lw[i]);
-      if (hm) ATdy_[i] = (V)((double)atyb[i] - laty[i]);
+      dx_[i] = (V)((double)xb[i] - (double)lx[i]);
+      dw_[i] = (V)((double)wb[i] - (double)lw[i]);
+      if (hm) ATdy_[i] = (V)((double)atyb[i] - (double)laty[i]);
     });
     V* dy_ = dy;
     const V* yb = y_bar;
-    const double* ly = last_y;
-    elem(cm, m, [=] __device__(int i) { dy_[i] = (V)((double)yb[i] - ly[i]); });
+    const V* ly = last_y;
+    elem(cm, m, [=] __device__(int i) { dy_[i] = (V)((double)yb[i] - (double)ly[i]); });
   }
   apply_Q(dw, dQw);
   if (m > 0) apply_Q(ATdy, QATdy);
@@ -1075,10 +1075,10 @@ void Engine<V>::restart() {
   else rows<V>(cm, 1, n, ZeroSrc{}, e);
   V *y_ = y;
   const V* yb = y_bar;
-  double* ly = last_y;
+  V* ly = last_y;
   elem(cm, m, [=] __device__(int i) {
     y_[i] = yb[i];
-    ly[i] = (double)yb[i];
+    ly[i] = yb[i];
   });
 }
 
@@ -1088,36 +1088,36 @@ void Engine<V>::initial_points(const double* x0, const double* y0) {
   if (x0) {
     cm.to_dev(stage_n, x0, sizeof(double) * n);
     V *x_ = x, *xb = x_bar, *w_ = w, *wb = w_bar;
-    double *lx = last_x, *lw = last_w;
+    V *lx = last_x, *lw = last_w;
     const double* st = stage_n;
     const V* cn = col_norm;
     const double bs = b_scale;
     elem(cm, n, [=] __device__(int i) {
       const double v = st[i] * (double)cn[i] / bs;
       x_[i] = xb[i] = w_[i] = wb[i] = (V)v;
-      lx[i] = lw[i] = (double)(V)v;
+      lx[i] = lw[i] = (V)v;
     });
   }
   if (y0) {
     if (m > 0) {
       cm.to_dev(stage_m, y0, sizeof(double) * m);
       V *y_ = y, *yb = y_bar;
-      double* ly = last_y;
+      V* ly = last_y;
       const double* st = stage_m;
       const V* rn = row_norm;
       const double cs = c_scale;
       elem(cm, m, [=] __device__(int i) {
         const double v = st[i] * (double)rn[i] / cs;
         y_[i] = yb[i] = (V)v;
-        ly[i] = (double)(V)v;
+        ly[i] = (V)v;
       });
       spmv(AT, y_bar, ATy_bar);
       V* aty = ATy;
       const V* atyb = ATy_bar;
-      double* laty = last_ATy;
+      V* laty = last_ATy;
       elem(cm, n, [=] __device__(int i) {
         aty[i] = atyb[i];
-        laty[i] = (double)atyb[i];
+        laty[i] = atyb[i];
       });
     }
     apply_Q(x_bar, Qx);
@@ -1575,8 +1575,8 @@ void Engine<V>::import_state(const Engine<W>& o) {
   auto cp = [&](double* dst, const double* src, int64_t len) {
     if (len) HPRQP_CUDA(cudaMemcpyAsync(dst, src, sizeof(double) * len, cudaMemcpyDeviceToDevice, cm.stream));
   };
-  cp(last_x, o.last_x, n); cp(last_w, o.last_w, n); cp(last_ATy, o.last_ATy, n); cp(last_Qw, o.last_Qw, n);
-  cp(last_y, o.last_y, m);
+  cv(last_x, o.last_x, n); cv(last_w, o.last_w, n); cv(last_ATy, o.last_ATy, n); cv(last_Qw, o.last_Qw, n);
+  cv(last_y, o.last_y, m);
   lamA = o.lamA;
   lamQ = o.lamQ;
   lam_l1 = o.lam_l1;

@@ -130,7 +130,10 @@ class Engine {
   V *x, *x_hat, *x_bar, *dx, *w, *w_bar, *dw, *z_bar, *Qw, *Qw_bar, *ATy, *ATy_bar, *ATdy, *QATdy,
       *dQw, *Qx, *tempv, *c, *l, *u, *col_norm, *fact1, *fact2, *fact, *fact_M, *diag_Q;
   V *y, *y_bar, *dy, *s, *Ax, *AL, *AU, *row_norm;
-  double *last_x, *last_w, *last_ATy, *last_Qw, *last_y;
+  // Halpern anchors: every value they take is an iterate of this engine's
+  // storage type (restart and initial points copy V values), so V holds
+  // them exactly
+  V *last_x, *last_w, *last_ATy, *last_Qw, *last_y;
   V* ltemp = nullptr;                 // LASSO A_d w
   V* ltemp2 = nullptr;                // LASSO A_d z of the Q power chain
   double *stage_n, *stage_m;          // FP64 staging for host copies

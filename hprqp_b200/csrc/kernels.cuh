@@ -7,7 +7,8 @@
 // (src/kernels.jl:2115-2832) expression by expression; `fma` stands where
 // the reference writes `muladd`.  Epilogue arithmetic is FP64; `V` is the
 // storage type of vectors and matrix values (double, or float in the FP32
-// phase), Halpern anchors (last_*) are always FP64.
+// phase); the Halpern anchors (last_*) are stored as V in the engines
+// (every value they take is a V iterate) and as FP64 in the batch engines.
 //
 // Reductions (KKT residuals, M-norm, sigma statistics, power method) are
 // single-pass: per-CTA shuffle/shared reduction, per-CTA partials, and the
@@ -293,11 +294,11 @@ struct EpiStore {
 };
 
 // QP step 1: Qw = Q w fused with update_zxw1_cpu! (src/kernels.jl:2301-2397)
-template <typename V, bool Full, bool Diag>
+template <typename V, bool Full, bool Diag, typename AV = double>
 struct EpiZxw1 {
   V *Qw, *x, *x_hat, *w_bar, *dx, *x_bar, *z_bar;
   const V *ATy, *c, *l, *u, *w, *fact1, *fact2;
-  const double* last_x;
+  const AV* last_x;
   double sigma, f1s, f2s, h1, h2;
   __device__ __forceinline__ void prefetch(int i, int lv) const {
     pf_rows(i, lv, x, w, ATy, c, l, u, last_x);
@@ -312,7 +313,7 @@ struct EpiZxw1 {
     const double z_raw = x_i + sigma * tmp;
     const double xb = clampd(z_raw, l[i], u[i]);
     const double xh = 2.0 * xb - x_i;
-    const double xn = fma(h2, xh, h1 * last_x[i]);
+    const double xn = fma(h2, xh, h1 * (double)last_x[i]);
     const double wb = Diag ? fma((double)fact1[i], w_i, (double)fact2[i] * xh) : fma(f1s, w_i, f2s * xh);
     if (Full) {
       dx[i] = (V)(xb - x_i);
@@ -342,11 +343,11 @@ struct EpiTempv {
 // unified_update_y_noQ_cpu! (src/kernels.jl:2242-2298, 2582-2658, 2682-2743).
 // YbarAlways: the QP / noC loops write y_bar in partial steps too, the LP
 // loop only in full steps.
-template <typename V, bool Full, bool YbarAlways>
+template <typename V, bool Full, bool YbarAlways, typename AV = double>
 struct EpiY {
   V *y, *y_bar, *s, *dy;
   const V *AL, *AU;
-  const double* last_y;
+  const AV* last_y;
   double f1, f2, h1, h2;
   __device__ __forceinline__ void prefetch(int i, int lv) const { pf_rows(i, lv, (const V*)y, AL, AU, last_y); }
   template <typename A>
@@ -356,7 +357,7 @@ struct EpiY {
     const double s_proj = clampd(s_raw, AL[i], AU[i]);
     const double yb = f2 * (s_proj - s_raw);
     const double yh = 2.0 * yb - yi;
-    const double yn = fma(h2, yh, h1 * last_y[i]);
+    const double yn = fma(h2, yh, h1 * (double)last_y[i]);
     if (Full) {
       s[i] = (V)s_proj;
       dy[i] = (V)(yb - yi);
@@ -367,11 +368,11 @@ struct EpiY {
 };
 
 // QP step 4: A'y_bar fused with update_w2_cpu! (src/kernels.jl:2747-2832)
-template <typename V, bool Full, bool Diag>
+template <typename V, bool Full, bool Diag, typename AV = double>
 struct EpiW2 {
   V *w, *ATy, *w_bar, *dw, *ATdy, *ATy_bar;
   const V* fact;
-  const double *last_w, *last_ATy;
+  const AV *last_w, *last_ATy;
   double fs, h1, h2;
   __device__ __forceinline__ void prefetch(int i, int lv) const {
     pf_rows(i, lv, (const V*)w, (const V*)ATy, (const V*)w_bar, last_w, last_ATy);
@@ -383,8 +384,8 @@ struct EpiW2 {
     const double w_i = w[i], aty = ATy[i];
     const double f = Diag ? (double)fact[i] : fs;
     const double wbn = (double)w_bar[i] + f * (atyb - aty);
-    const double wn = h1 * last_w[i] + h2 * (2.0 * wbn - w_i);
-    const double atyn = h1 * last_ATy[i] + h2 * (2.0 * atyb - aty);
+    const double wn = h1 * (double)last_w[i] + h2 * (2.0 * wbn - w_i);
+    const double atyn = h1 * (double)last_ATy[i] + h2 * (2.0 * atyb - aty);
     w[i] = (V)wn;
     ATy[i] = (V)atyn;
     if (Full) {
@@ -397,11 +398,11 @@ struct EpiW2 {
 };
 
 // QP-noC step 1: A'y fused with unified_update_zxw_cpu! (kernels.jl:2117-2223)
-template <typename V, bool Full, bool Diag>
+template <typename V, bool Full, bool Diag, typename AV = double>
 struct EpiZxwNoC {
   V *x, *x_hat, *w_bar, *w, *dx, *x_bar, *z_bar, *dw;
   const V *Qw, *c, *l, *u, *fact1, *fact2;
-  const double *last_x, *last_w;
+  const AV *last_x, *last_w;
   double sigma, f1s, f2s, h1, h2;
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
@@ -410,10 +411,10 @@ struct EpiZxwNoC {
     const double z_raw = x_i + sigma * tmp;
     const double xb = clampd(z_raw, l[i], u[i]);
     const double xh = 2.0 * xb - x_i;
-    const double xn = fma(h2, xh, h1 * last_x[i]);
+    const double xn = fma(h2, xh, h1 * (double)last_x[i]);
     const double wb = Diag ? fma((double)fact1[i], w_i, (double)fact2[i] * xh) : fma(f1s, w_i, f2s * xh);
     const double wh = 2.0 * wb - w_i;
-    const double wn = fma(h2, wh, h1 * last_w[i]);
+    const double wn = fma(h2, wh, h1 * (double)last_w[i]);
     if (Full) {
       dx[i] = (V)(xb - x_i);
       x_bar[i] = (V)xb;
@@ -428,28 +429,28 @@ struct EpiZxwNoC {
 };
 
 // QP-noC step 2: Q w_bar; Halpern-averaged Qw and tempv (kernels.jl:2226-2237)
-template <typename V, bool Full>
+template <typename V, bool Full, typename AV = double>
 struct EpiTempvNoC {
   V *Qw, *tempv, *Qw_bar;
   const V* x_hat;
-  const double* last_Qw;
+  const AV* last_Qw;
   double sigma, h1, h2;
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
     const double qwb = (double)acc, qw = Qw[i];
     const double qwh = 2.0 * qwb - qw;
-    Qw[i] = (V)fma(h2, qwh, h1 * last_Qw[i]);
+    Qw[i] = (V)fma(h2, qwh, h1 * (double)last_Qw[i]);
     tempv[i] = (V)((double)x_hat[i] + sigma * (qw - qwb));
     if (Full) Qw_bar[i] = (V)qwb;
   }
 };
 
 // LP step 1: A'y fused with unified_update_zx_cpu! (kernels.jl:2504-2578)
-template <typename V, bool Full>
+template <typename V, bool Full, typename AV = double>
 struct EpiZxLP {
   V *x, *x_hat, *dx, *x_bar, *z_bar;
   const V *c, *l, *u;
-  const double* last_x;
+  const AV* last_x;
   double sigma, h1, h2;
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
@@ -457,7 +458,7 @@ struct EpiZxLP {
     const double z_raw = x_i + sigma * ((double)acc - (double)c[i]);
     const double xb = clampd(z_raw, l[i], u[i]);
     const double xh = 2.0 * xb - x_i;
-    const double xn = fma(h2, xh, h1 * last_x[i]);
+    const double xn = fma(h2, xh, h1 * (double)last_x[i]);
     if (Full) {
       dx[i] = (V)(xb - x_i);
       x_bar[i] = (V)xb;
@@ -469,11 +470,11 @@ struct EpiZxLP {
 };
 
 // LASSO: A_d'(A_d w) fused with update_zxw_LASSO_cpu! (kernels.jl:2400-2496)
-template <typename V, bool Full>
+template <typename V, bool Full, typename AV = double>
 struct EpiLasso {
   V *x, *x_hat, *w_bar, *w, *dx, *x_bar, *z_bar, *dw;
   const V* c;
-  const double *last_x, *last_w;
+  const AV *last_x, *last_w;
   double sigma, lam, f1s, f2s, h1, h2;
   template <typename A>
   __device__ __forceinline__ void operator()(int i, A acc) const {
@@ -483,9 +484,9 @@ struct EpiLasso {
     const double shrink = fmax(fabs(z_raw) - lam * sigma, 0.0);
     const double xb = copysign(shrink, z_raw);
     const double xh = 2.0 * xb - x_i;
-    const double xn = fma(h2, xh, h1 * last_x[i]);
+    const double xn = fma(h2, xh, h1 * (double)last_x[i]);
     const double wb = fma(f1s, w_i, f2s * xh);
-    const double wn = fma(h2, 2.0 * wb - w_i, h1 * last_w[i]);
+    const double wn = fma(h2, 2.0 * wb - w_i, h1 * (double)last_w[i]);
     if (Full) {
       dx[i] = (V)(xb - x_i);
       x_bar[i] = (V)xb;
