@@ -1366,7 +1366,9 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   const bool cfQ = cm.pow_chunk_fold && cq.on && has_Q_sparse && !is_lasso && !is_qap;
   const int nblkA = cfA ? partials_grid(cm, G) : 0, nblkQ = cfQ ? partials_grid(cm, pQ) : 0;
   if ((cfA || cfQ) && !pow_cf_part) {
-    pow_cf_part = mem.alloc<double>((int64_t)2 * kPowChunk * kMaxReduceGrid * 3);
+    // one region per chain, each kPowChunk steps x (at most reduce_cap CTAs) x 3 sums
+    pow_cf_region = (int64_t)kPowChunk * std::max(cm.reduce_cap, 1) * 3;
+    pow_cf_part = mem.alloc<double>(2 * pow_cf_region);
     pow_cf_tot = mem.alloc<double>(2 * kPowChunk * 3);
   }
   // the unnormalised Q chain keeps an FP64 state: within a chunk it grows by
@@ -1392,7 +1394,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     d.K = kind == 0 ? 2 : 3;
     d.nblk = nblk;
     d.steps = kPowChunk;
-    d.partials = pow_cf_part + (size_t)kind * kPowChunk * kMaxReduceGrid * 3;
+    d.partials = pow_cf_part + (size_t)kind * pow_cf_region;
     d.totals = pow_cf_tot + kind * kPowChunk * 3;
     d.log = log;
     d.len = n;
@@ -1423,7 +1425,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
       const double* yc = (k & 1) ? gq1 : gq0;
       double* yn = (k & 1) ? gq0 : gq1;
       mat_partials<3>(cm, pQ, yc, EpiPowRaw<double>{yc, yn},
-                      pow_cf_part + (size_t)kPowChunk * kMaxReduceGrid * 3 + (size_t)k * nblkQ * 3);
+                      pow_cf_part + (size_t)pow_cf_region + (size_t)k * nblkQ * 3);
     } else if (c.which == 0 && use_gram) {  // u ping-pongs between gu0 and gu1
       const double* uc = (k & 1) ? gu1 : gu0;
       double* un = (k & 1) ? gu0 : gu1;

@@ -155,6 +155,7 @@ class Engine {
   int64_t pow_exec_launches[4] = {0, 0, 0, 0};
   int pow_exec_key = -1;
   double *pow_cf_part = nullptr, *pow_cf_tot = nullptr;  // chunk-fold partials and totals
+  int64_t pow_cf_region = 0;                              // doubles per chain in pow_cf_part
   double *gq0 = nullptr, *gq1 = nullptr;                  // the chunk-fold Q chain's FP64 state
   void power_setup(const Prepared& pp, int tpr_A, int tpr_Q);
   double *gu0 = nullptr, *gu1 = nullptr;  // the Gram chain's state u_k (FP64 in both engines)

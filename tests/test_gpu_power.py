@@ -158,3 +158,15 @@ def test_chunk_fold_falls_back_when_a_state_leaves_fp64_range():
     lq0, iq0, la0, ia0 = out["0"]
     assert lq0 > 1e11 and abs(lq1 - lq0) <= 1e-10 * lq0 and iq1 == iq0, (out["1"], out["0"])
     assert abs(la1 - la0) <= 1e-10 * abs(la0) and ia1 == ia0
+
+
+def test_chunk_fold_with_a_larger_reduction_grid():
+    """HPRQP_REDUCE_CAP above the default puts more CTAs, hence more per-CTA
+    sums, into every chunk-fold step: the same steps and lambda to rounding."""
+    big = _lambdas_with_env({"HPRQP_REDUCE_CAP": "4736"}, "fp64")
+    ref = _lambdas_with_env({}, "fp64")
+    for k in CASES:
+        lam1, it1, lq1, iq1 = big[k]
+        lam0, it0, lq0, iq0 = ref[k]
+        assert it1 == it0 and iq1 == iq0, (k, big[k], ref[k])
+        assert abs(lam1 - lam0) <= 1e-10 * abs(lam0) and abs(lq1 - lq0) <= 1e-10 * max(abs(lq0), 1e-300), k
