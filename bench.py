@@ -179,13 +179,14 @@ def run_reference(args):
         v, det = cpu_sample(model, iters if iters else args.cpu_sample_iters, threads, args.cpu_sample_iters)
         vals.append(v)
     value = statistics.mean(vals)
-    sample = (f"oracle power method in full + {args.cpu_sample_iters} HPR iterations of {WORKLOAD}, "
+    workload = WORKLOAD if args.grid == 700 else f"grid_qp_{args.grid}x{args.grid}"
+    sample = (f"oracle power method in full + {args.cpu_sample_iters} HPR iterations of {workload}, "
               f"extrapolated to {iters} iterations (oracle FP64 iteration count to 1e-6, "
               "tests/golden/grid_qp_oracle.json)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": value * 1e3, "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator)",
-            "config": {"workload": WORKLOAD, "n": model.n, "m": model.m, "precision": "fp64",
+            "config": {"workload": workload, "n": model.n, "m": model.m, "precision": "fp64",
                        "implementation": "reference CPU path restated in C++ (oracle/), OpenMP"},
             "cpu_baseline": {"value": value, "unit": "s", "cores": threads, "kind": "port", "sample": sample,
                              **det},
