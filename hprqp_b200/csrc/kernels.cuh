@@ -835,18 +835,21 @@ static __global__ void __launch_bounds__(kBlock) k_pow_chunk_fold(PowChunkChain 
 
 // The chunk's (lambda, err) recurrence (every CTA computes it from the
 // totals, CTA 0 writes the log) and the renormalisation of the last state.
-__device__ __forceinline__ double pow_chunk_recur(const PowChunkChain& c, bool write) {
+__device__ __forceinline__ bool pow_totals_ok(const double* t, int kind) {
+  return isfinite(t[0]) && isfinite(t[1]) && t[0] > 0.0 && t[1] > 0.0 &&
+         (kind == 0 || (isfinite(t[2]) && t[2] > 0.0));
+}
+
+// the chunk's (lambda, err) recurrence from its totals `tot` (steps x 3)
+__device__ __forceinline__ void pow_chunk_log(const PowChunkChain& c, const double* tot) {
   double s2 = 1.0;  // s_k^2 of the Gram chain (1 at the chunk start)
-  double scale = 1.0;
   for (int k = 0; k < c.steps; ++k) {
-    const double* t = c.totals + k * 3;
-    double lam, zz;
-    const bool ok = isfinite(t[0]) && isfinite(t[1]) && t[0] > 0.0 && t[1] > 0.0 &&
-                    (c.kind == 0 || (isfinite(t[2]) && t[2] > 0.0));
-    if (!ok) {
-      if (write) c.log[2 * k] = c.log[2 * k + 1] = nan("");
+    const double* t = tot + k * 3;
+    if (!pow_totals_ok(t, c.kind)) {
+      c.log[2 * k] = c.log[2 * k + 1] = nan("");
       continue;
     }
+    double lam, zz;
     if (c.kind == 0) {
       lam = s2 * t[1];
       zz = s2 * t[0];
@@ -855,23 +858,32 @@ __device__ __forceinline__ double pow_chunk_recur(const PowChunkChain& c, bool w
       lam = t[0] / t[1];
       zz = t[2] / t[1];
     }
-    if (write) {
-      c.log[2 * k] = lam;
-      c.log[2 * k + 1] = sqrt(fmax(zz - lam * lam, 0.0)) / (sqrt(zz) + lam);
-    }
-    if (k == c.steps - 1) scale = c.kind == 0 ? sqrt(s2) : 1.0 / sqrt(t[2]);
+    c.log[2 * k] = lam;
+    c.log[2 * k + 1] = sqrt(fmax(zz - lam * lam, 0.0)) / (sqrt(zz) + lam);
   }
-  return scale;
 }
 
+// CTA 0 writes the chunk's log (its totals staged in shared memory first,
+// so the recurrence does not wait on one load per step); every CTA
+// renormalises its slice of the last state by the factor that the last
+// step's totals give (Gram: 1 / sqrt(u_k . u_{k+1}), the s of the next
+// chunk's start; Q: 1 / ||y||), 1 when those totals are not usable.
 static __global__ void __launch_bounds__(kBlock) k_pow_chunk_finish(PowChunkChain c0, PowChunkChain c1) {
   pdl_enter();  // the fold must be complete
   const PowChunkChain& c = blockIdx.y == 0 ? c0 : c1;
-  if (c.steps == 0) return;
+  if (c.steps == 0 || c.steps > 32) return;
+  __shared__ double s_tot[32 * 3];
   __shared__ double s_scale;
+  if (blockIdx.x == 0)
+    for (int q = threadIdx.x; q < c.steps * 3; q += kBlock) s_tot[q] = c.totals[q];
+  __syncthreads();
   if (threadIdx.x == 0) {
-    s_scale = pow_chunk_recur(c, blockIdx.x == 0);
-    if (blockIdx.x == 0 && c.scale_out) *c.scale_out = s_scale;
+    if (blockIdx.x == 0) pow_chunk_log(c, s_tot);
+    const double* tl = c.totals + (c.steps - 1) * 3;
+    double sc = 1.0;
+    if (pow_totals_ok(tl, c.kind)) sc = c.kind == 0 ? sqrt(1.0 / tl[0]) : 1.0 / sqrt(tl[2]);
+    s_scale = sc;
+    if (blockIdx.x == 0 && c.scale_out) *c.scale_out = sc;
   }
   __syncthreads();
   const double sc = s_scale;
