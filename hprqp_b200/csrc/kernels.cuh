@@ -833,8 +833,8 @@ static __global__ void __launch_bounds__(kBlock) k_pow_chunk_fold(PowChunkChain 
     for (int q = 0; q < c.K; ++q) c.totals[k * 3 + q] = acc[q];
 }
 
-// The chunk's (lambda, err) recurrence (every CTA computes it from the
-// totals, CTA 0 writes the log) and the renormalisation of the last state.
+// A step's totals are usable when finite and positive (a state that left
+// FP64 range gives inf or 0).
 __device__ __forceinline__ bool pow_totals_ok(const double* t, int kind) {
   return isfinite(t[0]) && isfinite(t[1]) && t[0] > 0.0 && t[1] > 0.0 &&
          (kind == 0 || (isfinite(t[2]) && t[2] > 0.0));
