@@ -2,12 +2,18 @@
 // method on a caller-owned device CSR matrix, with no device allocation.
 //
 // Why it exists: some callers of this library cannot call cudaMalloc at the
-// point where they need the estimate — code running under a CUDA graph
-// capture that must not allocate, programs whose device memory belongs to
-// another framework's pool allocator, and real-time loops that forbid
-// allocation after start-up.  For them this entry point works entirely in
-// memory the caller already owns plus one fixed block of scratch that the
-// library reserves when it is loaded.
+// point where they need the estimate — programs whose device memory belongs
+// to another framework's pool allocator (a second allocator on the same GPU
+// would fragment or overcommit that pool), and real-time or long-running
+// loops that forbid allocation after start-up (an allocation there can
+// block on the driver or fail at an unpredictable moment).  For them this
+// entry point works entirely in memory the caller already owns plus one
+// fixed block of scratch that the library reserves when it is loaded.
+//
+// The call is synchronous: every 32 steps it reads the (lambda, err) log
+// back to the host, waiting on the caller's stream, and it returns after the
+// stream has finished its work.  The first call in each CUDA context does
+// the set-up below; make that first call before any stream capture.
 //
 // The scratch is the file-scope array g_noalloc_scratch below: the power
 // method's three work vectors (two m-vectors, one n-vector), the reduction
@@ -17,9 +23,12 @@
 // the process exits.  Problems with 2m + n > kNoAllocVecCap are rejected.
 //
 // Host code must not pass the array's name to a kernel: in host code it is
-// a host-side stand-in, not a device address.  The device address is
-// fetched once per device with cudaGetSymbolAddress (with that device
-// current) on the first call made on that device, and cached.
+// a host-side stand-in, not a device address.  The device address is looked
+// up with cudaGetSymbolAddress, with the device current, by the first call
+// made in each CUDA context (the primary context of a device, or a context
+// the caller made current), and cached under that context's unique id; a
+// new context (after cudaDeviceReset, say) gets a fresh look-up.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -27,7 +36,6 @@
 #include <string>
 
 #include "../../include/hprqp.h"
-#include "host_setup.h"
 #include "kernels.cuh"
 
 namespace hprqp {
@@ -49,8 +57,8 @@ static_assert(kOffPartials + (int64_t)kMaxReduceGrid * 16 <= kCtrl, "control blo
 static __device__ __align__(256) double g_noalloc_scratch[kCtrl + kNoAllocVecCap];
 
 std::mutex g_mu;                                   // serialises host-side use
-double* g_dev_ptr[kMaxDevices] = {nullptr};        // device address, per device
-double g_chunk_buf[4096];                          // host staging of the start vector
+double* g_dev_ptr[kMaxDevices] = {nullptr};        // device address, per device ...
+unsigned long long g_ctx_id[kMaxDevices] = {0};    // ... valid in this context only
 
 #define NA_CHECK(call)                                                                 \
   do {                                                                                 \
@@ -62,8 +70,11 @@ double g_chunk_buf[4096];                          // host staging of the start 
     }                                                                                  \
   } while (0)
 
-// Same launch geometry as the engine's power method, so results agree bit
-// for bit with hprqp_solve's lambda_max_A for the same matrix and schedule.
+// The products and the stopping test of the engine's power method (its
+// two-product form, one CTA fold per step), so lambda agrees with
+// hprqp_solve's lambda_max_A / eig_factor for the same matrix to rounding:
+// the engine folds the chains once per 32-step chunk or runs the A A' chain
+// on the Gram matrix A'A, which sums the same dot products in another order.
 template <int TPR>
 int power_steps(int m, int n, CsrSrc<double, double> At_z, CsrSrc<double, double> A_t, double* za, double* zb,
                 double* t, double* scal, double* log, ReduceWs ws, cudaStream_t st, int k) {
@@ -100,9 +111,13 @@ extern "C" int hprqp_power_lambda_noalloc(int64_t m, int64_t n, const int32_t* A
     set_global_error("hprqp_power_lambda_noalloc: invalid argument");
     return HPRQP_E_ARG;
   }
-  if (2 * m + n > kNoAllocVecCap) {
-    set_global_error("hprqp_power_lambda_noalloc: problem too large for the fixed scratch: needs 2m + n = " +
-                     std::to_string(2 * m + n) + " doubles, capacity is " + std::to_string(kNoAllocVecCap));
+  // m and n are each checked first, so 2m + n cannot overflow
+  if (m > kNoAllocVecCap || n > kNoAllocVecCap || 2 * m + n > kNoAllocVecCap) {
+    const std::string need = (m > kNoAllocVecCap || n > kNoAllocVecCap)
+                                  ? std::string("m = ") + std::to_string(m) + ", n = " + std::to_string(n)
+                                  : std::to_string(2 * m + n);
+    set_global_error("hprqp_power_lambda_noalloc: problem too large for the fixed scratch: needs 2m + n = " + need +
+                     " doubles, capacity is " + std::to_string(kNoAllocVecCap));
     return HPRQP_E_ARG;
   }
   int tpr = threads_per_row;
@@ -116,10 +131,39 @@ extern "C" int hprqp_power_lambda_noalloc(int64_t m, int64_t n, const int32_t* A
     set_global_error("hprqp_power_lambda_noalloc: device index out of range");
     return HPRQP_E_CUDA;
   }
-  if (!g_dev_ptr[dev]) {  // once per device, with that device current
+  // Set-up, once per context, with the device current: the array's device
+  // address.  The context's id (unique for the life of the process) tells
+  // whether a cached address still belongs to the current context.
+  unsigned long long ctx_id = 0;
+  {
+    static CUresult (*get_current)(CUcontext*) = nullptr;
+    static CUresult (*get_id)(CUcontext, unsigned long long*) = nullptr;
+    if (!get_current || !get_id) {
+      cudaDriverEntryPointQueryResult q1, q2;
+      NA_CHECK(cudaGetDriverEntryPoint("cuCtxGetCurrent", (void**)&get_current, cudaEnableDefault, &q1));
+      NA_CHECK(cudaGetDriverEntryPoint("cuCtxGetId", (void**)&get_id, cudaEnableDefault, &q2));
+      if (q1 != cudaDriverEntryPointSuccess || q2 != cudaDriverEntryPointSuccess || !get_current || !get_id) {
+        get_current = nullptr;
+        get_id = nullptr;
+        set_global_error("hprqp_power_lambda_noalloc: the driver lacks cuCtxGetCurrent / cuCtxGetId");
+        return HPRQP_E_CUDA;
+      }
+    }
+    CUcontext ctx = nullptr;
+    if (get_current(&ctx) == CUDA_SUCCESS && !ctx) {
+      NA_CHECK(cudaSetDevice(dev));  // no context yet: start the device's primary one
+      get_current(&ctx);
+    }
+    if (!ctx || get_id(ctx, &ctx_id) != CUDA_SUCCESS) {
+      set_global_error("hprqp_power_lambda_noalloc: no current CUDA context");
+      return HPRQP_E_CUDA;
+    }
+  }
+  if (!g_dev_ptr[dev] || g_ctx_id[dev] != ctx_id) {
     void* p = nullptr;
     NA_CHECK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     g_dev_ptr[dev] = (double*)p;
+    g_ctx_id[dev] = ctx_id;
   }
   cudaStream_t st = (cudaStream_t)stream;
   double* base = g_dev_ptr[dev];
@@ -132,13 +176,9 @@ extern "C" int hprqp_power_lambda_noalloc(int64_t m, int64_t n, const int32_t* A
   // The ticket and the scalar slots must start at zero; the rest of the
   // scratch keeps whatever the previous call left and is overwritten.
   NA_CHECK(cudaMemsetAsync(base, 0, sizeof(double) * kOffPartials, st));
-  StartVectorStream gen;  // same start vector as hprqp_solve's power method
-  for (int64_t off = 0; off < m; off += 4096) {
-    const int64_t cnt = std::min<int64_t>(4096, m - off);
-    gen.fill(g_chunk_buf, cnt);
-    NA_CHECK(cudaMemcpyAsync(za + off, g_chunk_buf, sizeof(double) * cnt, cudaMemcpyHostToDevice, st));
-    NA_CHECK(cudaStreamSynchronize(st));  // the staging buffer is reused
-  }
+  // the start vector of hprqp_solve's power method, generated in place
+  k_start_vector<double><<<(int)((m + kBlock - 1) / kBlock), kBlock, 0, st>>>(m, za);
+  NA_CHECK(cudaGetLastError());
   {
     const int grid = reduce_grid(m, 1);
     k_row_reduce<1, 1, 0u, double><<<grid, kBlock, 0, st>>>((int)m, ZeroSrc{}, EpiSumSq<double>{za}, ws, scal + 2);

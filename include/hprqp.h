@@ -248,15 +248,16 @@ int hprqp_get_pass_stats(hprqp_handle h, hprqp_pass_stats* fp64, hprqp_pass_stat
 /* lambda_max(A A') by the power method, for a CSR matrix A (m x n, int32,
  * 0-based) and its transpose A' (n x m) that the caller already holds in
  * device memory.  It allocates nothing; use it when device memory cannot be
- * allocated where the estimate is needed (inside a graph capture that must
- * not allocate, under another framework's memory pool, in a loop that must
- * not allocate after start-up).  No counterpart in the reference.
+ * allocated where the estimate is needed: in a program whose device memory
+ * belongs to another framework's pool allocator, or in a loop that must not
+ * allocate after start-up.  No counterpart in the reference.
  *  - Scratch: a fixed block inside the library (8 MiB of work vectors plus
  *    256 KiB of control), reserved on every GPU that loads the library until
  *    the process exits.  Requires 2m + n <= 1,048,576; larger problems get
  *    HPRQP_E_ARG with the reason in hprqp_last_error(NULL).
- *  - The first call on each device looks up the scratch address there;
- *    make that call before any stream capture.
+ *  - The first call in each CUDA context (a device's primary context, or
+ *    one the caller made current) looks up the scratch address there; make
+ *    that call before any stream capture.
  *  - All calls share the scratch: calls that overlap on the GPU (different
  *    streams, threads or processes on one device) race.  Each call clears
  *    what must start at zero.
@@ -264,7 +265,8 @@ int hprqp_get_pass_stats(hprqp_handle h, hprqp_pass_stats* fp64, hprqp_pass_stat
  *    max_iter steps) as the solver's power method (threads_per_row 1..32
  *    selects the CSR schedule), so lambda agrees with hprqp_solve's
  *    lambda_max_A / eig_factor for the same matrix to rounding (the solver
- *    sums its dot products in another order).
+ *    sums its dot products in another order).  When max_iter ends the
+ *    method, lambda is that step's estimate and *iters_out = max_iter.
  *  - stream: a cudaStream_t (NULL = legacy default stream); the call
  *    returns after the stream has finished the work.  */
 int hprqp_power_lambda_noalloc(int64_t m, int64_t n,

@@ -68,3 +68,19 @@ def test_no_gpu_is_an_error_not_a_fallback(lib_built):
     from hprqp_b200 import workloads as W
     with pytest.raises(_lib.HPRQPError):
         optimize(W.toy_qp())
+
+
+@pytest.mark.parametrize("m,n", [(1 << 20, 1 << 20), (1 << 62, 1), (1, 1 << 62), ((1 << 19) + 1, 0 + 1)])
+def test_power_lambda_noalloc_rejects_oversize(lib_built, m, n):
+    """The size check of the allocation-free entry point runs before any CUDA
+    call or dereference, so it is exercised here without a GPU; sizes that
+    would overflow 2m + n are rejected as well."""
+    L = _lib.load()
+    lam, its = C.c_double(), C.c_int32()
+    dummy = C.c_void_p(8)  # never dereferenced: the size check comes first
+    rc = L.hprqp_power_lambda_noalloc(m, n, dummy, dummy, dummy, dummy, dummy, dummy, 1, 1e-4, 10, None,
+                                      C.byref(lam), C.byref(its))
+    assert rc == _abi.HPRQP_E_ARG
+    assert b"too large" in L.hprqp_last_error(None)
+    with pytest.raises(_lib.HPRQPError):
+        _lib.check(rc)
