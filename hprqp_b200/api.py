@@ -170,7 +170,16 @@ class Solver:
         self._trace = (np.zeros((iters, n)), np.zeros((iters, m)), np.zeros((iters, n))) if iters else None
         t = self._trace
         check(self._L.hprqp_set_trace(self.h, iters, *( [_ptr(a) for a in t] if t else [None] * 3)), self.h)
+        self._strace = (np.zeros(iters), np.zeros(iters, dtype=np.int64)) if iters else None
+        st = self._strace
+        check(self._L.hprqp_set_trace_scalars(self.h, *([_ptr(a) for a in st] if st else [None] * 2)), self.h)
         return self._trace
+
+    def scalar_trace(self):
+        """(sigma, inner) of each iteration traced by the last solve after
+        set_trace: the sigma the step used and its Halpern counter (0 right
+        after a restart)."""
+        return self._strace
 
     def solve(self, params: HPRQP_parameters) -> HPRQP_results:
         model = self.model

@@ -175,6 +175,8 @@ struct Handle {
   std::string err;
   int64_t trace_iters = 0;
   double *xt = nullptr, *yt = nullptr, *wt = nullptr;
+  double* sig_t = nullptr;    // sigma of each traced iteration
+  int64_t* inner_t = nullptr; // inner (Halpern) counter of each traced iteration
   double setup_time = 0.0;
   int64_t h2d_at_solve_start = 0;
   PassProfiler prof64, prof32;
@@ -325,6 +327,7 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
     const bool to_check = (next % check_iter == 0) || (ri.restart_flag > 0) || on_print_schedule(next, p);
     // perform_iteration_step! (src/algorithm.jl:1881-1900)
     const double h1 = 1.0 / (ri.inner + 2.0), h2 = 1.0 - h1;
+    const int64_t inner_used = ri.inner;
     if (prof.on && !to_check && prof.begin(prof_view)) {
       E.prof = &prof_view;
       E.prof_k = 0;
@@ -340,9 +343,12 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
       L.pend_cur = PendingMnorm{true, S_MN_CUR, E.sigma, E.lamA, E.lamQ};
     }
     ri.inner++;
-    if (next <= H.trace_iters)
+    if (next <= H.trace_iters) {
       E.trace_copy(H.xt ? H.xt + (next - 1) * n : nullptr, H.yt ? H.yt + (next - 1) * m : nullptr,
                    H.wt ? H.wt + (next - 1) * n : nullptr);
+      if (H.sig_t) H.sig_t[next - 1] = E.sigma;
+      if (H.inner_t) H.inner_t[next - 1] = inner_used;
+    }
   }
   return HPRQP_STATUS_MAX_ITER;
 }
@@ -849,6 +855,13 @@ int hprqp_set_trace(hprqp_handle h, int64_t iters, double* x_trace, double* y_tr
   h->xt = x_trace;
   h->yt = y_trace;
   h->wt = w_trace;
+  return HPRQP_OK;
+}
+
+int hprqp_set_trace_scalars(hprqp_handle h, double* sigma_trace, int64_t* inner_trace) {
+  if (!h) return HPRQP_E_ARG;
+  h->sig_t = sigma_trace;
+  h->inner_t = inner_trace;
   return HPRQP_OK;
 }
 

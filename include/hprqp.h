@@ -232,6 +232,13 @@ int hprqp_solve(hprqp_handle h, const hprqp_params* params,
 int hprqp_set_trace(hprqp_handle h, int64_t iters,
                     double* x_trace, double* y_trace, double* w_trace);
 
+/* Parity hook, beside hprqp_set_trace: for each traced iteration k
+ * (k < iters of the last hprqp_set_trace) record the sigma the step used
+ * (after update_sigma!, src/algorithm.jl:323-423) and the inner counter of
+ * its Halpern weight 1/(inner + 2) (0 right after a restart, do_restart!,
+ * src/algorithm.jl:522-555).  Arrays of `iters` entries; NULL disables. */
+int hprqp_set_trace_scalars(hprqp_handle h, double* sigma_trace, int64_t* inner_trace);
+
 /* Measurement hook: prepare, estimate lambda_max, then run `iters` plain
  * (partial, `full` = 0) or full HPR iterations of the loaded problem from
  * the zero state and report the CUDA-event time and the algorithmic bytes

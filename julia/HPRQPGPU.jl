@@ -6,8 +6,14 @@
 # index_base = 1 — and the library returns an HPRQP_results-shaped record.
 # CUDA.jl, cuSPARSE and KernelAbstractions are not involved.
 #
+# Include it inside module HPRQP, after structs.jl:
+#     include(joinpath(@__DIR__, "..", "..", "hprqp_b200_repo", "julia", "HPRQPGPU.jl"))
+# (any path to this file), so that solve_gpu returns HPRQP.HPRQP_results.
+#
 # This file is not executed in the build container (no Julia there); the
-# same ABI is exercised from Python (hprqp_b200/_lib.py) by the test-suite.
+# same ABI is exercised from Python (hprqp_b200/_lib.py) by the test-suite,
+# and tests/test_julia_shim.py checks this file's struct mirrors and result
+# fields against include/hprqp.h and the reference's HPRQP_results.
 
 module HPRQPGPU
 
@@ -111,12 +117,27 @@ function cparams(p)
     return c
 end
 
-"""
-    solve_gpu(model::QP_info_cpu, params::HPRQP_parameters) -> NamedTuple
+# The reference's result type, HPRQP_results (src/structs.jl:292-309).  This
+# file is include()d inside module HPRQP after structs.jl (see the seam in
+# INTEGRATION.md), so the type is the parent module's own; a caller that
+# includes it elsewhere passes the type explicitly.
+function _results_type()
+    parent = parentmodule(@__MODULE__)
+    isdefined(parent, :HPRQP_results) || error("HPRQPGPU: include this file inside module HPRQP, " *
+                                               "or pass results_type = HPRQP.HPRQP_results")
+    return getfield(parent, :HPRQP_results)
+end
 
-The GPU body of `solve` through libhprqp.  Fields match HPRQP_results.
 """
-function solve_gpu(model, params)
+    solve_gpu(model::QP_info_cpu, params::HPRQP_parameters) -> HPRQP_results
+
+The GPU body of `solve` through libhprqp.  Returns the reference's own
+`HPRQP_results` (src/structs.jl:292-309), every field filled, so that
+`optimize` and `MOI.optimize!` (which stores it in a
+`Union{Nothing,HPRQP_results}` field, src/MOI_wrapper.jl:63,494) work
+unchanged.
+"""
+function solve_gpu(model, params; results_type = _results_type())
     m, n = size(model.A)
     A = model.A
     Acp, Arv = i32(A.colptr), i32(A.rowval)
@@ -163,10 +184,24 @@ function solve_gpu(model, params)
             ccall((:hprqp_destroy, libhprqp), Cint, (Ptr{Cvoid},), h[])
         end
     end
-    return (iter = res.iter, iter_4 = res.iter_4, iter_6 = res.iter_6, time = res.time,
-            time_4 = res.time_4, time_6 = res.time_6, power_time = res.power_time,
-            primal_obj = res.primal_obj, residuals = res.residuals, gap = res.gap,
-            status = STATUS[res.status], x = x, y = m > 0 ? y : Float64[], z = z, w = w)
+    # collect_results! / handle_termination (src/algorithm.jl:611-643,1039-1097)
+    out = results_type()
+    out.iter = res.iter
+    out.iter_4 = res.iter_4
+    out.iter_6 = res.iter_6
+    out.time = res.time
+    out.time_4 = res.time_4
+    out.time_6 = res.time_6
+    out.power_time = res.power_time
+    out.primal_obj = res.primal_obj
+    out.residuals = res.residuals
+    out.gap = res.gap
+    out.status = STATUS[res.status]
+    out.x = x
+    out.y = m > 0 ? y : Float64[]
+    out.z = z
+    out.w = w
+    return out
 end
 
 end # module

@@ -993,6 +993,15 @@ extern "C" {
 
 const char* oracle_last_error(void) { return g_err.c_str(); }
 
+// Scalar trace of the next oracle_solve (then cleared): per traced iteration
+// the sigma of the step and its Halpern inner counter (0 after a restart).
+static double* g_sig_trace = nullptr;
+static int64_t* g_inner_trace = nullptr;
+void oracle_set_scalar_trace(double* sigma_trace, int64_t* inner_trace) {
+  g_sig_trace = sigma_trace;
+  g_inner_trace = inner_trace;
+}
+
 // solve (src/algorithm.jl:1904-2039), CPU path, with optional iterate trace.
 // `threads` = 1 reproduces the reference's single-threaded CPU loops;
 // > 1 parallelises SpMV and the update loops with OpenMP (timing only).
@@ -1002,6 +1011,10 @@ int oracle_solve(const hprqp_problem* pr, const hprqp_params* params, const doub
                  int32_t threads) {
   g_err.clear();
   g_threads = threads < 1 ? 1 : threads;
+  double* const sig_t = g_sig_trace;
+  int64_t* const inner_t = g_inner_trace;
+  g_sig_trace = nullptr;
+  g_inner_trace = nullptr;
   if (!params || !res) return fail(HPRQP_E_ARG, "null params/result");
   const hprqp_params& p = *params;
   const double setup_start = now_s();
@@ -1134,6 +1147,7 @@ int oracle_solve(const hprqp_problem* pr, const hprqp_params* params, const doub
     const int64_t next = iter + 1;
     ws.to_check = (next % check_iter == 0) || (ri.restart_flag > 0) || on_print_schedule(next, p);
     // perform_iteration_step! (src/algorithm.jl:1881-1900)
+    const int64_t inner_used = ri.inner;
     main_update(ws, qp, ri);
     if (ri.restart_flag > 0) ri.last_gap = compute_M_norm(ws, qp);
     if ((iter + 1) % check_iter == 0) ri.current_gap = compute_M_norm(ws, qp);
@@ -1142,6 +1156,8 @@ int oracle_solve(const hprqp_problem* pr, const hprqp_params* params, const doub
       if (xt) std::memcpy(xt + (next - 1) * n, ws.x.data(), n * sizeof(double));
       if (yt && m) std::memcpy(yt + (next - 1) * m, ws.y.data(), m * sizeof(double));
       if (wt) std::memcpy(wt + (next - 1) * n, ws.w.data(), n * sizeof(double));
+      if (sig_t) sig_t[next - 1] = ws.sigma;
+      if (inner_t) inner_t[next - 1] = inner_used;
     }
   }
   return fail(HPRQP_E_STATE, "loop exited without status");

@@ -36,6 +36,8 @@ def lib():
             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
             C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int32]
         L.oracle_last_error.restype = C.c_char_p
+        L.oracle_set_scalar_trace.restype = None
+        L.oracle_set_scalar_trace.argtypes = [C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -67,6 +69,8 @@ def solve(model, params: Params | None = None, initial_x=None, initial_y=None,
     wt = np.zeros((trace_iters, n)) if trace_iters else None
     x0 = None if initial_x is None else np.ascontiguousarray(initial_x, dtype=np.float64)
     y0 = None if initial_y is None else np.ascontiguousarray(initial_y, dtype=np.float64)
+    st = (np.zeros(trace_iters), np.zeros(trace_iters, dtype=np.int64)) if trace_iters else (None, None)
+    L.oracle_set_scalar_trace(_p(st[0]), _p(st[1]))
     res = Result()
     rc = L.oracle_solve(C.addressof(view.struct), C.byref(params), _p(x0), _p(y0),
                         C.byref(res), _p(x), _p(y), _p(z), _p(w),
@@ -75,5 +79,5 @@ def solve(model, params: Params | None = None, initial_x=None, initial_y=None,
         raise RuntimeError(f"oracle_solve failed ({rc}): {L.oracle_last_error().decode()}")
     out = OracleResult({f: getattr(res, f) for f, _ in Result._fields_})
     out["status_name"] = STATUS_NAMES[res.status]
-    out.update(x=x, y=y, z=z, w=w, x_trace=xt, y_trace=yt, w_trace=wt)
+    out.update(x=x, y=y, z=z, w=w, x_trace=xt, y_trace=yt, w_trace=wt, sigma_trace=st[0], inner_trace=st[1])
     return out

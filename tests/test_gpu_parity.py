@@ -95,7 +95,7 @@ def test_full_solve_matches_oracle(name):
     assert ref.status_name == "OPTIMAL"
     assert res.status == "OPTIMAL" and res.residuals < 1e-6
     assert abs(res.primal_obj - ref.primal_obj) / (1 + abs(ref.primal_obj)) < OBJ_RTOL
-    assert abs(res.iter - ref.iter) <= max(20, 0.2 * ref.iter), (res.iter, ref.iter)
+    assert res.iter == ref.iter and res.restarts == ref.restarts, (res.iter, ref.iter, res.restarts, ref.restarts)
     assert res.gpu_launches > 0
     if ptype != "LASSO":
         k = kkt(m, res.x, res.y, res.z)
@@ -170,15 +170,24 @@ def test_unsupported_options_are_errors():
 
 
 def test_grid_qp_full_size_properties():
-    # 700 x 700 grid (n = 490,000, m = 974,408): too large for the oracle to
-    # finish quickly, so check size-independent properties: both precision
-    # modes reach 1e-6, agree on the objective, and pass the numpy KKT check.
+    # 700 x 700 grid (n = 490,000, m = 974,408), the benchmark problem: the
+    # oracle's recorded FP64 solve of it (tests/golden/grid_qp_oracle.json:
+    # OPTIMAL in 570 iterations, its objective) plus size-independent
+    # properties: both precision modes reach 1e-6, agree on the objective,
+    # and pass the numpy KKT check.
+    import json
+    import os
+    with open(os.path.join(os.path.dirname(__file__), "golden", "grid_qp_oracle.json")) as f:
+        gold = json.load(f)["700"]
     m = W.grid_qp()
     s = Solver().load(m)
     r64 = s.solve(gpu_params("QP"))
     r32 = s.solve(gpu_params("QP", precision="fp32_polish"))
     s.close()
-    assert r64.status == r32.status == "OPTIMAL"
+    assert r64.status == r32.status == gold["status"] == "OPTIMAL"
+    assert r64.iter == gold["iter"], (r64.iter, gold["iter"])
+    assert abs(r64.primal_obj - gold["primal_obj"]) / (1 + abs(gold["primal_obj"])) < OBJ_RTOL
+    assert abs(r32.primal_obj - gold["primal_obj"]) / (1 + abs(gold["primal_obj"])) < OBJ_RTOL
     assert abs(r64.primal_obj - r32.primal_obj) / (1 + abs(r64.primal_obj)) < 1e-5
     for r in (r64, r32):
         k = kkt(m, r.x, r.y, r.z)

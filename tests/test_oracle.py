@@ -2,7 +2,7 @@
 pinned against the analytic optimum of the reference's model.mps example,
 the reference tests' own status/tolerance assertions, scipy's HiGHS on LPs,
 sklearn on LASSO, an independent numpy KKT check, and the reference's MPS
-fixtures when the reference tree is present."""
+fixtures when the reference tree is given (HPRQP_REFERENCE_DATA)."""
 import os
 
 import numpy as np
@@ -13,7 +13,7 @@ from hprqp_b200._abi import default_params
 from oracle import oracle as O
 from tests.kkt import kkt
 
-REF_DATA = "/root/reference/data"
+REF_DATA = os.environ.get("HPRQP_REFERENCE_DATA", "")
 
 
 def params(**kw):
@@ -124,7 +124,7 @@ def test_max_iter_and_trace_shapes():
     assert r.x_trace.shape == (30, m.n) and np.all(np.isfinite(r.x_trace))
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference fixtures not present")
+@pytest.mark.skipif(not REF_DATA or not os.path.isdir(REF_DATA), reason="reference data files not given")
 @pytest.mark.parametrize("name", ["AUG3DCQP.mps", "AUG2D.mps"])
 def test_reference_mps_fixtures(name):
     # test/runtests.jl:254-280 (AUG2D) and :704-788 (AUG3DCQP): OPTIMAL, < 1e-6
