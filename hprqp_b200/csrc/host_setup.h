@@ -79,7 +79,10 @@ void load_problem(const hprqp_problem* pr, HostProblem& hp);
 void prepare_problem(const HostProblem& hp, const hprqp_params& p, Prepared& out);
 // The same for a sparse Q with the matrix scaling on the GPU (scale.cu):
 // bitwise the host result, with the scaled arrays copied back into `out`.
-void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared& out, cudaStream_t st);
+// h2d / d2h: byte counters of the handle, incremented by every host<->device
+// copy the scaling makes
+void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared& out, cudaStream_t st,
+                         int64_t* h2d, int64_t* d2h);
 // the tails shared by both: norms, check_Q_diagonal and Q_maxval on the
 // scaled sparse Q; the noC rule
 void finish_sparse(Prepared& o, int64_t n);

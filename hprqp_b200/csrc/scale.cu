@@ -116,7 +116,8 @@ inline int blocks(int64_t n) { return (int)((std::max<int64_t>(n, 1) + kT - 1) /
 
 }  // namespace
 
-void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared& o, cudaStream_t st) {
+void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared& o, cudaStream_t st,
+                         int64_t* h2d, int64_t* d2h) {
   if (hp.Q_kind != HPRQP_Q_SPARSE) {
     prepare_problem(hp, p, o);
     return;
@@ -203,8 +204,10 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   auto ds = std::make_shared<DevScaled>();
   DevBuf d;
   auto up = [&](auto* dst, const auto& v) {
-    if (!v.empty())
+    if (!v.empty()) {
       HPRQP_CUDA(cudaMemcpyAsync(dst, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice, st));
+      *h2d += (int64_t)(sizeof(v[0]) * v.size());
+    }
   };
   struct DM {
     int rows = 0;
@@ -277,8 +280,10 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   HPRQP_CUDA(cudaStreamSynchronize(st));
   tm[nt++] = wall();  // scaling kernels
   auto down = [&](std::vector<double>& dst, const double* src) {
-    if (!dst.empty())
+    if (!dst.empty()) {
       HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
+      *d2h += (int64_t)(sizeof(double) * dst.size());
+    }
   };
   down(S.val, sv);
   down(o.c, c);

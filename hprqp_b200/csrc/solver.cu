@@ -387,7 +387,7 @@ static void prepare(Handle& H, const hprqp_params& p) {
   const char* hs = std::getenv("HPRQP_HOST_SCALING");
   const int64_t work = H.hp.A.nnz() + H.hp.Q.nnz();
   if (H.hp.Q_kind == HPRQP_Q_SPARSE && work >= 100000 && !(hs && hs[0] == '1'))
-    prepare_problem_gpu(H.hp, p, H.pp, H.cm->stream);
+    prepare_problem_gpu(H.hp, p, H.pp, H.cm->stream, &H.cm->h2d, &H.cm->d2h);
   else
     prepare_problem(H.hp, p, H.pp);
   if (H.hp.Q_kind == HPRQP_Q_LASSO) H.path = PATH_LASSO;
@@ -459,7 +459,9 @@ static void start_engine(Handle& H, Engine<V>& E, const hprqp_params& p, double 
 static int solve(Handle& H, const hprqp_params& p, const double* x0, const double* y0, hprqp_result* res,
                  double* xo, double* yo, double* zo, double* wo) {
   const double setup_start = now_s();
+  // host<->device bytes of this call, set-up (scaling, uploads) included
   H.h2d_at_solve_start = H.cm->h2d;
+  const int64_t d2h0 = H.cm->d2h;
   prepare(H, p);
   const double setup_time = now_s() - setup_start;
   Common& cm = *H.cm;
@@ -467,7 +469,6 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   const Prepared& pp = H.pp;
   const int64_t m = H.hp.m;
   Engine<double>& E64 = *H.e64;
-  const int64_t h2d0 = cm.h2d - (setup_time > 0 ? 0 : 0), d2h0 = cm.d2h;
   cudaEvent_t ev0, ev1;
   HPRQP_CUDA(cudaEventCreate(&ev0));
   HPRQP_CUDA(cudaEventCreate(&ev1));
@@ -572,7 +573,6 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   res->power_bytes = pbytes;
   res->h2d_bytes = cm.h2d - H.h2d_at_solve_start;
   res->d2h_bytes = cm.d2h - d2h0;
-  (void)h2d0;
   if (p.verbose) {
     static const char* names[] = {"OPTIMAL", "MAX_ITER", "TIME_LIMIT", "NUMERICAL_ERROR"};
     std::printf("Status: %s  Iterations: %lld  Time: %.3f s  Primal Objective: %.12e  KKT: %.3e\n",
