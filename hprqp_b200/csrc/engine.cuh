@@ -82,6 +82,12 @@ struct Common {  // per-handle resources shared by the engines
   // on the 700x700 grid (FP32 iteration 40.3 vs 40.3 us, FP64 50.3 vs
   // 48.4 us), so off by default
   int epi_prefetch = 0;
+  // ELL passes load their constant data before waiting on the previous kernel
+  // (HPRQP_ELL_PROLOGUE: 0 off = k_row_pass, 1 the matrix rows, 2 the matrix
+  // rows and the epilogue's problem data).  Measured on the 700x700 grid, ELL
+  // for Q, A, A': FP32 plain iteration 43.4 / 28.6 / 29.5 us, FP64 48.3 /
+  // 45.1 / 46.4 us for 0 / 1 / 2
+  int ell_prologue = 1;
   // power chains folded once per chunk (HPRQP_POWER_CHUNK_FOLD=0: per step)
   bool pow_chunk_fold = true;
   // row-schedule autotuner (timed); HPRQP_AUTOTUNE=0 applies a fixed rule

@@ -126,6 +126,59 @@ __global__ void __launch_bounds__(kBlock) k_row_pass(int nrows, Src src, Epi epi
   if (lane == 0) epi(row, acc);
 }
 
+// An epilogue may split off `Pre pre(i)`: the operands of row i that are
+// constant over a solve (problem data written at set-up), and take them back
+// in operator()(i, acc, pre).  k_ell_pass loads them before it waits on the
+// previous kernel.
+template <typename E, typename = void>
+struct HasPre : std::false_type {};
+template <typename E>
+struct HasPre<E, std::void_t<typename E::Pre>> : std::true_type {};
+
+// ELL pass (one thread per row, width w <= WMAX) whose constant loads come
+// before the wait on the previous kernel.  Passes are launched with
+// programmatic dependent launch: CTAs of this pass become resident while the
+// previous pass drains, and here they already stream their rows' column
+// indices and values (constant over a solve) and the epilogue's constant
+// operands; only the gathers of the input vector and the epilogue's other
+// operands wait for the previous pass's writes.  Same products, same order
+// of summation as EllSrc::dot.
+template <int WMAX, typename Acc, typename V, typename X, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_ell_pass(int nrows, EllSrc<V, X> src, Epi epi, int with_pre) {
+  const int row = blockIdx.x * kBlock + threadIdx.x;
+  const bool live = row < nrows;
+  int c[WMAX];
+  V v[WMAX];
+  if (live) {
+#pragma unroll
+    for (int k = 0; k < WMAX; ++k)
+      if (k < src.w) {
+        c[k] = __ldg(src.col + (size_t)k * src.rows + row);
+        v[k] = __ldg(src.val + (size_t)k * src.rows + row);
+      }
+  }
+  if constexpr (HasPre<Epi>::value) {
+    typename Epi::Pre pre{};
+    if (live && with_pre) pre = epi.pre(row);
+    pdl_enter();
+    if (!live) return;
+    Acc s = Acc(0);
+#pragma unroll
+    for (int k = 0; k < WMAX; ++k)
+      if (k < src.w) s = fma((Acc)v[k], (Acc)__ldg(src.x + c[k]), s);
+    if (!with_pre) pre = epi.pre(row);
+    epi(row, s, pre);
+  } else {
+    pdl_enter();
+    if (!live) return;
+    Acc s = Acc(0);
+#pragma unroll
+    for (int k = 0; k < WMAX; ++k)
+      if (k < src.w) s = fma((Acc)v[k], (Acc)__ldg(src.x + c[k]), s);
+    epi(row, s);
+  }
+}
+
 // Block reduction of K slots; MaxMask bit k selects max (else sum).
 // Result valid in thread 0.
 template <int K, unsigned MaxMask>
@@ -304,14 +357,20 @@ struct EpiZxw1 {
     pf_rows(i, lv, x, w, ATy, c, l, u, last_x);
     if (Diag) pf_rows(i, lv, fact1, fact2);
   }
+  struct Pre {
+    V c, l, u;
+  };
+  __device__ __forceinline__ Pre pre(int i) const { return Pre{c[i], l[i], u[i]}; }
   template <typename A>
-  __device__ __forceinline__ void operator()(int i, A acc) const {
+  __device__ __forceinline__ void operator()(int i, A acc) const { (*this)(i, acc, pre(i)); }
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, const Pre& p) const {
     const double qw = (double)acc;
     Qw[i] = (V)qw;
     const double x_i = x[i], w_i = w[i];
-    const double tmp = -qw + (double)ATy[i] - (double)c[i];
+    const double tmp = -qw + (double)ATy[i] - (double)p.c;
     const double z_raw = x_i + sigma * tmp;
-    const double xb = clampd(z_raw, l[i], u[i]);
+    const double xb = clampd(z_raw, p.l, p.u);
     const double xh = 2.0 * xb - x_i;
     const double xn = fma(h2, xh, h1 * (double)last_x[i]);
     const double wb = Diag ? fma((double)fact1[i], w_i, (double)fact2[i] * xh) : fma(f1s, w_i, f2s * xh);
@@ -350,11 +409,17 @@ struct EpiY {
   const AV* last_y;
   double f1, f2, h1, h2;
   __device__ __forceinline__ void prefetch(int i, int lv) const { pf_rows(i, lv, (const V*)y, AL, AU, last_y); }
+  struct Pre {
+    V al, au;
+  };
+  __device__ __forceinline__ Pre pre(int i) const { return Pre{AL[i], AU[i]}; }
   template <typename A>
-  __device__ __forceinline__ void operator()(int i, A acc) const {
+  __device__ __forceinline__ void operator()(int i, A acc) const { (*this)(i, acc, pre(i)); }
+  template <typename A>
+  __device__ __forceinline__ void operator()(int i, A acc, const Pre& p) const {
     const double yi = y[i];
     const double s_raw = (double)acc - f1 * yi;
-    const double s_proj = clampd(s_raw, AL[i], AU[i]);
+    const double s_proj = clampd(s_raw, p.al, p.au);
     const double yb = f2 * (s_proj - s_raw);
     const double yh = 2.0 * yb - yi;
     const double yn = fma(h2, yh, h1 * (double)last_y[i]);
@@ -768,6 +833,63 @@ __global__ void __launch_bounds__(kBlock) k_row_partials(int nrows, Src src, Epi
   for (int row = (int)((blockIdx.x * kBlock + threadIdx.x) / TPR); row < nrows; row += rows_per_grid) {
     const Acc acc = src.template dot<TPR, Acc>(row, lane);
     if (lane == 0) epi(row, acc, r);
+  }
+  block_reduce<K, 0u>(r);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) partials[(size_t)blockIdx.x * K + k] = r[k];
+  }
+}
+
+// The same over a SELL-32 matrix, one thread per row, with the matrix
+// entries of the thread's first R rows (up to WMAX entries each: row
+// lengths, slice offsets, column indices, values; constant over a solve)
+// loaded before the wait on the previous kernel, so a CTA made resident
+// while the previous step drains already holds them.  Rows past R or entries
+// past WMAX are read after the wait.  Summation order as SellSrc::dot.
+template <int R, int WMAX, int K, typename Acc, typename V, typename X, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_sell_partials(int nrows, SellSrc<V, X> src, Epi epi,
+                                                          double* __restrict__ partials) {
+  double r[K];
+#pragma unroll
+  for (int k = 0; k < K; ++k) r[k] = 0.0;
+  const int stride = (int)(gridDim.x * kBlock);
+  const int row0 = (int)(blockIdx.x * kBlock + threadIdx.x);
+  int len[R], base[R], c[R][WMAX];
+  V v[R][WMAX];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int row = row0 + q * stride;
+    len[q] = 0;
+    base[q] = 0;
+    if (row < nrows) {
+      len[q] = __ldg(src.ptr + row + 1) - __ldg(src.ptr + row);
+      base[q] = __ldg(src.sptr + (row >> 5)) + (row & 31);
+#pragma unroll
+      for (int k = 0; k < WMAX; ++k)
+        if (k < len[q]) {
+          c[q][k] = __ldg(src.col + base[q] + 32 * k);
+          v[q][k] = __ldg(src.val + base[q] + 32 * k);
+        }
+    }
+  }
+  pdl_enter();
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int row = row0 + q * stride;
+    if (row < nrows) {
+      Acc s = Acc(0);
+#pragma unroll
+      for (int k = 0; k < WMAX; ++k)
+        if (k < len[q]) s = fma((Acc)v[q][k], (Acc)__ldg(src.x + c[q][k]), s);
+      for (int k = WMAX; k < len[q]; ++k)
+        s = fma((Acc)__ldg(src.val + base[q] + 32 * k), (Acc)__ldg(src.x + __ldg(src.col + base[q] + 32 * k)), s);
+      epi(row, s, r);
+    }
+  }
+  for (int row = row0 + R * stride; row < nrows; row += stride) {
+    const Acc acc = src.template dot<1, Acc>(row, 0);
+    epi(row, acc, r);
   }
   block_reduce<K, 0u>(r);
   if (threadIdx.x == 0) {
