@@ -14,10 +14,12 @@ the same run measures, into the same JSON line:
                 plain FP64 one instance at a time, on 1,000 held-out
                 instances (the network trained on 3,000 solver-made labels);
   qap_batch     256 QAP relaxations (n = 30..128): batched FP64 and FP32 +
-                polish against plain FP64 one instance at a time.
+                polish against plain FP64 one instance at a time;
+  lasso_large   the 20,000 x 150,000 LASSO (1.1e7 nonzeros, lognormal row
+                lengths): time to 1e-6 in FP64 and FP32 + polish.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-    python bench.py --mode iterations|solve|power|gemm|family|qap ...   (one part alone, for ncu)
+    python bench.py --mode iterations|solve|power|gemm|family|qap|lasso ...   (one part alone, for ncu)
 
 N > 1 runs one process per GPU (torchrun); the grid instance does not shard,
 so every rank solves its own replica ("scaling": "weak", replicas only) and
@@ -61,6 +63,7 @@ def parse():
     ap.add_argument("--no-one-thread", action="store_true", help="reference arm: skip the 1-thread solve")
     ap.add_argument("--no-family", action="store_true", help="skip the LASSO-family block")
     ap.add_argument("--no-qap", action="store_true", help="skip the QAP-batch block")
+    ap.add_argument("--no-lasso", action="store_true", help="skip the large-LASSO block")
     ap.add_argument("--family-train", type=int, default=3000)
     ap.add_argument("--family-test", type=int, default=1000)
     ap.add_argument("--family-epochs", type=int, default=150)
@@ -72,7 +75,7 @@ def parse():
     ap.add_argument("--qap-only", default="all", choices=["all", "batch_fp64", "batch_fp32_polish"],
                     help="one batched path alone (for profilers)")
     ap.add_argument("--mode", default="bench",
-                    choices=["bench", "iterations", "solve", "power", "gemm", "family", "qap"])
+                    choices=["bench", "iterations", "solve", "power", "gemm", "family", "qap", "lasso"])
     ap.add_argument("--workload", default="grid", choices=["grid", "random_qp", "lasso"])
     ap.add_argument("--iters", type=int, default=10)
     ap.add_argument("--n", type=int, default=2048)
@@ -385,6 +388,47 @@ def qap_block(args, rank, world, local_rank, log):
     return out
 
 
+def lasso_block(args, rank, world, local_rank, log):
+    """The large LASSO (A 20,000 x 150,000, ~1.1e7 nonzeros, lognormal row
+    lengths; implicit Q = A'A): time to 1e-6 (device time from after set-up,
+    power method included, like the headline) in plain FP64 and in FP32 +
+    FP64 polish, iterations/s, and each fused pass's achieved bandwidth (a
+    CUDA event on each side of every pass of one profiled solve).  A replica
+    per rank ("replicas only"); the time is the slowest rank's."""
+    from hprqp_b200 import HPRQP_parameters, Solver
+    from hprqp_b200 import workloads as W
+    from hprqp_b200.dist import max_over_ranks
+    dev = f"cuda:{local_rank}"
+    model = W.lasso()
+    out = dict(workload="lasso_20000x150000_lognormal", n=model.n, lasso_m=model.Q.A.shape[0], nnz=int(model.Q.A.nnz))
+    s = Solver(local_rank).load(model)
+    peak, peak_kind = measured_peak()
+    for prec in ("fp64", "fp32_polish"):
+        p = HPRQP_parameters(verbose=False, problem_type="LASSO", precision=prec)
+        s.prepare(p)
+        s.solve(p)  # warm-up
+        rs = [s.solve(p) for _ in range(3)]
+        r = rs[-1]
+        t = max_over_ranks(statistics.median(x.device_time for x in rs), device=dev)
+        loop_s = max(t - statistics.median(x.power_time for x in rs), 1e-9)
+        s.solve(HPRQP_parameters(verbose=False, problem_type="LASSO", precision=prec, profile_passes=True))
+        st = s.pass_stats()
+        passes = []
+        for eng in ("fp64", "fp32"):
+            for q in st[eng]["passes"]:
+                ach = q["bytes"] / (q["ms"] * 1e-3) / 1e9 if q["ms"] else 0.0
+                passes.append({"kernel": f"{eng}:{q['name']}", "ms_per_launch": q["ms"], "bytes": q["bytes"],
+                               "schedule": q["threads_per_row"], "achieved_GBps": round(ach, 1),
+                               "frac": round(ach / peak, 4)})
+        out[prec] = dict(time_s=t, status=r.status, iters=r.iter, iters_fp32=r.iter_fp32, kkt=r.residuals,
+                         primal_obj=r.primal_obj, power_s=r.power_time, iters_per_s=r.iter / loop_s,
+                         passes_with_events=passes, peak=peak, peak_source=peak_kind)
+        log(f"lasso {prec}: {t:.3f} s, {r.iter} iterations")
+    s.close()
+    out["speedup_fp32_vs_fp64"] = out["fp64"]["time_s"] / out["fp32_polish"]["time_s"]
+    return out
+
+
 def run_ours(args):
     rank, local_rank, world = dist_env()
     dist = _dist_init(local_rank, world)
@@ -549,6 +593,8 @@ def run_ours(args):
         line["lasso_family"] = family_block(args, rank, world, local_rank, log)
     if not args.no_qap:
         line["qap_batch"] = qap_block(args, rank, world, local_rank, log)
+    if not args.no_lasso:
+        line["lasso_large"] = lasso_block(args, rank, world, local_rank, log)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -585,11 +631,12 @@ def run_mode(a):
     tensor-core GEMM on --n x --n FP32 matrices.  --mode family / qap: the
     batched-family blocks of the default run alone.  Prints one JSON line."""
     from hprqp_b200 import HPRQP_parameters, Solver
-    if a.mode in ("family", "qap"):
+    if a.mode in ("family", "qap", "lasso"):
         rank, local_rank, world = dist_env()
         dist = _dist_init(local_rank, world)
         log = lambda *x: print(*x, file=sys.stderr, flush=True) if rank == 0 else None
-        out = (family_block if a.mode == "family" else qap_block)(a, rank, world, local_rank, log)
+        blk = {"family": family_block, "qap": qap_block, "lasso": lasso_block}[a.mode]
+        out = blk(a, rank, world, local_rank, log)
         if rank == 0:
             print(json.dumps(out), flush=True)
         if dist:

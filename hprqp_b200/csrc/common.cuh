@@ -56,6 +56,17 @@ struct DCsr {
   int ell_w = 0;
   const int* ecol = nullptr;
   const V* evalv = nullptr;
+  // Row-split schedule for a heavy tail of long rows: `npieces` pieces
+  // {row, begin, end, split index or -1}, heaviest first, one warp each; a
+  // row longer than split_T is cut into pieces of split_T entries whose
+  // partial sums go to spart[srow[s].x + j] (j = piece index in the row) and
+  // are folded in order by the row's last piece (counter scnt[s])
+  bool split = false;
+  int npieces = 0, split_T = 0;
+  const int4* pieces = nullptr;
+  const int2* srow = nullptr;
+  double* spart = nullptr;
+  unsigned* scnt = nullptr;
 };
 
 // Programmatic dependent launch: wait until the previous kernel in the

@@ -307,11 +307,16 @@ void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode, const DevCsr
     build_ell(h, d);
     d.ell = d.ell_w > 0;
     d.tpr = d.ell ? 1 : 4;
+  } else if (tpr_mode == 9) {  // row split requested
+    build_split(h, d);
+    d.split = d.npieces > 0;
+    d.tpr = 4;
   } else if (tpr_mode > 0) {
     d.tpr = 1 << std::min(tpr_mode - 1, 5);
   } else {
     build_sell(h, d);
     build_ell(h, d);
+    build_split(h, d);
     d.tpr = autotune(d);
   }
 }
@@ -358,6 +363,52 @@ void Engine<V>::build_ell(const HCsr& h, DCsr<V>& d) {
   d.ell_w = w;
 }
 
+// Row-split schedule (DCsr::split) for a matrix with a heavy tail of long
+// rows: built when the longest row exceeds 1,024 entries and 8x the mean.
+// Rows longer than T = max(1024, longest / 64) (a multiple of 32) are cut
+// into pieces of T entries; pieces are ordered by length, longest first.
+template <typename V>
+void Engine<V>::build_split(const HCsr& h, DCsr<V>& d) {
+  d.npieces = 0;
+  if (h.rows <= 0 || h.nnz() == 0) return;
+  int64_t maxlen = 0;
+  for (int64_t r = 0; r < h.rows; ++r) maxlen = std::max<int64_t>(maxlen, h.ptr[r + 1] - h.ptr[r]);
+  const double avg = (double)h.nnz() / (double)h.rows;
+  if (maxlen <= 1024 || (double)maxlen <= 8.0 * avg) return;
+  int64_t T = std::max<int64_t>(1024, (maxlen + 63) / 64);
+  T = (T + 31) / 32 * 32;
+  std::vector<int4> pcs;
+  std::vector<int2> srow;
+  int64_t slots = 0;
+  for (int64_t r = 0; r < h.rows; ++r) {
+    const int b = h.ptr[r], e = h.ptr[r + 1];
+    if (e - b <= T) {
+      pcs.push_back(make_int4((int)r, b, e, -1));
+      continue;
+    }
+    const int np = (int)((e - b + T - 1) / T);
+    const int s = (int)srow.size();
+    srow.push_back(make_int2((int)slots, np));
+    for (int j = 0; j < np; ++j) pcs.push_back(make_int4((int)r, b + (int)(j * T), (int)std::min<int64_t>(e, b + (j + 1) * T), s));
+    slots += np;
+  }
+  std::stable_sort(pcs.begin(), pcs.end(), [](const int4& a, const int4& b) { return (a.z - a.y) > (b.z - b.y); });
+  int4* dp = mem.alloc<int4>(pcs.size());
+  int2* ds = mem.alloc<int2>(std::max<size_t>(srow.size(), 1));
+  double* part = mem.alloc<double>(std::max<int64_t>(slots, 1));
+  unsigned* cnt = mem.alloc<unsigned>(std::max<size_t>(srow.size(), 1));
+  cm.to_dev(dp, pcs.data(), sizeof(int4) * pcs.size());
+  cm.to_dev(ds, srow.data(), sizeof(int2) * srow.size());
+  HPRQP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * std::max<size_t>(srow.size(), 1), cm.stream));
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));  // host staging vectors go out of scope
+  d.pieces = dp;
+  d.srow = ds;
+  d.spart = part;
+  d.scnt = cnt;
+  d.npieces = (int)pcs.size();
+  d.split_T = (int)T;
+}
+
 // SELL-32 copy of a CSR matrix, built on the device from its CSR; skipped
 // when padding would exceed 50%.
 template <typename V>
@@ -392,7 +443,11 @@ void Engine<V>::build_sell(const HCsr& h, DCsr<V>& d) {
 template <typename V>
 template <typename Epi>
 void Engine<V>::mat_rows(const DCsr<V>& M, const V* xin, const Epi& e) {
-  if (M.ell && M.ell_w <= 8 && cm.ell_prologue > 0 && M.rows > 0) {
+  if (M.split) {
+    const int grid = (int)(((int64_t)M.npieces * 32 + kBlock - 1) / kBlock);
+    launch(cm, k_split_pass<V, V, V, Epi>, grid, kBlock, M.npieces, M.pieces, M.ptr, M.col, M.val, xin, M.srow,
+           M.split_T, M.spart, M.scnt, e);
+  } else if (M.ell && M.ell_w <= 8 && cm.ell_prologue > 0 && M.rows > 0) {
     const int grid = (int)((M.rows + kBlock - 1) / kBlock);
     launch(cm, k_ell_pass<8, V, V, V, Epi>, grid, kBlock, (int)M.rows,
            EllSrc<V, V>{M.ecol, M.evalv, xin, (int)M.rows, M.ell_w}, e, cm.ell_prologue >= 2 ? 1 : 0);
@@ -462,7 +517,9 @@ int Engine<V>::autotune(DCsr<V>& d) {
   if (!cm.autotune) {  // fixed rule: ELL, else SELL-32, else threads per row by mean row length
     d.ell = d.ell_w > 0;
     d.sell = !d.ell && d.sell_len > 0;
+    d.split = !d.ell && !d.sell && d.npieces > 0;
     if (d.ell || d.sell) return 1;
+    if (d.split) return 32;
     int t = 1;
     while (t < 32 && avg >= 4.0 * t) t *= 2;
     return t;
@@ -475,6 +532,7 @@ int Engine<V>::autotune(DCsr<V>& d) {
   if (cm.ell_prologue > 0 && d.ell_w > 0 && d.ell_w <= 8) {
     d.ell = true;
     d.sell = false;
+    d.split = false;
     return 1;
   }
   cudaEvent_t e0, e1;
@@ -482,18 +540,20 @@ int Engine<V>::autotune(DCsr<V>& d) {
   HPRQP_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = 4;
-  bool best_sell = false, best_ell = false;
+  bool best_sell = false, best_ell = false, best_split = false;
   // candidate -1 = SELL-32, -2 = ELL (one thread per row each); each timed as
   // the best of 3 rounds of 4 back-to-back products, so a noisy round cannot
   // decide.
-  for (int t : {-2, -1, 1, 2, 4, 8, 16, 32}) {
+  for (int t : {-3, -2, -1, 1, 2, 4, 8, 16, 32}) {
+    if (t == -3 && d.npieces == 0) continue;
     if (t == -2 && d.ell_w == 0) continue;
     if (t == -1 && d.sell_len == 0) continue;
     if (t == 1 && avg > 12) continue;
     if (t == 32 && avg < 8) continue;
+    d.split = (t == -3);
     d.ell = (t == -2);
     d.sell = (t == -1);
-    d.tpr = t < 0 ? 1 : t;
+    d.tpr = t == -3 ? 32 : t < 0 ? 1 : t;  // (a split matrix's reductions run on CSR, 32 lanes per row)
     spmv(d, pz, pt);
     float tbest = 1e30f;
     for (int round = 0; round < 3; ++round) {
@@ -505,12 +565,13 @@ int Engine<V>::autotune(DCsr<V>& d) {
       HPRQP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       tbest = std::min(tbest, ms);
     }
-    if (tbest < best) { best = tbest; best_t = d.tpr; best_sell = d.sell; best_ell = d.ell; }
+    if (tbest < best) { best = tbest; best_t = d.tpr; best_sell = d.sell; best_ell = d.ell; best_split = d.split; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   d.sell = best_sell;
   d.ell = best_ell;
+  d.split = best_split;
   return best_t;
 }
 
@@ -980,7 +1041,7 @@ template <typename V>
 void Engine<V>::pass_info(int k, const char** name, double* bytes, int* tpr) const {
   const double v = sizeof(V), d = sizeof(V);  // d: the Halpern anchors (storage type too)
   auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
-  auto sched = [](const DCsr<V>& M) { return M.ell ? -1 : M.sell ? 0 : M.tpr; };  // 0 = SELL-32, -1 = ELL
+  auto sched = [](const DCsr<V>& M) { return M.split ? -3 : M.ell ? -1 : M.sell ? 0 : M.tpr; };  // 0 = SELL-32, -1 = ELL, -3 = row split
   const double N = (double)n, M_ = (double)m;
   const double dg = Q_is_diag ? 2 * N * v : 0.0;
   *name = "?";

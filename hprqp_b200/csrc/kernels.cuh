@@ -179,6 +179,48 @@ __global__ void __launch_bounds__(kBlock) k_ell_pass(int nrows, EllSrc<V, X> src
   }
 }
 
+// Row-split pass (DCsr::split): one warp per piece of a row, pieces in the
+// order of the schedule (heaviest first, so the long rows of a heavy-tailed
+// matrix start at once instead of finishing last).  A whole row runs its
+// epilogue at once; the pieces of a split row store their partial sums, and
+// the last one to arrive (atomic counter) folds them in piece order, resets
+// the counter and runs the epilogue, so results do not depend on timing.
+template <typename Acc, typename V, typename X, typename Epi>
+__global__ void __launch_bounds__(kBlock) k_split_pass(int npieces, const int4* __restrict__ pieces,
+                                                       const int* __restrict__ ptr, const int* __restrict__ col,
+                                                       const V* __restrict__ val, const X* __restrict__ x,
+                                                       const int2* __restrict__ srow, int T,
+                                                       double* __restrict__ part, unsigned* __restrict__ cnt,
+                                                       Epi epi) {
+  const int wid = (int)((blockIdx.x * kBlock + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
+  int4 pc = make_int4(0, 0, 0, -1);
+  if (wid < npieces) pc = __ldg(pieces + wid);  // the schedule is constant: before the wait
+  pdl_enter();
+  if (wid >= npieces) return;
+  Acc s = Acc(0);
+#pragma unroll 4
+  for (int k = pc.y + lane; k < pc.z; k += 32) s = fma((Acc)__ldg(val + k), (Acc)__ldg(x + __ldg(col + k)), s);
+  s = group_sum<32>(s);
+  if (lane != 0) return;
+  if (pc.w < 0) {
+    epi(pc.x, s);
+    return;
+  }
+  const int2 sr = __ldg(srow + pc.w);
+  const int j = (pc.y - __ldg(ptr + pc.x)) / T;
+  part[sr.x + j] = (double)s;
+  __threadfence();
+  const unsigned arrived = atomicAdd(cnt + pc.w, 1u);
+  if (arrived == (unsigned)(sr.y - 1)) {
+    __threadfence();
+    Acc t = Acc(0);
+    for (int q = 0; q < sr.y; ++q) t += (Acc)__ldcg(part + sr.x + q);
+    cnt[pc.w] = 0u;
+    epi(pc.x, t);
+  }
+}
+
 // Block reduction of K slots; MaxMask bit k selects max (else sum).
 // Result valid in thread 0.
 template <int K, unsigned MaxMask>

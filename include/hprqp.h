@@ -121,7 +121,9 @@ typedef struct hprqp_params {
     int32_t warm_up;                 /* 0; accepted, no JIT to warm                 */
     int32_t spmv_mode_Q;             /* 0 = auto (autotuned row schedule); 1..6 =
                                         CSR with 1,2,4,...,32 threads per row;
-                                        7 = SELL-32; 8 = ELL (short rows)           */
+                                        7 = SELL-32; 8 = ELL (short rows); 9 = row
+                                        split (long rows cut into equal pieces,
+                                        one warp each; CSR where no row is long)   */
     int32_t spmv_mode_A;             /* same, for A and A'                          */
     int32_t print_frequency;         /* -1 = adaptive (print_step)                  */
     int32_t device_number;           /* 0                                           */
