@@ -31,6 +31,8 @@ def _lib():
         L.hprqp_batch_load_lasso.argtypes = [vp, C.c_int32, vp]
         L.hprqp_batch_load_qap.argtypes = [vp, C.c_int32, vp]
         L.hprqp_batch_solve.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.hprqp_batch_qap_apply.argtypes = [vp, C.c_int32, vp, vp, C.POINTER(C.c_int32)]
+        L.hprqp_batch_qap_apply.restype = C.c_int
         L.hprqp_batch_last_error.argtypes = [vp]
         L.hprqp_batch_last_error.restype = C.c_char_p
         L.hprqp_batch_destroy.argtypes = [vp]
@@ -90,6 +92,17 @@ class BatchSolver:
             r.x = xs[k]
             out.append(r)
         return out
+
+    def qap_apply(self, X, precision="fp64"):
+        """Q_k(X_k) for every instance (X concatenated, each block
+        column-major); returns (Y, used the tensor-core operator)."""
+        from ._abi import PRECISIONS
+        X = np.ascontiguousarray(X, dtype=np.float64)
+        Y = np.zeros_like(X)
+        tc = C.c_int32()
+        self._check(self.L.hprqp_batch_qap_apply(self.h, PRECISIONS[precision], X.ctypes.data, Y.ctypes.data,
+                                                 C.byref(tc)))
+        return Y, bool(tc.value)
 
     def close(self):
         if getattr(self, "h", None):

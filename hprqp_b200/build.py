@@ -68,7 +68,7 @@ def build(verbose=False, force=False):
             print(o)
     objs = [os.path.join(BUILD, s + ".o") for s in SOURCES]
     if jobs or not os.path.exists(LIB):
-        run([cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcublas", "-lgomp", "-ccbin", "/usr/bin/g++"])
+        run([cc] + ARCH + ["-shared", "-o", LIB] + objs + ["-lgomp", "-ccbin", "/usr/bin/g++"])
     return LIB
 
 

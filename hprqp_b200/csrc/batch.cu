@@ -1230,6 +1230,16 @@ int hprqp_batch_solve(hprqp_batch_handle h, const hprqp_params* params, const do
   })
 }
 
+int hprqp_batch_qap_apply(hprqp_batch_handle h, int32_t precision, const double* X, double* Y,
+                          int32_t* tensor_cores) {
+  if (!h || !X || !Y) return HPRQP_E_ARG;
+  BATCH_GUARD(h, {
+    if (!h->qap || hprqp::bqp::count(h->qp) == 0) throw hprqp::Error(HPRQP_E_STATE, "no QAP batch loaded");
+    const int tc = hprqp::bqp::apply_q(h->qp, precision, X, Y);
+    if (tensor_cores) *tensor_cores = tc;
+  })
+}
+
 const char* hprqp_batch_last_error(hprqp_batch_handle h) { return h ? h->err.c_str() : g_batch_err.c_str(); }
 
 int hprqp_batch_destroy(hprqp_batch_handle h) {

@@ -19,6 +19,10 @@ void load(QpBatch* q, int count, const hprqp_problem* problems);
 int count(const QpBatch* q);
 void solve(QpBatch* q, const hprqp_params& p, const double* const* x0s, const double* sig0, hprqp_result* res,
            double* const* xs);
+// Y = Q_k(X_k) for every instance (X, Y concatenated, sum n_k^2 values) in
+// the engine of `precision`; returns 1 when the FP32 engine ran the fused
+// tensor-core operator, 0 for the CUDA-core GEMMs.
+int apply_q(QpBatch* q, int precision, const double* X, double* Y);
 
 }  // namespace bqp
 }  // namespace hprqp

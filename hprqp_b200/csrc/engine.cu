@@ -11,6 +11,7 @@
 #include <type_traits>
 
 #include "engine.cuh"
+#include "qap_gemm.cuh"
 #include "power.cuh"
 #include "tc_gemm.h"
 
@@ -71,7 +72,6 @@ Common::~Common() {
   const double t0 = wall_s();
   if (h_scal) pinned_give(h_scal, sizeof(double) * kNumSlots);
   const double t1 = wall_s();
-  if (cublas) cublasDestroy(cublas);
   if (stream) cudaStreamDestroy(stream);
   if (stream2) cudaStreamDestroy(stream2);
   const double t2 = wall_s();
@@ -835,6 +835,17 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
     qS = upload<V>(cm, mem, hp.qS, N2);
     qT = upload<V>(cm, mem, hp.qT, N2);
     qTmp = mem.alloc<V>(N2);
+    // the one-instance descriptor of the CUDA-core QAP products (k_qap_gemm)
+    const int qn1 = (int)hp.qn;
+    const int64_t off1 = 0;
+    const unsigned char on1 = 1;
+    qap_n_d = mem.alloc<int>(1);
+    qap_off_d = mem.alloc<int64_t>(1);
+    qap_on_d = mem.alloc<unsigned char>(16);
+    cm.to_dev(qap_n_d, &qn1, sizeof(int));
+    cm.to_dev(qap_off_d, &off1, sizeof(int64_t));
+    cm.to_dev(qap_on_d, &on1, 1);
+    HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   }
   Qp = Q;
   if (power_engine) power_setup(pp, tpr_A, tpr_Q);
@@ -867,23 +878,12 @@ void Engine<V>::spmv(const DCsr<V>& M, const V* xin, V* yout, double scale) {
   mat_rows(M, xin, EpiStore<V>{yout, scale});
 }
 
-template <typename V>
-static cublasStatus_t gemm(cublasHandle_t h, int N, double alpha, const V* A, const V* B, double beta, V* C);
-template <>
-cublasStatus_t gemm<double>(cublasHandle_t h, int N, double alpha, const double* A, const double* B,
-                            double beta, double* C) {
-  return cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &alpha, A, N, B, N, &beta, C, N);
-}
-template <>
-cublasStatus_t gemm<float>(cublasHandle_t h, int N, double alpha, const float* A, const float* B, double beta,
-                           float* C) {
-  const float a = (float)alpha, b = (float)beta;
-  return cublasSgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, N, N, N, &a, A, N, B, N, &b, C, N);
-}
-
 // QAP Qmap! (src/Q_operators/QAP_operator.jl:52-61): X = reshape(x, N, N)
-// column-major; TMP = A X; QX = 2 TMP B - 2 S X - 2 X T.  FP64: cuBLAS
-// DGEMM (the reference arithmetic); FP32 phase: the 3xTF32 tcgen05 GEMM.
+// column-major; TMP = A X; QX = 2 TMP B - 2 S X - 2 X T.  FP64: the
+// library's tiled CUDA-core GEMM (k_qap_gemm: TMP, then 2 TMP B - 2 S X -
+// 2 X T as one GEMM over three K segments, FP64 FMAs in a fixed order);
+// FP32 phase: the 3xTF32 tcgen05 GEMM (the same k_qap_gemm in FP32 when
+// HPRQP_QAP_TC=0).
 template <typename V>
 void Engine<V>::qap_apply(const V* xin, V* yout) {
   const int N = (int)std::lround(std::sqrt((double)n));
@@ -898,15 +898,15 @@ void Engine<V>::qap_apply(const V* xin, V* yout) {
       return;
     }
   }
-  auto ck = [](cublasStatus_t s) {
-    if (s != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cuBLAS GEMM failed");
-  };
-  cublasHandle_t hb = cm.blas();
-  ck(gemm<V>(hb, N, 1.0, qA, xin, 0.0, qTmp));
-  ck(gemm<V>(hb, N, 2.0, qTmp, qB, 0.0, yout));
-  ck(gemm<V>(hb, N, -2.0, qS, xin, 1.0, yout));
-  ck(gemm<V>(hb, N, -2.0, xin, qT, 1.0, yout));
-  cm.launches += 4;
+  const int nt = (N + kQT - 1) / kQT;
+  const dim3 g(1, nt * nt);
+  const QapSegs<V, 1> s1{{qA}, {xin}, {V(1)}};
+  k_qap_gemm<V, 1><<<g, 256, 0, cm.stream>>>(qap_n_d, qap_off_d, qap_on_d, s1, V(1), qTmp);
+  HPRQP_LAUNCH_CHECK();
+  const QapSegs<V, 3> s3{{qTmp, qS, xin}, {qB, xin, qT}, {V(1), V(-1), V(-1)}};
+  k_qap_gemm<V, 3><<<g, 256, 0, cm.stream>>>(qap_n_d, qap_off_d, qap_on_d, s3, V(2), yout);
+  HPRQP_LAUNCH_CHECK();
+  cm.launches += 2;
 }
 
 template <typename V>

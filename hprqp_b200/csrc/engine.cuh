@@ -10,7 +10,6 @@
 // that the host reads once per residual check.
 #pragma once
 
-#include <cublas_v2.h>
 
 #include <memory>
 #include <vector>
@@ -47,14 +46,6 @@ struct DeviceMem : PoolBlocks {  // owns blocks of the library's device memory p
 struct Common {  // per-handle resources shared by the engines
   cudaStream_t stream = nullptr;
   cudaStream_t stream2 = nullptr;  // second chain of the power method
-  cublasHandle_t cublas = nullptr;  // created on first use (the dense QAP operator)
-  cublasHandle_t blas() {
-    if (!cublas) {
-      if (cublasCreate(&cublas) != CUBLAS_STATUS_SUCCESS) throw Error(HPRQP_E_CUDA, "cublasCreate failed");
-      cublasSetStream(cublas, stream);
-    }
-    return cublas;
-  }
   double* d_scal = nullptr;
   double* h_scal = nullptr;  // pinned mirror
   ReduceWs rws{}, rws2{};
@@ -94,7 +85,7 @@ struct Common {  // per-handle resources shared by the engines
   // instead, e.g. under a profiler, whose serialisation makes the timings
   // meaningless
   bool autotune = true;
-  bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else cuBLAS SGEMM)
+  bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else the CUDA-core k_qap_gemm)
   DeviceMem mem;
   void init();
   ~Common();
@@ -166,6 +157,9 @@ class Engine {
   void power_setup(const Prepared& pp, int tpr_A, int tpr_Q);
   double *gu0 = nullptr, *gu1 = nullptr;  // the Gram chain's state u_k (FP64 in both engines)
   V *qA = nullptr, *qB = nullptr, *qS = nullptr, *qT = nullptr, *qTmp = nullptr;
+  int* qap_n_d = nullptr;              // one-instance descriptor of k_qap_gemm
+  int64_t* qap_off_d = nullptr;
+  unsigned char* qap_on_d = nullptr;
   float* qws = nullptr;  // TF32 operand images of the tensor-core QAP products
 
   void reset_state();

@@ -45,6 +45,17 @@ int hprqp_batch_load_qap(hprqp_batch_handle h, int32_t count, const hprqp_proble
 int hprqp_batch_solve(hprqp_batch_handle h, const hprqp_params* params, const double* const* initial_x,
                       const double* sigma0, hprqp_result* results, double* const* x_out);
 
+/* Test and measurement hook (no reference counterpart): Y = Q_k(X_k) for
+ * every instance of the loaded QAP family (Qmap!, src/Q_operators/
+ * QAP_operator.jl:52-75), X and Y concatenated in instance order (sum of
+ * n_k^2 values, each block column-major), computed by the batch engine of
+ * `precision`: HPRQP_PRECISION_FP64 runs the CUDA-core FP64 GEMMs,
+ * HPRQP_PRECISION_FP32_POLISH the FP32 phase's operator (the fused 3xTF32
+ * tensor-core kernel when every n_k <= 128).  *tensor_cores (may be NULL)
+ * tells which ran. */
+int hprqp_batch_qap_apply(hprqp_batch_handle h, int32_t precision, const double* X, double* Y,
+                          int32_t* tensor_cores);
+
 const char* hprqp_batch_last_error(hprqp_batch_handle h);
 int hprqp_batch_destroy(hprqp_batch_handle h);
 
