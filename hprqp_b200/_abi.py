@@ -17,7 +17,11 @@ HPRQP_E_UNSUPPORTED = -5
 
 STATUS_NAMES = {0: "OPTIMAL", 1: "MAX_ITER", 2: "TIME_LIMIT", 3: "NUMERICAL_ERROR"}
 
-Q_SPARSE, Q_LASSO, Q_QAP = 0, 1, 2
+Q_SPARSE, Q_LASSO, Q_QAP, Q_CUSTOM = 0, 1, 2, 3
+HPRQP_E_CALLBACK = -6
+
+# int32_t qmap(const void* x, void* Qx, int32_t precision, void* user, void* stream)
+QMAP_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.c_void_p, C.c_int32, C.c_void_p, C.c_void_p)
 PROBLEM_TYPES = {"QP": 0, "LASSO": 1, "QAP": 2}
 PRECISIONS = {"fp64": 0, "fp32_polish": 1}
 

@@ -160,7 +160,26 @@ class Solver:
         check(self._L.hprqp_load(self.h, C.addressof(self._view.struct)), self.h)
         self.model = model
         self._view = None
+        self._qmap_cb = None
+        if model.Q.kind == _abi.Q_CUSTOM:
+            self._bind_qmap(model.Q)
         return self
+
+    def _bind_qmap(self, op):
+        """Bind a CustomQ's device_qmap as the library's hprqp_qmap_fn; the
+        ctypes thunk is kept on the solver for as long as it may be called.
+        An exception in the operator becomes a nonzero return, which stops
+        the solve with HPRQP_E_CALLBACK (the exception is chained to it)."""
+        def thunk(x, qx, precision, user, stream):
+            try:
+                rc = op.device_qmap(x or 0, qx or 0, int(precision), stream or 0)
+                return int(rc or 0)
+            except Exception as e:  # noqa: BLE001 - reported through the return code
+                self._qmap_error = e
+                return -1
+        self._qmap_error = None
+        self._qmap_cb = _abi.QMAP_FN(thunk)
+        check(self._L.hprqp_set_qmap(self.h, self._qmap_cb, None), self.h)
 
     def prepare(self, params: HPRQP_parameters):
         check(self._L.hprqp_prepare(self.h, C.byref(params.to_struct())), self.h)
@@ -192,8 +211,15 @@ class Solver:
         if y0 is not None and len(y0) != m:
             raise ValueError("initial_y has the wrong length")
         r = Result()
-        check(self._L.hprqp_solve(self.h, C.byref(params.to_struct()), _ptr(x0), _ptr(y0), C.byref(r),
-                                  _ptr(x), _ptr(y), _ptr(z), _ptr(w)), self.h)
+        try:
+            check(self._L.hprqp_solve(self.h, C.byref(params.to_struct()), _ptr(x0), _ptr(y0), C.byref(r),
+                                      _ptr(x), _ptr(y), _ptr(z), _ptr(w)), self.h)
+        except Exception as e:
+            err = getattr(self, "_qmap_error", None)
+            if err is not None:
+                self._qmap_error = None
+                raise e from err
+            raise
         out = HPRQP_results()
         for f, _ in Result._fields_:
             if f == "status":

@@ -731,7 +731,7 @@ void Engine<V>::gram_values() {
 template <typename V>
 void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
   gram = false;
-  if (m <= 0 || is_qap || is_lasso || cm.pow_gram == 0 || pp.A.nnz() == 0) return;
+  if (m <= 0 || is_op || is_lasso || cm.pow_gram == 0 || pp.A.nnz() == 0) return;
   const bool force = cm.pow_gram == 1;
   const int64_t nnzA = pp.A.nnz();
   const double t0 = wall_s();
@@ -786,6 +786,8 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   path = path_;
   Q_is_diag = pp.Q_is_diag;
   is_qap = hp.Q_kind == HPRQP_Q_QAP;
+  is_custom = hp.Q_kind == HPRQP_Q_CUSTOM;
+  is_op = is_qap || is_custom;
   is_lasso = hp.Q_kind == HPRQP_Q_LASSO;
   has_Q_sparse = hp.Q_kind == HPRQP_Q_SPARSE;
   b_scale = pp.b_scale;
@@ -886,6 +888,13 @@ void Engine<V>::spmv(const DCsr<V>& M, const V* xin, V* yout, double scale) {
 // HPRQP_QAP_TC=0).
 template <typename V>
 void Engine<V>::qap_apply(const V* xin, V* yout) {
+  if (is_custom) {  // the user's Qmap! (hprqp_set_qmap), on the engine's current stream
+    if (!cm.qmap) throw Error(HPRQP_E_STATE, "custom Q operator: hprqp_set_qmap was not called");
+    const int32_t rc = cm.qmap((const void*)xin, (void*)yout, sizeof(V) == 8 ? 0 : 1, cm.qmap_user, (void*)cm.stream);
+    if (rc != 0) throw Error(HPRQP_E_CALLBACK, "custom Q operator callback returned " + std::to_string(rc));
+    HPRQP_CUDA(cudaGetLastError());
+    return;
+  }
   const int N = (int)std::lround(std::sqrt((double)n));
   if constexpr (std::is_same<V, float>::value) {
     if (cm.tc_qap) {
@@ -914,7 +923,7 @@ void Engine<V>::apply_Q(const V* xin, V* yout) {
   if (is_lasso) {
     spmv(L, xin, ltemp);
     spmv(LT, ltemp, yout);
-  } else if (is_qap) {
+  } else if (is_op) {
     qap_apply(xin, yout);
   } else {
     spmv(Q, xin, yout);
@@ -943,7 +952,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
     HPRQP_BOOL(full, F, HPRQP_BOOL(Q_is_diag, D, {
       EpiZxw1<V, F, D, V> e{Qw, x, x_hat, w_bar, dx, x_bar, z_bar, ATy, c, l, u, w, fact1, fact2, last_x,
                          sigma, f1s, f2s, h1, h2};
-      if (is_qap) {
+      if (is_op) {
         qap_apply(w, Qw);
         rows<V>(cm, 1, n, VecSrc<V>{Qw}, e);
       } else {
@@ -953,7 +962,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
     mark();
     if (m > 0) {
       EpiTempv<V> et{tempv, x_hat, Qw, sigma};
-      if (is_qap) {
+      if (is_op) {
         qap_apply(w_bar, Qw_bar);
         rows<V>(cm, 1, n, VecSrc<V>{Qw_bar}, et);
       } else {
@@ -985,7 +994,7 @@ void Engine<V>::step(bool full, double h1, double h2) {
     mark();
     HPRQP_BOOL(full, F, {
       EpiTempvNoC<V, F, V> e{Qw, tempv, Qw_bar, x_hat, last_Qw, sigma, h1, h2};
-      if (is_qap) {
+      if (is_op) {
         qap_apply(w_bar, Qw_bar);
         rows<V>(cm, 1, n, VecSrc<V>{Qw_bar}, e);
       } else {
@@ -1027,7 +1036,7 @@ double Engine<V>::power_step_bytes(int which) const {
   auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
   if (which == 0 && gram) return csr(G) + 2.0 * n * 8.0;  // FP64 state
   if (which == 0) return m > 0 ? csr(AT) + csr(A) + 2.0 * n * v + 3.0 * m * v : 0.0;
-  if (is_qap) return 0.0;
+  if (is_op) return 0.0;
   if (is_lasso) return csr(L) + csr(LT) + 2.0 * L.rows * v + 3.0 * n * v;
   // the chunk-fold Q chain reads and writes an FP64 state
   return csr(Q) + 2.0 * n * (cm.pow_chunk_fold ? 8.0 : v);
@@ -1052,8 +1061,8 @@ void Engine<V>::pass_info(int k, const char** name, double* bytes, int* tpr) con
     else { *name = "lasso2 A_d'*t+prox"; *bytes = csr(LT) + L.rows * v + 3 * N * v + 2 * N * d + 4 * N * v; *tpr = sched(LT); }
     return;
   }
-  const double cq = is_qap ? 0.0 : csr(Q);
-  const int tq = is_qap ? 1 : sched(Q);
+  const double cq = is_op ? 0.0 : csr(Q);
+  const int tq = is_op ? 1 : sched(Q);
   if (path == PATH_QP) {
     if (k == 0) { *name = "zxw1 Q*w"; *bytes = cq + N * v + 5 * N * v + N * d + dg + 4 * N * v; *tpr = tq; }
     else if (m > 0 && k == 1) { *name = "tempv Q*w_bar"; *bytes = cq + N * v + 2 * N * v + N * v; *tpr = tq; }
@@ -1399,7 +1408,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   const cudaStream_t main = cm.stream;
   const ReduceWs main_ws = cm.rws;
   // the QAP operator's cuBLAS calls are bound to the main stream: one stream then
-  const cudaStream_t qst = is_qap ? main : cm.stream2;
+  const cudaStream_t qst = is_op ? main : cm.stream2;
   Chain ca{want_A && m > 0, 0, pz, pq, pt, cm.d_scal + S_POW, cm.d_scal + S_POWLOG, cm.rws, main, m, 1.0, -1};
   Chain cq{want_Q, 1, pz2, pq2, pt2, cm.d_scal + S_POW_Q, cm.d_scal + S_POWLOG_Q, cm.rws2, qst, n, 1.0, -1};
   auto use = [&](const Chain& c, cudaStream_t st) {
@@ -1420,7 +1429,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
     reduce<1, 0u, double>(cm, 1, c->len, ZeroSrc{}, EpiSumSq<V>{c->z0}, c->scal + 2, InvNormFin{c->scal + 4});
     restore();
   }
-  if (cm.pow_persistent && !is_qap && power_persistent(ca.on, cq.on, tol, max_it, lamA_out, lamQ_out, itA, itQ))
+  if (cm.pow_persistent && !is_op && power_persistent(ca.on, cq.on, tol, max_it, lamA_out, lamQ_out, itA, itQ))
     return;
   // HPRQP_POWER_ELL=1: the chained steps use ELL wherever the matrix has an
   // ELL copy (its reduction keeps 4 rows per thread in flight); measured
@@ -1444,7 +1453,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   // renormalises the state (kernels.cuh).  The other chains keep the
   // per-step fold.
   const bool cfA = cm.pow_chunk_fold && use_gram;
-  const bool cfQ = cm.pow_chunk_fold && cq.on && has_Q_sparse && !is_lasso && !is_qap;
+  const bool cfQ = cm.pow_chunk_fold && cq.on && has_Q_sparse && !is_lasso && !is_op;
   const int nblkA = cfA ? partials_grid(cm, G) : 0, nblkQ = cfQ ? partials_grid(cm, pQ) : 0;
   if ((cfA || cfQ) && !pow_cf_part) {
     // one region per chain, each kPowChunk steps x (at most reduce_cap CTAs) x 3 sums
@@ -1527,7 +1536,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
       } else {
         mat_reduce<3, 0u>(cm, pLT, ltemp2, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
       }
-    } else if (is_qap) {
+    } else if (is_op) {
       elem(cm, n, ScaleInvNorm<V>{c.t, zc, zz});
       qap_apply(c.t, zn);
       reduce<3, 0u, double>(cm, 1, n, VecSrc<V>{zn}, EpiPowerFused<V>{zc, zn, zz, false, inv}, c.scal + 1, fin);
@@ -1587,7 +1596,7 @@ void Engine<V>::power_both(bool want_A, bool want_Q, double tol, int max_it, dou
   while (it < max_it && ((ca.on && ca.found < 0) || (cq.on && cq.found < 0))) {
     const bool doA = ca.on && ca.found < 0, doQ = cq.on && cq.found < 0;
     const int gi = (doA ? 1 : 0) | (doQ ? 2 : 0);
-    if (is_qap) {
+    if (is_op) {
       issue_chunk(doA, doQ);  // cuBLAS inside: run eagerly
     } else {
       if (!graphs[gi]) {

@@ -85,6 +85,8 @@ struct Common {  // per-handle resources shared by the engines
   // instead, e.g. under a profiler, whose serialisation makes the timings
   // meaningless
   bool autotune = true;
+  hprqp_qmap_fn qmap = nullptr;  // a custom Q operator's callback (HPRQP_Q_CUSTOM)
+  void* qmap_user = nullptr;
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else the CUDA-core k_qap_gemm)
   DeviceMem mem;
   void init();
@@ -118,6 +120,8 @@ class Engine {
   int64_t n, m;
   int path;
   bool Q_is_diag, has_Q_sparse, is_qap, is_lasso;
+  bool is_custom = false;  // Q through the user's callback
+  bool is_op = false;      // an operator Q applied as a whole product (QAP or custom)
   double b_scale, c_scale, norm_b_org, norm_c_org;
   double sigma = 1.0, lamA = 0.0, lamQ = 0.0;
   double lam_l1 = 0.0;   // lambda in the L1 objective term (problem_type LASSO)

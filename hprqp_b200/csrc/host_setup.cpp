@@ -322,6 +322,8 @@ void load_problem(const hprqp_problem* pr, HostProblem& hp) {
     h.qB = copy_vec(pr->qap_B, N * N, "QAP B", false);
     h.qS = copy_vec(pr->qap_S, N * N, "QAP S", false);
     h.qT = copy_vec(pr->qap_T, N * N, "QAP T", false);
+  } else if (h.Q_kind == HPRQP_Q_CUSTOM) {
+    // the operator is bound afterwards by hprqp_set_qmap
   } else {
     throw Error(HPRQP_E_ARG, "unknown Q_kind");
   }

@@ -392,7 +392,8 @@ static void prepare(Handle& H, const hprqp_params& p) {
   else
     prepare_problem(H.hp, p, H.pp);
   if (H.hp.Q_kind == HPRQP_Q_LASSO) H.path = PATH_LASSO;
-  else if (H.hp.Q_kind == HPRQP_Q_QAP || H.pp.Q.nnz() > 0) H.path = H.pp.noC ? PATH_NOC : PATH_QP;
+  else if (H.hp.Q_kind == HPRQP_Q_QAP || H.hp.Q_kind == HPRQP_Q_CUSTOM || H.pp.Q.nnz() > 0)
+    H.path = H.pp.noC ? PATH_NOC : PATH_QP;
   else H.path = PATH_LP;
   // the power method runs on the first phase's engine: only that one builds
   // the Gram matrix of the A A' chain
@@ -822,6 +823,8 @@ int hprqp_load(hprqp_handle h, const hprqp_problem* prob) {
     h->prepared = false;
     h->e64.reset();
     h->e32.reset();
+    h->cm->qmap = nullptr;  // a custom operator is bound per loaded problem
+    h->cm->qmap_user = nullptr;
     hprqp::load_problem(prob, h->hp);
   })
 }
@@ -857,6 +860,17 @@ int hprqp_set_trace(hprqp_handle h, int64_t iters, double* x_trace, double* y_tr
   h->yt = y_trace;
   h->wt = w_trace;
   return HPRQP_OK;
+}
+
+int hprqp_set_qmap(hprqp_handle h, hprqp_qmap_fn qmap, void* user) {
+  if (!h) return HPRQP_E_ARG;
+  HPRQP_GUARD(h, {
+    if (!h->hp.loaded || h->hp.Q_kind != HPRQP_Q_CUSTOM)
+      throw hprqp::Error(HPRQP_E_STATE, "hprqp_set_qmap: load a problem with Q_kind = HPRQP_Q_CUSTOM first");
+    if (!qmap) throw hprqp::Error(HPRQP_E_ARG, "hprqp_set_qmap: null callback");
+    h->cm->qmap = qmap;
+    h->cm->qmap_user = user;
+  })
 }
 
 int hprqp_set_trace_scalars(hprqp_handle h, double* sigma_trace, int64_t* inner_trace) {

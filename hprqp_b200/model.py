@@ -13,7 +13,7 @@ from dataclasses import dataclass, field
 import numpy as np
 import scipy.sparse as sp
 
-from ._abi import Q_LASSO, Q_QAP, Q_SPARSE
+from ._abi import Q_CUSTOM, Q_LASSO, Q_QAP, Q_SPARSE
 
 
 # ---------------------------------------------------------------------------
@@ -38,6 +38,40 @@ class AbstractQOperatorCPU:
 
     def Qmap(self, x: np.ndarray) -> np.ndarray:
         raise NotImplementedError
+
+
+@dataclass
+class CustomQ(AbstractQOperatorCPU):
+    """A user's Q operator on the GPU: the Python side of the library's
+    device-callback operator (hprqp_set_qmap; the reference's custom
+    AbstractQOperator with its own Qmap!, src/Q_operators/
+    Q_operator_interface.jl:33-92).
+
+    `device_qmap(x_ptr, qx_ptr, precision, stream_ptr)` computes Qx = Q x
+    for n-vectors in device memory (float64 when precision == 0, float32
+    when 1) and enqueues its work on the CUDA stream `stream_ptr`; it must
+    not change x, and it returns 0 (or raises / returns nonzero to stop the
+    solve).  `host_qmap(x)` (optional) is the same product on numpy arrays,
+    for checks on the host."""
+    n_vars: int
+    device_qmap: object
+    host_qmap: object = None
+    name: str = "Custom"
+    kind: int = Q_CUSTOM
+
+    def get_problem_size(self):
+        return self.n_vars
+
+    def get_temp_size(self):
+        return 0
+
+    def get_operator_name(self):
+        return self.name
+
+    def Qmap(self, x):
+        if self.host_qmap is None:
+            raise NotImplementedError("this custom operator has no host Qmap")
+        return self.host_qmap(x)
 
 
 @dataclass

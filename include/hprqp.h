@@ -43,6 +43,7 @@ extern "C" {
 #define HPRQP_E_OOM         -3   /* device allocation failed                        */
 #define HPRQP_E_STATE       -4   /* call order (solve before load, ...)             */
 #define HPRQP_E_UNSUPPORTED -5   /* option the library does not implement           */
+#define HPRQP_E_CALLBACK    -6   /* the custom Q operator's callback returned nonzero */
 
 /* ---- solver status (reference strings, src/algorithm.jl:558-576) --------- */
 #define HPRQP_STATUS_OPTIMAL          0   /* "OPTIMAL"          */
@@ -54,6 +55,7 @@ extern "C" {
 #define HPRQP_Q_SPARSE 0   /* explicit sparse Q (may have 0 nonzeros: LP)      */
 #define HPRQP_Q_LASSO  1   /* implicit Q = A_d' A_d  (LASSO_operator.jl)       */
 #define HPRQP_Q_QAP    2   /* implicit Q(X) = 2(A X B - S X - X T) (QAP_operator.jl) */
+#define HPRQP_Q_CUSTOM 3   /* user operator: Q x through a device callback (hprqp_set_qmap) */
 
 /* ---- problem_type (reference params.problem_type string) ----------------- */
 #define HPRQP_PROBLEM_QP    0
@@ -98,6 +100,7 @@ typedef struct hprqp_problem {
     const int32_t* L_rowval;
     const double*  L_nzval;
     /* HPRQP_Q_QAP: dense n_qap x n_qap column-major A, B, S, T; n = n_qap^2   */
+    /* HPRQP_Q_CUSTOM: no Q data here; the operator comes from hprqp_set_qmap */
     int64_t qap_n;
     const double* qap_A;
     const double* qap_B;
@@ -253,6 +256,26 @@ int hprqp_profile_iterations(hprqp_handle h, const hprqp_params* params, int64_t
  * params.profile_passes = 1: one hprqp_pass_stats per engine precision
  * (fp64, fp32; npass = 0 when that engine did not run). */
 int hprqp_get_pass_stats(hprqp_handle h, hprqp_pass_stats* fp64, hprqp_pass_stats* fp32);
+
+/* A user's Q operator (an AbstractQOperator with its own Qmap!,
+ * src/Q_operators/Q_operator_interface.jl:33-92): Qx = Q x for n-vectors in
+ * device memory, FP64 (precision 0: x, Qx are double*) or FP32 (precision 1:
+ * float*, the FP32 phase of HPRQP_PRECISION_FP32_POLISH), enqueued on
+ * `stream` (a cudaStream_t); x must not be changed.  The library calls it
+ * from the solving thread wherever the method applies Q: twice per HPR
+ * iteration on the QP path, in the residuals, the M-norm and the sigma
+ * update, and in every step of the power method on Q (give
+ * lambda_max_Q_override to skip that).  Returns 0, or nonzero to stop the
+ * solve with HPRQP_E_CALLBACK.  As for the reference's operators, Q must be
+ * symmetric positive semidefinite, and an operator Q gets no scaling
+ * (src/utils.jl:364-406). */
+typedef int32_t (*hprqp_qmap_fn)(const void* x, void* Qx, int32_t precision, void* user, void* stream);
+
+/* Bind the Q operator of a loaded HPRQP_Q_CUSTOM problem (replaces the
+ * reference's to_gpu + Qmap! of a custom operator type); `user` is passed
+ * back to every call.  Must follow hprqp_load and precede hprqp_prepare /
+ * hprqp_solve of that problem; hprqp_load drops the binding. */
+int hprqp_set_qmap(hprqp_handle h, hprqp_qmap_fn qmap, void* user);
 
 /* lambda_max(A A') by the power method, for a CSR matrix A (m x n, int32,
  * 0-based) and its transpose A' (n x m) that the caller already holds in

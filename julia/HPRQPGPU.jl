@@ -21,7 +21,8 @@ using SparseArrays
 
 const libhprqp = get(ENV, "HPRQP_LIB", joinpath(@__DIR__, "..", "hprqp_b200", "libhprqp.so"))
 
-const Q_SPARSE, Q_LASSO, Q_QAP = Int32(0), Int32(1), Int32(2)
+const Q_SPARSE, Q_LASSO, Q_QAP, Q_CUSTOM = Int32(0), Int32(1), Int32(2), Int32(3)
+const E_CALLBACK = -6
 const STATUS = Dict(0 => "OPTIMAL", 1 => "MAX_ITER", 2 => "TIME_LIMIT", 3 => "NUMERICAL_ERROR")
 
 # mirrors `hprqp_problem`
@@ -128,6 +129,46 @@ function _results_type()
     return getfield(parent, :HPRQP_results)
 end
 
+# ---------------------------------------------------------------------------
+# Custom Q operators (the reference's AbstractQOperatorCPU / AbstractQOperator
+# with their own to_gpu and Qmap!, src/Q_operators/Q_operator_interface.jl:
+# 33-92) cross the C ABI as a device callback (hprqp_set_qmap).  Their Qmap!
+# works on CuVectors, so this path uses CUDA.jl, which the enclosing module
+# HPRQP already loads; the built-in operators need no CUDA.jl.
+# ---------------------------------------------------------------------------
+_parent(name) = getfield(parentmodule(@__MODULE__), name)
+
+mutable struct QmapCtx
+    Qgpu::Any   # to_gpu(Q_cpu) of the user's operator
+    n::Int
+    err::Any    # an exception raised inside the callback, rethrown by solve_gpu
+end
+
+# hprqp_qmap_fn: Qx = Q x on n-vectors in device memory, precision 0 = Float64,
+# 1 = Float32 (the FP32 phase), ordered after the library's stream.
+function qmap_thunk(x::Ptr{Cvoid}, Qx::Ptr{Cvoid}, precision::Int32, user::Ptr{Cvoid}, stream::Ptr{Cvoid})::Int32
+    ctx = unsafe_pointer_to_objref(user)::QmapCtx
+    try
+        CU = _parent(:CUDA)
+        CU.cuStreamSynchronize(reinterpret(CU.CUstream, stream))  # the library's writes of x are done
+        T = precision == 0 ? Float64 : Float32
+        xv = unsafe_wrap(CU.CuArray, CU.CuPtr{T}(UInt(x)), ctx.n)
+        yv = unsafe_wrap(CU.CuArray, CU.CuPtr{T}(UInt(Qx)), ctx.n)
+        if T === Float64
+            _parent(:Qmap!)(xv, yv, ctx.Qgpu)
+        else  # the reference's operators compute in Float64
+            y64 = CU.zeros(Float64, ctx.n)
+            _parent(:Qmap!)(Float64.(xv), y64, ctx.Qgpu)
+            yv .= Float32.(y64)
+        end
+        CU.synchronize()  # Qx is complete before the library's next kernel reads it
+        return Int32(0)
+    catch e
+        ctx.err = e
+        return Int32(-1)
+    end
+end
+
 """
     solve_gpu(model::QP_info_cpu, params::HPRQP_parameters) -> HPRQP_results
 
@@ -147,6 +188,7 @@ function solve_gpu(model, params; results_type = _results_type())
     lm = 0; Lcp = Lrv = Ptr{Int32}(0); Lnz = Ptr{Float64}(0)
     qn = 0; qA = qB = qS = qT = Ptr{Float64}(0)
     Q = model.Q
+    qctx = nothing
     if Q isa SparseMatrixCSC
         a, b = i32(Q.colptr), i32(Q.rowval); push!(keep, a, b, Q.nzval)
         Qcp, Qrv, Qnz = pointer(a), pointer(b), pointer(Q.nzval)
@@ -158,8 +200,10 @@ function solve_gpu(model, params; results_type = _results_type())
         Qk = Q_QAP
         push!(keep, Q.A, Q.B, Q.S, Q.T)
         qn = Q.n; qA, qB, qS, qT = pointer(Q.A), pointer(Q.B), pointer(Q.S), pointer(Q.T)
-    else
-        error("custom Q operators need the device-callback ABI (not provided)")
+    else  # a custom operator: its GPU form and the callback that applies it
+        Qk = Q_CUSTOM
+        qctx = QmapCtx(_parent(:to_gpu)(Q), n, nothing)
+        push!(keep, qctx)
     end
     x = zeros(n); y = zeros(m); z = zeros(n); w = zeros(n)
     res = CResult()
@@ -172,13 +216,22 @@ function solve_gpu(model, params; results_type = _results_type())
         check(ccall((:hprqp_create, libhprqp), Cint, (Ref{Ptr{Cvoid}}, Int32), h, params.device_number), C_NULL)
         try
             check(ccall((:hprqp_load, libhprqp), Cint, (Ptr{Cvoid}, Ref{CProblem}), h[], prob), h[])
+            if Qk == Q_CUSTOM
+                fn = @cfunction(qmap_thunk, Int32, (Ptr{Cvoid}, Ptr{Cvoid}, Int32, Ptr{Cvoid}, Ptr{Cvoid}))
+                check(ccall((:hprqp_set_qmap, libhprqp), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}),
+                            h[], fn, pointer_from_objref(qctx)), h[])
+            end
             x0 = params.initial_x === nothing ? C_NULL : pointer(params.initial_x)
             y0 = params.initial_y === nothing ? C_NULL : pointer(params.initial_y)
             GC.@preserve params begin
-                check(ccall((:hprqp_solve, libhprqp), Cint,
-                            (Ptr{Cvoid}, Ref{CParams}, Ptr{Float64}, Ptr{Float64}, Ref{CResult},
-                             Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
-                            h[], cparams(params), x0, y0, res, x, y, z, w), h[])
+                rc = ccall((:hprqp_solve, libhprqp), Cint,
+                           (Ptr{Cvoid}, Ref{CParams}, Ptr{Float64}, Ptr{Float64}, Ref{CResult},
+                            Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}),
+                           h[], cparams(params), x0, y0, res, x, y, z, w)
+                if rc == E_CALLBACK && Qk == Q_CUSTOM && qctx.err !== nothing
+                    throw(qctx.err)  # the user's Qmap! failed: its own exception
+                end
+                check(rc, h[])
             end
         finally
             ccall((:hprqp_destroy, libhprqp), Cint, (Ptr{Cvoid},), h[])

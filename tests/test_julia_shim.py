@@ -5,6 +5,8 @@ here, so the file is checked as text):
    hprqp_problem, hprqp_params and hprqp_result in include/hprqp.h, in the
    same order and with matching types (a mismatch would corrupt every
    ccall);
+ - a custom operator (the reference's AbstractQOperator with its own Qmap!)
+   is bound through hprqp_set_qmap with a callback of the header's type;
  - solve_gpu builds and returns the reference's own HPRQP_results and fills
    every one of its fields (src/structs.jl:292-309), so that MOI.optimize!,
    which stores the result in a Union{Nothing,HPRQP_results} field
@@ -74,5 +76,11 @@ def test_solve_gpu_returns_reference_results_type():
     assert assigned == HPRQP_RESULTS_FIELDS, assigned
     # the default type is the reference's HPRQP_results of the enclosing module
     assert "getfield(parent, :HPRQP_results)" in src
+    # custom operators: the callback has the header's hprqp_qmap_fn signature
+    assert "@cfunction(qmap_thunk, Int32, (Ptr{Cvoid}, Ptr{Cvoid}, Int32, Ptr{Cvoid}, Ptr{Cvoid}))" in src
+    assert "hprqp_set_qmap" in src and 'error("custom Q operators' not in src
+    hdr = open(HDR).read()
+    assert ("typedef int32_t (*hprqp_qmap_fn)(const void* x, void* Qx, int32_t precision, void* user, "
+            "void* stream);") in hdr
     # statuses are the reference strings (src/algorithm.jl:558-576)
     assert '0 => "OPTIMAL"' in src and '1 => "MAX_ITER"' in src and '2 => "TIME_LIMIT"' in src
