@@ -16,7 +16,7 @@ LIB_PATH = os.path.join(HERE, "libhprqp.so")
 
 # Every entry point declared in include/hprqp.h
 EXPORTS = ("hprqp_abi_info", "hprqp_default_params", "hprqp_create", "hprqp_load", "hprqp_prepare",
-           "hprqp_solve", "hprqp_set_trace", "hprqp_set_trace_scalars", "hprqp_set_qmap", "hprqp_profile_iterations", "hprqp_get_pass_stats",
+           "hprqp_solve", "hprqp_set_save_file", "hprqp_solve_resume", "hprqp_set_trace", "hprqp_set_trace_scalars", "hprqp_set_qmap", "hprqp_profile_iterations", "hprqp_get_pass_stats",
            "hprqp_power_lambda_noalloc", "hprqp_gemm_3xtf32", "hprqp_gemm_3xtf32_ws_floats",
            "hprqp_gemm_3xtf32_ws", "hprqp_last_error", "hprqp_destroy")
 
@@ -52,6 +52,10 @@ def load():
     L.hprqp_solve.restype = C.c_int
     L.hprqp_set_trace.argtypes = [vp, C.c_int64, vp, vp, vp]
     L.hprqp_set_trace.restype = C.c_int
+    L.hprqp_set_save_file.argtypes = [vp, C.c_char_p]
+    L.hprqp_set_save_file.restype = C.c_int
+    L.hprqp_solve_resume.argtypes = [vp, C.POINTER(Params), C.c_char_p, C.POINTER(Result), vp, vp, vp, vp]
+    L.hprqp_solve_resume.restype = C.c_int
     L.hprqp_set_trace_scalars.argtypes = [vp, vp, vp]
     from ._abi import QMAP_FN
     L.hprqp_set_qmap.argtypes = [vp, QMAP_FN, vp]

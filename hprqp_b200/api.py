@@ -45,7 +45,7 @@ class HPRQP_parameters:
     initial_x: np.ndarray | None = None
     initial_y: np.ndarray | None = None
     auto_save: bool = False
-    save_filename: str = "hprqp_autosave.h5"
+    save_filename: str = "hprqp_autosave.ckpt"
     verbose: bool = True
     use_gpu: bool = True
     # extensions
@@ -201,6 +201,14 @@ class Solver:
         return self._strace
 
     def solve(self, params: HPRQP_parameters) -> HPRQP_results:
+        return self._run(params, None)
+
+    def resume(self, params: HPRQP_parameters, path: str) -> HPRQP_results:
+        """Continue a solve of the loaded model from a checkpoint that
+        params.auto_save wrote (hprqp_solve_resume)."""
+        return self._run(params, path)
+
+    def _run(self, params, resume_path):
         model = self.model
         n, m = model.n, model.m
         x, y, z, w = np.zeros(n), np.zeros(m), np.zeros(n), np.zeros(n)
@@ -210,10 +218,17 @@ class Solver:
             raise ValueError("initial_x has the wrong length")
         if y0 is not None and len(y0) != m:
             raise ValueError("initial_y has the wrong length")
+        if params.auto_save:
+            check(self._L.hprqp_set_save_file(self.h, str(params.save_filename).encode()), self.h)
         r = Result()
         try:
-            check(self._L.hprqp_solve(self.h, C.byref(params.to_struct()), _ptr(x0), _ptr(y0), C.byref(r),
-                                      _ptr(x), _ptr(y), _ptr(z), _ptr(w)), self.h)
+            if resume_path is None:
+                rc = self._L.hprqp_solve(self.h, C.byref(params.to_struct()), _ptr(x0), _ptr(y0), C.byref(r),
+                                         _ptr(x), _ptr(y), _ptr(z), _ptr(w))
+            else:
+                rc = self._L.hprqp_solve_resume(self.h, C.byref(params.to_struct()), str(resume_path).encode(),
+                                                C.byref(r), _ptr(x), _ptr(y), _ptr(z), _ptr(w))
+            check(rc, self.h)
         except Exception as e:
             err = getattr(self, "_qmap_error", None)
             if err is not None:

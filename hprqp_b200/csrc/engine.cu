@@ -1277,6 +1277,34 @@ void Engine<V>::trace_copy(double* xt, double* yt, double* wt) {
   out(w, n, stage_n, wt);
 }
 
+template <typename V>
+void Engine<V>::vec_to_host(const V* src, int64_t len, double* dst) {
+  if (!dst || len <= 0) return;
+  double* stage = len <= n ? stage_n : stage_m;
+  if (len > std::max(n, m)) throw Error(HPRQP_E_ARG, "vec_to_host: length beyond the staging buffers");
+  elem(cm, len, CastCopy<double, V>{stage, src});
+  cm.to_host(dst, stage, sizeof(double) * len);
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+}
+
+template <typename V>
+void Engine<V>::vec_from_host(V* dst, const double* src, int64_t len) {
+  if (!src || len <= 0) return;
+  double* stage = len <= n ? stage_n : stage_m;
+  if (len > std::max(n, m)) throw Error(HPRQP_E_ARG, "vec_from_host: length beyond the staging buffers");
+  cm.to_dev(stage, src, sizeof(double) * len);
+  elem(cm, len, CastCopy<V, double>{dst, stage});
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+}
+
+template <typename V>
+void Engine<V>::bars_to_device(double* xb, double* yb, double* zb, double* wb) {
+  elem(cm, n, CastCopy<double, V>{xb, x_bar});
+  elem(cm, n, CastCopy<double, V>{zb, z_bar});
+  elem(cm, n, CastCopy<double, V>{wb, w_bar});
+  if (m > 0) elem(cm, m, CastCopy<double, V>{yb, y_bar});
+}
+
 // ---------------------------------------------------------------------------
 // Power method (src/utils.jl:1335-1461).  One power step is one fused kernel
 // for a sparse Q (the product, z_next, and the q.z / z.z / q.q sums), two

@@ -177,6 +177,11 @@ class Engine {
   void initial_points(const double* x0, const double* y0);
   void collect(double* x_out, double* y_out, double* z_out, double* w_out);
   void trace_copy(double* xt, double* yt, double* wt);
+  // checkpoint helpers: a state vector to / from FP64 host memory (exact:
+  // every V value is a double), and the bar iterates into FP64 device copies
+  void vec_to_host(const V* src, int64_t len, double* dst);
+  void vec_from_host(V* dst, const double* src, int64_t len);
+  void bars_to_device(double* xb, double* yb, double* zb, double* wb);
   // Both power methods (A A' and Q) at once, on two streams; want_* select
   // which run.  Returns lambda estimates (not yet times eig_factor).
   void power_both(bool want_A, bool want_Q, double tol, int max_it, double* lamA_out, double* lamQ_out,

@@ -8,6 +8,7 @@
 // sigma blend and the scalar golden-section search (src/kernels.jl:1453-1486)
 // run on the host from those scalars.
 #include <chrono>
+#include <ctime>
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -17,6 +18,7 @@
 #include <memory>
 #include <string>
 
+#include "checkpoint.h"
 #include "engine.cuh"
 
 namespace hprqp {
@@ -86,9 +88,20 @@ struct LoopState {
   int stall = 0;
   bool force_residuals = false;
   int status = -1;
+  bool skip_checks_once = false;  // resume: the checkpoint's checks are done, run its step
 };
 
 constexpr int kSwitch = -100;
+
+// The best bar iterates so far (ws.saved_state, src/algorithm.jl:97-113),
+// kept on the device in FP64 while params.auto_save is set.
+struct SavedBest {
+  double *x = nullptr, *y = nullptr, *z = nullptr, *w = nullptr;
+  int64_t cap_n = 0, cap_m = 0;
+  double sigma = 0.0;
+  int64_t iter = 0;
+  double err_Rp = kInf, err_Rd = kInf, pobj = kInf, dobj = kInf, gap = kInf;
+};
 
 // Live per-pass timing: a pool of event sets, one set (npass + 1 marks) per
 // recorded plain iteration, harvested after each residual synchronisation.
@@ -175,6 +188,9 @@ struct Handle {
   std::string err;
   int64_t trace_iters = 0;
   double *xt = nullptr, *yt = nullptr, *wt = nullptr;
+  std::string save_file = "hprqp_autosave.ckpt";  // auto-save target (hprqp_set_save_file)
+  SavedBest best;
+  std::vector<double> init_x, init_y;  // the call's initial points (for the checkpoint's parameters/)
   double* sig_t = nullptr;    // sigma of each traced iteration
   int64_t* inner_t = nullptr; // inner (Halpern) counter of each traced iteration
   double setup_time = 0.0;
@@ -182,6 +198,161 @@ struct Handle {
   PassProfiler prof64, prof32;
   hprqp_pass_stats stats64{}, stats32{};
 };
+
+// A fingerprint of the loaded problem's data (FNV-1a over its arrays), so a
+// checkpoint is only resumed on the problem it was written for.
+static double problem_fingerprint(const HostProblem& hp) {
+  uint64_t h = 1469598103934665603ULL;
+  auto mix = [&](const void* p, size_t bytes) {
+    const unsigned char* b = (const unsigned char*)p;
+    for (size_t i = 0; i < bytes; ++i) h = (h ^ b[i]) * 1099511628211ULL;
+  };
+  auto vec = [&](const std::vector<double>& v) { mix(v.data(), sizeof(double) * v.size()); };
+  auto csr = [&](const HCsr& M) {
+    mix(M.ptr.data(), sizeof(int) * M.ptr.size());
+    mix(M.col.data(), sizeof(int) * M.col.size());
+    vec(M.val);
+  };
+  mix(&hp.n, 8);
+  mix(&hp.m, 8);
+  mix(&hp.Q_kind, sizeof(hp.Q_kind));
+  vec(hp.c); vec(hp.AL); vec(hp.AU); vec(hp.l); vec(hp.u);
+  csr(hp.A); csr(hp.Q); csr(hp.L);
+  vec(hp.qA); vec(hp.qB); vec(hp.qS); vec(hp.qT);
+  return (double)(h >> 11);  // exact in a double
+}
+
+static const char* problem_type_name(int t) { return t == HPRQP_PROBLEM_LASSO ? "LASSO" : t == HPRQP_PROBLEM_QAP ? "QAP" : "QP"; }
+
+// save_state_to_hdf5! (src/algorithm.jl:183-301): the current and the best
+// bar iterates unscaled as collect_results! does, their residuals, sigma and
+// the parameters, under the reference's dataset names (the z of the file
+// keeps the reference's c_scale * z_bar / col_norm, unlike collect_results!,
+// src/algorithm.jl:213 against :640), plus the resume/ section: the scaled
+// state the next step reads (x, w, y, A'y and the Halpern anchors; Qw on the
+// QP-noC path), sigma, the lambda_max values and the restart and loop
+// records.  A failed write warns (verbose) and the solve goes on, as in the
+// reference.
+template <typename V>
+static void save_checkpoint(Handle& H, Engine<V>& E, const hprqp_params& p, const LoopState& L, int status,
+                            bool fp32_phase) {
+  const int64_t n = E.n, m = E.m;
+  const double bs = E.b_scale, cs = E.c_scale;
+  std::vector<double> cn(n), rn(m), xb(n), zb(n), wb(n), yb(m), v(std::max(n, m));
+  E.vec_to_host(E.col_norm, n, cn.data());
+  if (m > 0) E.vec_to_host(E.row_norm, m, rn.data());
+  E.vec_to_host(E.x_bar, n, xb.data());
+  E.vec_to_host(E.z_bar, n, zb.data());
+  E.vec_to_host(E.w_bar, n, wb.data());
+  if (m > 0) E.vec_to_host(E.y_bar, m, yb.data());
+  ck::Writer w;
+  auto org = [&](const std::string& name, const std::vector<double>& s, const std::vector<double>& nrm, double sc,
+                 int64_t len) {
+    for (int64_t i = 0; i < len; ++i) v[i] = sc * (s[i] / nrm[i]);
+    w.f64(name, v.data(), len);
+  };
+  char stamp[32];
+  const std::time_t now = std::time(nullptr);
+  std::strftime(stamp, sizeof(stamp), "%Y-%m-%dT%H:%M:%S", std::localtime(&now));
+  w.i64("current/iteration", L.iter);
+  w.f64("current/time_elapsed", now_s() - L.t0);
+  w.str("current/timestamp", stamp);
+  org("current/x_org", xb, cn, bs, n);
+  org("current/w_org", wb, cn, bs, n);
+  if (m > 0) org("current/y_org", yb, rn, cs, m);
+  org("current/z_org", zb, cn, cs, n);
+  w.f64("current/sigma", E.sigma);
+  w.f64("current/err_Rp", L.res.err_Rp);
+  w.f64("current/err_Rd", L.res.err_Rd);
+  w.f64("current/primal_obj", L.res.pobj);
+  w.f64("current/dual_obj", L.res.dobj);
+  w.f64("current/rel_gap", L.res.gap);
+  w.f64("current/KKTx_and_gap", L.res.KKT);
+  const SavedBest& B = H.best;
+  auto down = [&](const double* d, int64_t len, std::vector<double>& h) {
+    if (len > 0) HPRQP_CUDA(cudaMemcpyAsync(h.data(), d, sizeof(double) * len, cudaMemcpyDeviceToHost, H.cm->stream));
+  };
+  down(B.x, n, xb);
+  down(B.z, n, zb);
+  down(B.w, n, wb);
+  if (m > 0) down(B.y, m, yb);
+  HPRQP_CUDA(cudaStreamSynchronize(H.cm->stream));
+  H.cm->d2h += (int64_t)sizeof(double) * (3 * n + m);
+  org("best/x_org", xb, cn, bs, n);
+  org("best/w_org", wb, cn, bs, n);
+  if (m > 0) org("best/y_org", yb, rn, cs, m);
+  org("best/z_org", zb, cn, cs, n);
+  w.f64("best/sigma", B.sigma);
+  w.i64("best/iteration", B.iter);
+  w.f64("best/err_Rp", B.err_Rp);
+  w.f64("best/err_Rd", B.err_Rd);
+  w.f64("best/primal_obj", B.pobj);
+  w.f64("best/dual_obj", B.dobj);
+  w.f64("best/rel_gap", B.gap);
+  w.f64("best/KKTx_and_gap", std::max(std::max(B.err_Rp, B.err_Rd), B.gap));
+  w.f64("parameters/stoptol", p.stoptol);
+  w.f64("parameters/sigma", p.sigma);
+  w.i64("parameters/max_iter", p.max_iter);
+  w.i64("parameters/sigma_fixed", p.sigma_fixed);
+  w.f64("parameters/time_limit", p.time_limit);
+  w.f64("parameters/eig_factor", p.eig_factor);
+  w.i64("parameters/check_iter", p.check_iter);
+  w.i64("parameters/warm_up", p.warm_up);
+  w.i64("parameters/spmv_mode_Q", p.spmv_mode_Q);
+  w.i64("parameters/spmv_mode_A", p.spmv_mode_A);
+  w.i64("parameters/print_frequency", p.print_frequency);
+  w.i64("parameters/device_number", p.device_number);
+  w.i64("parameters/use_Ruiz_scaling", p.use_Ruiz_scaling);
+  w.i64("parameters/use_bc_scaling", p.use_bc_scaling);
+  w.i64("parameters/use_l2_scaling", p.use_l2_scaling);
+  w.i64("parameters/use_Pock_Chambolle_scaling", p.use_Pock_Chambolle_scaling);
+  w.str("parameters/problem_type", problem_type_name(p.problem_type));
+  w.f64("parameters/lambda", p.lambda);
+  w.i64("parameters/auto_save", p.auto_save);
+  w.i64("parameters/precision", p.precision);
+  if (!H.init_x.empty()) w.f64("parameters/initial_x", H.init_x.data(), (int64_t)H.init_x.size());
+  if (!H.init_y.empty()) w.f64("parameters/initial_y", H.init_y.data(), (int64_t)H.init_y.size());
+  // resume/: the scaled state of the engine's storage type, exactly
+  w.f64("resume/fingerprint", problem_fingerprint(H.hp));
+  w.i64("resume/n", n);
+  w.i64("resume/m", m);
+  w.i64("resume/phase", fp32_phase ? 32 : 64);
+  w.i64("resume/status", status);
+  w.i64("resume/iter", L.iter);
+  w.f64("resume/sigma", E.sigma);
+  w.f64("resume/lambda_max_A", E.lamA);
+  w.f64("resume/lambda_max_Q", E.lamQ);
+  const RestartInfo& r = L.ri;
+  const double rinfo[14] = {r.first_restart ? 1.0 : 0.0, r.save_gap, r.current_gap, r.last_gap, r.best_gap,
+                            r.best_sigma, r.weighted_norm, (double)r.inner, (double)r.times, (double)r.sufficient,
+                            (double)r.necessary, (double)r.long_, (double)r.restart_flag, 0.0};
+  w.f64("resume/restart", rinfo, 14);
+  const double loop[16] = {L.res.err_Rp, L.res.err_Rd, L.res.KKT, L.res.pobj, L.res.dobj, L.res.gap,
+                           (double)L.iter_4, (double)L.iter_6, L.time_4, L.time_6, L.first_4 ? 1.0 : 0.0,
+                           L.first_6 ? 1.0 : 0.0, L.best_kkt, (double)L.stall, L.polish_tol, 0.0};
+  w.f64("resume/loop", loop, 16);
+  auto st = [&](const char* name, const V* d, int64_t len) {
+    if (len <= 0 || !d) return;
+    E.vec_to_host(d, len, v.data());
+    w.f64(std::string("resume/") + name, v.data(), len);
+  };
+  st("x", E.x, n);
+  st("w", E.w, n);
+  st("ATy", E.ATy, n);
+  st("last_x", E.last_x, n);
+  st("last_w", E.last_w, n);
+  st("last_ATy", E.last_ATy, n);
+  st("Qw", E.Qw, n);
+  st("last_Qw", E.last_Qw, n);
+  st("y", E.y, m);
+  st("last_y", E.last_y, m);
+  std::string err;
+  if (!w.write(H.save_file, err)) {
+    if (p.verbose) std::printf("Warning: Failed to save the checkpoint: %s\n", err.c_str());
+  } else if (p.verbose) {
+    std::printf("State saved to %s at iteration %lld\n", H.save_file.c_str(), (long long)L.iter);
+  }
+}
 
 // One phase of the HPR loop on engine E (src/algorithm.jl:1977-2038).
 // Returns a final status, or kSwitch when the FP32 phase hands over.
@@ -199,6 +370,11 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
     const int64_t iter = L.iter;
     const bool time_up = now_s() - L.t0 > p.time_limit;
     const bool print_yes = on_print_schedule(iter, p) || iter == p.max_iter || time_up;
+    // a resumed solve enters at its checkpoint's step: the checks of that
+    // iteration ran before the checkpoint was written
+    const bool checks = !L.skip_checks_once;
+    L.skip_checks_once = false;
+    if (checks) {
     if (iter % check_iter == 0 || print_yes || L.force_residuals) {
       L.force_residuals = false;
       E.residuals_launch(iter == 0);
@@ -229,6 +405,18 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
       if (iter == 0) R.err_Rp = std::max(R.err_Rp, r[S_RES_N + 7]);
       R.KKT = std::max(std::max(R.err_Rp, R.err_Rd), R.gap);
       if (!std::isfinite(R.KKT) || !std::isfinite(R.pobj) || !std::isfinite(R.dobj)) return HPRQP_STATUS_NUMERICAL_ERROR;
+      // the best iterates so far (compute_residuals!, src/algorithm.jl:97-113)
+      SavedBest& B = H.best;
+      if (p.auto_save && (iter == 0 || R.KKT < std::max(std::max(B.err_Rp, B.err_Rd), B.gap))) {
+        E.bars_to_device(B.x, B.y, B.z, B.w);
+        B.sigma = E.sigma;
+        B.iter = iter;
+        B.err_Rp = R.err_Rp;
+        B.err_Rd = R.err_Rd;
+        B.pobj = R.pobj;
+        B.dobj = R.dobj;
+        B.gap = R.gap;
+      }
       if (fp32_phase) {
         if (R.KKT < L.polish_tol) return kSwitch;
         if (R.KKT < 0.9 * L.best_kkt) {
@@ -321,8 +509,11 @@ static int run_loop(Handle& H, Engine<V>& E, const hprqp_params& p, LoopState& L
       std::printf("%5lld    %3.2e    %3.2e    %+7.6e    %+7.6e    %3.2e    %3.2e    %6.2f\n", (long long)iter,
                   L.res.err_Rp, L.res.err_Rd, L.res.pobj, L.res.dobj, L.res.gap, E.sigma, now_s() - L.t0);
     if (L.res.KKT < 1e-4 && L.first_4) { L.time_4 = now_s() - L.t0; L.iter_4 = iter; L.first_4 = false; }
+    if ((print_yes || status >= 0) && p.auto_save) save_checkpoint(H, E, p, L, status, fp32_phase);
+    if (L.res.KKT < 1e-4 && L.first_4) { L.time_4 = now_s() - L.t0; L.iter_4 = iter; L.first_4 = false; }
     if (L.res.KKT < 1e-6 && L.first_6) { L.time_6 = now_s() - L.t0; L.iter_6 = iter; L.first_6 = false; }
     if (status >= 0) return status;
+    }  // checks
     const int64_t next = iter + 1;
     const bool to_check = (next % check_iter == 0) || (ri.restart_flag > 0) || on_print_schedule(next, p);
     // perform_iteration_step! (src/algorithm.jl:1881-1900)
@@ -361,7 +552,6 @@ static void check_params(const hprqp_params& p) {
     throw Error(HPRQP_E_ARG, "Invalid sigma value. It should be a positive number or -1 for automatic.");
   if (!(p.print_frequency == -1 || p.print_frequency > 0))
     throw Error(HPRQP_E_ARG, "Invalid print_frequency. It should be a positive integer or -1 for automatic printing.");
-  if (p.auto_save) throw Error(HPRQP_E_UNSUPPORTED, "auto_save (HDF5) is not implemented by libhprqp");
   if (!p.use_gpu) throw Error(HPRQP_E_UNSUPPORTED, "use_gpu = false: libhprqp has no CPU path");
   if (p.precision != HPRQP_PRECISION_FP64 && p.precision != HPRQP_PRECISION_FP32_POLISH)
     throw Error(HPRQP_E_ARG, "unknown precision mode");
@@ -458,16 +648,122 @@ static void start_engine(Handle& H, Engine<V>& E, const hprqp_params& p, double 
   if (E.Q_is_diag) E.set_sigma(sigma0);
 }
 
+// Continue from a checkpoint: the engine's state, sigma, lambda_max and the
+// loop records as the checkpoint holds them; the loop then enters at the
+// checkpoint's step (LoopState::skip_checks_once).
+template <typename V>
+static void resume_engine(Handle& H, Engine<V>& E, const hprqp_params& p, const ck::Reader& rs, LoopState& L) {
+  auto f1 = [&](const char* name) { return rs.get(name)->f[0]; };
+  E.reset_state();
+  E.lamA = f1("resume/lambda_max_A");
+  E.lamQ = f1("resume/lambda_max_Q");
+  E.lam_l1 = p.problem_type == HPRQP_PROBLEM_LASSO ? H.hp.lambda : 0.0;
+  E.sigma = f1("resume/sigma");
+  auto put = [&](const char* name, V* d, int64_t len) {
+    const ck::Record* r = rs.get(std::string("resume/") + name);
+    if (len <= 0 || !d) return;
+    if (!r || (int64_t)r->f.size() != len) throw Error(HPRQP_E_ARG, std::string("checkpoint lacks resume/") + name);
+    E.vec_from_host(d, r->f.data(), len);
+  };
+  const int64_t n = E.n, m = E.m;
+  put("x", E.x, n);
+  put("w", E.w, n);
+  put("ATy", E.ATy, n);
+  put("last_x", E.last_x, n);
+  put("last_w", E.last_w, n);
+  put("last_ATy", E.last_ATy, n);
+  put("Qw", E.Qw, n);
+  put("last_Qw", E.last_Qw, n);
+  put("y", E.y, m);
+  put("last_y", E.last_y, m);
+  if (E.Q_is_diag) E.set_sigma(E.sigma);
+  const std::vector<double>& r = rs.get("resume/restart")->f;
+  RestartInfo& ri = L.ri;
+  ri.first_restart = r[0] != 0.0;
+  ri.save_gap = r[1];
+  ri.current_gap = r[2];
+  ri.last_gap = r[3];
+  ri.best_gap = r[4];
+  ri.best_sigma = r[5];
+  ri.weighted_norm = r[6];
+  ri.inner = (int64_t)r[7];
+  ri.times = (int64_t)r[8];
+  ri.sufficient = (int64_t)r[9];
+  ri.necessary = (int64_t)r[10];
+  ri.long_ = (int64_t)r[11];
+  ri.restart_flag = (int)r[12];
+  const std::vector<double>& q = rs.get("resume/loop")->f;
+  L.res.err_Rp = q[0];
+  L.res.err_Rd = q[1];
+  L.res.KKT = q[2];
+  L.res.pobj = q[3];
+  L.res.dobj = q[4];
+  L.res.gap = q[5];
+  L.iter_4 = (int64_t)q[6];
+  L.iter_6 = (int64_t)q[7];
+  L.time_4 = q[8];
+  L.time_6 = q[9];
+  L.first_4 = q[10] != 0.0;
+  L.first_6 = q[11] != 0.0;
+  L.best_kkt = q[12];
+  L.stall = (int)q[13];
+  L.iter = rs.get("resume/iter")->i[0];
+  L.skip_checks_once = true;
+}
+
+// The checkpoint must belong to the loaded problem and the parameters that
+// shape the scaled state; it must be of a solve that stopped early.
+static void check_resume(const Handle& H, const hprqp_params& p, const ck::Reader& rs) {
+  static const char* need_f[] = {"resume/fingerprint", "resume/sigma", "resume/lambda_max_A", "resume/lambda_max_Q",
+                                 "resume/restart", "resume/loop"};
+  static const char* need_i[] = {"resume/n", "resume/m", "resume/phase", "resume/status", "resume/iter",
+                                 "parameters/use_Ruiz_scaling", "parameters/use_Pock_Chambolle_scaling"};
+  for (const char* k : need_f)
+    if (!rs.get(k) || rs.get(k)->f.empty()) throw Error(HPRQP_E_ARG, std::string("checkpoint lacks ") + k);
+  for (const char* k : need_i)
+    if (!rs.get(k) || rs.get(k)->i.empty()) throw Error(HPRQP_E_ARG, std::string("checkpoint lacks ") + k);
+  if (rs.get("resume/restart")->f.size() < 13 || rs.get("resume/loop")->f.size() < 14)
+    throw Error(HPRQP_E_ARG, "checkpoint: short restart or loop record");
+  if (rs.get("resume/n")->i[0] != H.hp.n || rs.get("resume/m")->i[0] != H.hp.m ||
+      rs.get("resume/fingerprint")->f[0] != problem_fingerprint(H.hp))
+    throw Error(HPRQP_E_ARG, "checkpoint is of another problem than the loaded one");
+  if (rs.get("parameters/use_Ruiz_scaling")->i[0] != p.use_Ruiz_scaling ||
+      rs.get("parameters/use_Pock_Chambolle_scaling")->i[0] != p.use_Pock_Chambolle_scaling)
+    throw Error(HPRQP_E_ARG, "checkpoint was written with other scaling parameters");
+  const int64_t st = rs.get("resume/status")->i[0];
+  if (st == HPRQP_STATUS_OPTIMAL || st == HPRQP_STATUS_NUMERICAL_ERROR)
+    throw Error(HPRQP_E_ARG, "checkpoint is of a finished solve (status " + std::to_string(st) + ")");
+  if (rs.get("resume/phase")->i[0] == 32 && p.precision != HPRQP_PRECISION_FP32_POLISH)
+    throw Error(HPRQP_E_ARG, "checkpoint is of the FP32 phase: resume it with precision FP32_POLISH");
+}
+
 static int solve(Handle& H, const hprqp_params& p, const double* x0, const double* y0, hprqp_result* res,
-                 double* xo, double* yo, double* zo, double* wo) {
+                 double* xo, double* yo, double* zo, double* wo, const ck::Reader* rs = nullptr) {
   const double setup_start = now_s();
   // host<->device bytes of this call, set-up (scaling, uploads) included
   H.h2d_at_solve_start = H.cm->h2d;
   const int64_t d2h0 = H.cm->d2h;
   prepare(H, p);
+  if (rs) check_resume(H, p, *rs);
   const double setup_time = now_s() - setup_start;
   Common& cm = *H.cm;
   const int64_t launches0 = cm.launches;
+  if (p.auto_save) {  // the best-iterate copies (FP64, on the device)
+    SavedBest& B = H.best;
+    if (B.cap_n < H.hp.n || B.cap_m < H.hp.m) {
+      B.x = cm.mem.alloc<double>(H.hp.n);
+      B.z = cm.mem.alloc<double>(H.hp.n);
+      B.w = cm.mem.alloc<double>(H.hp.n);
+      B.y = cm.mem.alloc<double>(std::max<int64_t>(H.hp.m, 1));
+      B.cap_n = H.hp.n;
+      B.cap_m = H.hp.m;
+    }
+    B.sigma = 0.0;
+    B.iter = 0;
+    B.err_Rp = B.err_Rd = B.pobj = B.dobj = B.gap = kInf;
+    H.init_x.assign(x0 ? x0 : nullptr, x0 ? x0 + H.hp.n : nullptr);
+    H.init_y.assign(y0 ? y0 : nullptr, y0 ? y0 + H.hp.m : nullptr);
+  }
   const Prepared& pp = H.pp;
   const int64_t m = H.hp.m;
   Engine<double>& E64 = *H.e64;
@@ -485,7 +781,12 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
   int64_t pitA = 0, pitQ = 0;
   double pbytes = 0.0;
-  estimate_lambdas(H, p, fp32, &lamA, &lamQ, &pitA, &pitQ, &pbytes);
+  if (rs) {  // the checkpoint's lambda_max values
+    lamA = rs->get("resume/lambda_max_A")->f[0];
+    lamQ = rs->get("resume/lambda_max_Q")->f[0];
+  } else {
+    estimate_lambdas(H, p, fp32, &lamA, &lamQ, &pitA, &pitQ, &pbytes);
+  }
   const double power_time = now_s() - L.t0;
   // sigma of allocate_workspace (src/algorithm.jl:838-851)
   double sigma0 = p.sigma > 0 ? p.sigma : 1.0;
@@ -496,9 +797,13 @@ static int solve(Handle& H, const hprqp_params& p, const double* x0, const doubl
   int status;
   int64_t iter_fp32 = 0;
   bool final64 = true;
-  if (p.precision == HPRQP_PRECISION_FP32_POLISH) {
+  if (rs && rs->get("resume/phase")->i[0] == 64) {  // resumed in the FP64 phase (plain FP64 or the polish)
+    resume_engine(H, E64, p, *rs, L);
+    status = run_loop(H, E64, p, L, false);
+  } else if (p.precision == HPRQP_PRECISION_FP32_POLISH) {
     Engine<float>& E32 = *H.e32;
-    start_engine(H, E32, p, lamA, lamQ, sigma0, x0, y0);
+    if (rs) resume_engine(H, E32, p, *rs, L);
+    else start_engine(H, E32, p, lamA, lamQ, sigma0, x0, y0);
     status = run_loop(H, E32, p, L, true);
     iter_fp32 = L.iter;
     if (status == kSwitch) {
@@ -860,6 +1165,25 @@ int hprqp_set_trace(hprqp_handle h, int64_t iters, double* x_trace, double* y_tr
   h->yt = y_trace;
   h->wt = w_trace;
   return HPRQP_OK;
+}
+
+int hprqp_set_save_file(hprqp_handle h, const char* path) {
+  if (!h || !path || !path[0]) return HPRQP_E_ARG;
+  h->save_file = path;
+  return HPRQP_OK;
+}
+
+int hprqp_solve_resume(hprqp_handle h, const hprqp_params* params, const char* path, hprqp_result* result,
+                       double* x, double* y, double* z, double* w) {
+  if (!h || !params || !path || !result) return HPRQP_E_ARG;
+  HPRQP_GUARD(h, {
+    if (!h->hp.loaded) throw hprqp::Error(HPRQP_E_STATE, "load a problem first");
+    hprqp::check_params(*params);
+    hprqp::ck::Reader rs;
+    std::string err;
+    if (!rs.read(path, err)) throw hprqp::Error(HPRQP_E_ARG, err);
+    hprqp::solve(*h, *params, nullptr, nullptr, result, x, y, z, w, &rs);
+  })
 }
 
 int hprqp_set_qmap(hprqp_handle h, hprqp_qmap_fn qmap, void* user) {

@@ -137,7 +137,10 @@ typedef struct hprqp_params {
     int32_t problem_type;            /* HPRQP_PROBLEM_*; L1 term in the objective
                                         only when LASSO (algorithm.jl:66)           */
     double  lambda;                  /* params.lambda: never read (reference quirk) */
-    int32_t auto_save;               /* HDF5 auto-save: HPRQP_E_UNSUPPORTED if set  */
+    int32_t auto_save;               /* 1: write a checkpoint at every printed
+                                        iteration and at the end (the reference's
+                                        HDF5 datasets in the library's container,
+                                        to the file of hprqp_set_save_file)        */
     int32_t verbose;                 /* 1: iteration log on stdout                  */
     int32_t use_gpu;                 /* must be 1 for this library                  */
     /* ---- extensions ---- */
@@ -229,6 +232,30 @@ int hprqp_solve(hprqp_handle h, const hprqp_params* params,
                 const double* initial_x, const double* initial_y,
                 hprqp_result* result,
                 double* x, double* y, double* z, double* w);
+
+/* The file params.auto_save writes (the reference's save_filename,
+ * src/structs.jl:195-275; default "hprqp_autosave.ckpt").  save_state_to_hdf5!
+ * (src/algorithm.jl:183-301) writes HDF5; this library writes the same
+ * datasets (current/..., best/..., parameters/...) into its own container
+ * of named arrays (a u16-length name, a type byte, a u64 count and the
+ * little-endian payload per record after the magic "HPRQPCK1";
+ * hprqp_b200/checkpoint.py reads it), written to <path>.tmp and renamed,
+ * plus a resume/... section for hprqp_solve_resume. */
+int hprqp_set_save_file(hprqp_handle h, const char* path);
+
+/* Continue a solve from a checkpoint written by params.auto_save for the
+ * loaded problem (no reference counterpart: the reference writes its
+ * checkpoints but cannot continue from them).  The scaled state, sigma,
+ * lambda_max and the restart records come from the file, so the continued
+ * solve takes exactly the steps the interrupted one would have taken after
+ * the checkpoint's iteration.  `params` may change max_iter, time_limit,
+ * stoptol and the like; the scaling parameters must be those of the
+ * checkpoint.  A checkpoint of a solve that ended OPTIMAL (or in a
+ * numerical error) is rejected; one of the FP32 phase needs precision
+ * HPRQP_PRECISION_FP32_POLISH.  Results as hprqp_solve; iter counts the
+ * iterations of both parts. */
+int hprqp_solve_resume(hprqp_handle h, const hprqp_params* params, const char* path, hprqp_result* result,
+                       double* x, double* y, double* z, double* w);
 
 /* Parity hook: record the scaled working iterates x, y, w after each of the
  * first `iters` HPR iterations of the next hprqp_solve() into caller-owned

@@ -163,8 +163,6 @@ def test_invalid_device_is_an_error():
 def test_unsupported_options_are_errors():
     s = Solver().load(model("toy_diagQ"))
     with pytest.raises(HPRQPError):
-        s.solve(gpu_params("QP", auto_save=True))
-    with pytest.raises(HPRQPError):
         s.solve(gpu_params("QP", use_gpu=False))
     s.close()
 
