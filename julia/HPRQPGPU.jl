@@ -216,6 +216,10 @@ function solve_gpu(model, params; results_type = _results_type())
         check(ccall((:hprqp_create, libhprqp), Cint, (Ref{Ptr{Cvoid}}, Int32), h, params.device_number), C_NULL)
         try
             check(ccall((:hprqp_load, libhprqp), Cint, (Ptr{Cvoid}, Ref{CProblem}), h[], prob), h[])
+            if params.auto_save  # the reference's save_filename; the library's container, same datasets
+                check(ccall((:hprqp_set_save_file, libhprqp), Cint, (Ptr{Cvoid}, Cstring), h[],
+                            params.save_filename), h[])
+            end
             if Qk == Q_CUSTOM
                 fn = @cfunction(qmap_thunk, Int32, (Ptr{Cvoid}, Ptr{Cvoid}, Int32, Ptr{Cvoid}, Ptr{Cvoid}))
                 check(ccall((:hprqp_set_qmap, libhprqp), Cint, (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid}),
