@@ -84,3 +84,35 @@ def test_solve_gpu_returns_reference_results_type():
             "void* stream);") in hdr
     # statuses are the reference strings (src/algorithm.jl:558-576)
     assert '0 => "OPTIMAL"' in src and '1 => "MAX_ITER"' in src and '2 => "TIME_LIMIT"' in src
+
+
+MOI_EXTRAS = os.path.join(ROOT, "julia", "MOI_extras.jl")
+
+# HPRQP_parameters fields a user sets through MOI (src/structs.jl:195-275),
+# with the three the reference's wrapper leaves out (src/MOI_wrapper.jl:141-163)
+MOI_PARAMETERS = ["stoptol", "sigma", "max_iter", "sigma_fixed", "time_limit", "eig_factor", "check_iter",
+                  "warm_up", "spmv_mode_Q", "spmv_mode_A", "print_frequency", "device_number", "use_Ruiz_scaling",
+                  "use_bc_scaling", "use_l2_scaling", "use_Pock_Chambolle_scaling", "initial_x", "initial_y",
+                  "auto_save", "save_filename", "verbose", "use_gpu", "problem_type", "lambda"]
+
+
+def test_moi_extras_expose_the_missing_raw_attributes():
+    src = open(MOI_EXTRAS).read()
+    tup = re.search(r"const SUPPORTED_PARAMETERS = \((.*?)\n\)", src, flags=re.S).group(1)
+    names = re.findall(r'"(\w+)"', tup)
+    assert names == MOI_PARAMETERS, names
+    for name in ("use_gpu", "problem_type", "lambda"):
+        assert f'name == "{name}"' in src[src.index("function _set_extra!"):src.index("function _get_extra")]
+        assert f'name == "{name}" && return model.params.{name}' in src
+
+
+def test_moi_extras_constraint_primal_of_affine_rows():
+    src = open(MOI_EXTRAS).read()
+    body = src[src.index("function MOI.get(\n    model::Optimizer,\n    attr::MOI.ConstraintPrimal"):]
+    assert "MOI.ScalarAffineFunction{Float64},<:SCALAR_SETS" in body
+    assert "get_fallback" not in body
+    assert "_row_activity(model)[c.value]" in body
+    # the activity is A x from the cached constraint matrix and the returned x
+    act = src[src.index("function _compute_row_activity"):]
+    assert "model.cache.constraints.coefficients" in act and "model.results.x" in act
+    assert "ax[A.rowval[k]] += A.nzval[k] * xj" in act
