@@ -25,26 +25,51 @@ HCsr csc_to_csr(int64_t rows, int64_t cols, const int32_t* cp, const int32_t* rv
   const int64_t nnz = (int64_t)cp[cols] - base;
   if (nnz < 0 || nnz > INT32_MAX) throw Error(HPRQP_E_ARG, std::string(what) + ": bad nnz");
   if (nnz > 0 && (!rv || !nz)) throw Error(HPRQP_E_ARG, std::string(what) + ": null rowval/nzval");
+  for (int64_t j = 0; j < cols; ++j)
+    if (cp[j + 1] < cp[j]) throw Error(HPRQP_E_ARG, std::string(what) + ": colptr not monotone");
   M.ptr.assign(rows + 1, 0);
   M.col.resize(nnz);
   M.val.resize(nnz);
-  for (int64_t j = 0; j < cols; ++j)
-    if (cp[j + 1] < cp[j]) throw Error(HPRQP_E_ARG, std::string(what) + ": colptr not monotone");
+  // validation and row counts, in parallel (counts by atomic increments do
+  // not depend on the order)
+  int* cnt = M.ptr.data() + 1;
+  bool bad_row = false, bad_val = false;
+#pragma omp parallel for schedule(static) reduction(|| : bad_row, bad_val) num_threads(host_threads(nnz))
   for (int64_t k = 0; k < nnz; ++k) {
     const int64_t r = (int64_t)rv[k] - base;
-    if (r < 0 || r >= rows) throw Error(HPRQP_E_ARG, std::string(what) + ": row index out of range");
-    if (!std::isfinite(nz[k])) throw Error(HPRQP_E_ARG, std::string(what) + " contains NaN or Inf values.");
-    M.ptr[r + 1]++;
-  }
-  for (int64_t i = 0; i < rows; ++i) M.ptr[i + 1] += M.ptr[i];
-  std::vector<int> pos(M.ptr.begin(), M.ptr.end() - 1);
-  for (int64_t j = 0; j < cols; ++j)
-    for (int64_t k = cp[j] - base; k < cp[j + 1] - base; ++k) {
-      const int r = rv[k] - base;
-      M.col[pos[r]] = (int)j;
-      M.val[pos[r]] = nz[k];
-      pos[r]++;
+    if (r < 0 || r >= rows) {
+      bad_row = true;
+      continue;
     }
+    if (!std::isfinite(nz[k])) bad_val = true;
+    __atomic_fetch_add(cnt + r, 1, __ATOMIC_RELAXED);
+  }
+  if (bad_row) throw Error(HPRQP_E_ARG, std::string(what) + ": row index out of range");
+  if (bad_val) throw Error(HPRQP_E_ARG, std::string(what) + " contains NaN or Inf values.");
+  for (int64_t i = 0; i < rows; ++i) M.ptr[i + 1] += M.ptr[i];
+  // scatter: each thread owns a range of rows (balanced by entries) and
+  // walks all columns in order, so every row receives its entries in
+  // increasing column order, as a serial pass would
+  const int T = host_threads(nnz);
+#pragma omp parallel num_threads(T)
+  {
+    const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+    const int64_t e0 = nnz * t / nt, e1 = nnz * (t + 1) / nt;
+    const int64_t r0 = std::upper_bound(M.ptr.begin(), M.ptr.end(), (int)e0) - M.ptr.begin() - 1;
+    const int64_t r1 = t + 1 == nt ? rows : std::upper_bound(M.ptr.begin(), M.ptr.end(), (int)e1) - M.ptr.begin() - 1;
+    if (r0 < r1) {
+      std::vector<int> pos(M.ptr.begin() + r0, M.ptr.begin() + r1);
+      for (int64_t j = 0; j < cols; ++j)
+        for (int64_t k = cp[j] - base; k < cp[j + 1] - base; ++k) {
+          const int64_t r = (int64_t)rv[k] - base;
+          if (r < r0 || r >= r1) continue;
+          int& p = pos[r - r0];
+          M.col[p] = (int)j;
+          M.val[p] = nz[k];
+          ++p;
+        }
+    }
+  }
   // CSC rows sorted within each column give CSR columns sorted within rows.
   return M;
 }
