@@ -58,6 +58,8 @@ void Common::init() {
   pow_chunk_fold = !(cf && cf[0] == '0');
   const char* at = std::getenv("HPRQP_AUTOTUNE");
   autotune = !(at && at[0] == '0');
+  const char* ppr = std::getenv("HPRQP_POWER_PRELOAD_ROWS");
+  if (ppr) pow_rows_preloaded = std::atoi(ppr) == 1 ? 1 : 2;
   const char* ept = std::getenv("HPRQP_ELL_PROLOGUE");
   if (ept) ell_prologue = std::max(0, std::min(std::atoi(ept), 2));
   const char* ep = std::getenv("HPRQP_EPI_PREFETCH");
@@ -487,7 +489,10 @@ template <int K, typename V, typename X, typename Epi>
 static void mat_partials(Common& cm, const DCsr<V>& M, const X* xin, const Epi& e, double* partials) {
   const int grid = partials_grid(cm, M);
   if (M.sell || (M.ell && M.sell_len > 0)) {
-    if (cm.ell_prologue > 0)  // matrix entries of the first 2 rows per thread before the wait
+    if (cm.ell_prologue > 0 && cm.pow_rows_preloaded == 1)  // the first row's matrix entries before the wait
+      launch(cm, k_sell_partials<1, 8, K, double, V, X, Epi>, grid, kBlock, M.rows,
+             SellSrc<V, X>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, partials);
+    else if (cm.ell_prologue > 0)  // the first 2 rows' per thread
       launch(cm, k_sell_partials<2, 8, K, double, V, X, Epi>, grid, kBlock, M.rows,
              SellSrc<V, X>{M.sptr, M.ptr, M.scol, M.sval, xin}, e, partials);
     else

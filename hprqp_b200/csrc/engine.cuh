@@ -79,6 +79,7 @@ struct Common {  // per-handle resources shared by the engines
   // for Q, A, A': FP32 plain iteration 43.4 / 28.6 / 29.5 us, FP64 48.3 /
   // 45.1 / 46.4 us for 0 / 1 / 2
   int ell_prologue = 1;
+  int pow_rows_preloaded = 2;  // rows per thread whose power-step matrix entries load before the wait (1 or 2)
   // power chains folded once per chunk (HPRQP_POWER_CHUNK_FOLD=0: per step)
   bool pow_chunk_fold = true;
   // row-schedule autotuner (timed); HPRQP_AUTOTUNE=0 applies a fixed rule

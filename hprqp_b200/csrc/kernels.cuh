@@ -916,6 +916,13 @@ __global__ void __launch_bounds__(kBlock) k_sell_partials(int nrows, SellSrc<V, 
     }
   }
   pdl_enter();
+  // every preloaded row's gathers first, then the sums and epilogues: the
+  // epilogues' stores must not keep the next row's loads waiting
+  Acc g[R][WMAX];
+#pragma unroll
+  for (int q = 0; q < R; ++q)
+#pragma unroll
+    for (int k = 0; k < WMAX; ++k) g[q][k] = (k < len[q]) ? (Acc)__ldg(src.x + c[q][k]) : Acc(0);
 #pragma unroll
   for (int q = 0; q < R; ++q) {
     const int row = row0 + q * stride;
@@ -923,7 +930,7 @@ __global__ void __launch_bounds__(kBlock) k_sell_partials(int nrows, SellSrc<V, 
       Acc s = Acc(0);
 #pragma unroll
       for (int k = 0; k < WMAX; ++k)
-        if (k < len[q]) s = fma((Acc)v[q][k], (Acc)__ldg(src.x + c[q][k]), s);
+        if (k < len[q]) s = fma((Acc)v[q][k], g[q][k], s);
       for (int k = WMAX; k < len[q]; ++k)
         s = fma((Acc)__ldg(src.val + base[q] + 32 * k), (Acc)__ldg(src.x + __ldg(src.col + base[q] + 32 * k)), s);
       epi(row, s, r);
