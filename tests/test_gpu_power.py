@@ -1,10 +1,13 @@
 """GPU tests of the power method (src/utils.jl:1335-1461).
 
-The engine runs both chains (A A' and Q, or the LASSO operator) in one
-persistent cooperative kernel.  Its lambda_max estimates must agree with
-the oracle's power method (same start vector, same stopping rule, FP64) and
-with the engine's graph-captured one-launch-per-product chains, which
-HPRQP_POWER_PERSISTENT=0 selects."""
+The engine runs both chains (A A' and Q, or the LASSO operator) on two
+streams, 32 steps per CUDA graph: the A A' chain on the Gram matrix A'A
+where that is small, both chains folded once per 32-step chunk.  Its
+lambda_max estimates must agree with the oracle's power method (same start
+vector, same stopping rule, FP64), with the engine's reference-form chains
+(two products per step, HPRQP_POWER_GRAM=0; a fold per step,
+HPRQP_POWER_CHUNK_FOLD=0), and with the opt-in persistent cooperative
+kernel (HPRQP_POWER_PERSISTENT=1)."""
 import json
 import os
 import subprocess
