@@ -296,21 +296,69 @@ __global__ void k_each(int64_t len, F f) {
 
 // FP32 phase: the whole Q operator of one instance (n_k <= 128) in one CTA
 // on the tensor cores, 3xTF32 with FP32 accumulation in TMEM:
-//   phase 1: acc1 = A_k X, acc2 = S_k X        (K = n_k in chunks of 32)
-//   phase 2: acc3 = TMP B_k + (-X) T_k, TMP = acc1 read back from TMEM
-//   Y = 2 acc3 - 2 acc2
-// Operands are split into TF32 hi/lo and staged K-major (tcgen05.cuh);
-// rows and columns beyond n_k are zero.  Every mbarrier wait is bounded;
-// on a timeout the CTA raises g_bqp_err, frees its TMEM and returns.
+//   phase 1: acc1 = A_k X,  acc3 = (-S_k) X            (K = n_k in chunks of 32)
+//   phase 2: acc3 += TMP B_k,  acc3 += (-X) T_k,  TMP = acc1 read back
+//   Y = 2 acc3
+// The constant operands A_k, -S_k (A operands) and B_k, T_k (B operands)
+// are split into TF32 hi/lo once per batch (k_qap_images) in the K-major
+// layout of one 128 x 32 chunk, and each call fetches them with bulk copies
+// (cp.async.bulk, completion on an mbarrier) while the threads split only
+// X (or TMP) into shared memory.  Two accumulators (256 TMEM columns) and
+// 96 KiB of shared memory per CTA let two CTAs share an SM, so one CTA's
+// staging overlaps the other's MMAs.  Rows and columns beyond n_k are zero.
+// Every mbarrier wait is bounded; on a timeout the CTA raises g_bqp_err,
+// frees its TMEM and returns.
 __device__ int g_bqp_err = 0;
-constexpr int kQapTcSmem = 8 * tc::kOpBytes + 1024;
-constexpr uint32_t kQapTcCols = 512;  // acc1, acc2, acc3 (128 columns each), power of two
-
+constexpr int kQapImgChunk = 2 * tc::kTile * tc::kChunk;  // floats of one chunk image: hi, then lo
+constexpr int kQapTcSmem = 6 * tc::kOpBytes + 1024;          // three operand slots (hi + lo each)
+constexpr uint32_t kQapTcCols = 256;                          // acc1, acc3 (128 columns each)
 constexpr int kQapTcThreads = 256;  // 8 warps: two warp groups share the TMEM lanes by column halves
 
-__global__ void __launch_bounds__(kQapTcThreads) k_qap_tc(const int* qn, const int64_t* off, const unsigned char* on,
-                                                         const float* __restrict__ QA, const float* __restrict__ QB,
-                                                         const float* __restrict__ QS, const float* __restrict__ QT,
+// The images of instance k start at img_off[k] floats: [A | -S | B | T],
+// each ceil(n_k / 32) chunk images of kQapImgChunk floats.  A-operand
+// images hold element (row i, k = l) = M[i + l n], B-operand images
+// (row j, k = l) = M[l + j n].  One CTA per (instance, matrix, chunk).
+__global__ void __launch_bounds__(256) k_qap_images(const int* qn, const int64_t* off, const int64_t* img_off,
+                                                    const float* __restrict__ QA, const float* __restrict__ QB,
+                                                    const float* __restrict__ QS, const float* __restrict__ QT,
+                                                    float* img) {
+  using namespace tc;
+  const int k = blockIdx.x, mat = blockIdx.y, c = blockIdx.z;
+  const int n = qn[k];
+  const int nch = (n + kChunk - 1) / kChunk;
+  if (c >= nch || n > kTile) return;
+  const int64_t o = off[k];
+  const float* M = (mat == 0 ? QA : mat == 1 ? QS : mat == 2 ? QB : QT) + o;
+  const float sgn = mat == 1 ? -1.0f : 1.0f;
+  const bool a_operand = mat < 2;
+  unsigned char* hi = (unsigned char*)(img + img_off[k] + (int64_t)(mat * nch + c) * kQapImgChunk);
+  unsigned char* lo = hi + kOpBytes;
+  const int k0 = c * kChunk;
+  for (int e = threadIdx.x; e < kTile * kChunk / 4; e += 256) {
+    const int r = e & (kTile - 1), c4 = (e >> 7) * 4;  // row r, k = k0 + c4 .. + 3
+    float v[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int l = k0 + c4 + q;
+      const bool in = r < n && l < n;
+      v[q] = in ? sgn * (a_operand ? M[r + (int64_t)l * n] : M[l + (int64_t)r * n]) : 0.0f;
+    }
+    put_split4(hi, lo, kmaj_off(r, c4), v[0], v[1], v[2], v[3]);
+  }
+}
+
+__device__ __forceinline__ void qap_bulk(uint32_t dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(tc::smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void qap_expect(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc::smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__global__ void __launch_bounds__(kQapTcThreads) k_qap_tc(const int* qn, const int64_t* off, const int64_t* img_off,
+                                                         const unsigned char* on, const float* __restrict__ img,
                                                          const float* X, float* Y) {
   using namespace tc;
   const int k = blockIdx.x;
@@ -321,139 +369,149 @@ __global__ void __launch_bounds__(kQapTcThreads) k_qap_tc(const int* qn, const i
     return;
   }
   extern __shared__ unsigned char smem_raw[];
-  __shared__ __align__(8) uint64_t bar;
+  __shared__ __align__(8) uint64_t bar_full, bar_mma;
   __shared__ uint32_t tmem_base;
   __shared__ int s_fail;
   unsigned char* sm = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
-  unsigned char *sAh = sm, *sAl = sm + kOpBytes, *sSh = sm + 2 * kOpBytes, *sSl = sm + 3 * kOpBytes;
-  unsigned char *sBh = sm + 4 * kOpBytes, *sBl = sm + 5 * kOpBytes, *sTh = sm + 6 * kOpBytes,
-                *sTl = sm + 7 * kOpBytes;
+  unsigned char *s0h = sm, *s0l = sm + kOpBytes, *s1h = sm + 2 * kOpBytes, *s1l = sm + 3 * kOpBytes;
+  unsigned char *s2h = sm + 4 * kOpBytes, *s2l = sm + 5 * kOpBytes;
   const int tid = threadIdx.x, warp = tid >> 5;
   const int64_t o = off[k];
-  const float *Ak = QA + o, *Bk = QB + o, *Sk = QS + o, *Tk = QT + o, *Xk = X + o;
+  const float* Xk = X + o;
   float* Yk = Y + o;
+  const int nch = (n + kChunk - 1) / kChunk;
+  const float* Ik = img + img_off[k];
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base)),
                  "r"(kQapTcCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar)), "r"(1u));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_full)), "r"(1u));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(&bar_mma)), "r"(1u));
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     s_fail = 0;
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  const uint32_t tm = tmem_base, acc1 = tm, acc2 = tm + 128, acc3 = tm + 256;
+  const uint32_t tm = tmem_base, acc1 = tm, acc3 = tm + 128;
   const uint32_t lane_base = (uint32_t)((warp & 3) * 32) << 16;  // warp w reads TMEM lanes 32 (w % 4) ..
   const int half = warp >> 2;                                      // ... and column half w / 4
-  uint32_t parity = 0;
-  // phase 1
-  for (int k0 = 0; k0 < n; k0 += kChunk) {
-    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
-      const int r = e & (kTile - 1), c = (e >> 7) * 4;  // A operands: (row r, k = k0 + c .. +3), column-major source
-      float a[4], b[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int l = k0 + c + q;
-        const bool in = r < n && l < n;
-        a[q] = in ? Ak[r + (int64_t)l * n] : 0.0f;
-        b[q] = in ? Sk[r + (int64_t)l * n] : 0.0f;
-      }
-      put_split4(sAh, sAl, kmaj_off(r, c), a[0], a[1], a[2], a[3]);
-      put_split4(sSh, sSl, kmaj_off(r, c), b[0], b[1], b[2], b[3]);
-    }
-    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
-      const int c = (e & (kChunk / 4 - 1)) * 4, j = e >> 3;  // B operand X(l, j): row j, k = l
-      float x[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int l = k0 + c + q;
-        x[q] = (j < n && l < n) ? Xk[l + (int64_t)j * n] : 0.0f;
-      }
-      put_split4(sBh, sBl, kmaj_off(j, c), x[0], x[1], x[2], x[3]);
-    }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      mma_chunk_3x(acc1, smem_u32(sAh), smem_u32(sAl), smem_u32(sBh), smem_u32(sBl), k0 == 0);
-      mma_chunk_3x(acc2, smem_u32(sSh), smem_u32(sSl), smem_u32(sBh), smem_u32(sBl), k0 == 0);
-      mma_commit(&bar);
-    }
-    if (!mbar_wait(&bar, parity)) s_fail = 1;
-    parity ^= 1u;
-    __syncthreads();
-    if (s_fail) break;
-  }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  // phase 2
   const int row = (warp & 3) * 32 + (tid & 31);
-  for (int k0 = 0; k0 < n && !s_fail; k0 += kChunk) {
-    uint32_t v[16];
-    const int cb = half * 16;  // this warp group's 16 of the chunk's 32 columns
-    tmem_ld16(acc1 + lane_base + (uint32_t)(k0 + cb), v);  // TMP(row, k0 + cb .. +15)
-#pragma unroll
-    for (int c = 0; c < 16; c += 4) {
-      float t[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) t[q] = (row < n && k0 + cb + c + q < n) ? __uint_as_float(v[c + q]) : 0.0f;
-      put_split4(sAh, sAl, kmaj_off(row, cb + c), t[0], t[1], t[2], t[3]);
+  // tid 0's barrier bookkeeping: the parity it waits on next, and what is
+  // still in flight (waited for, bounded, before the CTA leaves on a failure)
+  uint32_t pf = 0, pm = 0;
+  bool full_pending = false, mma_pending = false;
+  uint32_t pf_pending = 0, pm_pending = 0;
+  // bulk copies of two constant chunk images (hi + lo each) into two slots
+  auto fetch = [&](unsigned char* d0h, const float* im0, unsigned char* d1h, const float* im1) {
+    if (tid != 0 || s_fail) return;
+    const int nimg = im1 ? 2 : 1;
+    qap_expect(&bar_full, (uint32_t)(nimg * 2 * kOpBytes));
+    qap_bulk(smem_u32(d0h), im0, kOpBytes, &bar_full);
+    qap_bulk(smem_u32(d0h + kOpBytes), im0 + kTile * kChunk, kOpBytes, &bar_full);
+    if (im1) {
+      qap_bulk(smem_u32(d1h), im1, kOpBytes, &bar_full);
+      qap_bulk(smem_u32(d1h + kOpBytes), im1 + kTile * kChunk, kOpBytes, &bar_full);
     }
-    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
-      const int r = e & (kTile - 1), c = (e >> 7) * 4;  // -X(r, l) as an A operand
-      float x[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int l = k0 + c + q;
-        x[q] = (r < n && l < n) ? -Xk[r + (int64_t)l * n] : 0.0f;
-      }
-      put_split4(sSh, sSl, kmaj_off(r, c), x[0], x[1], x[2], x[3]);
-    }
-    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
-      const int c = (e & (kChunk / 4 - 1)) * 4, j = e >> 3;  // B_k(l, j), T_k(l, j): row j, k = l
-      float b[4], t[4];
-#pragma unroll
-      for (int q = 0; q < 4; ++q) {
-        const int l = k0 + c + q;
-        const bool in = j < n && l < n;
-        b[q] = in ? Bk[l + (int64_t)j * n] : 0.0f;
-        t[q] = in ? Tk[l + (int64_t)j * n] : 0.0f;
-      }
-      put_split4(sBh, sBl, kmaj_off(j, c), b[0], b[1], b[2], b[3]);
-      put_split4(sTh, sTl, kmaj_off(j, c), t[0], t[1], t[2], t[3]);
-    }
+    full_pending = true;
+    pf_pending = pf;
+  };
+  // the rest of a step: the threads' staging is in shared memory; tid 0 waits
+  // for the bulk copies, issues the MMAs, commits and waits for them
+  auto finish = [&](auto mmas) {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      mma_chunk_3x(acc3, smem_u32(sAh), smem_u32(sAl), smem_u32(sBh), smem_u32(sBl), k0 == 0);
-      mma_chunk_3x(acc3, smem_u32(sSh), smem_u32(sSl), smem_u32(sTh), smem_u32(sTl), false);
-      mma_commit(&bar);
+    if (tid == 0 && !s_fail) {
+      if (!mbar_wait(&bar_full, pf)) {
+        s_fail = 1;
+      } else {
+        full_pending = false;
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        mmas();
+        mma_commit(&bar_mma);
+        mma_pending = true;
+        pm_pending = pm;
+        if (!mbar_wait(&bar_mma, pm)) s_fail = 1;
+        else mma_pending = false;
+      }
+      pf ^= 1u;
+      pm ^= 1u;
     }
-    if (!mbar_wait(&bar, parity)) s_fail = 1;
-    parity ^= 1u;
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  };
+  auto image = [&](int mat, int c) { return Ik + (int64_t)(mat * nch + c) * kQapImgChunk; };
+  // phase 1: acc1 = A X, acc3 = (-S) X; X as the B operand (row j, k = l)
+  for (int c = 0; c < nch && !s_fail; ++c) {
+    const int k0 = c * kChunk;
+    fetch(s0h, image(0, c), s1h, image(1, c));
+    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
+      const int c4 = (e & (kChunk / 4 - 1)) * 4, j = e >> 3;
+      float x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int l = k0 + c4 + q;
+        x[q] = (j < n && l < n) ? Xk[l + (int64_t)j * n] : 0.0f;
+      }
+      put_split4(s2h, s2l, kmaj_off(j, c4), x[0], x[1], x[2], x[3]);
+    }
+    finish([&] {
+      mma_chunk_3x(acc1, smem_u32(s0h), smem_u32(s0l), smem_u32(s2h), smem_u32(s2l), c == 0);
+      mma_chunk_3x(acc3, smem_u32(s1h), smem_u32(s1l), smem_u32(s2h), smem_u32(s2l), c == 0);
+    });
   }
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  // phase 2: acc3 += TMP B, acc3 += (-X) T; A operands in slot 0, B in slot 1
+  for (int c = 0; c < nch && !s_fail; ++c) {
+    const int k0 = c * kChunk;
+    fetch(s1h, image(2, c), nullptr, nullptr);
+    {
+      uint32_t v[16];
+      const int cb = half * 16;  // this warp group's 16 of the chunk's 32 columns
+      tmem_ld16(acc1 + lane_base + (uint32_t)(k0 + cb), v);  // TMP(row, k0 + cb .. +15)
+#pragma unroll
+      for (int c4 = 0; c4 < 16; c4 += 4) {
+        float t[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) t[q] = (row < n && k0 + cb + c4 + q < n) ? __uint_as_float(v[c4 + q]) : 0.0f;
+        put_split4(s0h, s0l, kmaj_off(row, cb + c4), t[0], t[1], t[2], t[3]);
+      }
+    }
+    finish([&] { mma_chunk_3x(acc3, smem_u32(s0h), smem_u32(s0l), smem_u32(s1h), smem_u32(s1l), false); });
+    if (s_fail) break;
+    fetch(s1h, image(3, c), nullptr, nullptr);
+    for (int e = tid; e < kTile * kChunk / 4; e += kQapTcThreads) {
+      const int r = e & (kTile - 1), c4 = (e >> 7) * 4;  // -X(r, l) as an A operand
+      float x[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        const int l = k0 + c4 + q;
+        x[q] = (r < n && l < n) ? -Xk[r + (int64_t)l * n] : 0.0f;
+      }
+      put_split4(s0h, s0l, kmaj_off(r, c4), x[0], x[1], x[2], x[3]);
+    }
+    finish([&] { mma_chunk_3x(acc3, smem_u32(s0h), smem_u32(s0l), smem_u32(s1h), smem_u32(s1l), false); });
+  }
   if (!s_fail) {
     for (int c0 = half * 64; c0 < half * 64 + 64; c0 += 32) {
-      uint32_t a3[32], a2[32];
+      uint32_t a3[32];
       tmem_ld32(acc3 + lane_base + (uint32_t)c0, a3);
-      tmem_ld32(acc2 + lane_base + (uint32_t)c0, a2);
       if (row < n) {
 #pragma unroll
         for (int q = 0; q < 32; ++q) {
           const int j = c0 + q;
-          if (j < n) Yk[row + (int64_t)j * n] = 2.0f * __uint_as_float(a3[q]) - 2.0f * __uint_as_float(a2[q]);
+          if (j < n) Yk[row + (int64_t)j * n] = 2.0f * __uint_as_float(a3[q]);
         }
       }
     }
   } else if (tid == 0) {
     atomicExch(&g_bqp_err, 1);
-    mbar_wait(&bar, parity ^ 1u);  // give MMAs still in flight a bounded chance to drain
+    // give what is still in flight a bounded chance to land before the CTA leaves
+    if (full_pending) mbar_wait(&bar_full, pf_pending);
+    if (mma_pending) mbar_wait(&bar_mma, pm_pending);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -719,8 +777,22 @@ struct Engine {
     if constexpr (std::is_same<V, float>::value) {
       const char* e = std::getenv("HPRQP_QAP_TC");
       use_tc = nmax <= tc::kTile && !(e && e[0] == '0');
-      if (use_tc)
+      if (use_tc) {
         HPRQP_CUDA(cudaFuncSetAttribute(k_qap_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, kQapTcSmem));
+        // the constant operands' TF32 images, once per batch (k_qap_images)
+        std::vector<int64_t> io(B);
+        int64_t tot = 0;
+        for (int k = 0; k < B; ++k) {
+          io[k] = tot;
+          tot += 4 * (int64_t)((F.qn[k] + tc::kChunk - 1) / tc::kChunk) * kQapImgChunk;
+        }
+        qimg_off = up(io);
+        qimg = mem.alloc<float>(std::max<int64_t>(tot, 1));
+        k_qap_images<<<dim3((unsigned)B, 4, (unsigned)((nmax + tc::kChunk - 1) / tc::kChunk)), 256, 0, st>>>(
+            qn, off, qimg_off, (const float*)QA, (const float*)QB, (const float*)QS, (const float*)QT, (float*)qimg);
+        HPRQP_LAUNCH_CHECK();
+        HPRQP_CUDA(cudaStreamSynchronize(st));
+      }
     }
   }
   // true (and the flag cleared) when a tensor-core operator launch gave up
@@ -738,11 +810,13 @@ struct Engine {
     HPRQP_LAUNCH_CHECK();
   }
   bool use_tc = false;  // FP32 engine, every n_k <= 128: the tensor-core operator
+  float* qimg = nullptr;        // its constant operands' TF32 hi/lo images
+  int64_t* qimg_off = nullptr;  // per instance, in floats
   // Q operator for the instances in `mk`: yout = Q_k(xin)
   void qmap(const V* xin, V* yout, const unsigned char* mk) {
     if constexpr (std::is_same<V, float>::value) {
       if (use_tc) {
-        k_qap_tc<<<B, kQapTcThreads, kQapTcSmem, st>>>(qn, off, mk, QA, QB, QS, QT, xin, yout);
+        k_qap_tc<<<B, kQapTcThreads, kQapTcSmem, st>>>(qn, off, qimg_off, mk, qimg, xin, yout);
         check();
         return;
       }
