@@ -81,7 +81,7 @@ def parse():
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--lam-A", type=float, default=0.44866094653915195)
     ap.add_argument("--lam-Q", type=float, default=0.8051445993716677)
-    ap.add_argument("--tpr", default="0", help="CSR threads per row, 'sell', 'ell', or 0 = autotune")
+    ap.add_argument("--tpr", default="0", help="CSR threads per row, 'sell', 'ell', 'split', 'staged', or 0 = autotune")
     return ap.parse_args()
 
 
@@ -617,7 +617,7 @@ def _profile_model(a):
 
 def _pin(p, a):
     if a.tpr != "0":
-        p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr in ("sell", "ell") else int(a.tpr)
+        p.spmv_mode_Q = p.spmv_mode_A = a.tpr if a.tpr in ("sell", "ell", "split", "staged") else int(a.tpr)
     return p
 
 

@@ -82,9 +82,10 @@ class HPRQP_parameters:
 def _spmv_mode(v) -> int:
     """'auto' (autotuned), 'CUSPARSE'/'customized' (reference names, treated
     as auto), 'sell' (SELL-32), 'ell' (ELL), 'split' (long rows cut into
-    equal pieces), or an explicit CSR threads-per-row 1..32."""
+    equal pieces), 'staged' (column blocks of the input vector in shared
+    memory), or an explicit CSR threads-per-row 1..32."""
     if isinstance(v, str):
-        return {"sell": 7, "ell": 8, "split": 9}.get(v.lower(), 0)
+        return {"sell": 7, "ell": 8, "split": 9, "staged": 10}.get(v.lower(), 0)
     t = int(v)
     if t not in (1, 2, 4, 8, 16, 32):
         raise ValueError("threads per row must be 1, 2, 4, 8, 16 or 32")

@@ -30,6 +30,8 @@ struct Error : std::runtime_error {
 
 #ifdef __CUDACC__
 constexpr int kBlock = 256;  // threads per CTA for every row/element kernel
+constexpr int kStageSmem = 200 * 1024;     // its shared-memory budget for one column block
+constexpr int kStageSlots = 2048;          // and the row-sum slots of one tile (FP64 at most: 16 KiB)
 
 // Device view of a sparse matrix: CSR (0-based, int32 indices), plus
 // optional ELL and SELL-32 copies (slices of 32 consecutive rows stored column-major,
@@ -67,6 +69,33 @@ struct DCsr {
   const int2* srow = nullptr;
   double* spart = nullptr;
   unsigned* scnt = nullptr;
+  // Column-blocked staged schedule (k_stage_pass), for products whose input
+  // gathers dominate: the columns are cut into st_nblk blocks of st_bw
+  // columns, each small enough for one CTA's shared memory.  Block b's part
+  // of every row is a run of 8-entry chunks (zero-padded, at least one per
+  // row) holding 16-bit block-local columns and the values; chunk offsets
+  // st_cptr[b * (rows + 1) + r].  Tiles {first warp tile, chunks, first row,
+  // end row} are runs of whole rows with at most kStageSlots row-sum slots,
+  // starting at a whole warp tile (32 chunks; the values of a warp tile are
+  // stored lane-interleaved in 16-byte slices); each warp tile has a
+  // descriptor {first slot, segment-head mask}, and a row has one slot per
+  // warp tile it touches (first slot st_srow[b * (rows + 1) + r]).  CTA i
+  // of the one-wave grid takes block st_item[i].x and tiles [st_item[i].y,
+  // st_item[i].z).  With several blocks a row's block sums go to
+  // st_part[b * rows + r] and the last block to arrive (counter st_cnt[r])
+  // folds them in block order.
+  bool stage = false;
+  int st_nblk = 0, st_bw = 0, st_grid = 0, st_ntile = 0;
+  int64_t st_chunks = 0, st_nwt = 0;
+  const int* st_cptr = nullptr;
+  const int* st_srow = nullptr;
+  const uint16_t* st_col = nullptr;
+  const V* st_val = nullptr;
+  const int2* st_wt = nullptr;
+  const int4* st_tile = nullptr;
+  const int4* st_item = nullptr;
+  double* st_part = nullptr;
+  unsigned* st_cnt = nullptr;
 };
 
 // Programmatic dependent launch: wait until the previous kernel in the

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -107,6 +108,40 @@ static void launch(Common& cm, void (*kernel)(KArgs...), dim3 grid, int block, A
   cfg.numAttrs = cm.pdl ? 1 : 0;
   HPRQP_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
   cm.launches++;
+}
+
+// launch() with dynamic shared memory; the kernel's limit is raised once per
+// device to the staged pass's column block and row-sum slots
+template <typename... KArgs, typename... Args>
+static void launch_smem(Common& cm, void (*kernel)(KArgs...), dim3 grid, int block, size_t smem, Args... args) {
+  static std::atomic<uint64_t> raised{0};  // bit d: done on device d
+  int dev = 0;
+  HPRQP_CUDA(cudaGetDevice(&dev));
+  const uint64_t bit = 1ull << (dev & 63);
+  if (!(raised.load() & bit)) {
+    HPRQP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    kStageSmem + kStageSlots * (int)sizeof(double)));
+    raised.fetch_or(bit);
+  }
+  cudaLaunchConfig_t cfg{};
+  cfg.gridDim = grid;
+  cfg.blockDim = dim3((unsigned)block);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = cm.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = cm.pdl ? 1 : 0;
+  HPRQP_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
+  cm.launches++;
+}
+
+// threads per row of a CSR pass by the mean row length (the fixed rule)
+static int csr_tpr(double avg) {
+  int t = 1;
+  while (t < 32 && avg >= 4.0 * t) t *= 2;
+  return t;
 }
 
 template <int TPR, typename Acc, typename Src, typename Epi>
@@ -313,12 +348,18 @@ void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode, const DevCsr
     build_split(h, d);
     d.split = d.npieces > 0;
     d.tpr = 4;
+  } else if (tpr_mode == 10) {  // staged column blocks requested
+    build_stage(h, d);
+    d.stage = d.st_nblk > 0;
+    d.tpr = csr_tpr((double)d.nnz / std::max(d.rows, 1));
   } else if (tpr_mode > 0) {
     d.tpr = 1 << std::min(tpr_mode - 1, 5);
   } else {
     build_sell(h, d);
     build_ell(h, d);
     build_split(h, d);
+    // (an ELL copy of width <= 8 is taken untimed: no other copy is needed)
+    if (!(cm.ell_prologue > 0 && d.ell_w > 0 && d.ell_w <= 8)) build_stage(h, d);
     d.tpr = autotune(d);
   }
 }
@@ -411,6 +452,220 @@ void Engine<V>::build_split(const HCsr& h, DCsr<V>& d) {
   d.split_T = (int)T;
 }
 
+// Set-up of the staged copy.  Chunks of row r in block b: the entries of
+// row r whose column lies in [b bw, (b + 1) bw), 8 per chunk, at least one
+// chunk per row.  One thread per (row, block).
+__global__ void __launch_bounds__(kBlock) k_stage_count(int rows, int nblk, int bw, const int* __restrict__ ptr,
+                                                        const int* __restrict__ col, int* __restrict__ chunks) {
+  const int64_t t = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (t >= (int64_t)rows * nblk) return;
+  const int r = (int)(t % rows), b = (int)(t / rows);
+  const int lo = b * bw, hi = lo + bw;
+  int n = 0;
+  for (int k = ptr[r]; k < ptr[r + 1]; ++k) n += (col[k] >= lo && col[k] < hi) ? 1 : 0;
+  chunks[t] = n > 0 ? (n + 7) / 8 : 1;
+}
+
+// Fill: row r's entries of block b, in CSR order, from chunk cptr[b][r]
+// on (the copy was zeroed first, so the padding is column 0, value 0).
+// Entry e of chunk c = 32 g + l: its column at 8 c + e; its value in the
+// lane-interleaved slices of warp tile g (slice e / S of lane l, S values
+// of 16 bytes each).
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_stage_fill(int rows, int nblk, int bw, const int* __restrict__ ptr,
+                                                       const int* __restrict__ col, const V* __restrict__ val,
+                                                       const int* __restrict__ cptr, uint16_t* __restrict__ scol,
+                                                       V* __restrict__ sval) {
+  constexpr int S = 16 / (int)sizeof(V);
+  const int64_t t = (int64_t)blockIdx.x * kBlock + threadIdx.x;
+  if (t >= (int64_t)rows * nblk) return;
+  const int r = (int)(t % rows), b = (int)(t / rows);
+  const int lo = b * bw, hi = lo + bw;
+  int64_t j = (int64_t)cptr[(int64_t)b * (rows + 1) + r] * 8;
+  for (int k = ptr[r]; k < ptr[r + 1]; ++k) {
+    const int c = col[k];
+    if (c >= lo && c < hi) {
+      const int64_t ch = j >> 3, g = ch >> 5, l = ch & 31;
+      const int e = (int)(j & 7);
+      scol[j] = (uint16_t)(c - lo);
+      sval[((g * (8 / S) + e / S) * 32 + l) * S + e % S] = val[k];
+      ++j;
+    }
+  }
+}
+
+// Staged copy (DCsr::stage) of a CSR matrix whose products are bound by their
+// gathers: built for rows of at least 16 entries on average, at least 65,536
+// entries, and an input vector of at most 32 column blocks of kStageSmem
+// bytes.  Counts on the device; slots, windows, tiles and the CTA split on
+// the host; the scatter on the device.
+template <typename V>
+void Engine<V>::build_stage(const HCsr& h, DCsr<V>& d) {
+  d.st_nblk = 0;
+  if (h.rows <= 0 || h.cols <= 0 || h.nnz() < 65536) return;
+  if ((double)h.nnz() / (double)h.rows < 16.0) return;
+  const int64_t per = kStageSmem / (int64_t)sizeof(V);
+  const int64_t nblk = (h.cols + per - 1) / per;
+  if (nblk > 32 || nblk >= cm.num_sms) return;
+  // block width a multiple of 8 (16-byte staging loads); at most
+  // kStageSmem / 4 = 51,200 columns, so block-local columns fit 16 bits
+  const int bw = (int)(((h.cols + nblk - 1) / nblk + 7) / 8 * 8);
+  const int rows = (int)h.rows;
+  const int nb = (int)nblk;
+  const int64_t pairs = (int64_t)rows * nb;
+  int* dch = mem.alloc<int>(pairs);
+  const int g1 = (int)((pairs + kBlock - 1) / kBlock);
+  k_stage_count<<<g1, kBlock, 0, cm.stream>>>(rows, nb, bw, d.ptr, d.col, dch);
+  HPRQP_LAUNCH_CHECK();
+  std::vector<int> ch((size_t)pairs);
+  cm.to_host(ch.data(), dch, sizeof(int) * (size_t)pairs);
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+  // chunk offsets, block-major
+  const size_t R1 = (size_t)rows + 1;
+  std::vector<int> cptr((size_t)nb * R1), srow((size_t)nb * R1);
+  int64_t tot = 0;
+  std::vector<double> bcost(nb, 0.0);  // chunks + 1 a row (its slot and epilogue)
+  for (int b = 0; b < nb; ++b) {
+    const int64_t b0 = tot;
+    for (int r = 0; r < rows; ++r) {
+      cptr[(size_t)b * R1 + r] = (int)tot;
+      tot += ch[(size_t)b * rows + r];
+      if (tot > INT32_MAX / 8) return;
+    }
+    cptr[(size_t)b * R1 + rows] = (int)tot;
+    bcost[b] = (double)(tot - b0) + rows;
+  }
+  // one CTA per SM; block b gets a share of them by its cost (at least one,
+  // at most one per row)
+  const int G = cm.num_sms;
+  double total = 0;
+  for (double c : bcost) total += c;
+  std::vector<int> kb(nb);
+  int sum = 0;
+  for (int b = 0; b < nb; ++b) {
+    kb[b] = std::max(1, std::min(rows, (int)std::floor(G * bcost[b] / total)));
+    sum += kb[b];
+  }
+  while (sum < G) {  // the block with the most cost per CTA gets one more
+    int best = -1;
+    double bv = 0;
+    for (int b = 0; b < nb; ++b)
+      if (kb[b] < rows && bcost[b] / kb[b] > bv) { bv = bcost[b] / kb[b]; best = b; }
+    if (best < 0) break;
+    ++kb[best];
+    ++sum;
+  }
+  while (sum > G) {  // the block with the least cost per CTA gives one back
+    int best = -1;
+    double bv = 1e300;
+    for (int b = 0; b < nb; ++b)
+      if (kb[b] > 1 && bcost[b] / kb[b] < bv) { bv = bcost[b] / kb[b]; best = b; }
+    if (best < 0) return;
+    --kb[best];
+    --sum;
+  }
+  // Each block's rows cut into kb[b] runs of about equal cost, each run into
+  // tiles of whole rows with at most kStageSlots slots.  A tile's chunks are
+  // cut into 32-chunk warp tiles from its first chunk on, and a tile starts at
+  // a whole warp tile of the copy (pc = a row's first chunk there); a row has
+  // one slot per warp tile it touches (its segments), numbered in row order.
+  std::vector<int> pc((size_t)nb * R1);
+  std::vector<int2> wt;
+  std::vector<int4> tile, item;
+  std::vector<unsigned> heads;
+  std::vector<int> first;
+  for (int b = 0; b < nb; ++b) {
+    const int* cb = ch.data() + (size_t)b * rows;
+    const int* pb = cptr.data() + (size_t)b * R1;
+    int* sb = srow.data() + (size_t)b * R1;
+    int* pcb = pc.data() + (size_t)b * R1;
+    int64_t slot = 0;
+    int r = 0;
+    double acc = 0;
+    for (int i = 0; i < kb[b]; ++i) {
+      const double end = bcost[b] * (double)(i + 1) / kb[b];
+      int re = r;
+      if (i == kb[b] - 1) {
+        re = rows;
+      } else {
+        while (re < rows && (re == r || acc + 0.5 * (cb[re] + 1) <= end)) acc += cb[re++] + 1;
+      }
+      const int t0 = (int)tile.size();
+      int q = r;
+      while (q < re) {  // one tile from row q
+        const int r0 = q;
+        int64_t slots = 0;
+        while (q < re) {  // the warp tiles row q touches, from the tile's first chunk
+          const int o = pb[q] - pb[r0];
+          const int64_t touch = (o + cb[q] - 1) / 32 - o / 32 + 1;
+          if (slots + touch > kStageSlots) break;
+          slots += touch;
+          ++q;
+        }
+        if (q == r0) return;  // one row with more slots than a tile holds
+        const int nwt = (pb[q] - pb[r0] + 31) / 32;
+        heads.assign(nwt, 0u);
+        first.assign(nwt, -1);
+        if ((int64_t)(wt.size() + nwt) * 32 > INT32_MAX / 8) return;
+        for (int rr = r0; rr < q; ++rr) {
+          const int o = pb[rr] - pb[r0];
+          sb[rr] = (int)slot;
+          pcb[rr] = (int)(32 * wt.size()) + o;
+          for (int w = o / 32; w <= (o + cb[rr] - 1) / 32; ++w) {
+            heads[w] |= 1u << (std::max(o, 32 * w) - 32 * w);
+            if (first[w] < 0) first[w] = (int)slot;
+            ++slot;
+          }
+        }
+        if (slot > INT32_MAX / 2) return;
+        tile.push_back(make_int4((int)wt.size(), pb[q] - pb[r0], r0, q));
+        for (int w = 0; w < nwt; ++w) wt.push_back(make_int2(first[w], (int)heads[w]));
+      }
+      item.push_back(make_int4(b, t0, (int)tile.size(), 0));
+      r = re;
+    }
+    sb[rows] = (int)slot;
+  }
+  tot = 32 * (int64_t)wt.size();  // chunks of the copy, the tiles' tails padded
+  int* dcp = mem.alloc<int>((int64_t)pc.size());
+  int* dsr = mem.alloc<int>((int64_t)srow.size());
+  int2* dwt = mem.alloc<int2>((int64_t)wt.size());
+  int4* dtile = mem.alloc<int4>((int64_t)tile.size());
+  int4* ditem = mem.alloc<int4>((int64_t)item.size());
+  uint16_t* scol = mem.alloc<uint16_t>(tot * 8);
+  V* sval = mem.alloc<V>(tot * 8);
+  if ((reinterpret_cast<uintptr_t>(scol) | reinterpret_cast<uintptr_t>(sval)) & 15u) return;  // 16-byte chunk loads
+  cm.to_dev(dcp, pc.data(), sizeof(int) * pc.size());
+  cm.to_dev(dsr, srow.data(), sizeof(int) * srow.size());
+  cm.to_dev(dwt, wt.data(), sizeof(int2) * wt.size());
+  cm.to_dev(dtile, tile.data(), sizeof(int4) * tile.size());
+  cm.to_dev(ditem, item.data(), sizeof(int4) * item.size());
+  HPRQP_CUDA(cudaMemsetAsync(scol, 0, sizeof(uint16_t) * (size_t)tot * 8, cm.stream));
+  HPRQP_CUDA(cudaMemsetAsync(sval, 0, sizeof(V) * (size_t)tot * 8, cm.stream));
+  k_stage_fill<V><<<g1, kBlock, 0, cm.stream>>>(rows, nb, bw, d.ptr, d.col, d.val, dcp, scol, sval);
+  HPRQP_LAUNCH_CHECK();
+  if (nb > 1) {
+    d.st_part = mem.alloc<double>(pairs);
+    unsigned* cnt = mem.alloc<unsigned>(rows);
+    HPRQP_CUDA(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * rows, cm.stream));
+    d.st_cnt = cnt;
+  }
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));  // host staging vectors go out of scope
+  d.st_col = scol;
+  d.st_val = sval;
+  d.st_wt = dwt;
+  d.st_tile = dtile;
+  d.st_item = ditem;
+  d.st_cptr = dcp;
+  d.st_srow = dsr;
+  d.st_chunks = tot;
+  d.st_nwt = (int64_t)wt.size();
+  d.st_ntile = (int)tile.size();
+  d.st_grid = (int)item.size();
+  d.st_bw = bw;
+  d.st_nblk = nb;
+}
+
 // SELL-32 copy of a CSR matrix, built on the device from its CSR; skipped
 // when padding would exceed 50%.
 template <typename V>
@@ -445,7 +700,12 @@ void Engine<V>::build_sell(const HCsr& h, DCsr<V>& d) {
 template <typename V>
 template <typename Epi>
 void Engine<V>::mat_rows(const DCsr<V>& M, const V* xin, const Epi& e) {
-  if (M.split) {
+  if (M.stage) {
+    const StageView<V> sv{(int)M.rows, (int)M.cols, M.st_bw, M.st_nblk, M.st_col, M.st_val, M.st_wt,
+                          M.st_tile, M.st_item, M.st_srow, M.st_part, M.st_cnt};
+    launch_smem(cm, k_stage_pass<V, V, V, Epi>, M.st_grid, stage_block<V>(),
+                (size_t)kStageSlots * sizeof(V) + (size_t)M.st_bw * sizeof(V), sv, xin, e);
+  } else if (M.split) {
     const int grid = (int)(((int64_t)M.npieces * 32 + kBlock - 1) / kBlock);
     launch(cm, k_split_pass<V, V, V, Epi>, grid, kBlock, M.npieces, M.pieces, M.ptr, M.col, M.val, xin, M.srow,
            M.split_T, M.spart, M.scnt, e);
@@ -519,15 +779,14 @@ template <typename V>
 int Engine<V>::autotune(DCsr<V>& d) {
   if (d.rows <= 0 || d.nnz == 0) return 1;
   const double avg = (double)d.nnz / d.rows;
-  if (!cm.autotune) {  // fixed rule: ELL, else SELL-32, else threads per row by mean row length
+  if (!cm.autotune) {  // fixed rule: ELL, else staged, else SELL-32, else threads per row by mean row length
     d.ell = d.ell_w > 0;
-    d.sell = !d.ell && d.sell_len > 0;
-    d.split = !d.ell && !d.sell && d.npieces > 0;
+    d.stage = !d.ell && d.st_nblk > 0;
+    d.sell = !d.ell && !d.stage && d.sell_len > 0;
+    d.split = !d.ell && !d.stage && !d.sell && d.npieces > 0;
     if (d.ell || d.sell) return 1;
     if (d.split) return 32;
-    int t = 1;
-    while (t < 32 && avg >= 4.0 * t) t *= 2;
-    return t;
+    return csr_tpr(avg);
   }
   // An ELL copy of width <= 8 runs the passes with its loads before the wait
   // on the previous pass (k_ell_pass).  Timing products alone cannot see that
@@ -538,6 +797,7 @@ int Engine<V>::autotune(DCsr<V>& d) {
     d.ell = true;
     d.sell = false;
     d.split = false;
+    d.stage = false;
     return 1;
   }
   cudaEvent_t e0, e1;
@@ -545,20 +805,24 @@ int Engine<V>::autotune(DCsr<V>& d) {
   HPRQP_CUDA(cudaEventCreate(&e1));
   float best = 1e30f;
   int best_t = 4;
-  bool best_sell = false, best_ell = false, best_split = false;
-  // candidate -1 = SELL-32, -2 = ELL (one thread per row each); each timed as
-  // the best of 3 rounds of 4 back-to-back products, so a noisy round cannot
-  // decide.
-  for (int t : {-3, -2, -1, 1, 2, 4, 8, 16, 32}) {
+  bool best_sell = false, best_ell = false, best_split = false, best_stage = false;
+  // candidate -1 = SELL-32, -2 = ELL (one thread per row each), -3 = row
+  // split, -4 = staged column blocks; each timed as the best of 3 rounds of 4
+  // back-to-back products, so a noisy round cannot decide.
+  for (int t : {-4, -3, -2, -1, 1, 2, 4, 8, 16, 32}) {
+    if (t == -4 && d.st_nblk == 0) continue;
     if (t == -3 && d.npieces == 0) continue;
     if (t == -2 && d.ell_w == 0) continue;
     if (t == -1 && d.sell_len == 0) continue;
     if (t == 1 && avg > 12) continue;
     if (t == 32 && avg < 8) continue;
+    d.stage = (t == -4);
     d.split = (t == -3);
     d.ell = (t == -2);
     d.sell = (t == -1);
-    d.tpr = t == -3 ? 32 : t < 0 ? 1 : t;  // (a split matrix's reductions run on CSR, 32 lanes per row)
+    // (the reductions of a split matrix run on CSR with 32 lanes per row, of
+    // a staged one with the fixed rule's lanes)
+    d.tpr = t == -4 ? csr_tpr(avg) : t == -3 ? 32 : t < 0 ? 1 : t;
     spmv(d, pz, pt);
     float tbest = 1e30f;
     for (int round = 0; round < 3; ++round) {
@@ -570,13 +834,21 @@ int Engine<V>::autotune(DCsr<V>& d) {
       HPRQP_CUDA(cudaEventElapsedTime(&ms, e0, e1));
       tbest = std::min(tbest, ms);
     }
-    if (tbest < best) { best = tbest; best_t = d.tpr; best_sell = d.sell; best_ell = d.ell; best_split = d.split; }
+    if (tbest < best) {
+      best = tbest;
+      best_t = d.tpr;
+      best_sell = d.sell;
+      best_ell = d.ell;
+      best_split = d.split;
+      best_stage = d.stage;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   d.sell = best_sell;
   d.ell = best_ell;
   d.split = best_split;
+  d.stage = best_stage;
   return best_t;
 }
 
@@ -1054,8 +1326,18 @@ double Engine<V>::power_step_bytes(int which) const {
 template <typename V>
 void Engine<V>::pass_info(int k, const char** name, double* bytes, int* tpr) const {
   const double v = sizeof(V), d = sizeof(V);  // d: the Halpern anchors (storage type too)
-  auto csr = [&](const DCsr<V>& M) { return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1); };
-  auto sched = [](const DCsr<V>& M) { return M.split ? -3 : M.ell ? -1 : M.sell ? 0 : M.tpr; };  // 0 = SELL-32, -1 = ELL, -3 = row split
+  // the staged copy streams its padded chunks (16-bit columns), the warp-tile
+  // descriptors, the row slot offsets and, with several column blocks, the
+  // block sums
+  auto csr = [&](const DCsr<V>& M) {
+    if (M.stage)
+      return (double)M.st_chunks * 8.0 * (v + 2.0) + 8.0 * M.st_nwt + 16.0 * (M.st_ntile + M.st_grid) +
+             4.0 * M.st_nblk * (M.rows + 1) +
+             (M.st_nblk > 1 ? 16.0 * M.st_nblk * M.rows + 8.0 * M.rows : 0.0);
+    return (double)M.nnz * (v + 4.0) + 4.0 * (M.rows + 1);
+  };
+  // 0 = SELL-32, -1 = ELL, -3 = row split, -4 = staged column blocks
+  auto sched = [](const DCsr<V>& M) { return M.stage ? -4 : M.split ? -3 : M.ell ? -1 : M.sell ? 0 : M.tpr; };
   const double N = (double)n, M_ = (double)m;
   const double dg = Q_is_diag ? 2 * N * v : 0.0;
   *name = "?";

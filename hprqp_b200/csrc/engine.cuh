@@ -222,6 +222,7 @@ class Engine {
   void build_sell(const HCsr& h, DCsr<V>& d);
   void build_ell(const HCsr& h, DCsr<V>& d);
   void build_split(const HCsr& h, DCsr<V>& d);
+  void build_stage(const HCsr& h, DCsr<V>& d);
   void qap_apply(const V* xin, V* yout);
   void build_gram(const Prepared& pp, int tpr_mode);  // tpr_mode: A's (pinned when > 0)
   void gram_values();

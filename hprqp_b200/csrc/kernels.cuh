@@ -221,6 +221,210 @@ __global__ void __launch_bounds__(kBlock) k_split_pass(int npieces, const int4* 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Staged pass (DCsr::stage): the input vector's column block sits in shared
+// memory, so the gathers cost a shared-memory access (a few bank conflicts)
+// instead of one L1 wavefront per lane; the matrix streams as 16-byte
+// loads of 8 16-bit columns and 8 values per lane.
+// ---------------------------------------------------------------------------
+template <typename V>
+struct StageView {
+  int rows, cols, bw, nblk;
+  const uint16_t* __restrict__ col;
+  const V* __restrict__ val;
+  const int2* __restrict__ wt;    // per 32-chunk warp tile {first slot, segment-head mask}
+  const int4* __restrict__ tile;  // {first warp tile, chunks, first row, end row}
+  const int4* __restrict__ item;  // per CTA {block, first tile, end tile, 0}
+  const int* __restrict__ srow;   // nblk x (rows + 1): first slot of each row
+  double* __restrict__ part;      // nblk x rows block sums (nblk > 1)
+  unsigned* __restrict__ cnt;     // per-row arrivals (nblk > 1)
+};
+
+// Chunk c = 32 g + l (lane l of warp tile g) of the staged copy in registers:
+// 8 16-bit columns (two per word; the 32 chunks of a warp tile are 512
+// contiguous bytes) and 8 values, stored lane-interleaved in 16-byte slices
+// (slice q of the 32 lanes contiguous), so every load of a warp reads 512
+// contiguous bytes.
+template <typename V>
+struct StageChunk {
+  uint4 c;
+  V v[8];
+};
+
+template <typename V>
+__device__ __forceinline__ void stage_load(StageChunk<V>& k, const uint16_t* __restrict__ col,
+                                           const V* __restrict__ val, int64_t g, int l) {
+  k.c = __ldg(reinterpret_cast<const uint4*>(col) + g * 32 + l);
+  if constexpr (sizeof(V) == 4) {
+    const float4 a = __ldg(reinterpret_cast<const float4*>(val) + (g * 2 + 0) * 32 + l);
+    const float4 b = __ldg(reinterpret_cast<const float4*>(val) + (g * 2 + 1) * 32 + l);
+    k.v[0] = a.x; k.v[1] = a.y; k.v[2] = a.z; k.v[3] = a.w; k.v[4] = b.x; k.v[5] = b.y; k.v[6] = b.z; k.v[7] = b.w;
+  } else {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const double2 a = __ldg(reinterpret_cast<const double2*>(val) + (g * 4 + q) * 32 + l);
+      k.v[2 * q] = a.x;
+      k.v[2 * q + 1] = a.y;
+    }
+  }
+}
+
+// Sum of the chunk's 8 products val[k] * xs[col[k]], in entry order.
+template <typename Acc, typename V, typename X>
+__device__ __forceinline__ Acc stage_dot(const StageChunk<V>& k, const X* xs) {
+  const unsigned idx[4] = {k.c.x, k.c.y, k.c.z, k.c.w};
+  Acc s = Acc(0);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    s = fma((Acc)k.v[2 * q], (Acc)xs[idx[q] & 0xffffu], s);
+    s = fma((Acc)k.v[2 * q + 1], (Acc)xs[idx[q] >> 16], s);
+  }
+  return s;
+}
+
+// Row r's sum over block b: the epilogue at once with one block; else the
+// block sum is stored and the last block to arrive folds the sums in block
+// order, resets the row's counter and runs the epilogue.
+template <typename Acc, typename V, typename Epi>
+__device__ __forceinline__ void stage_finish(const StageView<V>& s, int b, int r, Acc v, const Epi& epi) {
+  if (s.nblk == 1) {
+    epi(r, v);
+    return;
+  }
+  s.part[(size_t)b * s.rows + r] = (double)v;
+  __threadfence();
+  const unsigned a = atomicAdd(s.cnt + r, 1u);
+  if (a == (unsigned)(s.nblk - 1)) {
+    __threadfence();
+    Acc t = Acc(0);
+    for (int q = 0; q < s.nblk; ++q) t += (Acc)__ldcg(s.part + (size_t)q * s.rows + r);
+    s.cnt[r] = 0u;
+    epi(r, t);
+  }
+}
+
+// Threads of a staged-pass CTA (32 warps), and warp tiles a warp keeps in
+// flight: two in FP32; one in FP64, whose chunks take twice the registers
+// (two with 24 warps and 80 registers measured slower).
+template <typename V>
+__host__ __device__ constexpr int stage_block() { return 1024; }
+template <typename V>
+__host__ __device__ constexpr int stage_unroll() { return sizeof(V) == 8 ? 1 : 2; }
+
+// One CTA per SM (one wave).  CTA i stages block b = item[i].x of the input
+// into shared memory and runs its tiles [item.y, item.z) one after another,
+// each in two phases.  Phase 1: a tile's chunks [C0, C1) (C0 = 32 x its
+// first warp tile) are cut into warp tiles of 32 chunks; warp k takes warp
+// tiles k, k + NW, ... (two at a time in FP32, their loads in flight
+// together); lane l sums chunk l, and a segmented scan over the warp tile's
+// segment heads (row starts, and lane 0 where a row continues from the
+// previous warp tile) leaves each segment's sum in its last lane, which
+// stores it in the segment's shared-memory slot.
+// Phase 2: one thread per row of the tile (consecutive rows, so the
+// epilogue's accesses coalesce) folds the row's slots in order and finishes
+// the row.  Every lane but the tile's last warp tile's tail has a chunk, no
+// epilogue latency stalls the streaming phase, and every sum runs in a fixed
+// order.  The first tile's first loads (constant data) are issued before the
+// wait on the previous kernel.
+template <typename Acc, typename V, typename X, typename Epi>
+__global__ void __launch_bounds__(stage_block<V>(), 1) k_stage_pass(StageView<V> s, const X* __restrict__ x, Epi epi) {
+  extern __shared__ __align__(16) unsigned char stage_smem[];
+  Acc* sums = reinterpret_cast<Acc*>(stage_smem);
+  X* xs = reinterpret_cast<X*>(stage_smem + kStageSlots * sizeof(Acc));
+  constexpr int NT = stage_block<V>(), NW = NT / 32;
+  constexpr int U = stage_unroll<V>();  // warp tiles per step
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int4 it = __ldg(s.item + blockIdx.x);  // the schedule and the matrix are constant: before the wait
+  const int b = it.x;
+  const int* srow = s.srow + (size_t)b * (s.rows + 1);
+  int t = it.y;
+  int4 tl = make_int4(0, 0, 0, 0);
+  int C0 = 0, C1 = 0, k = warp;
+  StageChunk<V> ck[U];
+  int2 d[U];
+  auto load_step = [&]() {  // warp tiles k + u NW of tile tl
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int wt = k + u * NW;
+      d[u] = C0 + 32 * wt < C1 ? __ldg(s.wt + tl.x + wt) : make_int2(0, 0);
+      if (C0 + 32 * wt + lane < C1) stage_load(ck[u], s.col, s.val, (int64_t)tl.x + wt, lane);
+    }
+  };
+  if (t < it.z) {
+    tl = __ldg(s.tile + t);
+    C0 = 32 * tl.x;
+    C1 = C0 + tl.y;
+    load_step();
+  }
+  pdl_enter();
+  const int c0 = b * s.bw;
+  const int len = min(s.bw, s.cols - c0);
+  const X* src = x + c0;
+  if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+    constexpr int P = 16 / (int)sizeof(X);
+    const int nv = len / P;
+    for (int q = threadIdx.x; q < nv; q += NT)
+      reinterpret_cast<uint4*>(xs)[q] = __ldg(reinterpret_cast<const uint4*>(src) + q);
+    for (int q = nv * P + threadIdx.x; q < len; q += NT) xs[q] = __ldg(src + q);
+  } else {
+    for (int q = threadIdx.x; q < len; q += NT) xs[q] = __ldg(src + q);
+  }
+  __syncthreads();
+  for (; t < it.z;) {
+    const int slot0 = __ldg(srow + tl.z);
+    const int nwt = (C1 - C0 + 31) / 32;
+    while (k < nwt) {
+      Acc v[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {  // every gather before any slot store
+        v[u] = C0 + 32 * (k + u * NW) + lane < C1 ? stage_dot<Acc>(ck[u], xs) : Acc(0);
+      }
+      unsigned f[U], heads[U];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        heads[u] = (unsigned)d[u].y;  // bit l: chunk l starts a segment
+        f[u] = (heads[u] >> lane) & 1u;  // my segment's head is inside the lanes summed so far
+      }
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+          const Acc o = __shfl_up_sync(0xffffffffu, v[u], off);
+          const unsigned fo = __shfl_up_sync(0xffffffffu, f[u], off);
+          if (lane >= off) {
+            if (!f[u]) v[u] += o;
+            f[u] |= fo;
+          }
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int base = 32 * (k + u * NW);
+        const int last = min(31, C1 - C0 - base - 1);  // (negative: no such warp tile)
+        if (lane <= last && (lane == last || ((heads[u] >> (lane + 1)) & 1u)))
+          sums[d[u].x - slot0 + __popc(heads[u] & (0xffffffffu >> (31 - lane))) - 1] = v[u];
+      }
+      k += U * NW;
+      if (k < nwt) load_step();
+    }
+    __syncthreads();
+    for (int r = tl.z + (int)threadIdx.x; r < tl.w; r += NT) {
+      const int a = __ldg(srow + r) - slot0, e = __ldg(srow + r + 1) - slot0;
+      Acc acc = sums[a];
+      for (int q = a + 1; q < e; ++q) acc += sums[q];
+      stage_finish(s, b, r, acc, epi);
+    }
+    __syncthreads();  // the slots are the next tile's
+    if (++t < it.z) {
+      tl = __ldg(s.tile + t);
+      C0 = 32 * tl.x;
+      C1 = C0 + tl.y;
+      k = warp;
+      load_step();
+    }
+  }
+}
+
 // Block reduction of K slots; MaxMask bit k selects max (else sum).
 // Result valid in thread 0.
 template <int K, unsigned MaxMask>

@@ -555,9 +555,9 @@ static void check_params(const hprqp_params& p) {
   if (!p.use_gpu) throw Error(HPRQP_E_UNSUPPORTED, "use_gpu = false: libhprqp has no CPU path");
   if (p.precision != HPRQP_PRECISION_FP64 && p.precision != HPRQP_PRECISION_FP32_POLISH)
     throw Error(HPRQP_E_ARG, "unknown precision mode");
-  if (p.spmv_mode_Q < 0 || p.spmv_mode_Q > 9 || p.spmv_mode_A < 0 || p.spmv_mode_A > 9)
-    throw Error(HPRQP_E_ARG, "spmv_mode must be 0 (auto), 1..6 (CSR, 1..32 threads per row), 7 (SELL-32), 8 (ELL) "
-                             "or 9 (row split)");
+  if (p.spmv_mode_Q < 0 || p.spmv_mode_Q > 10 || p.spmv_mode_A < 0 || p.spmv_mode_A > 10)
+    throw Error(HPRQP_E_ARG, "spmv_mode must be 0 (auto), 1..6 (CSR, 1..32 threads per row), 7 (SELL-32), 8 (ELL), "
+                             "9 (row split) or 10 (staged column blocks)");
 }
 
 static void prepare(Handle& H, const hprqp_params& p) {

@@ -126,7 +126,11 @@ typedef struct hprqp_params {
                                         CSR with 1,2,4,...,32 threads per row;
                                         7 = SELL-32; 8 = ELL (short rows); 9 = row
                                         split (long rows cut into equal pieces,
-                                        one warp each; CSR where no row is long)   */
+                                        one warp each; CSR where no row is long);
+                                        10 = staged column blocks (the input
+                                        vector's blocks in shared memory, 16-bit
+                                        columns; CSR where the matrix is small,
+                                        its rows short or its input too long)      */
     int32_t spmv_mode_A;             /* same, for A and A'                          */
     int32_t print_frequency;         /* -1 = adaptive (print_step)                  */
     int32_t device_number;           /* 0                                           */
