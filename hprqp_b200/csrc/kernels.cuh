@@ -269,6 +269,16 @@ __device__ __forceinline__ void stage_load(StageChunk<V>& k, const uint16_t* __r
   }
 }
 
+// Bulk prefetch of warp tile g (its 512 bytes of columns and 256 values)
+// into L2: the loads of the warp's next step then wait for L2, not HBM, and
+// no register holds the data in flight.
+template <typename V>
+__device__ __forceinline__ void stage_prefetch(const uint16_t* col, const V* val, int64_t g) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(col + g * 256), "r"(512u) : "memory");
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(val + g * 256), "r"((unsigned)(256 * sizeof(V)))
+               : "memory");
+}
+
 // Sum of the chunk's 8 products val[k] * xs[col[k]], in entry order.
 template <typename Acc, typename V, typename X>
 __device__ __forceinline__ Acc stage_dot(const StageChunk<V>& k, const X* xs) {
@@ -325,7 +335,8 @@ __host__ __device__ constexpr int stage_unroll() { return sizeof(V) == 8 ? 1 : 2
 // the row.  Every lane but the tile's last warp tile's tail has a chunk, no
 // epilogue latency stalls the streaming phase, and every sum runs in a fixed
 // order.  The first tile's first loads (constant data) are issued before the
-// wait on the previous kernel.
+// wait on the previous kernel, and every step prefetches the warp's next
+// step into L2.
 template <typename Acc, typename V, typename X, typename Epi>
 __global__ void __launch_bounds__(stage_block<V>(), 1) k_stage_pass(StageView<V> s, const X* __restrict__ x, Epi epi) {
   extern __shared__ __align__(16) unsigned char stage_smem[];
@@ -342,12 +353,19 @@ __global__ void __launch_bounds__(stage_block<V>(), 1) k_stage_pass(StageView<V>
   int C0 = 0, C1 = 0, k = warp;
   StageChunk<V> ck[U];
   int2 d[U];
-  auto load_step = [&]() {  // warp tiles k + u NW of tile tl
+  auto load_step = [&]() {  // warp tiles k + u NW of tile tl; the next step's into L2
 #pragma unroll
     for (int u = 0; u < U; ++u) {
       const int wt = k + u * NW;
       d[u] = C0 + 32 * wt < C1 ? __ldg(s.wt + tl.x + wt) : make_int2(0, 0);
       if (C0 + 32 * wt + lane < C1) stage_load(ck[u], s.col, s.val, (int64_t)tl.x + wt, lane);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int wt = k + (U + u) * NW;
+        if (C0 + 32 * wt < C1) stage_prefetch(s.col, s.val, (int64_t)tl.x + wt);
+      }
     }
   };
   if (t < it.z) {
