@@ -1058,6 +1058,7 @@ template <typename V>
 Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int path_, int tpr_Q, int tpr_A,
                   bool power_engine)
     : cm(c_) {
+  const double t0 = wall_s();
   n = hp.n;
   m = hp.m;
   path = path_;
@@ -1099,9 +1100,14 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   AL = vec_in(pp.AL, ds ? ds->AL : nullptr, m);
   AU = vec_in(pp.AU, ds ? ds->AU : nullptr, m);
   row_norm = vec_in(pp.row_norm, ds ? ds->row_norm : nullptr, m);
+  HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+  const double t_vec = wall_s();
   upload_csr(pp.A, A, tpr_A, ds ? &ds->A : nullptr);
+  const double t_A = wall_s();
   upload_csr(pp.AT, AT, tpr_A, ds ? &ds->AT : nullptr);
+  const double t_AT = wall_s();
   if (has_Q_sparse) upload_csr(pp.Q, Q, tpr_Q, ds ? &ds->Q : nullptr);
+  const double t_Q = wall_s();
   if (is_lasso) {
     ltemp = mem.alloc<V>(hp.L.rows);
     upload_csr(hp.L, L, tpr_Q);
@@ -1127,9 +1133,16 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
     HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   }
   Qp = Q;
+  const double t_op = wall_s();
   if (power_engine) power_setup(pp, tpr_A, tpr_Q);
   reset_state();
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
+  if (const char* tv = std::getenv("HPRQP_TIMING"))
+    if (tv[0] == '1')
+      std::fprintf(stderr,
+                   "[hprqp] FP%d engine: vectors %.4f s, A %.4f s, A' %.4f s, Q %.4f s, LASSO/QAP %.4f s, "
+                   "power set-up %.4f s\n",
+                   (int)(8 * sizeof(V)), t_vec - t0, t_A - t_vec, t_AT - t_A, t_Q - t_AT, t_op - t_Q, wall_s() - t_op);
 }
 
 template <typename V>

@@ -104,11 +104,18 @@ bool csc_as_transpose(int64_t rows, int64_t cols, const int32_t* cp, const int32
 
 std::vector<double> copy_vec(const double* p, int64_t len, const char* what, bool allow_inf) {
   if (len > 0 && !p) throw Error(HPRQP_E_ARG, std::string(what) + ": null pointer");
-  std::vector<double> v(p, p + len);
-  for (double x : v) {
-    if (std::isnan(x)) throw Error(HPRQP_E_ARG, std::string(what) + " contains NaN values.");
-    if (!allow_inf && std::isinf(x)) throw Error(HPRQP_E_ARG, std::string(what) + " contains Inf values.");
+  std::vector<double> v;
+  par_copy(v, p, len);
+  // the first offending entry decides the message, as in a serial scan
+  int64_t first_nan = len, first_inf = len;
+#pragma omp parallel for schedule(static) reduction(min : first_nan, first_inf) num_threads(host_threads(len))
+  for (int64_t i = 0; i < len; ++i) {
+    if (std::isnan(v[i])) first_nan = std::min(first_nan, i);
+    if (std::isinf(v[i])) first_inf = std::min(first_inf, i);
   }
+  if (allow_inf) first_inf = len;
+  if (first_nan < first_inf) throw Error(HPRQP_E_ARG, std::string(what) + " contains NaN values.");
+  if (first_inf < len) throw Error(HPRQP_E_ARG, std::string(what) + " contains Inf values.");
   return v;
 }
 
@@ -196,6 +203,25 @@ int host_threads(int64_t work) {
   if (work < 65536) return 1;
   return std::max(1, std::min(16, omp_get_max_threads()));
 }
+
+template <typename T>
+void par_copy(std::vector<T>& dst, const T* src, int64_t len) {
+  dst.resize((size_t)len);
+  const int nt = host_threads(len);
+#pragma omp parallel for schedule(static) num_threads(nt)
+  for (int t = 0; t < nt; ++t) {
+    const int64_t a = len * t / nt, b = len * (t + 1) / nt;
+    if (b > a) std::memcpy(dst.data() + a, src + a, sizeof(T) * (size_t)(b - a));
+  }
+}
+template <typename T>
+void par_copy(std::vector<T>& dst, const std::vector<T>& src) {
+  par_copy(dst, src.data(), (int64_t)src.size());
+}
+template void par_copy<int>(std::vector<int>&, const std::vector<int>&);
+template void par_copy<double>(std::vector<double>&, const std::vector<double>&);
+template void par_copy<int>(std::vector<int>&, const int*, int64_t);
+template void par_copy<double>(std::vector<double>&, const double*, int64_t);
 
 HCsr transpose(const HCsr& A) {
   HCsr T;
@@ -491,6 +517,11 @@ void finish_sparse(Prepared& o, int64_t n) {
     }
     o.Q_maxval = Q.nnz() ? *std::max_element(Q.val.begin(), Q.val.end()) : 0.0;
   }
+}
+
+void finish_norms(Prepared& o) {
+  o.norm_b = norm_b_of(o.AL, o.AU, false);
+  o.norm_c = norm2(o.c);
 }
 
 void finish_common(const HostProblem& hp, Prepared& o) {

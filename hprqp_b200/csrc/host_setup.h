@@ -86,6 +86,9 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
 // the tails shared by both: norms, check_Q_diagonal and Q_maxval on the
 // scaled sparse Q; the noC rule
 void finish_sparse(Prepared& o, int64_t n);
+// the vector norms of finish_sparse alone (the GPU scaling checks Q's
+// diagonal on the device)
+void finish_norms(Prepared& o);
 void finish_common(const HostProblem& hp, Prepared& o);
 double norm_b_inf_org(const std::vector<double>& AL, const std::vector<double>& AU);
 double norm_inf(const std::vector<double>& v);
@@ -98,6 +101,13 @@ HCsr transpose(const HCsr& A);
 // merge needs sorted rows) or when the product's work, sum over the rows of
 // A of their length squared, exceeds max_work.
 bool gram_pattern(const HCsr& A, const HCsr& AT, int64_t max_work, HCsr& G);
+// dst = src with the copy split over host threads (the preparation copies
+// ~100 MB of patterns and vectors; one thread moves ~6 GB/s).
+template <typename T>
+void par_copy(std::vector<T>& dst, const std::vector<T>& src);
+// dst = src[0, len) likewise, from a caller's array
+template <typename T>
+void par_copy(std::vector<T>& dst, const T* src, int64_t len);
 // Host threads for a row-parallel loop over `work` items: 1 below ~64k
 // items (a parallel region costs more than it saves there), else at most
 // 16 (the loops are memory-bound; more threads only add wake-up cost).

@@ -8,8 +8,9 @@
 // sqrt / reciprocal / multiply in the host's order.  The symmetrised
 // pattern and its index maps come from the host (the pattern does not
 // change under scaling); the values are merged on the device.  The scaled
-// arrays are copied back into the host Prepared record, from which the
-// engines upload their copies as before.
+// vectors are copied back into the host Prepared record; the matrices'
+// scaled values stay on the device, where the engines copy them from, and
+// Q's diagonal check runs there too (k_qcheck).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -17,6 +18,7 @@
 #include <cstdlib>
 #include <cmath>
 #include <type_traits>
+#include <limits>
 #include <vector>
 
 #include "pool.h"
@@ -105,6 +107,42 @@ __global__ void k_sym(int nnz, const int* ia, const int* ib, const double* qv, c
   sv[p] = v / 2.0;
 }
 
+// check_Q_diagonal on the scaled S (src/utils.jl:827-855) and its largest
+// entry, on the device: row i's diagonal entry and the sum of |S_ij| in
+// stored (column) order.  S is exactly symmetric (entries (i,j) and (j,i)
+// are the same sum of the same two scaled values), so that row sum is
+// bitwise the column sum the host restatement accumulates in row order.  A
+// row fails when the sum and |diagonal| differ by more than rtol relative;
+// the failures are counted, and each CTA stores the largest entry it saw.
+__global__ void k_qcheck(int n, const int* __restrict__ ptr, const int* __restrict__ col,
+                         const double* __restrict__ val, double rtol, double* __restrict__ diag,
+                         unsigned* __restrict__ bad, double* __restrict__ bmax) {
+  __shared__ double sh[kT / 32];
+  const int i = blockIdx.x * kT + threadIdx.x;
+  double mx = -INFINITY;
+  if (i < n) {
+    double d = 0.0, sum = 0.0;
+    for (int k = ptr[i]; k < ptr[i + 1]; ++k) {
+      const double v = val[k];
+      sum += fabs(v);
+      if (col[k] == i) d = v;
+      mx = fmax(mx, v);
+    }
+    diag[i] = d;
+    const double x = sum, y = fabs(d);
+    const bool ok = (x == y) || (isfinite(x) && isfinite(y) && fabs(x - y) <= rtol * fmax(fabs(x), fabs(y)));
+    if (!ok) atomicAdd(bad, 1u);
+  }
+  for (int off = 16; off > 0; off >>= 1) mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, off));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = mx;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = sh[0];
+    for (int w = 1; w < kT / 32; ++w) m = fmax(m, sh[w]);
+    bmax[blockIdx.x] = m;
+  }
+}
+
 struct DevBuf : PoolBlocks {  // pool scratch freed at scope exit
   template <typename T>
   T* take(int64_t n) {
@@ -139,17 +177,17 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
     HCsr x;
     x.rows = h.rows;
     x.cols = h.cols;
-    x.ptr = h.ptr;
-    x.col = h.col;
+    par_copy(x.ptr, h.ptr);
+    par_copy(x.col, h.col);
     return x;
   };
   o.A = pattern_of(hp.A);
   o.AT = pattern_of(hp.AT);
-  o.c = hp.c;
-  o.AL = hp.AL;
-  o.AU = hp.AU;
-  o.l = hp.l;
-  o.u = hp.u;
+  par_copy(o.c, hp.c);
+  par_copy(o.AL, hp.AL);
+  par_copy(o.AU, hp.AU);
+  par_copy(o.l, hp.l);
+  par_copy(o.u, hp.u);
   o.row_norm.assign(m, 1.0);
   o.col_norm.assign(n, 1.0);
   o.norm_b_org = m > 0 ? norm_b_inf_org(o.AL, o.AU) : 0.0;
@@ -157,7 +195,13 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   const HCsr &Q = hp.Q, &QT = hp.QT;
   // merged pattern of Q + Q' with index maps (the values come later); a
   // structurally symmetric Q (the common case) is its own merged pattern
-  const bool sym_pattern = Q.ptr == QT.ptr && Q.col == QT.col;
+  bool sym_pattern = Q.ptr.size() == QT.ptr.size() && Q.col.size() == QT.col.size();
+  if (sym_pattern) {
+    const int64_t np = (int64_t)Q.ptr.size(), nc = (int64_t)Q.col.size();
+#pragma omp parallel for schedule(static) reduction(&& : sym_pattern) num_threads(host_threads(np + nc))
+    for (int64_t k = 0; k < np + nc; ++k)
+      sym_pattern = sym_pattern && (k < np ? Q.ptr[k] == QT.ptr[k] : Q.col[k - np] == QT.col[k - np]);
+  }
   std::vector<int> len(sym_pattern ? 0 : n, 0);
   auto merge = [&](int64_t i, int* cols, int* ia, int* ib) {
     int a = Q.ptr[i], b = QT.ptr[i], cnt = 0;
@@ -182,8 +226,8 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   S.rows = S.cols = n;
   std::vector<int> ia, ib;
   if (sym_pattern) {
-    S.ptr = Q.ptr;
-    S.col = Q.col;
+    par_copy(S.ptr, Q.ptr);
+    par_copy(S.col, Q.col);
   } else {
 #pragma omp parallel for schedule(static) num_threads(host_threads(n))
     for (int64_t i = 0; i < n; ++i) len[i] = merge(i, nullptr, nullptr, nullptr);
@@ -196,7 +240,7 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
     for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], ia.data() + S.ptr[i], ib.data() + S.ptr[i]);
   }
   const int64_t nnzS = S.ptr[n];
-  S.val.resize(nnzS);
+  // (S's values stay on the device: the engines copy them from there)
 
   tm[nt++] = wall();  // merged pattern
   // device copies: what the engines copy from afterwards lives in ds->mem,
@@ -277,22 +321,6 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   }
   k_sym<<<blocks(nnzS), kT, 0, st>>>((int)nnzS, dia, dib, dQ.val, dQT.val, sv);
   HPRQP_LAUNCH_CHECK();
-  HPRQP_CUDA(cudaStreamSynchronize(st));
-  tm[nt++] = wall();  // scaling kernels
-  auto down = [&](std::vector<double>& dst, const double* src) {
-    if (!dst.empty()) {
-      HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
-      *d2h += (int64_t)(sizeof(double) * dst.size());
-    }
-  };
-  down(S.val, sv);
-  down(o.c, c);
-  down(o.l, l);
-  down(o.u, u);
-  down(o.col_norm, cn);
-  down(o.AL, AL);
-  down(o.AU, AU);
-  down(o.row_norm, rn);
   // S's pattern on the device (Q's when that is symmetric)
   const int *sptr = dQ.ptr, *scol = dQ.col;
   if (!sym_pattern) {
@@ -303,7 +331,39 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
     sptr = p2;
     scol = c2;
   }
+  double* dg = d.take<double>(n);
+  unsigned* bad = d.take<unsigned>(1);
+  const int nb = blocks(n);
+  double* bmax = d.take<double>(nb);
+  HPRQP_CUDA(cudaMemsetAsync(bad, 0, sizeof(unsigned), st));
+  k_qcheck<<<nb, kT, 0, st>>>((int)n, sptr, scol, sv, std::sqrt(std::numeric_limits<double>::epsilon()), dg, bad,
+                              bmax);
+  HPRQP_LAUNCH_CHECK();
   HPRQP_CUDA(cudaStreamSynchronize(st));
+  tm[nt++] = wall();  // scaling kernels
+  auto down = [&](std::vector<double>& dst, const double* src) {
+    if (!dst.empty()) {
+      HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
+      *d2h += (int64_t)(sizeof(double) * dst.size());
+    }
+  };
+  o.diag_Q.assign(n, 0.0);
+  down(o.diag_Q, dg);
+  std::vector<double> hmax(nb);
+  down(hmax, bmax);
+  unsigned nbad = 0;
+  HPRQP_CUDA(cudaMemcpyAsync(&nbad, bad, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+  *d2h += (int64_t)sizeof(unsigned);
+  down(o.c, c);
+  down(o.l, l);
+  down(o.u, u);
+  down(o.col_norm, cn);
+  down(o.AL, AL);
+  down(o.AU, AU);
+  down(o.row_norm, rn);
+  HPRQP_CUDA(cudaStreamSynchronize(st));
+  o.Q_is_diag = nbad == 0;
+  o.Q_maxval = nnzS > 0 ? *std::max_element(hmax.begin(), hmax.end()) : 0.0;
   ds->A = DevCsrView{dA.ptr, dA.col, dA.val};
   ds->AT = DevCsrView{dAT.ptr, dAT.col, dAT.val};
   ds->Q = DevCsrView{sptr, scol, sv};
@@ -316,7 +376,7 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   ds->col_norm = cn;
   o.dev = ds;
   tm[nt++] = wall();  // downloads
-  finish_sparse(o, n);
+  finish_norms(o);
   finish_common(hp, o);
   tm[nt++] = wall();
   if (timing)
