@@ -289,9 +289,11 @@ __global__ void k_each(int len, F f) {
 // ---------------------------------------------------------------------------
 struct Mem : PoolBlocks {  // blocks of the library's device memory pool
   template <typename T>
-  T* alloc(int64_t n) {  // zeroed
+  T* alloc(int64_t n) {  // zeroed, complete on return (the engines' streams do
+                         // not wait for the legacy stream that runs cudaMemset)
     T* p = alloc_raw<T>(n);
     HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    HPRQP_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
     return p;
   }
   template <typename T>
@@ -379,26 +381,29 @@ struct BEngine {
     }
     int* p = mem.alloc_raw<int>(h.rows + 1);
     int* cc = mem.alloc_raw<int>(d.nnz);
-    HPRQP_CUDA(cudaMemcpy(p, h.ptr.get(), sizeof(int) * (h.rows + 1), cudaMemcpyHostToDevice));
-    if (d.nnz) HPRQP_CUDA(cudaMemcpy(cc, h.col.get(), sizeof(int) * d.nnz, cudaMemcpyHostToDevice));
+    h2d_staged(p, h.ptr.get(), sizeof(int) * (h.rows + 1), st);
+    if (d.nnz) h2d_staged(cc, h.col.get(), sizeof(int) * d.nnz, st);
     if (d.nnz) {
       if constexpr (std::is_same<V, double>::value) {
-        HPRQP_CUDA(cudaMemcpy(v, h.val.get(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
+        h2d_staged(v, h.val.get(), sizeof(V) * d.nnz, st);
       } else {
         std::vector<V> vv(d.nnz);
 #pragma omp parallel for schedule(static) num_threads(host_threads(d.nnz))
         for (int64_t q = 0; q < d.nnz; ++q) vv[q] = (V)h.val[q];
-        HPRQP_CUDA(cudaMemcpy(v, vv.data(), sizeof(V) * d.nnz, cudaMemcpyHostToDevice));
+        h2d_staged(v, vv.data(), sizeof(V) * d.nnz, st);
       }
     }
+    HPRQP_CUDA(cudaStreamSynchronize(st));
     d.ptr = p;
     d.col = cc;
     d.val = v;
   }
   template <typename T>
   T* up(const std::vector<T>& h) {
-    T* d = mem.alloc<T>((int64_t)h.size());
-    if (!h.empty()) HPRQP_CUDA(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    if (h.empty()) return mem.alloc<T>(0);
+    T* d = mem.alloc_raw<T>((int64_t)h.size());
+    h2d_staged(d, h.data(), sizeof(T) * h.size(), st);
+    HPRQP_CUDA(cudaStreamSynchronize(st));
     return d;
   }
 
@@ -476,7 +481,7 @@ struct BEngine {
   // (all instances active, plain products into scratch).
   void autotune() {
     unsigned char* all = mem.alloc<unsigned char>(B);
-    HPRQP_CUDA(cudaMemset(all, 1, B));
+    HPRQP_CUDA(cudaMemsetAsync(all, 1, B, st));
     cudaEvent_t a, b;
     HPRQP_CUDA(cudaEventCreate(&a));
     HPRQP_CUDA(cudaEventCreate(&b));
@@ -637,7 +642,8 @@ static std::vector<double> power_batch(BEngine<V>& E, const Family& F, double to
     HPRQP_CUDA(cudaStreamSynchronize(E.st));
   }
   std::vector<unsigned char> act(B, 1);
-  HPRQP_CUDA(cudaMemcpy(E.on_pw, act.data(), B, cudaMemcpyHostToDevice));
+  HPRQP_CUDA(cudaMemcpyAsync(E.on_pw, act.data(), B, cudaMemcpyHostToDevice, E.st));
+  HPRQP_CUDA(cudaStreamSynchronize(E.st));
   E.template seg_plain<1, 0u>(EpiSumSqB<V>{E.pz}, E.on_pw, E.out_tmp, ZzFin{E.zz});
   std::vector<double> lam(B, 1.0);
   std::vector<int> done(B, 0);
@@ -1109,10 +1115,12 @@ static void solve(Handle& H, const hprqp_params& p, const double* const* x0s, co
   launches = E64.launches + (H.e32 ? H.e32->launches : 0);
   // collect_results! (operator Q: x = x_bar)
   std::vector<double> x64(F.N), x32(fp32 ? F.N : 0);
-  HPRQP_CUDA(cudaMemcpy(x64.data(), E64.x_bar, sizeof(double) * F.N, cudaMemcpyDeviceToHost));
+  HPRQP_CUDA(cudaMemcpyAsync(x64.data(), E64.x_bar, sizeof(double) * F.N, cudaMemcpyDeviceToHost, E64.st));
+  HPRQP_CUDA(cudaStreamSynchronize(E64.st));
   if (fp32) {
     std::vector<float> xf(F.N);
-    HPRQP_CUDA(cudaMemcpy(xf.data(), H.e32->x_bar, sizeof(float) * F.N, cudaMemcpyDeviceToHost));
+    HPRQP_CUDA(cudaMemcpyAsync(xf.data(), H.e32->x_bar, sizeof(float) * F.N, cudaMemcpyDeviceToHost, H.e32->st));
+    HPRQP_CUDA(cudaStreamSynchronize(H.e32->st));
     for (int64_t i = 0; i < F.N; ++i) x32[i] = xf[i];
   }
   for (int k = 0; k < B; ++k) {

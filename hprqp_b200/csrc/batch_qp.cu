@@ -524,12 +524,18 @@ __global__ void __launch_bounds__(kQapTcThreads) k_qap_tc(const int* qn, const i
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-struct Mem : PoolBlocks {  // zeroed blocks of the library's device memory pool
+struct Mem : PoolBlocks {  // blocks of the library's device memory pool
   template <typename T>
-  T* alloc(int64_t n) {
+  T* alloc(int64_t n) {  // zeroed, complete on return (the engines' streams do
+                         // not wait for the legacy stream that runs cudaMemset)
     void* p = get(sizeof(T) * (size_t)std::max<int64_t>(n, 1));
     HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    HPRQP_CUDA(cudaStreamSynchronize(cudaStreamLegacy));
     return (T*)p;
+  }
+  template <typename T>
+  T* alloc_raw(int64_t n) {  // for buffers that are written in full right away
+    return (T*)get(sizeof(T) * (size_t)std::max<int64_t>(n, 1));
   }
 };
 
@@ -662,8 +668,10 @@ struct Engine {
 
   template <typename T>
   T* up(const std::vector<T>& h) {
-    T* d = mem.alloc<T>((int64_t)h.size());
-    if (!h.empty()) HPRQP_CUDA(cudaMemcpy(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    if (h.empty()) return mem.alloc<T>(0);
+    T* d = mem.alloc_raw<T>((int64_t)h.size());
+    h2d_staged(d, h.data(), sizeof(T) * h.size(), st);
+    HPRQP_CUDA(cudaStreamSynchronize(st));
     return d;
   }
   V* upv(const std::vector<double>& h) {
@@ -748,7 +756,7 @@ struct Engine {
     // row, the fastest of 3 timed rounds of 3 launches
     {
       unsigned char* all = mem.alloc<unsigned char>(B);
-      HPRQP_CUDA(cudaMemset(all, 1, B));
+      HPRQP_CUDA(cudaMemsetAsync(all, 1, B, st));
       cudaEvent_t a, b;
       HPRQP_CUDA(cudaEventCreate(&a));
       HPRQP_CUDA(cudaEventCreate(&b));
@@ -1475,10 +1483,12 @@ void solve(QpBatch* H, const hprqp_params& p, const double* const* x0s, const do
                    t_all - power_time);
   const int64_t launches = E64.launches + (H->e32 ? H->e32->launches : 0);
   std::vector<double> x64(F.N), x32(fp32 ? F.N : 0);
-  HPRQP_CUDA(cudaMemcpy(x64.data(), E64.x_bar, sizeof(double) * F.N, cudaMemcpyDeviceToHost));
+  HPRQP_CUDA(cudaMemcpyAsync(x64.data(), E64.x_bar, sizeof(double) * F.N, cudaMemcpyDeviceToHost, E64.st));
+  HPRQP_CUDA(cudaStreamSynchronize(E64.st));
   if (fp32) {
     std::vector<float> xf(F.N);
-    HPRQP_CUDA(cudaMemcpy(xf.data(), H->e32->x_bar, sizeof(float) * F.N, cudaMemcpyDeviceToHost));
+    HPRQP_CUDA(cudaMemcpyAsync(xf.data(), H->e32->x_bar, sizeof(float) * F.N, cudaMemcpyDeviceToHost, H->e32->st));
+    HPRQP_CUDA(cudaStreamSynchronize(H->e32->st));
     for (int64_t i = 0; i < F.N; ++i) x32[i] = xf[i];
   }
   for (int k = 0; k < B; ++k) {

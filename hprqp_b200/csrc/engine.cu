@@ -30,14 +30,15 @@ void Common::init() {
   HPRQP_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   HPRQP_CUDA(cudaStreamCreateWithFlags(&stream2, cudaStreamNonBlocking));
   d_scal = mem.alloc<double>(kNumSlots);
-  HPRQP_CUDA(cudaMemset(d_scal, 0, sizeof(double) * kNumSlots));
+  HPRQP_CUDA(cudaMemsetAsync(d_scal, 0, sizeof(double) * kNumSlots, stream));
   h_scal = (double*)pinned_take(sizeof(double) * kNumSlots);
   rws.partials = mem.alloc<double>((int64_t)kReduceGridLimit * 16);
   rws.counter = mem.alloc<unsigned>(4);
-  HPRQP_CUDA(cudaMemset(rws.counter, 0, sizeof(unsigned) * 4));
+  HPRQP_CUDA(cudaMemsetAsync(rws.counter, 0, sizeof(unsigned) * 4, stream));
   rws2.partials = mem.alloc<double>((int64_t)kReduceGridLimit * 16);
   rws2.counter = mem.alloc<unsigned>(4);
-  HPRQP_CUDA(cudaMemset(rws2.counter, 0, sizeof(unsigned) * 4));
+  HPRQP_CUDA(cudaMemsetAsync(rws2.counter, 0, sizeof(unsigned) * 4, stream));
+  HPRQP_CUDA(cudaStreamSynchronize(stream));  // (the second chain's stream uses rws2 too)
   int dev = 0;
   HPRQP_CUDA(cudaGetDevice(&dev));
   HPRQP_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -1086,7 +1087,7 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   pz = mem.alloc<V>(mx);
   pq = mem.alloc<V>(mx);
   pt = mem.alloc<V>(mx);
-  HPRQP_CUDA(cudaMemset(pz, 0, sizeof(V) * mx));
+  HPRQP_CUDA(cudaMemsetAsync(pz, 0, sizeof(V) * mx, cm.stream));
   pz2 = mem.alloc<V>(n);
   pq2 = mem.alloc<V>(n);
   pt2 = mem.alloc<V>(n);

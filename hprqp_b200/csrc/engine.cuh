@@ -95,7 +95,7 @@ struct Common {  // per-handle resources shared by the engines
   void sync_read(int first, int count);
   void to_dev(void* d, const void* h, size_t bytes) {
     if (!bytes) return;
-    HPRQP_CUDA(cudaMemcpyAsync(d, h, bytes, cudaMemcpyHostToDevice, stream));
+    h2d_staged(d, h, bytes, stream);
     h2d += (int64_t)bytes;
   }
   void to_host(void* h, const void* d, size_t bytes) {

@@ -254,6 +254,7 @@ struct Net {
   T* alloc(int64_t n) {
     void* p = mem.get(sizeof(T) * (size_t)std::max<int64_t>(n, 1));
     HPRQP_CUDA(cudaMemset(p, 0, sizeof(T) * (size_t)std::max<int64_t>(n, 1)));
+    HPRQP_CUDA(cudaStreamSynchronize(cudaStreamLegacy));  // the net's stream does not wait for it
     return (T*)p;
   }
   ~Net() {
@@ -404,8 +405,10 @@ int hprqp_mlp_create(hprqp_mlp_handle* out, int32_t device, int32_t n_in, int32_
         for (int i = 0; i < l.in; ++i) w[(size_t)o * l.ldi + i] = (float)(a * rnd());
       std::vector<bf16> wb(nw);
       for (int64_t i = 0; i < nw; ++i) wb[i] = __float2bfloat16(w[i]);
-      HPRQP_CUDA(cudaMemcpy(l.W, w.data(), sizeof(float) * nw, cudaMemcpyHostToDevice));
-      HPRQP_CUDA(cudaMemcpy(l.Wb, wb.data(), sizeof(bf16) * nw, cudaMemcpyHostToDevice));
+      HPRQP_CUDA(cudaMemcpyAsync(l.W, w.data(), sizeof(float) * nw, cudaMemcpyHostToDevice, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
+      HPRQP_CUDA(cudaMemcpyAsync(l.Wb, wb.data(), sizeof(bf16) * nw, cudaMemcpyHostToDevice, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
       h->L.push_back(l);
     }
     const int R = h->batch;
@@ -475,8 +478,10 @@ int hprqp_mlp_gradients(hprqp_mlp_handle h, const float* X, const float* T, int3
     size_t off = 0;
     for (auto& l : h->L) {
       std::vector<float> g((size_t)l.ldo * l.ldi), gb(l.ldo);
-      HPRQP_CUDA(cudaMemcpy(g.data(), l.gW, sizeof(float) * g.size(), cudaMemcpyDeviceToHost));
-      HPRQP_CUDA(cudaMemcpy(gb.data(), l.gb, sizeof(float) * gb.size(), cudaMemcpyDeviceToHost));
+      HPRQP_CUDA(cudaMemcpyAsync(g.data(), l.gW, sizeof(float) * g.size(), cudaMemcpyDeviceToHost, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
+      HPRQP_CUDA(cudaMemcpyAsync(gb.data(), l.gb, sizeof(float) * gb.size(), cudaMemcpyDeviceToHost, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
       for (int o = 0; o < l.out; ++o)
         for (int i = 0; i < l.in; ++i) grads[off++] = g[(size_t)o * l.ldi + i];
       for (int o = 0; o < l.out; ++o) grads[off++] = gb[o];
@@ -510,8 +515,10 @@ int hprqp_mlp_get_params(hprqp_mlp_handle h, float* params, int64_t* count) {
       size_t off = 0;
       for (auto& l : h->L) {
         std::vector<float> w((size_t)l.ldo * l.ldi), b(l.ldo);
-        HPRQP_CUDA(cudaMemcpy(w.data(), l.W, sizeof(float) * w.size(), cudaMemcpyDeviceToHost));
-        HPRQP_CUDA(cudaMemcpy(b.data(), l.b, sizeof(float) * b.size(), cudaMemcpyDeviceToHost));
+        HPRQP_CUDA(cudaMemcpyAsync(w.data(), l.W, sizeof(float) * w.size(), cudaMemcpyDeviceToHost, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
+        HPRQP_CUDA(cudaMemcpyAsync(b.data(), l.b, sizeof(float) * b.size(), cudaMemcpyDeviceToHost, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
         for (int o = 0; o < l.out; ++o)
           for (int i = 0; i < l.in; ++i) params[off++] = w[(size_t)o * l.ldi + i];
         for (int o = 0; o < l.out; ++o) params[off++] = b[o];
@@ -532,9 +539,12 @@ int hprqp_mlp_set_params(hprqp_mlp_handle h, const float* params) {
       for (int o = 0; o < l.out; ++o) b[o] = params[off++];
       std::vector<bf16> wb(w.size());
       for (size_t i = 0; i < w.size(); ++i) wb[i] = __float2bfloat16(w[i]);
-      HPRQP_CUDA(cudaMemcpy(l.W, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice));
-      HPRQP_CUDA(cudaMemcpy(l.Wb, wb.data(), sizeof(bf16) * wb.size(), cudaMemcpyHostToDevice));
-      HPRQP_CUDA(cudaMemcpy(l.b, b.data(), sizeof(float) * b.size(), cudaMemcpyHostToDevice));
+      HPRQP_CUDA(cudaMemcpyAsync(l.W, w.data(), sizeof(float) * w.size(), cudaMemcpyHostToDevice, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
+      HPRQP_CUDA(cudaMemcpyAsync(l.Wb, wb.data(), sizeof(bf16) * wb.size(), cudaMemcpyHostToDevice, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
+      HPRQP_CUDA(cudaMemcpyAsync(l.b, b.data(), sizeof(float) * b.size(), cudaMemcpyHostToDevice, h->st));
+      HPRQP_CUDA(cudaStreamSynchronize(h->st));
     }
   })
 }

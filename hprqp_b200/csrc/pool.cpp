@@ -3,9 +3,12 @@
 #include "pool.h"
 
 #include <cuda_runtime.h>
+#include <omp.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <cstring>
 #include <mutex>
 
 #include "../../include/hprqp.h"
@@ -108,6 +111,50 @@ void pinned_give(void* p, size_t bytes) {
   if (!p) return;
   std::lock_guard<std::mutex> lk(g_pin_mu);
   g_pinned.emplace_back(bytes, p);
+}
+
+void h2d_staged(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  constexpr size_t kChunk = 8u << 20;
+  if (bytes < (1u << 20)) {
+    if (bytes) HPRQP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st));
+    return;
+  }
+  char* buf[2] = {(char*)pinned_take(kChunk), (char*)pinned_take(kChunk)};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  bool used[2] = {false, false};
+  try {
+    for (int b = 0; b < 2; ++b) HPRQP_CUDA(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+    const char* s = (const char*)src;
+    char* d = (char*)dst;
+    int b = 0;
+    for (size_t off = 0; off < bytes; off += kChunk, b ^= 1) {
+      const size_t len = std::min(kChunk, bytes - off);
+      if (used[b]) HPRQP_CUDA(cudaEventSynchronize(ev[b]));  // the chunk's previous DMA has read it
+      const int nt = std::max(1, std::min(16, omp_get_max_threads()));
+#pragma omp parallel for schedule(static) num_threads(nt)
+      for (int t = 0; t < nt; ++t) {
+        const size_t a = len * (size_t)t / (size_t)nt, e = len * (size_t)(t + 1) / (size_t)nt;
+        if (e > a) std::memcpy(buf[b] + a, s + off + a, e - a);
+      }
+      HPRQP_CUDA(cudaMemcpyAsync(d + off, buf[b], len, cudaMemcpyHostToDevice, st));
+      HPRQP_CUDA(cudaEventRecord(ev[b], st));
+      used[b] = true;
+    }
+    for (int k = 0; k < 2; ++k)
+      if (used[k]) HPRQP_CUDA(cudaEventSynchronize(ev[k]));  // the chunks go back to the free list
+  } catch (...) {
+    for (int k = 0; k < 2; ++k)
+      if (ev[k]) {
+        cudaEventSynchronize(ev[k]);
+        cudaEventDestroy(ev[k]);
+      }
+    pinned_give(buf[0], kChunk);
+    pinned_give(buf[1], kChunk);
+    throw;
+  }
+  for (int k = 0; k < 2; ++k) cudaEventDestroy(ev[k]);
+  pinned_give(buf[0], kChunk);
+  pinned_give(buf[1], kChunk);
 }
 
 void* PoolBlocks::get(size_t bytes) {

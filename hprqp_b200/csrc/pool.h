@@ -12,6 +12,8 @@
 // retries.  HPRQP_POOL_KEEP_MB caps the reserve kept across frees instead.
 #pragma once
 
+#include <cuda_runtime.h>
+
 #include <cstddef>
 #include <vector>
 
@@ -30,6 +32,13 @@ void pool_free(std::vector<void*>& blocks, int dev);
 // cudaFreeHost synchronises the device and measured up to a second here.
 void* pinned_take(size_t bytes);
 void pinned_give(void* p, size_t bytes);
+
+// Host -> device copy of `bytes` from pageable memory, enqueued on `st`:
+// copies of 1 MiB and more go through two pinned 8 MiB chunks, each filled
+// by the host threads while the other one's DMA runs (a plain copy from
+// pageable memory is staged by one thread).  `src` may be reused on return;
+// the copy completes in stream order.
+void h2d_staged(void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 // Owner of a list of pool blocks of one device, freed together.
 struct PoolBlocks {

@@ -249,7 +249,7 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   DevBuf d;
   auto up = [&](auto* dst, const auto& v) {
     if (!v.empty()) {
-      HPRQP_CUDA(cudaMemcpyAsync(dst, v.data(), sizeof(v[0]) * v.size(), cudaMemcpyHostToDevice, st));
+      h2d_staged(dst, v.data(), sizeof(v[0]) * v.size(), st);
       *h2d += (int64_t)(sizeof(v[0]) * v.size());
     }
   };
