@@ -9,6 +9,8 @@
 #include <cstring>
 #include <cstdlib>
 #include <functional>
+#include <unordered_map>
+#include <mutex>
 #include <type_traits>
 
 #include "engine.cuh"
@@ -60,6 +62,8 @@ void Common::init() {
   pow_chunk_fold = !(cf && cf[0] == '0');
   const char* at = std::getenv("HPRQP_AUTOTUNE");
   autotune = !(at && at[0] == '0');
+  const char* sc = std::getenv("HPRQP_SCHED_CACHE");
+  sched_cache = !(sc && sc[0] == '0');
   const char* ppr = std::getenv("HPRQP_POWER_PRELOAD_ROWS");
   if (ppr) pow_rows_preloaded = std::atoi(ppr) == 1 ? 1 : 2;
   const char* ept = std::getenv("HPRQP_ELL_PROLOGUE");
@@ -137,6 +141,62 @@ static void launch_smem(Common& cm, void (*kernel)(KArgs...), dim3 grid, int blo
   HPRQP_CUDA(cudaLaunchKernelEx(&cfg, kernel, args...));
   cm.launches++;
 }
+
+// ---------------------------------------------------------------------------
+// Schedule cache: the autotuner's timed choices by sparsity signature, for
+// the process.  A handle that loads a problem of a pattern tuned before (the
+// load -> solve -> destroy cycle of a caller solving a family of problems)
+// builds only the chosen format copy and times nothing.
+// ---------------------------------------------------------------------------
+namespace {
+enum SchedKind { SK_CSR = 0, SK_SELL = 1, SK_ELL = 2, SK_SPLIT = 3, SK_STAGE = 4 };
+struct SchedChoice {
+  int kind, tpr;
+};
+std::mutex g_sched_mu;
+std::unordered_map<uint64_t, SchedChoice>& sched_map() {
+  static std::unordered_map<uint64_t, SchedChoice> m;
+  return m;
+}
+
+uint64_t mix64(uint64_t z) {  // splitmix64 finaliser
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+  return z ^ (z >> 31);
+}
+
+// Signature of a pattern (sizes, row pointers, columns) and a tag: 64 fixed
+// chunks hashed in parallel, combined in order, so the key does not depend
+// on the thread count.
+uint64_t pattern_key(const HCsr& h, uint64_t tag) {
+  constexpr int kParts = 64;
+  const int64_t np = (int64_t)h.ptr.size(), nc = (int64_t)h.col.size(), total = np + nc;
+  uint64_t part[kParts];
+#pragma omp parallel for schedule(static) num_threads(host_threads(total))
+  for (int q = 0; q < kParts; ++q) {
+    uint64_t x = 0x9E3779B97F4A7C15ULL * (uint64_t)(q + 1);
+    for (int64_t i = total * q / kParts; i < total * (q + 1) / kParts; ++i)
+      x = mix64(x ^ (uint64_t)(uint32_t)(i < np ? h.ptr[i] : h.col[i - np]));
+    part[q] = x;
+  }
+  uint64_t k = mix64(tag ^ 0xD6E8FEB86659FD93ULL);
+  k = mix64(k ^ (uint64_t)h.rows) ^ mix64((uint64_t)h.cols + 0x2545F4914F6CDD1DULL);
+  for (int q = 0; q < kParts; ++q) k = mix64(k ^ part[q]);
+  return k;
+}
+
+bool sched_lookup(uint64_t key, SchedChoice& c) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  auto it = sched_map().find(key);
+  if (it == sched_map().end()) return false;
+  c = it->second;
+  return true;
+}
+void sched_store(uint64_t key, SchedChoice c) {
+  std::lock_guard<std::mutex> lk(g_sched_mu);
+  sched_map()[key] = c;
+}
+}  // namespace
 
 // threads per row of a CSR pass by the mean row length (the fixed rule)
 static int csr_tpr(double avg) {
@@ -356,12 +416,33 @@ void Engine<V>::upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode, const DevCsr
   } else if (tpr_mode > 0) {
     d.tpr = 1 << std::min(tpr_mode - 1, 5);
   } else {
+    // a pattern timed before: only the chosen copy is built
+    const bool cached = cm.autotune && cm.sched_cache && h.nnz() > 0;
+    const uint64_t key = cached ? pattern_key(h, 0x100 * sizeof(V) + cm.ell_prologue) : 0;
+    SchedChoice c{};
+    if (cached && sched_lookup(key, c)) {
+      if (c.kind == SK_SELL) build_sell(h, d);
+      if (c.kind == SK_ELL) build_ell(h, d);
+      if (c.kind == SK_SPLIT) build_split(h, d);
+      if (c.kind == SK_STAGE) build_stage(h, d);
+      d.sell = c.kind == SK_SELL && d.sell_len > 0;
+      d.ell = c.kind == SK_ELL && d.ell_w > 0;
+      d.split = c.kind == SK_SPLIT && d.npieces > 0;
+      d.stage = c.kind == SK_STAGE && d.st_nblk > 0;
+      if (d.sell || d.ell || d.split || d.stage || c.kind == SK_CSR) {
+        d.tpr = c.tpr;
+        return;
+      }
+    }
     build_sell(h, d);
     build_ell(h, d);
     build_split(h, d);
     // (an ELL copy of width <= 8 is taken untimed: no other copy is needed)
     if (!(cm.ell_prologue > 0 && d.ell_w > 0 && d.ell_w <= 8)) build_stage(h, d);
     d.tpr = autotune(d);
+    if (cached)
+      sched_store(key, SchedChoice{d.stage ? SK_STAGE : d.split ? SK_SPLIT : d.ell ? SK_ELL : d.sell ? SK_SELL : SK_CSR,
+                                   d.tpr});
   }
 }
 
@@ -898,7 +979,14 @@ __global__ void __launch_bounds__(kBlock) k_gram_vals(int rows, const int* __res
 // rounds of 8 chained steps on a unit start.
 template <typename V>
 template <typename Step>
-void Engine<V>::tune_reduce(DCsr<V>& M, Step step) {
+void Engine<V>::tune_reduce(DCsr<V>& M, Step step, uint64_t key) {
+  SchedChoice c{};
+  if (key && sched_lookup(key, c)) {
+    M.ell = false;
+    M.sell = c.kind == SK_SELL && M.sell_len > 0;
+    M.tpr = c.tpr;
+    return;
+  }
   cudaEvent_t e0, e1;
   HPRQP_CUDA(cudaEventCreate(&e0));
   HPRQP_CUDA(cudaEventCreate(&e1));
@@ -933,10 +1021,11 @@ void Engine<V>::tune_reduce(DCsr<V>& M, Step step) {
   cudaEventDestroy(e1);
   M.sell = best_sell;
   M.tpr = best_t;
+  if (key) sched_store(key, SchedChoice{best_sell ? SK_SELL : SK_CSR, best_t});
 }
 
 template <typename V>
-void Engine<V>::autotune_gram() {
+void Engine<V>::autotune_gram(uint64_t key) {
   double* inv = cm.d_scal + S_POW + 5;
   double* lg = cm.d_scal + S_POWLOG;
   double* u0 = gu0;
@@ -948,7 +1037,7 @@ void Engine<V>::autotune_gram() {
     double* un = (k & 1) ? gu0 : gu1;
     mat_reduce<2, 0u>(cm, G, uc, EpiGramPower<double>{uc, un, inv}, cm.d_scal + S_POW + 6,
                       GramPowerFin{lg, k & 31, inv});
-  });
+  }, key);
 }
 
 // What the power method needs beyond the iteration's matrices (the Gram
@@ -961,13 +1050,14 @@ void Engine<V>::power_setup(const Prepared& pp, int tpr_A, int tpr_Q) {
   if (power_ready) return;
   power_ready = true;
   build_gram(pp, tpr_A);
-  if (tpr_Q <= 0) autotune_power_Q();
+  if (tpr_Q <= 0)
+    autotune_power_Q(cm.sched_cache && pp.Q.nnz() > 0 ? pattern_key(pp.Q, 0x300 + sizeof(V)) : 0);
 }
 
 // The sparse Q's power step runs on its own copy of Q's schedule, chosen by
 // timing that step (Q's own schedule is chosen for the iteration's passes).
 template <typename V>
-void Engine<V>::autotune_power_Q() {
+void Engine<V>::autotune_power_Q(uint64_t key) {
   Qp = Q;
   if (!has_Q_sparse || Q.nnz == 0 || !cm.autotune || cm.pow_prefer_ell) return;
   double* inv = cm.d_scal + S_POW_Q + 5;
@@ -985,7 +1075,7 @@ void Engine<V>::autotune_power_Q() {
     V* zn = (k & 1) ? pz2 : pq2;
     mat_reduce<3, 0u>(cm, Qp, zc, EpiPowerFused<V>{zc, zn, zz, true, inv}, cm.d_scal + S_POW_Q + 1,
                       PowerFin{lg, k & 31, inv});
-  });
+  }, key);
 }
 
 // Values of G into the format its products use (the padding of ELL / SELL
@@ -1044,7 +1134,7 @@ void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
     G.sell = G.sell_len > 0;
     G.tpr = 1;
   } else {
-    autotune_gram();
+    autotune_gram(cm.sched_cache ? pattern_key(h, 0x200 + sizeof(V)) : 0);
   }
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   gram = true;

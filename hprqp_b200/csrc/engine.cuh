@@ -86,6 +86,9 @@ struct Common {  // per-handle resources shared by the engines
   // instead, e.g. under a profiler, whose serialisation makes the timings
   // meaningless
   bool autotune = true;
+  // timed schedule choices are kept per process by sparsity signature and
+  // reused for a matrix of the same pattern (HPRQP_SCHED_CACHE=0: time always)
+  bool sched_cache = true;
   hprqp_qmap_fn qmap = nullptr;  // a custom Q operator's callback (HPRQP_Q_CUSTOM)
   void* qmap_user = nullptr;
   bool tc_qap = true;  // FP32 QAP products on the 3xTF32 tensor-core GEMM (else the CUDA-core k_qap_gemm)
@@ -146,10 +149,10 @@ class Engine {
   // formed on the device at every power method (gram_values)
   DCsr<V> G;
   bool gram = false;
-  void autotune_gram();  // (public: it launches device lambdas)
-  void autotune_power_Q();
+  void autotune_gram(uint64_t key);  // (public: it launches device lambdas); key: schedule cache, 0 = none
+  void autotune_power_Q(uint64_t key);
   template <typename Step>
-  void tune_reduce(DCsr<V>& M, Step step);
+  void tune_reduce(DCsr<V>& M, Step step, uint64_t key = 0);
   DCsr<V> Qp;  // Q under the schedule of its power step
   bool power_ready = false;
   ~Engine();
