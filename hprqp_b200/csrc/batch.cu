@@ -18,6 +18,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -64,6 +65,140 @@ __global__ void __launch_bounds__(kBlock) k_rows(int nrows, Inst I, CsrSrc<V, V>
   const int lane = threadIdx.x & (TPR - 1);
   const V acc = src.template dot<TPR, V>(row, lane);
   if (lane == 0) epi(row, k, acc);
+}
+
+// Staged pass over a block-diagonal batch (BStage): instance k's rows only
+// touch its own columns [coff[k], coff[k] + ncol[k]), so that column block is
+// the CTA's shared-memory copy of the input.  One CTA per tile (whole rows
+// of one instance, at most kStageSlots row-sum slots): the CTA stages its
+// instance's block, streams the tile's 32-chunk warp tiles (two per warp
+// and step, loads in flight together, the next step prefetched into L2) with
+// the segmented scan into slots, then one thread per row folds the row's
+// slots in order and runs the epilogue.  The chunk layout, the scan and the
+// order of every sum are those of k_stage_pass; tiles of inactive instances
+// return at once.
+template <typename V>
+struct BStageView {
+  const uint16_t* __restrict__ col;
+  const V* __restrict__ val;
+  const int2* __restrict__ wt;    // per warp tile {first slot, segment-head mask}
+  const int4* __restrict__ tile;  // {first warp tile, chunks, first row, end row}
+  const int* __restrict__ tinst;  // tile -> instance
+  const int* __restrict__ srow;   // first slot of each row (rows + 1)
+  const int* __restrict__ coff;   // instance -> first column
+  const int* __restrict__ ncol;   // instance -> columns
+};
+
+constexpr int kBStageBlock = 512;  // two CTAs per SM at 64 registers
+
+template <typename V, typename Epi>
+__global__ void __launch_bounds__(kBStageBlock, 2) k_bstage_pass(BStageView<V> s, const V* __restrict__ x,
+                                                                 const unsigned char* __restrict__ on, Epi epi) {
+  extern __shared__ __align__(16) unsigned char bstage_smem[];
+  V* sums = reinterpret_cast<V*>(bstage_smem);
+  V* xs = reinterpret_cast<V*>(bstage_smem + kStageSlots * sizeof(V));
+  constexpr int NW = kBStageBlock / 32, U = 2;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int4 tl = __ldg(s.tile + blockIdx.x);  // the schedule and the matrix are constant: before the wait
+  const int k = __ldg(s.tinst + blockIdx.x);
+  const int C0 = 32 * tl.x, C1 = C0 + tl.y;
+  StageChunk<V> ck[U];
+  int2 d[U];
+  int kw = warp;
+  auto load_step = [&]() {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int w = kw + u * NW;
+      d[u] = C0 + 32 * w < C1 ? __ldg(s.wt + tl.x + w) : make_int2(0, 0);
+      if (C0 + 32 * w + lane < C1) stage_load(ck[u], s.col, s.val, (int64_t)tl.x + w, lane);
+    }
+    if (lane == 0) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int w = kw + (U + u) * NW;
+        if (C0 + 32 * w < C1) stage_prefetch(s.col, s.val, (int64_t)tl.x + w);
+      }
+    }
+  };
+  load_step();
+  pdl_enter();
+  if (!on[k]) return;  // (uniform over the CTA)
+  const int c0 = __ldg(s.coff + k), len = __ldg(s.ncol + k);
+  const V* src = x + c0;
+  if ((reinterpret_cast<uintptr_t>(src) & 15u) == 0) {
+    constexpr int P = 16 / (int)sizeof(V);
+    const int nv = len / P;
+    for (int q = threadIdx.x; q < nv; q += kBStageBlock)
+      reinterpret_cast<uint4*>(xs)[q] = __ldg(reinterpret_cast<const uint4*>(src) + q);
+    for (int q = nv * P + threadIdx.x; q < len; q += kBStageBlock) xs[q] = __ldg(src + q);
+  } else {
+    for (int q = threadIdx.x; q < len; q += kBStageBlock) xs[q] = __ldg(src + q);
+  }
+  __syncthreads();
+  const int slot0 = __ldg(s.srow + tl.z);
+  const int nwt = (C1 - C0 + 31) / 32;
+  while (kw < nwt) {
+    V v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u)  // every gather before any slot store
+      v[u] = C0 + 32 * (kw + u * NW) + lane < C1 ? stage_dot<V>(ck[u], xs) : V(0);
+    unsigned f[U], heads[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      heads[u] = (unsigned)d[u].y;
+      f[u] = (heads[u] >> lane) & 1u;
+    }
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const V o = __shfl_up_sync(0xffffffffu, v[u], off);
+        const unsigned fo = __shfl_up_sync(0xffffffffu, f[u], off);
+        if (lane >= off) {
+          if (!f[u]) v[u] += o;
+          f[u] |= fo;
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const int last = min(31, C1 - C0 - 32 * (kw + u * NW) - 1);
+      if (lane <= last && (lane == last || ((heads[u] >> (lane + 1)) & 1u)))
+        sums[d[u].x - slot0 + __popc(heads[u] & (0xffffffffu >> (31 - lane))) - 1] = v[u];
+    }
+    kw += U * NW;
+    if (kw < nwt) load_step();
+  }
+  __syncthreads();
+  for (int r = tl.z + (int)threadIdx.x; r < tl.w; r += kBStageBlock) {
+    const int a = __ldg(s.srow + r) - slot0, e = __ldg(s.srow + r + 1) - slot0;
+    V acc = sums[a];
+    for (int q = a + 1; q < e; ++q) acc += sums[q];
+    epi(r, k, acc);
+  }
+}
+
+// Fill of a batch's staged copy: row r's entries in CSR order from chunk
+// pc[r] on, columns local to the row's instance (the copy was zeroed
+// first; no columns when scol is null: a second precision's values for the
+// same structure); values lane-interleaved as in k_stage_fill.
+template <typename V>
+__global__ void __launch_bounds__(kBlock) k_bstage_fill(int rows, const int* __restrict__ ptr,
+                                                        const int* __restrict__ col, const V* __restrict__ val,
+                                                        const int* __restrict__ inst, const int* __restrict__ coff,
+                                                        const int* __restrict__ pc, uint16_t* __restrict__ scol,
+                                                        V* __restrict__ sval) {
+  constexpr int S = 16 / (int)sizeof(V);
+  const int r = blockIdx.x * kBlock + threadIdx.x;
+  if (r >= rows) return;
+  const int lo = coff[inst[r]];
+  int64_t j = (int64_t)pc[r] * 8;
+  for (int q = ptr[r]; q < ptr[r + 1]; ++q, ++j) {
+    const int64_t ch = j >> 3, g = ch >> 5, l = ch & 31;
+    const int e = (int)(j & 7);
+    if (scol) scol[j] = (uint16_t)(col[q] - lo);
+    sval[((g * (8 / S) + e / S) * 32 + l) * S + e % S] = val[q];
+  }
 }
 
 template <typename V>
@@ -338,6 +473,28 @@ struct Family {  // host copy of the batch
   std::vector<double> obj_constant, norm_c_org;
 };
 
+// A batch matrix's staged copy (k_bstage_pass) on the device
+template <typename V>
+struct BStage {
+  bool built = false, use = false;
+  int ntile = 0, ncol_max = 0;
+  int64_t chunks = 0;
+  const int* pc = nullptr;  // each row's first chunk (for a copy in the other precision)
+  BStageView<V> v{};
+};
+
+// the dynamic shared-memory limit of a kernel raised once per device
+template <typename K>
+static void raise_smem(K kernel, int bytes) {
+  static std::atomic<uint64_t> done{0};
+  int dev = 0;
+  HPRQP_CUDA(cudaGetDevice(&dev));
+  const uint64_t bit = 1ull << (dev & 63);
+  if (done.load() & bit) return;
+  HPRQP_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.fetch_or(bit);
+}
+
 template <typename V>
 struct BEngine {
   cudaStream_t st = nullptr;
@@ -345,6 +502,7 @@ struct BEngine {
   int B;
   int64_t N, R;
   DCsr<V> L, LT;
+  BStage<V> SL, SLT;  // staged copies of L and LT (built when their rows are long enough)
   int tprL = 8, tprLT = 4;
   V *x, *x_hat, *x_bar, *dx, *w, *w_bar, *dw, *z_bar, *c, *ltemp, *Qv, *pz, *pq;
   double *last_x, *last_w;
@@ -407,7 +565,8 @@ struct BEngine {
     return d;
   }
 
-  BEngine(const Family& F, cudaStream_t s, const DCsr<double>* L64 = nullptr, const DCsr<double>* LT64 = nullptr)
+  BEngine(const Family& F, cudaStream_t s, const DCsr<double>* L64 = nullptr, const DCsr<double>* LT64 = nullptr,
+          const BStage<double>* SL64 = nullptr, const BStage<double>* SLT64 = nullptr)
       : st(s), B(F.B), N(F.N), R(F.R) {
     upload_csr(F.L, L, L64);
     upload_csr(F.LT, LT, LT64);
@@ -426,6 +585,11 @@ struct BEngine {
     }
     inst_n = up(in);
     inst_r = up(ir);
+    const char* bst = std::getenv("HPRQP_BATCH_STAGED");
+    if (!(bst && bst[0] == '0')) {
+      build_bstage(F.L, L, F.roff, F.noff, inst_r, SL, SL64);
+      build_bstage(F.LT, LT, F.noff, F.roff, inst_n, SLT, SLT64);
+    }
     on = mem.alloc<unsigned char>(B);
     on_pw = mem.alloc<unsigned char>(B);
     sigma = mem.alloc<double>(B);
@@ -455,6 +619,154 @@ struct BEngine {
     autotune();
   }
 
+  // Staged copy of a block-diagonal batch matrix M (rows of instance k in
+  // [rof[k], rof[k+1]), its columns in [cof[k], cof[k+1])): chunk counts from
+  // the host pattern, tiles of whole rows of one instance with at most
+  // kStageSlots slots, each starting at a whole warp tile; the scatter on the
+  // device from M's device CSR.  Not built when an instance has more
+  // columns than 16 bits index or its block does not fit a CTA's shared
+  // memory, or when rows average fewer than 8 entries (padding to 8-entry
+  // chunks would cost more than the staging saves).
+  void build_bstage(const FlatCsr& h, const DCsr<V>& M, const std::vector<int64_t>& rof,
+                    const std::vector<int64_t>& cof, const int* inst, BStage<V>& S,
+                    const BStage<double>* from = nullptr) {
+    S = BStage<V>();
+    const int64_t rows = h.rows;
+    if (from) {  // the FP64 engine's structure: only the values in this precision
+      if (!from->built) return;
+      if ((int64_t)from->ncol_max * (int64_t)sizeof(V) > kStageSmem) return;
+      V* sval = mem.alloc_raw<V>(from->chunks * 8);
+      if (reinterpret_cast<uintptr_t>(sval) & 15u) return;
+      HPRQP_CUDA(cudaMemsetAsync(sval, 0, sizeof(V) * (size_t)from->chunks * 8, st));
+      k_bstage_fill<V><<<(int)((rows + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+          (int)rows, M.ptr, M.col, M.val, inst, from->v.coff, from->pc, nullptr, sval);
+      HPRQP_LAUNCH_CHECK();
+      const BStageView<double>& f = from->v;
+      S.v = BStageView<V>{f.col, sval, f.wt, f.tile, f.tinst, f.srow, f.coff, f.ncol};
+      S.ntile = from->ntile;
+      S.ncol_max = from->ncol_max;
+      S.chunks = from->chunks;
+      S.pc = from->pc;
+      HPRQP_CUDA(cudaStreamSynchronize(st));
+      S.built = true;
+      return;
+    }
+    if (rows <= 0 || h.nnz() < 65536 || (double)h.nnz() / (double)rows < 8.0) return;
+    int ncol_max = 0;
+    for (int k = 0; k < B; ++k) ncol_max = std::max<int>(ncol_max, (int)(cof[k + 1] - cof[k]));
+    if (ncol_max > 65535 || (int64_t)ncol_max * (int64_t)sizeof(V) > kStageSmem) return;
+    std::vector<int> ch(rows), pc(rows), srow(rows + 1);
+    // each instance planned on its own (local warp-tile and slot numbers),
+    // in parallel; then shifted by the instances' prefix offsets
+    struct Plan {
+      std::vector<int4> tiles;
+      std::vector<int2> wts;
+      int64_t nslot = 0;
+      bool ok = true;
+    };
+    std::vector<Plan> plans(B);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(host_threads(rows))
+    for (int k = 0; k < B; ++k) {
+      Plan& P = plans[k];
+      std::vector<unsigned> heads;
+      std::vector<int> first;
+      for (int64_t r = rof[k]; r < rof[k + 1]; ++r) {
+        const int len = h.ptr[r + 1] - h.ptr[r];
+        ch[r] = len > 0 ? (len + 7) / 8 : 1;
+      }
+      int64_t q = rof[k], slot = 0;
+      while (q < rof[k + 1]) {  // one tile from row q
+        const int64_t r0 = q;
+        int64_t o = 0, slots = 0;
+        while (q < rof[k + 1]) {
+          const int64_t touch = (o + ch[q] - 1) / 32 - o / 32 + 1;
+          if (slots + touch > kStageSlots) break;
+          slots += touch;
+          o += ch[q];
+          ++q;
+        }
+        if (q == r0) {  // a row with more slots than a tile holds
+          P.ok = false;
+          break;
+        }
+        const int nwt = (int)((o + 31) / 32);
+        heads.assign(nwt, 0u);
+        first.assign(nwt, -1);
+        int64_t off = 0;
+        for (int64_t rr = r0; rr < q; ++rr) {
+          srow[rr] = (int)slot;
+          pc[rr] = (int)(32 * (int64_t)P.wts.size() + off);
+          for (int64_t w = off / 32; w <= (off + ch[rr] - 1) / 32; ++w) {
+            heads[w] |= 1u << (std::max<int64_t>(off, 32 * w) - 32 * w);
+            if (first[w] < 0) first[w] = (int)slot;
+            ++slot;
+          }
+          off += ch[rr];
+        }
+        P.tiles.push_back(make_int4((int)P.wts.size(), (int)o, (int)r0, (int)q));
+        for (int w = 0; w < nwt; ++w) P.wts.push_back(make_int2(first[w], (int)heads[w]));
+      }
+      P.nslot = slot;
+    }
+    std::vector<int64_t> wb(B + 1, 0), sb(B + 1, 0), tb(B + 1, 0);
+    for (int k = 0; k < B; ++k) {
+      if (!plans[k].ok) return;
+      wb[k + 1] = wb[k] + (int64_t)plans[k].wts.size();
+      sb[k + 1] = sb[k] + plans[k].nslot;
+      tb[k + 1] = tb[k] + (int64_t)plans[k].tiles.size();
+    }
+    if (32 * wb[B] > INT32_MAX / 8 || sb[B] > INT32_MAX / 2) return;
+    std::vector<int2> wt(wb[B]);
+    std::vector<int4> tile(tb[B]);
+    std::vector<int> tinst(tb[B]);
+#pragma omp parallel for schedule(dynamic, 4) num_threads(host_threads(rows))
+    for (int k = 0; k < B; ++k) {
+      const Plan& P = plans[k];
+      for (size_t i = 0; i < P.tiles.size(); ++i) {
+        const int4 t = P.tiles[i];
+        tile[tb[k] + (int64_t)i] = make_int4((int)(t.x + wb[k]), t.y, t.z, t.w);
+        tinst[tb[k] + (int64_t)i] = k;
+      }
+      for (size_t j = 0; j < P.wts.size(); ++j)
+        wt[wb[k] + (int64_t)j] = make_int2((int)(P.wts[j].x + sb[k]), P.wts[j].y);
+      for (int64_t rr = rof[k]; rr < rof[k + 1]; ++rr) {
+        srow[rr] += (int)sb[k];
+        pc[rr] += (int)(32 * wb[k]);
+      }
+    }
+    srow[rows] = (int)sb[B];
+    const int64_t tot = 32 * wb[B];
+    std::vector<int> co(B), nc(B);
+    for (int k = 0; k < B; ++k) {
+      co[k] = (int)cof[k];
+      nc[k] = (int)(cof[k + 1] - cof[k]);
+    }
+    uint16_t* scol = mem.alloc_raw<uint16_t>(tot * 8);
+    V* sval = mem.alloc_raw<V>(tot * 8);
+    if ((reinterpret_cast<uintptr_t>(scol) | reinterpret_cast<uintptr_t>(sval)) & 15u) return;
+    HPRQP_CUDA(cudaMemsetAsync(scol, 0, sizeof(uint16_t) * (size_t)tot * 8, st));
+    HPRQP_CUDA(cudaMemsetAsync(sval, 0, sizeof(V) * (size_t)tot * 8, st));
+    const int* dpc = up(pc);
+    const int* dco = up(co);
+    k_bstage_fill<V><<<(int)((rows + kBlock - 1) / kBlock), kBlock, 0, st>>>((int)rows, M.ptr, M.col, M.val, inst,
+                                                                             dco, dpc, scol, sval);
+    HPRQP_LAUNCH_CHECK();
+    S.v = BStageView<V>{scol, sval, up(wt), up(tile), up(tinst), up(srow), dco, up(nc)};
+    S.ntile = (int)tile.size();
+    S.ncol_max = ncol_max;
+    S.chunks = tot;
+    S.pc = dpc;
+    HPRQP_CUDA(cudaStreamSynchronize(st));
+    S.built = true;
+  }
+  template <typename Epi>
+  void rows_stage(const BStage<V>& S, const V* xin, const Epi& e, const unsigned char* mask) {
+    const int smem = (int)(sizeof(V) * ((size_t)kStageSlots + (size_t)S.ncol_max));
+    raise_smem(k_bstage_pass<V, Epi>, (int)(sizeof(V) * kStageSlots) + kStageSmem);
+    k_bstage_pass<V, Epi><<<S.ntile, kBStageBlock, smem, st>>>(S.v, xin, mask, e);
+    launches++;
+    HPRQP_LAUNCH_CHECK();
+  }
   template <typename Epi>
   void rows_csr(const DCsr<V>& M, const int* inst, int tpr, const V* xin, const Epi& e, const unsigned char* mask) {
     const Inst I{inst, mask};
@@ -473,9 +785,15 @@ struct BEngine {
     HPRQP_LAUNCH_CHECK();
   }
   template <typename Epi>
-  void rows_L(const V* xin, const Epi& e, const unsigned char* mask) { rows_csr(L, inst_r, tprL, xin, e, mask); }
+  void rows_L(const V* xin, const Epi& e, const unsigned char* mask) {
+    if (SL.use) rows_stage(SL, xin, e, mask);
+    else rows_csr(L, inst_r, tprL, xin, e, mask);
+  }
   template <typename Epi>
-  void rows_LT(const V* xin, const Epi& e) { rows_csr(LT, inst_n, tprLT, xin, e, on); }
+  void rows_LT(const V* xin, const Epi& e) {
+    if (SLT.use) rows_stage(SLT, xin, e, on);
+    else rows_csr(LT, inst_n, tprLT, xin, e, on);
+  }
   // Row-schedule autotuner for this instance class: threads per row of the
   // A_d and A_d' products, the fastest of 3 timed rounds of 3 launches each
   // (all instances active, plain products into scratch).
@@ -506,6 +824,30 @@ struct BEngine {
     };
     tprL = tune(L, inst_r, pz, ltemp, {2, 4, 8, 16, 32});
     tprLT = tune(LT, inst_n, ltemp, Qv, {1, 2, 4, 8, 16});
+    // the staged copies against the best CSR schedule, timed the same way
+    auto time_of = [&](auto&& launch) {
+      launch();
+      float tb = 1e30f;
+      for (int r = 0; r < 3; ++r) {
+        HPRQP_CUDA(cudaEventRecord(a, st));
+        for (int q = 0; q < 3; ++q) launch();
+        HPRQP_CUDA(cudaEventRecord(b, st));
+        HPRQP_CUDA(cudaEventSynchronize(b));
+        float ms = 0;
+        HPRQP_CUDA(cudaEventElapsedTime(&ms, a, b));
+        tb = std::min(tb, ms);
+      }
+      return tb;
+    };
+    // (HPRQP_BATCH_STAGED=1 takes them untimed)
+    const char* bs = std::getenv("HPRQP_BATCH_STAGED");
+    const bool force = bs && bs[0] == '1';
+    if (SL.built)
+      SL.use = force || time_of([&] { rows_stage(SL, pz, EpiStoreB<V>{ltemp, nullptr}, all); }) <
+                            time_of([&] { rows_csr(L, inst_r, tprL, pz, EpiStoreB<V>{ltemp, nullptr}, all); });
+    if (SLT.built)
+      SLT.use = force || time_of([&] { rows_stage(SLT, ltemp, EpiStoreB<V>{Qv, nullptr}, all); }) <
+                             time_of([&] { rows_csr(LT, inst_n, tprLT, ltemp, EpiStoreB<V>{Qv, nullptr}, all); });
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     launches = 0;
@@ -875,7 +1217,8 @@ static void solve(Handle& H, const hprqp_params& p, const double* const* x0s, co
   const bool fp32 = p.precision == HPRQP_PRECISION_FP32_POLISH;
   const double tc0 = now_s();
   if (!H.e64) H.e64 = std::make_unique<BEngine<double>>(F, H.st);
-  if (fp32 && !H.e32) H.e32 = std::make_unique<BEngine<float>>(F, H.st, &H.e64->L, &H.e64->LT);
+  if (fp32 && !H.e32)
+    H.e32 = std::make_unique<BEngine<float>>(F, H.st, &H.e64->L, &H.e64->LT, &H.e64->SL, &H.e64->SLT);
   const double t_engines = now_s() - tc0;
   BEngine<double>& E64 = *H.e64;
   const double t0 = now_s();
