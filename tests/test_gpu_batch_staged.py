@@ -8,7 +8,11 @@ large enough for the staged copies (8 instances of 500 x 3,000 at 2%):
    objective to 1e-9 and, in FP64, iteration counts within 2%: the two
    differ only in the order of the row sums;
  - the staged batch matches each instance's own single solve (status,
-   objective to 1e-6), in both precision modes.
+   objective to 1e-6), in both precision modes;
+ - one instance of the staged FP64 batch against the oracle: its status,
+   objective (1e-6), and an iteration count within 10% (the batch's lockstep
+   power method starts from its own vector, so lambda differs in the last
+   digits of its 1e-4 stopping test).
 """
 import os
 
@@ -18,6 +22,8 @@ import pytest
 from hprqp_b200 import HPRQP_parameters, Solver
 from hprqp_b200 import workloads as W
 from hprqp_b200.batch import solve_batch
+from oracle import oracle as O
+from tests.test_gpu_parity import oracle_params
 
 pytestmark = pytest.mark.gpu
 
@@ -61,3 +67,12 @@ def test_staged_batch_matches_csr_batch_and_single_solves(precision):
         tol = 1e-6 if precision == "fp64" else 1e-5
         assert abs(rs.primal_obj - r1.primal_obj) / (1 + abs(r1.primal_obj)) < tol
         assert np.max(np.abs(rs.x - r1.x)) / max(1.0, np.max(np.abs(r1.x))) < 1e-3
+
+
+def test_staged_batch_instance_matches_oracle():
+    m = family()[3]
+    rb = run("1", "fp64")[3]
+    ref = O.solve(m, oracle_params("LASSO", max_iter=50000))
+    assert ref.status_name == rb.status == "OPTIMAL"
+    assert abs(rb.primal_obj - ref.primal_obj) / (1 + abs(ref.primal_obj)) < 1e-6
+    assert abs(rb.iter - ref.iter) <= max(20, 0.1 * ref.iter), (rb.iter, ref.iter)
