@@ -666,15 +666,16 @@ struct Engine {
   double *out_rn, *out_rm, *out_mn_cur, *out_mn_last, *out_mm_cur, *out_mm_last, *out_sn, *out_sm, *out_tmp;
   int64_t launches = 0;
 
-  template <typename T>
-  T* up(const std::vector<T>& h) {
+  template <typename T, typename A>
+  T* up(const std::vector<T, A>& h) {
     if (h.empty()) return mem.alloc<T>(0);
     T* d = mem.alloc_raw<T>((int64_t)h.size());
     h2d_staged(d, h.data(), sizeof(T) * h.size(), st);
     HPRQP_CUDA(cudaStreamSynchronize(st));
     return d;
   }
-  V* upv(const std::vector<double>& h) {
+  template <typename A>
+  V* upv(const std::vector<double, A>& h) {
     std::vector<V> t(h.size());
 #pragma omp parallel for schedule(static) num_threads(host_threads((int64_t)h.size()))
     for (int64_t i = 0; i < (int64_t)h.size(); ++i) t[i] = (V)h[i];

@@ -346,8 +346,8 @@ __global__ void __launch_bounds__(1024) k_golden_diag(int n, double a, double b,
 // ---------------------------------------------------------------------------
 // Engine: construction and uploads
 // ---------------------------------------------------------------------------
-template <typename V>
-static V* upload(Common& cm, DeviceMem& mem, const std::vector<double>& h, int64_t len) {
+template <typename V, typename A>
+static V* upload(Common& cm, DeviceMem& mem, const std::vector<double, A>& h, int64_t len) {
   V* d = mem.alloc<V>(len);
   if (len > 0) {
     if constexpr (std::is_same<V, double>::value) {
@@ -367,7 +367,7 @@ static V* upload(Common& cm, DeviceMem& mem, const std::vector<double>& h, int64
 // A vector of the scaled problem: copied (FP64) or cast (FP32) from the
 // GPU scaling's device copy when there is one, else uploaded from the host.
 template <typename V>
-V* Engine<V>::vec_in(const std::vector<double>& h, const double* dsrc, int64_t len) {
+V* Engine<V>::vec_in(const hvec<double>& h, const double* dsrc, int64_t len) {
   if (!dsrc || len <= 0) return upload<V>(cm, mem, h, len);
   V* d = mem.alloc<V>(len);
   if constexpr (std::is_same<V, double>::value)

@@ -219,7 +219,7 @@ class Engine {
  private:
   DeviceMem mem;
   void upload_csr(const HCsr& h, DCsr<V>& d, int tpr_mode, const DevCsrView* dsrc = nullptr);
-  V* vec_in(const std::vector<double>& h, const double* dsrc, int64_t len);
+  V* vec_in(const hvec<double>& h, const double* dsrc, int64_t len);
   int autotune(DCsr<V>& d);
   void spmv(const DCsr<V>& M, const V* xin, V* yout, double scale = 1.0);
   void build_sell(const HCsr& h, DCsr<V>& d);

@@ -102,9 +102,9 @@ bool csc_as_transpose(int64_t rows, int64_t cols, const int32_t* cp, const int32
   return true;
 }
 
-std::vector<double> copy_vec(const double* p, int64_t len, const char* what, bool allow_inf) {
+hvec<double> copy_vec(const double* p, int64_t len, const char* what, bool allow_inf) {
   if (len > 0 && !p) throw Error(HPRQP_E_ARG, std::string(what) + ": null pointer");
-  std::vector<double> v;
+  hvec<double> v;
   par_copy(v, p, len);
   // the first offending entry decides the message, as in a serial scan
   int64_t first_nan = len, first_inf = len;
@@ -119,7 +119,7 @@ std::vector<double> copy_vec(const double* p, int64_t len, const char* what, boo
   return v;
 }
 
-double norm_b_of(const std::vector<double>& AL, const std::vector<double>& AU, bool inf) {
+double norm_b_of(const hvec<double>& AL, const hvec<double>& AU, bool inf) {
   double s = 0.0;
   for (size_t i = 0; i < AL.size(); ++i) {
     const double a = AL[i] == -kInf ? 0.0 : AL[i];
@@ -129,12 +129,12 @@ double norm_b_of(const std::vector<double>& AL, const std::vector<double>& AU, b
   }
   return inf ? s : std::sqrt(s);
 }
-double norm2(const std::vector<double>& v) {
+double norm2(const hvec<double>& v) {
   double s = 0.0;
   for (double x : v) s += x * x;
   return std::sqrt(s);
 }
-double norminf(const std::vector<double>& v) {
+double norminf(const hvec<double>& v) {
   double s = 0.0;
   for (double x : v) s = std::max(s, std::fabs(x));
   return s;
@@ -205,7 +205,7 @@ int host_threads(int64_t work) {
 }
 
 template <typename T>
-void par_copy(std::vector<T>& dst, const T* src, int64_t len) {
+void par_copy(hvec<T>& dst, const T* src, int64_t len) {
   dst.resize((size_t)len);
   const int nt = host_threads(len);
 #pragma omp parallel for schedule(static) num_threads(nt)
@@ -215,13 +215,13 @@ void par_copy(std::vector<T>& dst, const T* src, int64_t len) {
   }
 }
 template <typename T>
-void par_copy(std::vector<T>& dst, const std::vector<T>& src) {
+void par_copy(hvec<T>& dst, const hvec<T>& src) {
   par_copy(dst, src.data(), (int64_t)src.size());
 }
-template void par_copy<int>(std::vector<int>&, const std::vector<int>&);
-template void par_copy<double>(std::vector<double>&, const std::vector<double>&);
-template void par_copy<int>(std::vector<int>&, const int*, int64_t);
-template void par_copy<double>(std::vector<double>&, const double*, int64_t);
+template void par_copy<int>(hvec<int>&, const hvec<int>&);
+template void par_copy<double>(hvec<double>&, const hvec<double>&);
+template void par_copy<int>(hvec<int>&, const int*, int64_t);
+template void par_copy<double>(hvec<double>&, const double*, int64_t);
 
 HCsr transpose(const HCsr& A) {
   HCsr T;
@@ -530,7 +530,7 @@ void finish_common(const HostProblem& hp, Prepared& o) {
   o.noC = nfree > 0.8 * hp.n;
 }
 
-double norm_b_inf_org(const std::vector<double>& AL, const std::vector<double>& AU) { return norm_b_of(AL, AU, true); }
-double norm_inf(const std::vector<double>& v) { return norminf(v); }
+double norm_b_inf_org(const hvec<double>& AL, const hvec<double>& AU) { return norm_b_of(AL, AU, true); }
+double norm_inf(const hvec<double>& v) { return norminf(v); }
 
 }  // namespace hprqp

@@ -16,6 +16,8 @@
 
 #include <memory>
 #include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/hprqp.h"
@@ -23,10 +25,36 @@
 
 namespace hprqp {
 
+// Allocator whose value-initialisation of trivial elements is default-
+// initialisation: resize leaves them uninitialised.  The host arrays of a
+// problem (hundreds of MB for the large configurations) are filled in full
+// right after they are sized, mostly by parallel loops; std::allocator's
+// zero-fill would first touch every page on one thread (38 ms per 100 MB
+// on the B200 host, against 4 ms for the parallel first touch).
+template <typename T, typename A = std::allocator<T>>
+struct NoInitAlloc : A {
+  template <typename U>
+  struct rebind {
+    using other = NoInitAlloc<U, typename std::allocator_traits<A>::template rebind_alloc<U>>;
+  };
+  using A::A;
+  NoInitAlloc() = default;
+  template <typename U>
+  void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+    ::new (static_cast<void*>(p)) U;
+  }
+  template <typename U, typename... Args>
+  void construct(U* p, Args&&... args) {
+    std::allocator_traits<A>::construct(static_cast<A&>(*this), p, std::forward<Args>(args)...);
+  }
+};
+template <typename T>
+using hvec = std::vector<T, NoInitAlloc<T>>;
+
 struct HCsr {
   int64_t rows = 0, cols = 0;
-  std::vector<int> ptr, col;
-  std::vector<double> val;
+  hvec<int> ptr, col;
+  hvec<double> val;
   int64_t nnz() const { return (int64_t)col.size(); }
 };
 
@@ -36,13 +64,13 @@ struct HostProblem {  // the loaded, unscaled problem
   HCsr A;   // m x n
   HCsr AT;  // n x m: the caller's CSC of A read as CSR of A'
   HCsr QT;  // n x n: the caller's CSC of Q read as CSR of Q' (sparse kind)
-  std::vector<double> c, AL, AU, l, u;
+  hvec<double> c, AL, AU, l, u;
   double obj_constant = 0.0, lambda = 0.0;
   HCsr Q;  // n x n (sparse kind)
   HCsr L;   // lasso data, lasso_m x n
   HCsr LT;  // its transpose (the caller's CSC read as CSR)
   int64_t qn = 0;
-  std::vector<double> qA, qB, qS, qT;  // column-major qn x qn
+  hvec<double> qA, qB, qS, qT;  // column-major qn x qn
   bool loaded = false;
 };
 
@@ -64,7 +92,7 @@ struct DevScaled {
 struct Prepared {  // scaled problem + scaling info (Scaling_info_cpu)
   std::shared_ptr<DevScaled> dev;  // set by the GPU scaling, null after host scaling
   HCsr A, AT, Q;  // with `dev`, A and A' carry their patterns only (values on the device)
-  std::vector<double> c, AL, AU, l, u, row_norm, col_norm, diag_Q;
+  hvec<double> c, AL, AU, l, u, row_norm, col_norm, diag_Q;
   double norm_b = 0, norm_c = 0, norm_b_org = 0, norm_c_org = 0;
   double b_scale = 1.0, c_scale = 1.0;
   bool Q_is_diag = false;
@@ -90,8 +118,8 @@ void finish_sparse(Prepared& o, int64_t n);
 // diagonal on the device)
 void finish_norms(Prepared& o);
 void finish_common(const HostProblem& hp, Prepared& o);
-double norm_b_inf_org(const std::vector<double>& AL, const std::vector<double>& AU);
-double norm_inf(const std::vector<double>& v);
+double norm_b_inf_org(const hvec<double>& AL, const hvec<double>& AU);
+double norm_inf(const hvec<double>& v);
 HCsr transpose(const HCsr& A);
 // Pattern of the Gram matrix G = A'A (n x n) from A (CSR) and A' (CSR of
 // the transpose): row p holds the columns of every row of A that has an
@@ -101,13 +129,13 @@ HCsr transpose(const HCsr& A);
 // merge needs sorted rows) or when the product's work, sum over the rows of
 // A of their length squared, exceeds max_work.
 bool gram_pattern(const HCsr& A, const HCsr& AT, int64_t max_work, HCsr& G);
-// dst = src with the copy split over host threads (the preparation copies
-// ~100 MB of patterns and vectors; one thread moves ~6 GB/s).
+// dst = src with the copy split over host threads, which also first-touch
+// dst's pages (the preparation copies ~100 MB of patterns and vectors).
 template <typename T>
-void par_copy(std::vector<T>& dst, const std::vector<T>& src);
+void par_copy(hvec<T>& dst, const hvec<T>& src);
 // dst = src[0, len) likewise, from a caller's array
 template <typename T>
-void par_copy(std::vector<T>& dst, const T* src, int64_t len);
+void par_copy(hvec<T>& dst, const T* src, int64_t len);
 // Host threads for a row-parallel loop over `work` items: 1 below ~64k
 // items (a parallel region costs more than it saves there), else at most
 // 16 (the loops are memory-bound; more threads only add wake-up cost).

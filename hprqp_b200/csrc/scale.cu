@@ -341,13 +341,13 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   HPRQP_LAUNCH_CHECK();
   HPRQP_CUDA(cudaStreamSynchronize(st));
   tm[nt++] = wall();  // scaling kernels
-  auto down = [&](std::vector<double>& dst, const double* src) {
+  auto down = [&](auto& dst, const double* src) {
     if (!dst.empty()) {
       HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
       *d2h += (int64_t)(sizeof(double) * dst.size());
     }
   };
-  o.diag_Q.assign(n, 0.0);
+  o.diag_Q.resize(n);  // (filled by the download)
   down(o.diag_Q, dg);
   std::vector<double> hmax(nb);
   down(hmax, bmax);

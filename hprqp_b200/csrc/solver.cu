@@ -207,7 +207,7 @@ static double problem_fingerprint(const HostProblem& hp) {
     const unsigned char* b = (const unsigned char*)p;
     for (size_t i = 0; i < bytes; ++i) h = (h ^ b[i]) * 1099511628211ULL;
   };
-  auto vec = [&](const std::vector<double>& v) { mix(v.data(), sizeof(double) * v.size()); };
+  auto vec = [&](const auto& v) { mix(v.data(), sizeof(double) * v.size()); };
   auto csr = [&](const HCsr& M) {
     mix(M.ptr.data(), sizeof(int) * M.ptr.size());
     mix(M.col.data(), sizeof(int) * M.col.size());
