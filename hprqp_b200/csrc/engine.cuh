@@ -101,9 +101,10 @@ struct Common {  // per-handle resources shared by the engines
     h2d_staged(d, h, bytes, stream);
     h2d += (int64_t)bytes;
   }
-  void to_host(void* h, const void* d, size_t bytes) {
+  void to_host(void* h, const void* d, size_t bytes) {  // (1 MiB and more: synchronous, pinned chunks)
     if (!bytes) return;
-    HPRQP_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, stream));
+    if (bytes >= (1u << 20)) d2h_staged(h, d, bytes, stream);
+    else HPRQP_CUDA(cudaMemcpyAsync(h, d, bytes, cudaMemcpyDeviceToHost, stream));
     d2h += (int64_t)bytes;
   }
 };

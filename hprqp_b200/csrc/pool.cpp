@@ -157,6 +157,57 @@ void h2d_staged(void* dst, const void* src, size_t bytes, cudaStream_t st) {
   pinned_give(buf[1], kChunk);
 }
 
+void d2h_staged(void* dst, const void* src, size_t bytes, cudaStream_t st) {
+  constexpr size_t kChunk = 8u << 20;
+  if (bytes < (1u << 20)) {
+    if (bytes) {
+      HPRQP_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, st));
+      HPRQP_CUDA(cudaStreamSynchronize(st));
+    }
+    return;
+  }
+  char* buf[2] = {(char*)pinned_take(kChunk), (char*)pinned_take(kChunk)};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  auto out = [&](int b, size_t off, size_t len) {  // pinned chunk b -> dst + off
+    const int nt = std::max(1, std::min(16, omp_get_max_threads()));
+#pragma omp parallel for schedule(static) num_threads(nt)
+    for (int t = 0; t < nt; ++t) {
+      const size_t a = len * (size_t)t / (size_t)nt, e = len * (size_t)(t + 1) / (size_t)nt;
+      if (e > a) std::memcpy((char*)dst + off + a, buf[b] + a, e - a);
+    }
+  };
+  try {
+    for (int b = 0; b < 2; ++b) HPRQP_CUDA(cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming));
+    size_t prev_off = 0, prev_len = 0;
+    int b = 0;
+    for (size_t off = 0; off < bytes; off += kChunk, b ^= 1) {
+      const size_t len = std::min(kChunk, bytes - off);
+      HPRQP_CUDA(cudaMemcpyAsync(buf[b], (const char*)src + off, len, cudaMemcpyDeviceToHost, st));
+      HPRQP_CUDA(cudaEventRecord(ev[b], st));
+      if (prev_len) {  // the previous chunk, whose DMA was enqueued before this one
+        HPRQP_CUDA(cudaEventSynchronize(ev[b ^ 1]));
+        out(b ^ 1, prev_off, prev_len);
+      }
+      prev_off = off;
+      prev_len = len;
+    }
+    HPRQP_CUDA(cudaEventSynchronize(ev[b ^ 1]));
+    out(b ^ 1, prev_off, prev_len);
+  } catch (...) {
+    for (int k = 0; k < 2; ++k)
+      if (ev[k]) {
+        cudaEventSynchronize(ev[k]);
+        cudaEventDestroy(ev[k]);
+      }
+    pinned_give(buf[0], kChunk);
+    pinned_give(buf[1], kChunk);
+    throw;
+  }
+  for (int k = 0; k < 2; ++k) cudaEventDestroy(ev[k]);
+  pinned_give(buf[0], kChunk);
+  pinned_give(buf[1], kChunk);
+}
+
 void* PoolBlocks::get(size_t bytes) {
   if (dev < 0) HPRQP_CUDA(cudaGetDevice(&dev));
   void* p = pool_alloc(bytes);

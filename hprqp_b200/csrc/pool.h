@@ -39,6 +39,10 @@ void pinned_give(void* p, size_t bytes);
 // pageable memory is staged by one thread).  `src` may be reused on return;
 // the copy completes in stream order.
 void h2d_staged(void* dst, const void* src, size_t bytes, cudaStream_t st);
+// Device -> host copy of `bytes` into pageable memory, the mirror image: the
+// DMA of each 8 MiB chunk into a pinned buffer runs while the host threads
+// copy the previous chunk out.  Synchronous: `dst` holds the data on return.
+void d2h_staged(void* dst, const void* src, size_t bytes, cudaStream_t st);
 
 // Owner of a list of pool blocks of one device, freed together.
 struct PoolBlocks {

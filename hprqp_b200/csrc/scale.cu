@@ -341,9 +341,9 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   HPRQP_LAUNCH_CHECK();
   HPRQP_CUDA(cudaStreamSynchronize(st));
   tm[nt++] = wall();  // scaling kernels
-  auto down = [&](auto& dst, const double* src) {
+  auto down = [&](auto& dst, const double* src) {  // (synchronous: pinned chunks, copied out in parallel)
     if (!dst.empty()) {
-      HPRQP_CUDA(cudaMemcpyAsync(dst.data(), src, sizeof(double) * dst.size(), cudaMemcpyDeviceToHost, st));
+      d2h_staged(dst.data(), src, sizeof(double) * dst.size(), st);
       *d2h += (int64_t)(sizeof(double) * dst.size());
     }
   };
