@@ -392,9 +392,11 @@ def lasso_block(args, rank, world, local_rank, log):
     """The large LASSO (A 20,000 x 150,000, ~1.1e7 nonzeros, lognormal row
     lengths; implicit Q = A'A): time to 1e-6 (device time from after set-up,
     power method included, like the headline) in plain FP64 and in FP32 +
-    FP64 polish, iterations/s, and each fused pass's achieved bandwidth (a
-    CUDA event on each side of every pass of one profiled solve).  A replica
-    per rank ("replicas only"); the time is the slowest rank's."""
+    FP64 polish, iterations/s, the plain iteration's achieved bandwidth (its
+    passes back to back, 50 iterations between two CUDA events), and each
+    fused pass's (a CUDA event on each side of every pass of one profiled
+    solve).  A replica per rank ("replicas only"); the time is the slowest
+    rank's."""
     from hprqp_b200 import HPRQP_parameters, Solver
     from hprqp_b200 import workloads as W
     from hprqp_b200.dist import max_over_ranks
@@ -420,9 +422,19 @@ def lasso_block(args, rank, world, local_rank, log):
                 passes.append({"kernel": f"{eng}:{q['name']}", "ms_per_launch": q["ms"], "bytes": q["bytes"],
                                "schedule": q["threads_per_row"], "achieved_GBps": round(ach, 1),
                                "frac": round(ach / peak, 4)})
+        # the plain iteration of this precision's first engine, its passes back to back as in the loop
+        # (50 iterations between two CUDA events, lambda given: no power method before them)
+        it = s.profile_iterations(HPRQP_parameters(verbose=False, problem_type="LASSO", precision=prec,
+                                                   lambda_max_Q_override=r.lambda_max_Q), 50)
+        it_ach = it["bytes_per_iter"] / (it["ms_per_iter"] * 1e-3) / 1e9 if it["ms_per_iter"] else 0.0
+        iteration = {"engine": "fp32" if prec == "fp32_polish" else "fp64", "ms_per_iter": it["ms_per_iter"],
+                     "bytes_per_iter": it["bytes_per_iter"], "achieved_GBps": round(it_ach, 1),
+                     "frac": round(it_ach / peak, 4),
+                     "note": "bytes the passes' formats stream (staged copies: 16-bit columns, padded chunks)"}
         out[prec] = dict(time_s=t, status=r.status, iters=r.iter, iters_fp32=r.iter_fp32, kkt=r.residuals,
                          primal_obj=r.primal_obj, power_s=r.power_time, iters_per_s=r.iter / loop_s,
-                         passes_with_events=passes, peak=peak, peak_source=peak_kind)
+                         roofline_iteration=iteration, passes_with_events=passes, peak=peak,
+                         peak_source=peak_kind)
         log(f"lasso {prec}: {t:.3f} s, {r.iter} iterations")
     s.close()
     out["speedup_fp32_vs_fp64"] = out["fp64"]["time_s"] / out["fp32_polish"]["time_s"]
