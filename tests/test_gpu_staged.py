@@ -13,12 +13,19 @@ by the last block to arrive.
    solves in FP64 and FP32 + polish give the oracle's status, iteration
    count (FP64) and objective;
  - two solves give bit-identical solutions (the fold does not depend on
-   which block arrives last).
+   which block arrives last);
+ - a QP built for the layout's edge cases (rows whose entries all sit in
+   the first or in the last column block, so that they are empty in the
+   others; rows of more than 32 chunks in every block; a last block
+   narrower than the others): the first 50 iterates match the oracle to
+   1e-10 with A pinned to the staged schedule.
 """
 import numpy as np
 import pytest
 
-from hprqp_b200 import Solver
+import scipy.sparse as sp
+
+from hprqp_b200 import Solver, build_from_QAbc
 from hprqp_b200 import workloads as W
 from oracle import oracle as O
 from tests.test_gpu_parity import ITER_RTOL, OBJ_RTOL, gpu_params, oracle_params, rel
@@ -99,3 +106,45 @@ def test_wide_lasso_staged_full_solve_matches_oracle():
     assert r32.status == "OPTIMAL" and r32.residuals < 1e-6 and r32.iter_fp32 > 0
     assert abs(r32.primal_obj - ref.primal_obj) / (1 + abs(ref.primal_obj)) < 1e-5
     assert again.iter == r.iter and np.array_equal(again.x, r.x)
+
+
+def edge_qp():
+    """n = 61,001 (three FP64 column blocks of 20,336 columns, the last one
+    20,329; two in FP32), m = 2,000 rows of A: 10% with every entry among
+    the last 15,000 columns, 10% among the first 500, 20 rows of 800 entries
+    (about 34 chunks in each block), the rest 30 entries; Q diagonal plus a
+    sparse low-rank term; bounds around a point."""
+    rng = np.random.default_rng(77)
+    n, m = 61001, 2000
+    rows, cols = [], []
+    for r in range(m):
+        if r % 10 == 0:
+            c = n - 1 - rng.choice(15000, 30, replace=False)
+        elif r % 10 == 1:
+            c = rng.choice(500, 30, replace=False)
+        elif r < 40 and r % 2 == 0:
+            c = rng.choice(n, 800, replace=False)
+        else:
+            c = rng.choice(n, 30, replace=False)
+        rows += [r] * len(c)
+        cols += list(c)
+    A = sp.csr_matrix((rng.standard_normal(len(rows)), (rows, cols)), shape=(m, n))
+    A.sum_duplicates()
+    Bm = sp.random(200, n, density=2e-4, random_state=5, format="csr")
+    Q = (Bm.T @ Bm + sp.diags(rng.uniform(0.1, 1.0, n))).tocsc()
+    Q = (0.5 * (Q + Q.T)).tocsc()
+    x0 = rng.uniform(-1, 1, n)
+    Ax0 = A @ x0
+    return build_from_QAbc(Q, rng.standard_normal(n), A.tocsc(), Ax0 - rng.uniform(0, 1, m),
+                           Ax0 + rng.uniform(0, 1, m), -5.0 * np.ones(n), 5.0 * np.ones(n), verbose=False)
+
+
+def test_edge_layout_qp_staged_iterates_match_oracle():
+    m = edge_qp()
+    ref, xt, yt, wt, stats = _iterates(m, "QP", spmv_mode_A="staged", spmv_mode_Q=1)
+    sched = {p["name"]: p["threads_per_row"] for p in stats["passes"]}
+    assert sched["y A*tempv"] == STAGED, sched
+    for k in range(50):
+        assert rel(xt[k], ref.x_trace[k]) < ITER_RTOL, ("x", k, rel(xt[k], ref.x_trace[k]))
+        assert rel(yt[k], ref.y_trace[k]) < ITER_RTOL, ("y", k)
+        assert rel(wt[k], ref.w_trace[k]) < ITER_RTOL, ("w", k)
