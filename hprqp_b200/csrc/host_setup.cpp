@@ -27,6 +27,76 @@ HCsr csc_to_csr(int64_t rows, int64_t cols, const int32_t* cp, const int32_t* rv
   if (nnz > 0 && (!rv || !nz)) throw Error(HPRQP_E_ARG, std::string(what) + ": null rowval/nzval");
   for (int64_t j = 0; j < cols; ++j)
     if (cp[j + 1] < cp[j]) throw Error(HPRQP_E_ARG, std::string(what) + ": colptr not monotone");
+  // A stable counting sort of the entries (column-major order) by row,
+  // split among H threads by columns: thread t counts its columns' entries
+  // per row in its own histogram, an exclusive sum over the threads gives
+  // each thread its first slot in every row, and each thread then scatters
+  // its columns in order.  Rows receive their entries in increasing column
+  // order, as from a serial pass, with O(nnz / H + rows) work a thread.
+  // The H x rows histograms are capped at max(8 nnz, 2^22) entries; past
+  // that, the row-range scatter below runs instead.
+  const int T = host_threads(nnz);
+  const int64_t cap = std::max<int64_t>(8 * nnz, int64_t(1) << 22);
+  const int H = rows > 0 ? (int)std::min<int64_t>(T, cap / rows) : 0;
+  if (H >= 2) {
+    M.ptr.resize(rows + 1);
+    M.col.resize(nnz);
+    M.val.resize(nnz);
+    std::vector<int64_t> cb(H + 1);  // column ranges of about nnz / H entries
+    cb[0] = 0;
+    cb[H] = cols;
+    for (int t = 1; t < H; ++t) {
+      const int64_t e = nnz * t / H + base;
+      cb[t] = std::max<int64_t>(cb[t - 1], std::upper_bound(cp, cp + cols + 1, (int32_t)e) - cp - 1);
+    }
+    hvec<int> hist;
+    hist.resize((size_t)H * rows);
+    bool bad_row = false, bad_val = false;
+#pragma omp parallel num_threads(H) reduction(|| : bad_row, bad_val)
+    {
+      const int t = omp_get_thread_num();
+      int* h = hist.data() + (size_t)t * rows;
+      std::memset(h, 0, sizeof(int) * (size_t)rows);
+      for (int64_t k = cp[cb[t]] - base; k < cp[cb[t + 1]] - base; ++k) {
+        const int64_t r = (int64_t)rv[k] - base;
+        if (r < 0 || r >= rows) {
+          bad_row = true;
+          continue;
+        }
+        if (!std::isfinite(nz[k])) bad_val = true;
+        h[r]++;
+      }
+#pragma omp barrier
+#pragma omp for schedule(static)
+      for (int64_t r = 0; r < rows; ++r) {
+        int sum = 0;
+        for (int q = 0; q < H; ++q) {
+          int& c = hist[(size_t)q * rows + r];
+          const int v = c;
+          c = sum;
+          sum += v;
+        }
+        M.ptr[r + 1] = sum;
+      }
+    }
+    if (bad_row) throw Error(HPRQP_E_ARG, std::string(what) + ": row index out of range");
+    if (bad_val) throw Error(HPRQP_E_ARG, std::string(what) + " contains NaN or Inf values.");
+    M.ptr[0] = 0;
+    for (int64_t i = 0; i < rows; ++i) M.ptr[i + 1] += M.ptr[i];
+#pragma omp parallel num_threads(H)
+    {
+      const int t = omp_get_thread_num();
+      int* h = hist.data() + (size_t)t * rows;
+      for (int64_t j = cb[t]; j < cb[t + 1]; ++j)
+        for (int64_t k = cp[j] - base; k < cp[j + 1] - base; ++k) {
+          const int64_t r = (int64_t)rv[k] - base;
+          const int q = M.ptr[r] + h[r]++;
+          M.col[q] = (int)j;
+          M.val[q] = nz[k];
+        }
+    }
+    return M;
+  }
   M.ptr.assign(rows + 1, 0);
   M.col.resize(nnz);
   M.val.resize(nnz);
@@ -50,7 +120,6 @@ HCsr csc_to_csr(int64_t rows, int64_t cols, const int32_t* cp, const int32_t* rv
   // scatter: each thread owns a range of rows (balanced by entries) and
   // walks all columns in order, so every row receives its entries in
   // increasing column order, as a serial pass would
-  const int T = host_threads(nnz);
 #pragma omp parallel num_threads(T)
   {
     const int t = omp_get_thread_num(), nt = omp_get_num_threads();
@@ -259,42 +328,52 @@ bool gram_pattern(const HCsr& A, const HCsr& AT, int64_t max_work, HCsr& G) {
   for (int64_t p = 0; p < n; ++p)
     for (int k = AT.ptr[p] + 1; k < AT.ptr[p + 1]; ++k) sorted = sorted && AT.col[k - 1] < AT.col[k];
   if (!sorted) return false;
-  std::vector<int> len(n, 0);
-  // pass 0 counts, pass 1 writes; a per-thread marker array dedupes
-  for (int pass = 0; pass < 2; ++pass) {
-#pragma omp parallel num_threads(host_threads(n))
-    {
-      std::vector<int> mark(n, -1), list;
-#pragma omp for schedule(static)
-      for (int64_t p = 0; p < n; ++p) {
-        list.clear();
-        for (int k = AT.ptr[p]; k < AT.ptr[p + 1]; ++k) {
-          const int r = AT.col[k];
-          for (int t = A.ptr[r]; t < A.ptr[r + 1]; ++t) {
-            const int j = A.col[t];
-            if (mark[j] != (int)p) {
-              mark[j] = (int)p;
-              list.push_back(j);
-            }
+  // one pass: each thread lists its contiguous range of rows p into its own
+  // buffer (each row sorted, a per-thread marker array dedupes), then copies
+  // the buffer to its place in G.col
+  const int T = host_threads(n);
+  std::vector<hvec<int>> buf(T);
+  hvec<int> len;
+  len.resize(n);
+  std::vector<int64_t> pb(T + 1, 0);
+#pragma omp parallel num_threads(T)
+  {
+    const int t = omp_get_thread_num(), nt = omp_get_num_threads();
+    const int64_t p0 = n * t / nt, p1 = n * (t + 1) / nt;
+    std::vector<int> mark(n, -1);
+    hvec<int>& out = buf[t];
+    size_t used = 0;
+    out.resize((size_t)std::max<int64_t>(1024, (p1 - p0) * 8));
+    for (int64_t p = p0; p < p1; ++p) {
+      const size_t start = used;
+      for (int k = AT.ptr[p]; k < AT.ptr[p + 1]; ++k) {
+        const int r = AT.col[k];
+        for (int q = A.ptr[r]; q < A.ptr[r + 1]; ++q) {
+          const int j = A.col[q];
+          if (mark[j] != (int)p) {
+            mark[j] = (int)p;
+            if (used == out.size()) out.resize(out.size() * 2);
+            out[used++] = j;
           }
         }
-        if (pass == 0) {
-          len[p] = (int)list.size();
-        } else {
-          std::sort(list.begin(), list.end());
-          std::copy(list.begin(), list.end(), G.col.begin() + G.ptr[p]);
-        }
       }
+      std::sort(out.begin() + start, out.begin() + used);
+      len[p] = (int)(used - start);
     }
-    if (pass == 0) {
-      int64_t total = 0;
-      for (int64_t p = 0; p < n; ++p) total += len[p];
-      if (total > std::numeric_limits<int>::max()) return false;  // int row pointers
-      G.rows = G.cols = n;
-      G.ptr.assign(n + 1, 0);
-      for (int64_t p = 0; p < n; ++p) G.ptr[p + 1] = G.ptr[p] + len[p];
-      G.col.resize(total);
-    }
+    pb[t + 1] = (int64_t)used;
+  }
+  for (int t = 0; t < T; ++t) pb[t + 1] += pb[t];
+  if (pb[T] > std::numeric_limits<int>::max()) return false;  // int row pointers
+  G.rows = G.cols = n;
+  G.ptr.resize(n + 1);
+  G.ptr[0] = 0;
+  for (int64_t p = 0; p < n; ++p) G.ptr[p + 1] = G.ptr[p] + len[p];
+  G.col.resize(pb[T]);
+#pragma omp parallel num_threads(T)
+  {
+    const int t = omp_get_thread_num();
+    if (pb[t + 1] > pb[t])
+      std::memcpy(G.col.data() + pb[t], buf[t].data(), sizeof(int) * (size_t)(pb[t + 1] - pb[t]));
   }
   return true;
 }
@@ -346,10 +425,16 @@ void load_problem(const hprqp_problem* pr, HostProblem& hp) {
   h.AU = copy_vec(pr->AU, h.m, "Constraint bounds AU", true);
   h.l = copy_vec(pr->l, h.n, "Variable bounds l", true);
   h.u = copy_vec(pr->u, h.n, "Variable bounds u", true);
+  // the first offending index is reported, as by a serial scan
+  int64_t bad_l = h.n, bad_A = h.m;
+#pragma omp parallel for schedule(static) reduction(min : bad_l) num_threads(host_threads(h.n))
   for (int64_t i = 0; i < h.n; ++i)
-    if (h.l[i] > h.u[i]) throw Error(HPRQP_E_ARG, "Infeasible variable bounds: l > u at index " + std::to_string(i));
+    if (h.l[i] > h.u[i]) bad_l = std::min(bad_l, i);
+#pragma omp parallel for schedule(static) reduction(min : bad_A) num_threads(host_threads(h.m))
   for (int64_t i = 0; i < h.m; ++i)
-    if (h.AL[i] > h.AU[i]) throw Error(HPRQP_E_ARG, "Infeasible constraint bounds: AL > AU at row " + std::to_string(i));
+    if (h.AL[i] > h.AU[i]) bad_A = std::min(bad_A, i);
+  if (bad_l < h.n) throw Error(HPRQP_E_ARG, "Infeasible variable bounds: l > u at index " + std::to_string(bad_l));
+  if (bad_A < h.m) throw Error(HPRQP_E_ARG, "Infeasible constraint bounds: AL > AU at row " + std::to_string(bad_A));
   h.obj_constant = pr->obj_constant;
   h.lambda = pr->lambda;
   if (h.Q_kind == HPRQP_Q_SPARSE) {
