@@ -14,11 +14,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
-#include <sys/mman.h>
-
-#include <cstdlib>
 #include <memory>
-#include <new>
 #include <string>
 #include <type_traits>
 #include <utility>
@@ -35,8 +31,9 @@ namespace hprqp {
 // right after they are sized, mostly by parallel loops; std::allocator's
 // zero-fill would first touch every page on one thread (38 ms per 100 MB
 // on the B200 host, against 4 ms for the parallel first touch).  Arrays of
-// 4 MiB and more are 2 MiB-aligned and advised for transparent huge pages,
-// so that their first touch takes one fault per 2 MiB instead of per 4 KiB.
+// 4 MiB and more come from the process's host block cache (host_take), so
+// that the next problem's arrays of similar sizes reuse pages that are
+// already mapped and faulted in.
 template <typename T, typename A = std::allocator<T>>
 struct NoInitAlloc : A {
   template <typename U>
@@ -45,19 +42,14 @@ struct NoInitAlloc : A {
   };
   using A::A;
   NoInitAlloc() = default;
-  static constexpr size_t kHugePage = size_t(2) << 20;
+  static constexpr size_t kLarge = size_t(4) << 20;
   T* allocate(size_t n) {
-    const size_t bytes = n * sizeof(T);
-    if (bytes < 2 * kHugePage) return A::allocate(n);
-    const size_t rounded = (bytes + kHugePage - 1) / kHugePage * kHugePage;
-    void* p = std::aligned_alloc(kHugePage, rounded);
-    if (!p) throw std::bad_alloc();
-    madvise(p, rounded, MADV_HUGEPAGE);  // a hint: without THP the pages stay 4 KiB
-    return static_cast<T*>(p);
+    if (n * sizeof(T) < kLarge) return A::allocate(n);
+    return static_cast<T*>(host_take(n * sizeof(T)));
   }
   void deallocate(T* p, size_t n) {
-    if (n * sizeof(T) < 2 * kHugePage) return A::deallocate(p, n);
-    std::free(p);
+    if (n * sizeof(T) < kLarge) return A::deallocate(p, n);
+    host_give(p);
   }
   template <typename U>
   void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {

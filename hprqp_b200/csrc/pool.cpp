@@ -9,7 +9,12 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <new>
+#include <unordered_map>
+
+#include <sys/mman.h>
 
 #include "../../include/hprqp.h"
 #include "common.cuh"
@@ -91,6 +96,59 @@ namespace {
 std::mutex g_pin_mu;
 std::vector<std::pair<size_t, void*>> g_pinned;  // free pinned buffers by size
 }  // namespace
+
+namespace {
+std::mutex g_host_mu;
+std::multimap<size_t, void*> g_host_free;     // kept blocks by size
+std::unordered_map<void*, size_t> g_host_live;  // blocks handed out, with their sizes
+size_t g_host_kept = 0;
+size_t host_keep_limit() {
+  static const size_t lim = [] {
+    size_t mb = 4096;
+    if (const char* e = std::getenv("HPRQP_HOST_KEEP_MB")) mb = (size_t)std::strtoull(e, nullptr, 10);
+    return mb << 20;
+  }();
+  return lim;
+}
+constexpr size_t kHostPage = size_t(2) << 20;
+}  // namespace
+
+void* host_take(size_t bytes) {
+  const size_t want = (std::max<size_t>(bytes, 1) + kHostPage - 1) / kHostPage * kHostPage;
+  {
+    std::lock_guard<std::mutex> lk(g_host_mu);
+    auto it = g_host_free.lower_bound(want);
+    if (it != g_host_free.end() && it->first <= want + want / 4) {
+      void* p = it->second;
+      g_host_kept -= it->first;
+      g_host_live.emplace(p, it->first);
+      g_host_free.erase(it);
+      return p;
+    }
+  }
+  void* p = std::aligned_alloc(kHostPage, want);
+  if (!p) throw std::bad_alloc();
+  madvise(p, want, MADV_HUGEPAGE);  // a hint: without transparent huge pages the pages stay 4 KiB
+  std::lock_guard<std::mutex> lk(g_host_mu);
+  g_host_live.emplace(p, want);
+  return p;
+}
+
+void host_give(void* p) {
+  if (!p) return;
+  std::unique_lock<std::mutex> lk(g_host_mu);
+  auto it = g_host_live.find(p);
+  if (it == g_host_live.end()) return;  // not ours: nothing to do
+  const size_t size = it->second;
+  g_host_live.erase(it);
+  if (g_host_kept + size > host_keep_limit()) {
+    lk.unlock();
+    std::free(p);
+    return;
+  }
+  g_host_kept += size;
+  g_host_free.emplace(size, p);
+}
 
 void* pinned_take(size_t bytes) {
   {

@@ -33,6 +33,17 @@ void pool_free(std::vector<void*>& blocks, int dev);
 void* pinned_take(size_t bytes);
 void pinned_give(void* p, size_t bytes);
 
+// Host blocks for the library's large host arrays: 2 MiB-aligned, advised
+// for transparent huge pages, and kept by the process once given back, so
+// that the arrays of the next problem (the load -> solve -> destroy cycle)
+// reuse pages that are mapped and faulted in already instead of paying a
+// page fault per 4 KiB again.  A request takes the smallest kept block of
+// at least its size and at most 1.25 times it, else maps a new one.  At
+// most HPRQP_HOST_KEEP_MB (default 4096) MiB of free blocks are kept; the
+// rest go back to the system.  Throws std::bad_alloc when out of memory.
+void* host_take(size_t bytes);
+void host_give(void* p);
+
 // Host -> device copy of `bytes` from pageable memory, enqueued on `st`:
 // copies of 1 MiB and more go through two pinned 8 MiB chunks, each filled
 // by the host threads while the other one's DMA runs (a plain copy from
