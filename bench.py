@@ -549,8 +549,16 @@ def run_ours(args):
                       "seconds": head["power_s"], "peak_source": peak_kind,
                       "share_of_solve": round(head["power_s"] / head["value"], 3) if head["value"] else None}
     # end to end through the public API from host buffers (load -> solve -> x,y,z,w on the host)
+    # one untimed cycle first (its time is reported as first_call_s): the
+    # process's first load maps and registers the host blocks that later
+    # problems reuse, as the device metric's warm-up steps exclude first-use costs
     e2e_t, h2d, d2h, setup, parts = [], 0, 0, 0.0, []
-    for _ in range(max(1, min(args.steps, 3))):
+    t = time.perf_counter()
+    s2 = Solver(local_rank).load(model)
+    s2.solve(HPRQP_parameters(verbose=False, precision=args.precision))
+    s2.close()
+    first_call = time.perf_counter() - t
+    for _ in range(max(3, min(args.steps, 5))):
         t = time.perf_counter()
         s2 = Solver(local_rank).load(model)
         t1 = time.perf_counter()
@@ -564,7 +572,8 @@ def run_ours(args):
                       "setup_s": round(r.setup_time, 4), "solve_s": round(r.time, 4),
                       "close_s": round(e2e_t[-1] - (t2 - t), 4)})
     e2e = {"value": barrier_max(statistics.median(e2e_t)), "unit": "s", "statistic": "median",
-           "samples_s": [round(t, 4) for t in e2e_t], "parts": parts, "h2d_bytes_per_step": h2d,
+           "samples_s": [round(t, 4) for t in e2e_t], "first_call_s": round(first_call, 4), "parts": parts,
+           "h2d_bytes_per_step": h2d,
            "d2h_bytes_per_step": d2h, "setup_s_last": setup,
            "note": "hprqp_load + hprqp_solve from host arrays (scaling, uploads, solve, solution copy-back); "
                    "bytes counted by the library over every host<->device copy of the call"}
