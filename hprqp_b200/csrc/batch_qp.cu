@@ -619,7 +619,7 @@ static void build_family(int count, const hprqp_problem* probs, Family& F) {
   for (int k = 0; k < count; ++k) {
     const HostProblem& hp = hps[k];
     const HCsr& Ak = hp.A;
-    const HCsr& Tk = pps[k].AT;
+    const HCsr& Tk = pps[k].ATpat();
     const int64_t z = zoff[k], no = F.noff[k], mo = F.moff[k];
     for (int64_t r = 0; r < Ak.rows; ++r) A.ptr[mo + r + 1] = (int)(z + Ak.ptr[r + 1]);
     for (int64_t q = 0; q < Ak.nnz(); ++q) {

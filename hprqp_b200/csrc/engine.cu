@@ -1051,7 +1051,7 @@ void Engine<V>::power_setup(const Prepared& pp, int tpr_A, int tpr_Q) {
   power_ready = true;
   build_gram(pp, tpr_A);
   if (tpr_Q <= 0)
-    autotune_power_Q(cm.sched_cache && pp.Q.nnz() > 0 ? pattern_key(pp.Q, 0x300 + sizeof(V)) : 0);
+    autotune_power_Q(cm.sched_cache && pp.Qpat().nnz() > 0 ? pattern_key(pp.Qpat(), 0x300 + sizeof(V)) : 0);
 }
 
 // The sparse Q's power step runs on its own copy of Q's schedule, chosen by
@@ -1099,12 +1099,12 @@ void Engine<V>::gram_values() {
 template <typename V>
 void Engine<V>::build_gram(const Prepared& pp, int tpr_mode) {
   gram = false;
-  if (m <= 0 || is_op || is_lasso || cm.pow_gram == 0 || pp.A.nnz() == 0) return;
+  if (m <= 0 || is_op || is_lasso || cm.pow_gram == 0 || pp.Apat().nnz() == 0) return;
   const bool force = cm.pow_gram == 1;
-  const int64_t nnzA = pp.A.nnz();
+  const int64_t nnzA = pp.Apat().nnz();
   const double t0 = wall_s();
   HCsr h;
-  if (!gram_pattern(pp.A, pp.AT, (force ? 64 : 6) * nnzA, h)) return;
+  if (!gram_pattern(pp.Apat(), pp.ATpat(), (force ? 64 : 6) * nnzA, h)) return;
   const double t_pat = wall_s();
   if (!force && h.nnz() > 3 * nnzA) return;
   G = DCsr<V>();
@@ -1193,11 +1193,11 @@ Engine<V>::Engine(Common& c_, const HostProblem& hp, const Prepared& pp, int pat
   row_norm = vec_in(pp.row_norm, ds ? ds->row_norm : nullptr, m);
   HPRQP_CUDA(cudaStreamSynchronize(cm.stream));
   const double t_vec = wall_s();
-  upload_csr(pp.A, A, tpr_A, ds ? &ds->A : nullptr);
+  upload_csr(pp.Apat(), A, tpr_A, ds ? &ds->A : nullptr);
   const double t_A = wall_s();
-  upload_csr(pp.AT, AT, tpr_A, ds ? &ds->AT : nullptr);
+  upload_csr(pp.ATpat(), AT, tpr_A, ds ? &ds->AT : nullptr);
   const double t_AT = wall_s();
-  if (has_Q_sparse) upload_csr(pp.Q, Q, tpr_Q, ds ? &ds->Q : nullptr);
+  if (has_Q_sparse) upload_csr(pp.Qpat(), Q, tpr_Q, ds ? &ds->Q : nullptr);
   const double t_Q = wall_s();
   if (is_lasso) {
     ltemp = mem.alloc<V>(hp.L.rows);

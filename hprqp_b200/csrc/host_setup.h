@@ -104,6 +104,16 @@ struct DevScaled {
 struct Prepared {  // scaled problem + scaling info (Scaling_info_cpu)
   std::shared_ptr<DevScaled> dev;  // set by the GPU scaling, null after host scaling
   HCsr A, AT, Q;  // with `dev`, A and A' carry their patterns only (values on the device)
+  // With `dev`, the patterns of A, A' and (when Q's pattern is symmetric,
+  // so that it is S's) Q are the loaded problem's, not copied: these point
+  // to its records, and A, AT, Q above stay empty.  Apat() etc. give the
+  // pattern in either case.
+  const HCsr* A_pat = nullptr;
+  const HCsr* AT_pat = nullptr;
+  const HCsr* Q_pat = nullptr;
+  const HCsr& Apat() const { return A_pat ? *A_pat : A; }
+  const HCsr& ATpat() const { return AT_pat ? *AT_pat : AT; }
+  const HCsr& Qpat() const { return Q_pat ? *Q_pat : Q; }
   hvec<double> c, AL, AU, l, u, row_norm, col_norm, diag_Q;
   double norm_b = 0, norm_c = 0, norm_b_org = 0, norm_c_org = 0;
   double b_scale = 1.0, c_scale = 1.0;

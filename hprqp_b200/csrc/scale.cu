@@ -82,6 +82,11 @@ __global__ void k_scale(int rows, const int* __restrict__ ptr, const int* __rest
   }
 }
 
+__global__ void k_fill(int len, double* p, double v) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < len) p[i] = v;
+}
+
 __global__ void k_scale_n(int n, const double* tc, double* c, double* l, double* u) {
   const int j = blockIdx.x * kT + threadIdx.x;
   if (j >= n) return;
@@ -170,28 +175,14 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   o = Prepared();
   o.ruiz = p.use_Ruiz_scaling;
   o.pc = p.use_Pock_Chambolle_scaling;
-  // A and A' keep their scaled values on the device only (o.dev): the host
-  // records hold the patterns (the engines' formats and the Gram pattern
-  // are built from them)
-  auto pattern_of = [](const HCsr& h) {
-    HCsr x;
-    x.rows = h.rows;
-    x.cols = h.cols;
-    par_copy(x.ptr, h.ptr);
-    par_copy(x.col, h.col);
-    return x;
-  };
-  o.A = pattern_of(hp.A);
-  o.AT = pattern_of(hp.AT);
-  par_copy(o.c, hp.c);
-  par_copy(o.AL, hp.AL);
-  par_copy(o.AU, hp.AU);
-  par_copy(o.l, hp.l);
-  par_copy(o.u, hp.u);
-  o.row_norm.assign(m, 1.0);
-  o.col_norm.assign(n, 1.0);
-  o.norm_b_org = m > 0 ? norm_b_inf_org(o.AL, o.AU) : 0.0;
-  o.norm_c_org = norm_inf(o.c);
+  // A and A' keep their scaled values on the device only (o.dev); their
+  // patterns (from which the engines' formats and the Gram pattern are
+  // built) are the loaded problem's.  The vectors are uploaded from the
+  // loaded problem and their scaled values downloaded at the end.
+  o.A_pat = &hp.A;
+  o.AT_pat = &hp.AT;
+  o.norm_b_org = m > 0 ? norm_b_inf_org(hp.AL, hp.AU) : 0.0;
+  o.norm_c_org = norm_inf(hp.c);
   const HCsr &Q = hp.Q, &QT = hp.QT;
   // merged pattern of Q + Q' with index maps (the values come later); a
   // structurally symmetric Q (the common case) is its own merged pattern
@@ -226,8 +217,7 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   S.rows = S.cols = n;
   std::vector<int> ia, ib;
   if (sym_pattern) {
-    par_copy(S.ptr, Q.ptr);
-    par_copy(S.col, Q.col);
+    o.Q_pat = &hp.Q;  // S's pattern is Q's
   } else {
 #pragma omp parallel for schedule(static) num_threads(host_threads(n))
     for (int64_t i = 0; i < n; ++i) len[i] = merge(i, nullptr, nullptr, nullptr);
@@ -239,7 +229,7 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
 #pragma omp parallel for schedule(static) num_threads(host_threads(n))
     for (int64_t i = 0; i < n; ++i) merge(i, S.col.data() + S.ptr[i], ia.data() + S.ptr[i], ib.data() + S.ptr[i]);
   }
-  const int64_t nnzS = S.ptr[n];
+  const int64_t nnzS = sym_pattern ? Q.nnz() : S.ptr[n];
   // (S's values stay on the device: the engines copy them from there)
 
   tm[nt++] = wall();  // merged pattern
@@ -282,13 +272,14 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
   double *AL = keep((double*)nullptr, m), *AU = keep((double*)nullptr, m), *rn = keep((double*)nullptr, m);
   double *ca = d.take<double>(n), *cq = d.take<double>(n), *tc = d.take<double>(n), *tci = d.take<double>(n);
   double *ra = d.take<double>(m), *tr = d.take<double>(m), *tri = d.take<double>(m);
-  up(c, o.c);
-  up(l, o.l);
-  up(u, o.u);
-  up(cn, o.col_norm);
-  up(AL, o.AL);
-  up(AU, o.AU);
-  up(rn, o.row_norm);
+  up(c, hp.c);
+  up(l, hp.l);
+  up(u, hp.u);
+  up(AL, hp.AL);
+  up(AU, hp.AU);
+  k_fill<<<blocks(n), kT, 0, st>>>((int)n, cn, 1.0);  // the norms' products start at 1
+  if (m > 0) k_fill<<<blocks(m), kT, 0, st>>>((int)m, rn, 1.0);
+  HPRQP_LAUNCH_CHECK();
   HPRQP_CUDA(cudaStreamSynchronize(st));
   tm[nt++] = wall();  // uploads
   auto pass = [&](int mode) {  // one Ruiz (0) or Pock-Chambolle (1) pass
@@ -347,7 +338,15 @@ void prepare_problem_gpu(const HostProblem& hp, const hprqp_params& p, Prepared&
       *d2h += (int64_t)(sizeof(double) * dst.size());
     }
   };
-  o.diag_Q.resize(n);  // (filled by the download)
+  // (filled by the downloads)
+  o.diag_Q.resize(n);
+  o.c.resize(n);
+  o.l.resize(n);
+  o.u.resize(n);
+  o.col_norm.resize(n);
+  o.AL.resize(m);
+  o.AU.resize(m);
+  o.row_norm.resize(m);
   down(o.diag_Q, dg);
   std::vector<double> hmax(nb);
   down(hmax, bmax);

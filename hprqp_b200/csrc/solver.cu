@@ -582,7 +582,7 @@ static void prepare(Handle& H, const hprqp_params& p) {
   else
     prepare_problem(H.hp, p, H.pp);
   if (H.hp.Q_kind == HPRQP_Q_LASSO) H.path = PATH_LASSO;
-  else if (H.hp.Q_kind == HPRQP_Q_QAP || H.hp.Q_kind == HPRQP_Q_CUSTOM || H.pp.Q.nnz() > 0)
+  else if (H.hp.Q_kind == HPRQP_Q_QAP || H.hp.Q_kind == HPRQP_Q_CUSTOM || H.pp.Qpat().nnz() > 0)
     H.path = H.pp.noC ? PATH_NOC : PATH_QP;
   else H.path = PATH_LP;
   // the power method runs on the first phase's engine: only that one builds
@@ -610,7 +610,7 @@ static void estimate_lambdas(Handle& H, const hprqp_params& p, bool fp32, double
                              int64_t* itA_out = nullptr, int64_t* itQ_out = nullptr, double* bytes_out = nullptr) {
   const Prepared& pp = H.pp;
   const bool needA = H.hp.m > 0 && !(p.lambda_max_A_override > 0);
-  const bool opQ = H.hp.Q_kind != HPRQP_Q_SPARSE || (pp.Q.nnz() > 0 && !pp.Q_is_diag);
+  const bool opQ = H.hp.Q_kind != HPRQP_Q_SPARSE || (pp.Qpat().nnz() > 0 && !pp.Q_is_diag);
   const bool needQ = opQ && !(p.lambda_max_Q_override > 0);
   double a = 0.0, q = 0.0;
   int64_t ia = 0, iq = 0;
@@ -633,7 +633,7 @@ static void estimate_lambdas(Handle& H, const hprqp_params& p, bool fp32, double
   }
   *lamA = H.hp.m > 0 ? (needA ? a * p.eig_factor : p.lambda_max_A_override) : 0.0;
   if (opQ) *lamQ = needQ ? q * p.eig_factor : p.lambda_max_Q_override;
-  else *lamQ = pp.Q.nnz() > 0 ? pp.Q_maxval : 0.0;
+  else *lamQ = pp.Qpat().nnz() > 0 ? pp.Q_maxval : 0.0;
 }
 
 template <typename V>
